@@ -1,0 +1,378 @@
+"""Test infrastructure, not product code: Python driver for the C oracle.
+
+Restates, step for step, the sequence the reference's `mttkrp` main runs to
+build each format (src/mttkrp.cu:72-389), using the C primitives in
+oracle/mmcsf_oracle.c, and returns every array under the same names the
+reference harness (oracle/ref_harness.cpp) dumps, so the two can be compared
+key by key. Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline
+leg may import this module, and only as the checker.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_BUILD = os.path.join(HERE, "_build")
+_LIB_PATH = os.path.join(_BUILD, "libmmcsf_oracle.so")
+_REF_LIB = os.path.join(HERE, "_ref", "libmmcsf_ref.so")
+INF_TH = 99999999  # the reference's default -f (src/util.h:212)
+FBRS_TH_MMCSF = 128  # 4-D fbrS split for -t 12 (src/util.h:1325-1326)
+FBRS_TH_OFF = 999999999
+
+_u64p = ctypes.POINTER(ctypes.c_uint64)
+_lib = None
+
+
+def build(force=False):
+    """Compile the C restatement into oracle/_build/libmmcsf_oracle.so."""
+    os.makedirs(_BUILD, exist_ok=True)
+    src = os.path.join(HERE, "mmcsf_oracle.c")
+    if force or not os.path.exists(_LIB_PATH) or os.path.getmtime(_LIB_PATH) < os.path.getmtime(src):
+        subprocess.run(["gcc", "-O2", "-ffp-contract=off", "-fPIC", "-shared", "-o", _LIB_PATH, src],
+                       check=True)
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        _lib = ctypes.CDLL(_LIB_PATH)
+    return _lib
+
+
+def _ptr_array(arrs, ctype=ctypes.c_uint64):
+    P = ctypes.POINTER(ctype)
+    return (P * len(arrs))(*[a.ctypes.data_as(P) for a in arrs])
+
+
+# --------------------------------------------------------------------------
+# .tns text format: src/util.h:313-370 (load_tensor)
+# --------------------------------------------------------------------------
+def load_tns(path):
+    """Parse a .tns file: line 1 = order, line 2 = dims, then 1-based
+    coordinates and a value per line. Returns (dims, inds[nd] uint64 0-based,
+    vals float32). The count is the number of parsed entries; the reference
+    uses (#lines - 2), which agrees for files without trailing blank lines."""
+    with open(path) as fh:
+        toks = fh.read().split()
+    nd = int(toks[0])
+    dims = [int(t) for t in toks[1:1 + nd]]
+    body = toks[1 + nd:]
+    n = len(body) // (nd + 1)
+    a = np.array(body[:n * (nd + 1)], dtype=object).reshape(n, nd + 1) if n else np.zeros((0, nd + 1))
+    inds = [np.array(a[:, m], dtype=np.float64).astype(np.uint64) - 1 if n else np.zeros(0, np.uint64)
+            for m in range(nd)]
+    vals = np.array(a[:, nd], dtype=np.float32) if n else np.zeros(0, np.float32)
+    return dims, [np.ascontiguousarray(i, dtype=np.uint64) for i in inds], vals
+
+
+def write_tns(path, dims, inds, vals):
+    """Write a .tns file (1-based coordinates) readable by the reference."""
+    nd = len(dims)
+    with open(path, "w") as fh:
+        fh.write(f"{nd}\n" + " ".join(str(d) for d in dims) + "\n")
+        cols = [np.asarray(i, dtype=np.uint64) + 1 for i in inds]
+        for x in range(len(vals)):
+            fh.write(" ".join(str(int(c[x])) for c in cols) + " " + repr(float(vals[x])) + "\n")
+
+
+# --------------------------------------------------------------------------
+# primitives
+# --------------------------------------------------------------------------
+def order_modes(dims, mode, natural=False):
+    nd = len(dims)
+    d = (ctypes.c_uint64 * nd)(*dims)
+    out = (ctypes.c_int * nd)()
+    lib().orc_order_modes(nd, d, mode, int(natural), out)
+    return list(out)
+
+
+def redundant_mode(orders):
+    """src/mttkrp.cu:314-343: the last mode whose (slice, fiber) pair repeats
+    an earlier mode's pair swapped; -1 when there is none."""
+    redun = -1
+    for m in range(1, len(orders)):
+        if any(orders[m][1] == orders[p][0] and orders[m][0] == orders[p][1] for p in range(m)):
+            redun = m
+    return redun
+
+
+def sort_coo(inds, vals, keys):
+    """Stable in-place sort on the key prefix (src/util.h:389-527)."""
+    nd = len(inds)
+    n = len(vals)
+    k = (ctypes.c_int * len(keys))(*keys)
+    rc = lib().orc_sort_coo(nd, ctypes.c_uint64(n), _ptr_array(inds),
+                            vals.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), k, len(keys))
+    assert rc == 0
+
+
+def create_csf(inds, order, fbr_th, fbrs_th):
+    """src/util.h:1320-1436 / 760-850. Returns (ptr[l], idx[l]) lists."""
+    nd = len(inds)
+    n = len(inds[0])
+    L = nd - 1
+    ptr = [np.zeros(n + 2, np.uint64) for _ in range(L)]
+    idx = [np.zeros(n + 2, np.uint64) for _ in range(L)]
+    nptr = (ctypes.c_uint64 * L)()
+    nidx = (ctypes.c_uint64 * L)()
+    o = (ctypes.c_int * nd)(*order)
+    lib().orc_create_csf(nd, ctypes.c_uint64(n), _ptr_array(inds), o, ctypes.c_uint64(fbr_th),
+                         ctypes.c_uint64(fbrs_th), _ptr_array(ptr), _ptr_array(idx), nptr, nidx)
+    return [ptr[l][:nptr[l]].copy() for l in range(L)], [idx[l][:nidx[l]].copy() for l in range(L)]
+
+
+def fbr_like_slc(ptr0, idx0):
+    nslc = len(idx0)
+    nf = int(ptr0[-1]) if len(ptr0) else 0
+    out = np.zeros(max(nf, 1), np.uint64)
+    lib().orc_fbr_like_slc(ptr0.ctypes.data_as(_u64p), idx0.ctypes.data_as(_u64p),
+                           ctypes.c_uint64(nslc), out.ctypes.data_as(_u64p))
+    return out[:nf]
+
+
+def _bins(fn, nd, ptr, tot_nnz):
+    nslc = len(ptr[0]) - 1
+    bin_of = np.zeros(max(nslc, 1), np.int32)
+    fn(nd, _ptr_array(ptr), ctypes.c_uint64(max(nslc, 0)), ctypes.c_uint64(tot_nnz),
+       bin_of.ctypes.data_as(ctypes.POINTER(ctypes.c_int)))
+    bin_of = bin_of[:nslc]
+    return [np.nonzero(bin_of == b)[0].astype(np.uint64) for b in range(10)]
+
+
+def keys_per_sort(nd):
+    """3-D sorts compare two keys, 4-D sorts three (src/util.h:389-410)."""
+    return 2 if nd == 3 else 3
+
+
+def _csf_dict(pfx, order, ptr, idx, inds, vals, with_fbr_like=True):
+    d = {f"{pfx}.nnz": np.array([len(vals)], np.uint64), f"{pfx}.modeOrder": np.array(order, np.uint64)}
+    for l in range(len(ptr)):
+        d[f"{pfx}.fbrPtr{l}"] = ptr[l]
+        d[f"{pfx}.fbrIdx{l}"] = idx[l]
+    nfib = len(ptr[1]) if len(ptr) > 1 else 0
+    d[f"{pfx}.nFibers"] = np.array([nfib], np.uint64)
+    if with_fbr_like:
+        d[f"{pfx}.fbrLikeSlcInds"] = fbr_like_slc(ptr[0], idx[0])[:max(nfib - 1, 0)]
+    for m in range(len(inds)):
+        d[f"{pfx}.inds{m}"] = inds[m].copy()
+    d[f"{pfx}.vals"] = vals.copy()
+    return d
+
+
+# --------------------------------------------------------------------------
+# format builders (mirror the reference main's call sequence)
+# --------------------------------------------------------------------------
+def build_mmcsf(dims, inds, vals, mode=0, fbr_th=INF_TH, partition="all-to-last"):
+    """mttkrp -t 12: src/mttkrp.cu:72-389. partition="all-to-last" is the
+    reference as shipped (src/util.h:2517 assigns every nonzero to partition
+    2). Returns a dict keyed like the reference harness dump."""
+    nd = len(dims)
+    K = keys_per_sort(nd)
+    inds = [np.array(i, dtype=np.uint64) for i in inds]
+    vals = np.array(vals, dtype=np.float32)
+    xorder = order_modes(dims, mode)
+    sort_coo(inds, vals, xorder[:K])
+    orders = []
+    redun = -1
+    for m in range(nd):
+        orders.append(order_modes(dims, m))
+        if m >= 1 and any(orders[m][1] == orders[p][0] and orders[m][0] == orders[p][1] for p in range(m)):
+            redun = m
+        if m != redun:
+            sort_coo(inds, vals, orders[m][:K])
+    if partition != "all-to-last":
+        raise NotImplementedError(partition)
+    part = 2
+    out = {"redunMode": np.array([redun], np.int64), "X.modeOrder": np.array(xorder, np.uint64)}
+    for p in range(nd):
+        pfx = f"part{p}"
+        if p != part or len(vals) == 0:
+            out[f"{pfx}.nnz"] = np.array([0], np.uint64)
+            out[f"{pfx}.modeOrder"] = np.array(orders[p], np.uint64)
+            continue
+        pin = [i.copy() for i in inds]
+        pv = vals.copy()
+        sort_coo(pin, pv, orders[p][:K])
+        ptr, idx = create_csf(pin, orders[p], fbr_th, FBRS_TH_MMCSF)
+        out.update(_csf_dict(pfx, orders[p], ptr, idx, pin, pv))
+    return out
+
+
+def build_bcsf(dims, inds, vals, mode=0, fbr_th=INF_TH):
+    """mttkrp -t 8: src/mttkrp.cu:72-100, 167-236 (create_HCSR, make_KTiling,
+    create_TiledHCSR, make_TiledBin, create_fbrLikeSlcInds)."""
+    nd = len(dims)
+    K = keys_per_sort(nd)
+    inds = [np.array(i, dtype=np.uint64) for i in inds]
+    vals = np.array(vals, dtype=np.float32)
+    order = order_modes(dims, mode)
+    sort_coo(inds, vals, order[:K])
+    ptr, idx = create_csf(inds, order, fbr_th, FBRS_TH_OFF)
+    out = _csf_dict("bcsf", order, ptr, idx, inds, vals)
+    for b, sl in enumerate(_bins(lib().orc_tiled_bins, nd, ptr, len(vals))):
+        out[f"bcsf.bin{b}"] = sl
+    return out
+
+
+def build_hyb(dims, inds, vals, mode=0, fbr_th=INF_TH):
+    """mttkrp -t 10: src/mttkrp.cu:138-151 (create_HCSR, create_HYB[_4D],
+    make_HybBin)."""
+    nd = len(dims)
+    K = keys_per_sort(nd)
+    inds = [np.array(i, dtype=np.uint64) for i in inds]
+    vals = np.array(vals, dtype=np.float32)
+    order = order_modes(dims, mode)
+    sort_coo(inds, vals, order[:K])
+    ptr, idx = create_csf(inds, order, fbr_th, FBRS_TH_OFF)
+    n = len(vals)
+    cap = n + 2
+    coo = [np.zeros(cap, np.uint64) for _ in range(nd)]
+    coov = np.zeros(cap, np.float32)
+    cslp, csli, csl1, csl2 = (np.zeros(cap, np.uint64) for _ in range(4))
+    cslv = np.zeros(cap, np.float32)
+    hptr = [np.zeros(cap, np.uint64) for _ in range(3)]
+    hidx = [np.zeros(cap, np.uint64) for _ in range(3)]
+    hleaf = np.zeros(cap, np.uint64)
+    hv = np.zeros(cap, np.float32)
+    counts = np.zeros(10, np.uint64)
+    nidx = np.array([len(i) for i in idx], np.uint64)
+    fp = ctypes.POINTER(ctypes.c_float)
+    o = (ctypes.c_int * nd)(*order)
+    lib().orc_create_hyb(nd, ctypes.c_uint64(n), _ptr_array(inds), vals.ctypes.data_as(fp), o,
+                         _ptr_array(ptr), _ptr_array(idx), nidx.ctypes.data_as(_u64p), _ptr_array(coo),
+                         coov.ctypes.data_as(fp), cslp.ctypes.data_as(_u64p), csli.ctypes.data_as(_u64p),
+                         csl1.ctypes.data_as(_u64p), csl2.ctypes.data_as(_u64p), cslv.ctypes.data_as(fp),
+                         _ptr_array(hptr), _ptr_array(hidx), hleaf.ctypes.data_as(_u64p),
+                         hv.ctypes.data_as(fp), counts.ctypes.data_as(_u64p))
+    ncoo, ncsl, nh, ncslslc = (int(c) for c in counts[:4])
+    out = {"hyb.COOnnz": np.array([ncoo], np.uint64), "hyb.CSLnnz": np.array([ncsl], np.uint64),
+           "hyb.HCSRnnz": np.array([nh], np.uint64), "hyb.modeOrder": np.array(order, np.uint64)}
+    for m in range(nd):
+        out[f"hyb.COOinds{m}"] = coo[m][:ncoo]
+    out["hyb.COOvals"] = coov[:ncoo]
+    hp = [hptr[l][:int(counts[4 + l])] for l in range(nd - 1)]
+    if nd == 3:
+        out["hyb.CSLslicePtr"] = cslp[:ncslslc + 1]
+        out["hyb.CSLsliceIdx"] = csli[:ncslslc]
+        out["hyb.CSLinds1"] = csl1[:ncsl]
+        out["hyb.CSLinds2"] = csl2[:ncsl]
+        out["hyb.CSLvals"] = cslv[:ncsl]
+    for l in range(nd - 1):
+        out[f"hyb.fbrPtr{l}"] = hp[l]
+        out[f"hyb.fbrIdx{l}"] = hidx[l][:int(counts[7 + l])]
+    out["hyb.indsLeaf"] = hleaf[:nh]
+    out["hyb.vals"] = hv[:nh]
+    for b, sl in enumerate(_bins(lib().orc_hyb_bins, nd, hp, n)):
+        out[f"hyb.bin{b}"] = sl
+    if nd == 3:
+        cslcnt = np.diff(cslp[:ncslslc + 1].astype(np.int64))
+        TB = 512
+        LB = [0, 2, 4, 8, 16, 1024, 4 * TB, 8 * TB, 16 * TB, 32 * TB]
+        UB = [1025, 5, 9, 17, 1025, 4 * TB + 1, 8 * TB + 1, 16 * TB + 1, 32 * TB + 1, n + 1]
+        cb = np.full(ncslslc, -1)
+        for s in range(ncslslc):
+            for b in range(10):
+                if LB[b] < cslcnt[s] < UB[b]:
+                    cb[s] = b
+                    break
+        for b in range(10):
+            out[f"hyb.cslbin{b}"] = np.nonzero(cb == b)[0].astype(np.uint64)
+    return out
+
+
+# --------------------------------------------------------------------------
+# MTTKRP
+# --------------------------------------------------------------------------
+def mttkrp_coo_f32(inds, vals, mode, factors):
+    """MTTKRP_COO_CPU semantics (src/mttkrp_cpu.cpp:60-113) with the output
+    zeroed first. factors: list of float32 (dim, R) arrays (not modified)."""
+    nd = len(inds)
+    R = factors[0].shape[1]
+    U = [np.ascontiguousarray(f, dtype=np.float32).copy() for f in factors]
+    U[mode][:] = 0
+    fp = ctypes.POINTER(ctypes.c_float)
+    ind = [np.ascontiguousarray(i, dtype=np.uint64) for i in inds]
+    v = np.ascontiguousarray(vals, dtype=np.float32)
+    lib().orc_mttkrp_coo_f32(nd, ctypes.c_uint64(len(v)), _ptr_array(ind), v.ctypes.data_as(fp), mode, R,
+                             (fp * nd)(*[u.ctypes.data_as(fp) for u in U]))
+    return U[mode]
+
+
+def mttkrp_coo_f64(dims, inds, vals, mode, factors):
+    """FP64-accumulated MTTKRP: the precision oracle."""
+    nd = len(inds)
+    R = factors[0].shape[1]
+    U = [np.ascontiguousarray(f, dtype=np.float32) for f in factors]
+    out = np.zeros((dims[mode], R), np.float64)
+    fp = ctypes.POINTER(ctypes.c_float)
+    ind = [np.ascontiguousarray(i, dtype=np.uint64) for i in inds]
+    v = np.ascontiguousarray(vals, dtype=np.float32)
+    d = (ctypes.c_uint64 * nd)(*dims)
+    lib().orc_mttkrp_coo_f64(nd, ctypes.c_uint64(len(v)), _ptr_array(ind), v.ctypes.data_as(fp), mode, R,
+                             (fp * nd)(*[u.ctypes.data_as(fp) for u in U]), d,
+                             out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+    return out
+
+
+# --------------------------------------------------------------------------
+# the reference itself (oracle/_ref), when it was built here
+# --------------------------------------------------------------------------
+def ref_available():
+    return os.path.exists(_REF_LIB)
+
+
+_ref = None
+
+
+def ref_lib():
+    global _ref
+    if _ref is None:
+        _ref = ctypes.CDLL(_REF_LIB)
+    return _ref
+
+
+def parse_dump(path):
+    d = {}
+    with open(path) as fh:
+        for line in fh:
+            t = line.split()
+            if not t:
+                continue
+            name, n = t[0], int(t[1])
+            vals = t[2:2 + n]
+            if name.endswith("vals") or name.endswith("Vals"):
+                d[name] = np.array(vals, dtype=np.float64).astype(np.float32)
+            elif name == "redunMode":
+                d[name] = np.array(vals, dtype=np.int64)
+            else:
+                d[name] = np.array(vals, dtype=np.uint64)
+    return d
+
+
+def ref_dump(kind, tns_path, mode, fbr_th, out_path):
+    """Run the reference's own builder for `kind` in {"mmcsf","bcsf","hyb"}."""
+    fn = {"mmcsf": "ref_mmcsf_dump", "bcsf": "ref_bcsf_dump", "hyb": "ref_hyb_dump"}[kind]
+    rc = getattr(ref_lib(), fn)(tns_path.encode(), int(mode), ctypes.c_long(int(fbr_th)), out_path.encode())
+    if rc != 0:
+        raise RuntimeError(f"{fn} failed")
+    return parse_dump(out_path)
+
+
+def ref_mttkrp_coo(dims, inds, vals, mode, factors):
+    """The reference's MTTKRP_COO_CPU on these arrays, output zeroed first."""
+    nd = len(dims)
+    R = factors[0].shape[1]
+    U = [np.ascontiguousarray(f, dtype=np.float32).copy() for f in factors]
+    U[mode][:] = 0
+    fp = ctypes.POINTER(ctypes.c_float)
+    ind = [np.ascontiguousarray(i, dtype=np.uint64) for i in inds]
+    v = np.ascontiguousarray(vals, dtype=np.float32)
+    d = (ctypes.c_uint64 * nd)(*dims)
+    rc = ref_lib().ref_coo_mttkrp(nd, d, ctypes.c_uint64(len(v)), _ptr_array(ind), v.ctypes.data_as(fp),
+                                  mode, R, (fp * nd)(*[u.ctypes.data_as(fp) for u in U]))
+    assert rc == 0
+    return U[mode]

@@ -1,0 +1,115 @@
+#!/usr/bin/env python3
+"""Generate the golden fixtures in tests/golden/ from the reference itself.
+
+Runs the reference's own format builders and COO CPU MTTKRP (built as
+oracle/_ref/libmmcsf_ref.so by oracle/build_ref.py from the reference's
+sources) on the reference's toy.tns and on seeded synthetic tensors, and
+writes inputs and outputs as JSON. The tests compare both the C oracle and
+the CUDA library against these files, so they run without the reference.
+
+Usage: python tests/golden/make_golden.py [--reference /root/reference]
+"""
+import argparse
+import json
+import os
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+from oracle import build_ref  # noqa: E402
+from oracle import oracle as O  # noqa: E402
+
+R_GOLD = 8
+
+
+def _tolist(a):
+    a = np.asarray(a)
+    if a.dtype.kind == "f":
+        return [float(x) for x in a]
+    return [int(x) for x in a]
+
+
+def _rand_tensor(rng, dims, n, skew=False, dup=False, ints=False):
+    if skew:
+        inds = [np.minimum(rng.zipf(1.6, n) - 1, d - 1).astype(np.uint64) for d in dims]
+    else:
+        inds = [rng.integers(0, d, n).astype(np.uint64) for d in dims]
+    if not dup:
+        key = np.zeros(n, np.uint64)
+        for m, d in enumerate(dims):
+            key = key * np.uint64(d) + inds[m]
+        _, first = np.unique(key, return_index=True)
+        first = np.sort(first)
+        inds = [i[first] for i in inds]
+    k = len(inds[0])
+    vals = (rng.integers(1, 51, k).astype(np.float32) if ints
+            else (rng.random(k) + 0.25).astype(np.float32))
+    return inds, vals
+
+
+def make_case(name, dims, inds, vals, tmp, runs, seed):
+    path = os.path.join(tmp, name + ".tns")
+    O.write_tns(path, dims, inds, vals)
+    dims2, inds2, vals2 = O.load_tns(path)
+    case = {"name": name, "dims": [int(d) for d in dims], "inds": [_tolist(i) for i in inds2],
+            "vals": _tolist(vals2), "formats": [], "mttkrp": []}
+    for kind, mode, fth in runs:
+        d = O.ref_dump(kind, path, mode, fth, os.path.join(tmp, "dump.txt"))
+        case["formats"].append({"kind": kind, "mode": mode, "f": int(fth),
+                                "arrays": {k: _tolist(v) for k, v in d.items()}})
+    rng = np.random.default_rng(seed)
+    U = [rng.random((d, R_GOLD)).astype(np.float32) for d in dims]
+    case["factors"] = [[_tolist(row) for row in u] for u in U]
+    for m in range(len(dims)):
+        out = O.ref_mttkrp_coo(dims2, inds2, vals2, m, U)
+        case["mttkrp"].append({"mode": m, "R": R_GOLD, "out": [_tolist(row) for row in out]})
+    with open(os.path.join(HERE, name + ".json"), "w") as fh:
+        json.dump(case, fh, separators=(",", ":"))
+    return name
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--reference", default="/root/reference")
+    a = ap.parse_args()
+    build_ref.build(os.path.join(a.reference, "src"))
+    tmp = tempfile.mkdtemp()
+    names = []
+    INF = O.INF_TH
+    # the reference's own fixture
+    dims, inds, vals = O.load_tns(os.path.join(a.reference, "toy.tns"))
+    runs = [(k, m, f) for k in ("mmcsf", "bcsf", "hyb") for m in range(3) for f in (1, 2, 128)]
+    names.append(make_case("toy", dims, inds, vals, tmp, runs, seed=0))
+
+    rng = np.random.default_rng(20261203)
+    specs = [
+        ("uni3d", [30, 25, 20], 400, dict()),
+        ("skew3d", [40, 60, 25], 600, dict(skew=True)),
+        ("dup3d", [6, 5, 7], 150, dict(dup=True)),
+        ("equal3d", [12, 12, 12], 300, dict()),
+        ("uni4d", [15, 9, 11, 5], 500, dict(ints=True)),
+        ("skew4d", [50, 20, 10, 4], 900, dict(skew=True, ints=True)),
+        ("fbrs4d", [3, 2, 4, 60], 700, dict()),
+        ("single3d", [4, 4, 4], 1, dict()),
+        ("single4d", [3, 3, 3, 3], 1, dict()),
+    ]
+    for name, dims, n, kw in specs:
+        inds, vals = _rand_tensor(rng, dims, n, **kw)
+        nd = len(dims)
+        runs = []
+        for kind in ("mmcsf", "bcsf", "hyb"):
+            for f in (1, 3, INF):
+                runs.append((kind, int(rng.integers(0, nd)), f))
+        names.append(make_case(name, dims, inds, vals, tmp, runs, seed=len(names)))
+    with open(os.path.join(HERE, "manifest.json"), "w") as fh:
+        json.dump({"cases": names, "R": R_GOLD,
+                   "source": "reference host code built by oracle/build_ref.py"}, fh, indent=1)
+    print("wrote", names)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,372 @@
+#!/usr/bin/env python3
+"""All-mode MTTKRP benchmark (MM-CSF, B200).
+
+Workload (default): 3-mode tensor 500,000 x 2,000,000 x 20,000 with 100M
+nonzeros, every mode index Zipf(s=1.1) after a seeded permutation, values
+lognormal(0,1), rank R=32 FP32 factors uniform in [0,1); MM-CSF format
+(-t 12, -m 0, no fiber split). A step is one all-mode MTTKRP (every mode from
+the same input factors), the reference's MTTKRP_MIHCSR_GPU loop.
+
+value      = effective HBM GB/s over all ranks: the MM-CSF traversal's
+             algorithmic bytes per all-mode MTTKRP (structure read once per
+             mode, every touched factor row once, the dense output written
+             once) / device time per step.
+e2e        = the same bytes / time of the host-buffer C-ABI call
+             (mmcsf_mttkrp_all_host: factors H2D, all modes, outputs D2H).
+roofline   = the dominant mode's kernel: its algorithmic bytes / its average
+             CUDA-event duration, against MEASURED_PEAKS.json's HBM copy rate.
+cpu_baseline / --impl reference = the reference's own MTTKRP_COO_CPU
+             (oracle/_ref, single-threaded as shipped) on a bounded sample of
+             the same nonzeros, extrapolated to the full workload.
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+import argparse
+import csv
+import io
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "mm-csf_b200")
+for _p in (ROOT, PKG):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+METRIC = "all-mode MTTKRP ms & HBM GB/s (effective GB/s = MM-CSF algorithmic bytes / all-mode time)"
+
+WORKLOADS = {
+    "skewed3d": dict(dims=[500000, 2000000, 20000], nnz=100_000_000, dist=[1, 1, 1], zipf=1.1, val=1, R=32,
+                     desc="500000x2000000x20000, 100M nnz, Zipf(1.1) per mode, lognormal values, R=32"),
+    "uniform3d": dict(dims=[1000, 1000, 1000], nnz=100_000, dist=[0, 0, 0], zipf=1.0, val=0, R=32,
+                      desc="1000^3, 100k uniform nnz, R=32"),
+}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="skewed3d", choices=list(WORKLOADS))
+    ap.add_argument("--nnz", type=int, default=0, help="override nonzero count (profiling on a small case)")
+    ap.add_argument("--rank", type=int, default=0, help="override R")
+    ap.add_argument("--fiber-threshold", type=int, default=0)
+    ap.add_argument("--dtype", default="f32", choices=["f32", "bf16"])
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def traffic_from_profiles(workload, R, dtype):
+    """dram bytes per launch of the dominant kernel from a committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", f"traffic_{workload}_R{R}_{dtype}.txt")
+    if not os.path.exists(p):
+        return None
+    with open(p) as fh:
+        for line in fh:
+            if line.startswith("traffic_bytes_per_launch:"):
+                return float(line.split(":", 1)[1])
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, dev):
+        self.dev = dev
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.dev), "-lms", "100"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        time.sleep(0.3)
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.2)
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        rows = [r for r in csv.reader(io.StringIO(out)) if len(r) >= 9]
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+            except ValueError:
+                continue
+            for i, n in enumerate(names):
+                if r[5 + i].strip().lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def algorithmic_bytes(nd, dims, nnz, R, esz, nfib, nfbrs, rows_touched):
+    """Per-mode compulsory bytes of the MM-CSF traversal (3-D: vals, leaf
+    index, fiber pointer/index/slice map; 4-D adds fiber->fbrS and the fbrS
+    index and slice map), every touched input-factor row once, and the dense
+    output written once."""
+    per_mode = []
+    struct = nnz * 8 + (nfib * 12 if nd == 3 else nfib * 12 + nfbrs * 8)
+    for m in range(nd):
+        fact = sum(rows_touched[q] * R * esz for q in range(nd) if q != m)
+        per_mode.append(struct + fact + dims[m] * R * 4)
+    return per_mode
+
+
+def workload_stats(inds_dev, dims, order):
+    """Rows touched per mode and fiber count (no split) with torch ops."""
+    import torch
+    rows = [int(torch.unique(i).numel()) for i in inds_dev]
+    o0, o1 = order[0], order[1]
+    key = inds_dev[o0].long() * dims[o1] + inds_dev[o1].long()
+    nfib = int(torch.unique(key).numel())
+    return rows, nfib
+
+
+def device_coo(X):
+    """Device index arrays of a CooTensor as torch int32 tensors (copies)."""
+    inds, vals = X.device_tensors()
+    return [i.clone() for i in inds], vals.clone()
+
+
+def reference_sample_time(inds_host, vals_host, dims, R, target_s=12.0, max_n=None):
+    """Time the reference's MTTKRP_COO_CPU (all modes) on the first S nonzeros,
+    S sized so the run takes about target_s seconds. Returns (seconds, S, kind)."""
+    import numpy as np
+
+    from oracle import oracle as O
+    use_ref = O.ref_available()
+    kind = "reference" if use_ref else "port"
+    fn = O.ref_mttkrp_coo if use_ref else (lambda d, i, v, m, U: O.mttkrp_coo_f32(i, v, m, U))
+    n_all = len(vals_host)
+    rng = np.random.default_rng(0)
+    U = [rng.random((d, R)).astype(np.float32) for d in dims]
+
+    def run(S):
+        ind = [np.ascontiguousarray(i[:S].astype(np.uint64)) for i in inds_host]
+        v = np.ascontiguousarray(vals_host[:S])
+        t = time.perf_counter()
+        for m in range(len(dims)):
+            fn(dims, ind, v, m, U)
+        return time.perf_counter() - t
+
+    S = min(200_000, n_all)
+    t = run(S)
+    S2 = int(min(max_n or n_all, n_all, max(S, S * target_s / max(t, 1e-3))))
+    if S2 > S * 1.5:
+        t = run(S2)
+        S = S2
+    return t, S, kind
+
+
+def main():
+    a = parse()
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    W = WORKLOADS[a.workload]
+    dims = W["dims"]
+    nd = len(dims)
+    nnz = a.nnz or W["nnz"]
+    R = a.rank or W["R"]
+    esz = 4 if a.dtype == "f32" else 2
+    hbm_peak, peak_kind = peaks()
+    config = {"workload": a.workload, "desc": W["desc"], "nnz": nnz, "R": R, "format": "MM-CSF (-t 12, -m 0)",
+              "fiber_threshold": a.fiber_threshold or "none", "factor_dtype": a.dtype,
+              "l2": "inputs larger than L2 (structure > 800 MB per step)", "seed": a.seed,
+              "parallelism": f"replicas x{world} (each rank its own tensor)"}
+
+    if a.impl == "reference":
+        if rank != 0:
+            return
+        torch.cuda.set_device(local)
+        import mmcsf
+        X = mmcsf.CooTensor.generate(dims, nnz, dist=W["dist"], zipf_s=W["zipf"], val_dist=W["val"],
+                                     seed=a.seed)
+        inds_dev, _ = device_coo(X)
+        from oracle import oracle as O
+        order = O.order_modes(dims, 2)
+        rows, nfib = workload_stats(inds_dev, dims, order)
+        per_mode = algorithmic_bytes(nd, dims, nnz, R, esz, nfib, 0, rows)
+        step_bytes = sum(per_mode)
+        inds_h, vals_h = X.host_arrays()
+        del inds_dev
+        # one step = the reference's MTTKRP_COO_CPU over all modes on a sample
+        # of the nonzeros, sized so warmup + steps finish in a few minutes
+        budget = 150.0 / max(1, a.steps + a.warmup)
+        _, S, kind = reference_sample_time(inds_h, vals_h, dims, R, target_s=min(20.0, budget))
+        ind = [np.ascontiguousarray(x[:S].astype(np.uint64)) for x in inds_h]
+        v = np.ascontiguousarray(vals_h[:S])
+        rng = np.random.default_rng(0)
+        Uh = [rng.random((d, R)).astype(np.float32) for d in dims]
+        fn = O.ref_mttkrp_coo if kind == "reference" else (lambda d, i_, v_, m, U_: O.mttkrp_coo_f32(i_, v_, m, U_))
+        times = []
+        for i in range(a.warmup + a.steps):
+            t0 = time.perf_counter()
+            for m in range(nd):
+                fn(dims, ind, v, m, Uh)
+            if i >= a.warmup:
+                times.append(time.perf_counter() - t0)
+        ts = statistics.mean(times) * nnz / S
+        val = step_bytes / ts / 1e9
+        line = {"metric": METRIC, "value": val, "unit": "GB/s", "n_gpus": a.gpus, "steps": a.steps,
+                "warmup": a.warmup, "ms_per_step": ts * 1e3, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator)", "impl": "reference",
+                "config": config,
+                "cpu_baseline": {"value": val, "unit": "GB/s", "cores": 1, "kind": kind,
+                                 "sample": f"first {S} of {nnz} nonzeros, all {nd} modes, MTTKRP_COO_CPU "
+                                           f"(serial as shipped: src/mttkrp_cpu.cpp:79), extrapolated x{nnz / S:.1f}"},
+                "e2e": {"value": val, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+
+    # ---- our arm ---------------------------------------------------------------
+    if world > 1:
+        torch.cuda.set_device(local)
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    else:
+        torch.cuda.set_device(0)
+    import mmcsf
+    X = mmcsf.CooTensor.generate(dims, nnz, dist=W["dist"], zipf_s=W["zipf"], val_dist=W["val"],
+                                 seed=a.seed + rank)
+    F = mmcsf.Format(X, impl=mmcsf.IMPL_MMCSF, mode=0, fiber_threshold=a.fiber_threshold)
+    info = F.info(2)
+    inds_dev, _ = device_coo(X)
+    rows, nfib_nosplit = workload_stats(inds_dev, dims, info["mode_order"])
+    del inds_dev
+    per_mode = algorithmic_bytes(nd, dims, nnz, R, esz, info["n_fibers"], info["n_fbrs"], rows)
+    step_bytes = sum(per_mode)
+    g = torch.Generator(device="cuda").manual_seed(1234 + rank)
+    tdt = torch.float32 if a.dtype == "f32" else torch.bfloat16
+    U = [torch.rand(d, R, device="cuda", generator=g).to(tdt) for d in dims]
+    outs = [torch.empty(d, R, device="cuda") for d in dims]
+    stream = torch.cuda.current_stream()
+
+    for _ in range(a.warmup):
+        F.mttkrp_all(U, outs)
+    launches_per_step = F.last_launches
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    sampler = ClockSampler(local) if rank == 0 else None
+    if sampler:
+        sampler.start()
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(nd + 1)] for _ in range(a.steps)]
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for k in range(a.steps):
+        ev[k][0].record(stream)
+        for m in range(nd):
+            F.mttkrp(m, U, outs[m])
+            ev[k][m + 1].record(stream)
+    t1.record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = sampler.stop() if sampler else None
+    total_ms = t0.elapsed_time(t1)
+    mode_ms = [statistics.mean(ev[k][m].elapsed_time(ev[k][m + 1]) for k in range(a.steps)) for m in range(nd)]
+    tmax = torch.tensor([total_ms], device="cuda")
+    if world > 1:
+        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+    total_ms = float(tmax.item())
+    ms_per_step = total_ms / a.steps
+    value = world * step_bytes * a.steps / (total_ms / 1e3) / 1e9
+
+    # e2e through the host-buffer C-ABI call (pinned host memory)
+    e2e = None
+    if not a.no_e2e and a.dtype == "f32":
+        hU = [u.float().cpu().pin_memory() for u in U]
+        hO = [torch.empty(d, R).pin_memory() for d in dims]
+        for _ in range(min(a.warmup, 2)):
+            F.mttkrp_all_host(hU, hO)
+        ke = max(1, min(a.steps, 20))
+        if world > 1:
+            dist.barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(ke):
+            F.mttkrp_all_host(hU, hO)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        em = torch.tensor([e0.elapsed_time(e1)], device="cuda")
+        if world > 1:
+            dist.all_reduce(em, op=dist.ReduceOp.MAX)
+        e_ms = float(em.item()) / ke
+        hb = sum(d * R * 4 for d in dims)
+        e2e = {"value": world * step_bytes / (e_ms / 1e3) / 1e9, "unit": "GB/s", "ms_per_step": e_ms,
+               "h2d_bytes_per_step": hb, "d2h_bytes_per_step": hb}
+
+    if rank != 0:
+        if world > 1:
+            dist.destroy_process_group()
+        return
+    dom = max(range(nd), key=lambda m: mode_ms[m])
+    achieved = per_mode[dom] / (mode_ms[dom] / 1e3) / 1e9
+    traffic = traffic_from_profiles(a.workload, R, a.dtype)
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
+                "traffic": traffic, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                "kernel": f"k_mttkrp mode {dom} (level {info['mode_order'].index(dom)} of order "
+                          f"{info['mode_order']})",
+                "algorithmic_bytes": per_mode[dom], "avg_ms": mode_ms[dom]}
+    cpu = None
+    if not a.no_cpu and world == 1:
+        inds_h, vals_h = X.host_arrays()
+        t, S, kind = reference_sample_time(inds_h, vals_h, dims, R, target_s=12.0)
+        ts = t * nnz / S
+        cpu = {"value": step_bytes / ts / 1e9, "unit": "GB/s", "cores": 1, "kind": kind,
+               "ms_per_step": ts * 1e3,
+               "sample": f"first {S} of {nnz} nonzeros, all {nd} modes, MTTKRP_COO_CPU serial as shipped, "
+                         f"extrapolated x{nnz / S:.1f}"}
+    line = {"metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": a.dtype, "data": "synthetic (seeded device generator)",
+            "config": config, "mode_ms": mode_ms, "format": info, "roofline": roofline, "cpu_baseline": cpu,
+            "e2e": e2e, "gpu_launches": launches_per_step * a.steps, "clocks": clocks}
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,189 @@
+/*
+ * mmcsf.h — C ABI of the B200-native MM-CSF sparse MTTKRP library.
+ *
+ * Plain C types only (pointers, sizes, integers); CUDA streams are passed as
+ * `void*` (a cudaStream_t, NULL = the legacy default stream). Every call
+ * returns an mmcsf_status and never exits or asserts; mmcsf_last_error()
+ * gives a message for the last failure on the calling thread.
+ *
+ * Each declaration names the reference (isratnisa/MM-CSF) interface it
+ * replaces. The reference has no plugin layer; its boundary is the C++
+ * function API in src/mttkrp_gpu.h:59-81 plus the builders in src/util.h.
+ *
+ * Index limits: every mode length and the nonzero count must be below 2^32
+ * (indices are stored as uint32 on the device; the reference uses size_t).
+ */
+#ifndef MMCSF_H
+#define MMCSF_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status ------------------------------------------------------------ */
+typedef enum {
+  MMCSF_OK = 0,
+  MMCSF_ERR_INVALID = 1,     /* bad argument; the reference prints and exit(0)s (src/util.h:238-248) */
+  MMCSF_ERR_CUDA = 2,        /* a CUDA call failed; the reference asserts (src/mttkrp_gpu.cu:60-67) */
+  MMCSF_ERR_NOMEM = 3,       /* host or device allocation failed */
+  MMCSF_ERR_IO = 4,          /* file missing or malformed; the reference exit(0)s (src/util.h:327-330) */
+  MMCSF_ERR_UNSUPPORTED = 5, /* valid request this build does not implement */
+  MMCSF_ERR_TIMEOUT = 6      /* a bounded device-side wait gave up */
+} mmcsf_status;
+
+/* Text for a status code. */
+const char* mmcsf_status_string(int status);
+/* Message for the last failure on this thread ("" if none). */
+const char* mmcsf_last_error(void);
+/* Library version as 10000*major + 100*minor + patch. */
+int mmcsf_version(void);
+
+/* ---- implementation types: the reference's -t values (src/mttkrp.cu) --- */
+#define MMCSF_IMPL_COO_CPU 1 /* -t 1: reference CPU path (not provided here; see the oracle) */
+#define MMCSF_IMPL_BCSF 8    /* -t 8: B-CSF, single mode */
+#define MMCSF_IMPL_HBCSF 10  /* -t 10: HB-CSF, single mode */
+#define MMCSF_IMPL_MMCSF 12  /* -t 12: MM-CSF, all modes from one partitioned format */
+
+/* Factor element types for MTTKRP inputs (outputs are always float32). */
+#define MMCSF_DTYPE_F32 0
+#define MMCSF_DTYPE_BF16 1
+
+/* ---- COO tensors --------------------------------------------------------
+ * Replaces Tensor + load_tensor (src/util.h:80-104, 313-370). A COO handle
+ * holds 0-based uint32 indices per mode and float32 values, on the host, on
+ * the device, or both. */
+typedef struct mmcsf_coo mmcsf_coo;
+
+/* Parse a .tns file (line 1: order; line 2: mode lengths; then 1-based
+ * coordinates and a value per line). Replaces load_tensor
+ * (src/util.h:313-370); the nonzero count is the number of parsed entries. */
+int mmcsf_coo_load_tns(const char* path, mmcsf_coo** out);
+/* Copy caller host arrays into a new handle (inds[m][x] 0-based). */
+int mmcsf_coo_create(int nd, const uint64_t* dims, uint64_t nnz, const uint32_t* const* inds,
+                     const float* vals, mmcsf_coo** out);
+/* Wrap-copy caller DEVICE arrays into a new handle (stream-ordered copy). */
+int mmcsf_coo_create_device(int nd, const uint64_t* dims, uint64_t nnz, const uint32_t* const* d_inds,
+                            const float* d_vals, void* stream, mmcsf_coo** out);
+int mmcsf_coo_info(const mmcsf_coo* X, int* nd, uint64_t* dims, uint64_t* nnz);
+/* Make sure the host (resp. device) copy exists; synchronous. */
+int mmcsf_coo_to_host(mmcsf_coo* X);
+int mmcsf_coo_to_device(mmcsf_coo* X, void* stream);
+/* Borrow array pointers (host or device copy; NULL if absent). inds must
+ * have room for nd pointers. */
+int mmcsf_coo_host_arrays(const mmcsf_coo* X, const uint32_t** inds, const float** vals);
+int mmcsf_coo_device_arrays(const mmcsf_coo* X, const uint32_t** d_inds, const float** d_vals);
+/* Write as .tns (1-based). */
+int mmcsf_coo_write_tns(mmcsf_coo* X, const char* path);
+void mmcsf_coo_destroy(mmcsf_coo* X);
+
+/* ---- synthetic tensors --------------------------------------------------
+ * Seeded generator for the benchmark shapes (no counterpart in the
+ * reference, whose tools/generate_tensor.py writes .tns text). Coordinates
+ * per mode are uniform or Zipf(s) mapped through a seeded permutation;
+ * duplicates are dropped keeping the first occurrence, and new candidates are
+ * drawn until `nnz` distinct coordinates exist. Runs on the device. */
+#define MMCSF_DIST_UNIFORM 0
+#define MMCSF_DIST_ZIPF 1
+#define MMCSF_VAL_UNIFORM01 0 /* uniform in (0, 1] */
+#define MMCSF_VAL_LOGNORMAL 1 /* lognormal(0, 1) */
+#define MMCSF_VAL_INT1_50 2   /* integer counts 1..50 stored as float */
+typedef struct {
+  int nd;
+  uint64_t dims[4];
+  uint64_t nnz;
+  int dist[4];        /* MMCSF_DIST_* per mode */
+  double zipf_s[4];   /* exponent for Zipf modes */
+  int val_dist;       /* MMCSF_VAL_* */
+  uint64_t seed;
+} mmcsf_gen_spec;
+int mmcsf_generate(const mmcsf_gen_spec* spec, void* stream, mmcsf_coo** out);
+
+/* ---- formats ------------------------------------------------------------
+ * Replaces the host-side builders the reference's main runs before a GPU
+ * call: sort_COOtensor, create_HCSR, mm_partition_reuseBased,
+ * populate_paritions, sort_MI_CSF, create_TiledHCSR, create_fbrLikeSlcInds,
+ * make_TiledBin, create_HYB, make_HybBin (src/util.h:389-2526,
+ * src/mttkrp.cu:72-389). Built on the device with radix-sort and scan
+ * kernels; every index array is bit-exact to the reference's (with its sort
+ * made stable). */
+typedef struct {
+  int impl;                 /* MMCSF_IMPL_MMCSF, _BCSF or _HBCSF (-t) */
+  int mode;                 /* -m: drives the first sort; the computed mode for B-CSF/HB-CSF */
+  uint64_t fiber_threshold; /* -f: max nonzeros per fiber; 0 = the reference default (99999999) */
+  int partition_rule;       /* 0: the reference as shipped (all nonzeros to partition 2, src/util.h:2517) */
+  int keep_coo;             /* 1: keep every mode's sorted index array on the device for export */
+} mmcsf_build_opts;
+
+typedef struct mmcsf_format mmcsf_format;
+int mmcsf_build(mmcsf_coo* X, const mmcsf_build_opts* opts, void* stream, mmcsf_format** out);
+void mmcsf_format_destroy(mmcsf_format* F);
+
+/* Per-partition summary (the numbers the reference prints at
+ * src/mttkrp_gpu.cu:3757-3767). part: 0..nd-1 for MM-CSF (a partition per
+ * mode), 0 for B-CSF, 0 = CSF part / 1 = COO part / 2 = CSL part for HB-CSF. */
+typedef struct {
+  int present;
+  int nd;
+  int mode_order[4];
+  uint64_t nnz;
+  uint64_t n_slices;  /* level-0 entries */
+  uint64_t n_fbrs;    /* level-1 entries (4-D: fbrS) */
+  uint64_t n_fibers;  /* leaf-fiber entries (3-D: = n_fbrs) */
+  uint64_t device_bytes;
+} mmcsf_part_info;
+int mmcsf_format_info(const mmcsf_format* F, int part, mmcsf_part_info* info);
+/* Reference-side scalars: redunMode (-1 if none) and X's mode order. */
+int mmcsf_format_meta(const mmcsf_format* F, int* redun_mode, int* x_mode_order);
+
+/* Copy one array to host, named as the reference names it (widened to
+ * uint64): "fbrPtr<l>", "fbrIdx<l>", "fbrLikeSlcInds", "inds<m>" (needs
+ * keep_coo; m = tensor mode), "indsLeaf", "bin<b>" (B-CSF/HB-CSF), and for
+ * HB-CSF parts 1/2 "COOinds<l>", "CSLslicePtr", "CSLsliceIdx", "CSLinds<l>",
+ * "cslbin<b>". Pass dst=NULL to query the count. Values: "vals", "COOvals",
+ * "CSLvals" through mmcsf_format_export_f32. */
+int mmcsf_format_export(const mmcsf_format* F, int part, const char* name, uint64_t* dst, uint64_t cap,
+                        uint64_t* count);
+int mmcsf_format_export_f32(const mmcsf_format* F, int part, const char* name, float* dst, uint64_t cap,
+                            uint64_t* count);
+
+/* ---- MTTKRP -------------------------------------------------------------
+ * Replaces MTTKRP_MIHCSR_GPU (src/mttkrp_gpu.cu:3380-3784), MTTKRP_B_HCSR_GPU
+ * (:1850-2129) and MTTKRP_HYB_GPU (:2530-2851). Factor matrices are
+ * row-major dims[m] x R on the device; out (dims[mode] x R float32) is
+ * overwritten with X_(mode) (Khatri-Rao of the other factors). Correct for
+ * any R >= 1 (the reference's kernels are only correct for R <= 32).
+ * Stream-ordered; nothing is synchronised. */
+typedef struct {
+  int chunk;         /* nonzeros per worker team; 0 = auto */
+  int block_threads; /* threads per CTA; 0 = auto (256) */
+  int leaf_variant;  /* leaf-mode kernel: 0 auto, 1 scatter atomics, 2 privatised hot rows */
+  int reserved[5];
+} mmcsf_kernel_cfg;
+
+/* One mode. factor_dtype: MMCSF_DTYPE_F32 (d_factors are float*) or
+ * MMCSF_DTYPE_BF16 (d_factors are __nv_bfloat16*, FP32 accumulation). For
+ * B-CSF/HB-CSF formats only the built mode is available. */
+int mmcsf_mttkrp(const mmcsf_format* F, int mode, int R, int factor_dtype, const void* const* d_factors,
+                 float* d_out, const mmcsf_kernel_cfg* cfg, void* stream);
+/* All modes, each from the same input factors: d_outs[m] gets mode m.
+ * (The reference's all-mode loop, src/mttkrp_gpu.cu:3548-3724.) */
+int mmcsf_mttkrp_all(const mmcsf_format* F, int R, int factor_dtype, const void* const* d_factors,
+                     float* const* d_outs, const mmcsf_kernel_cfg* cfg, void* stream);
+/* All modes through HOST buffers: copies the factors host->device, runs
+ * every mode, copies every output device->host and synchronises the stream.
+ * The end-to-end form of MTTKRP_MIHCSR_GPU, which takes host Matrix objects.
+ * Device staging buffers are kept by the format between calls. */
+int mmcsf_mttkrp_all_host(mmcsf_format* F, int R, const float* const* h_factors, float* const* h_outs,
+                          const mmcsf_kernel_cfg* cfg, void* stream);
+
+/* Number of kernel launches the last MTTKRP/build call on this format made
+ * (instrumentation for launch accounting). */
+int mmcsf_format_last_launches(const mmcsf_format* F, int* launches);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MMCSF_H */

@@ -1,0 +1,536 @@
+// Format construction on the device.
+//
+// The reference builds every format on the host (src/util.h:255-2526) with a
+// chain of unstable sample sorts, pointer-chasing scans and push_backs. Here
+// the same arrays come out of:
+//   1. host planning that replays the reference's decisions (mode orders,
+//      redundant mode, which sorts run in which order, partition rule);
+//   2. ONE stable LSD radix sort on a composite key: a chain of stable sorts
+//      equals a single stable sort keyed by the last sort's keys, then the
+//      previous sort's, and so on (keys already present are dropped), with
+//      ties left in file order;
+//   3. boundary flags + exclusive scans + compactions for every CSF level,
+//      fiber splitting at the -f threshold by position-in-run arithmetic, and
+//      the 4-D fbrS split at 128 nonzeros by a warp-per-run greedy scan.
+#include <algorithm>
+#include <memory>
+#include <cstring>
+#include <vector>
+
+#include "format.h"
+#include "prims.cuh"
+
+using mmcsf::set_error;
+
+namespace mmcsf {
+namespace {
+
+constexpr uint64_t REF_DEFAULT_FBR_TH = 99999999ull;  // src/util.h:212
+constexpr uint64_t FBRS_TH_MMCSF = 128;               // src/util.h:1325-1326
+constexpr uint64_t FBRS_TH_OFF = 999999999ull;
+
+struct Idx4 {
+  const uint32_t* p[4];
+};
+
+// ---- kernels --------------------------------------------------------------
+
+__global__ void k_pack(Idx4 in, const uint32_t* __restrict__ perm, int nk, Idx4 dummy, uint64_t n,
+                       int4 modes, int4 shifts, uint64_t* __restrict__ keys) {
+  (void)dummy;
+  const int md[4] = {modes.x, modes.y, modes.z, modes.w};
+  const int sh[4] = {shifts.x, shifts.y, shifts.z, shifts.w};
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    uint32_t src = perm ? perm[i] : (uint32_t)i;
+    uint64_t k = 0;
+    for (int j = 0; j < nk; ++j) k |= (uint64_t)in.p[md[j]][src] << sh[j];
+    keys[i] = k;
+  }
+}
+
+// flag[x] = 1 where any of the first L level keys changes (x == 0 included)
+__global__ void k_run_flags(Idx4 lev, int L, uint64_t n, uint32_t* __restrict__ flag) {
+  for (uint64_t x = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; x < n; x += (uint64_t)gridDim.x * blockDim.x) {
+    uint32_t f = (x == 0);
+    if (!f)
+      for (int l = 0; l < L; ++l) f |= (lev.p[l][x] != lev.p[l][x - 1]);
+    flag[x] = f;
+  }
+}
+
+// out[excl[i]] = i where flag[i]
+__global__ void k_compact_pos(const uint32_t* __restrict__ flag, const uint32_t* __restrict__ excl, uint64_t n,
+                              uint32_t* __restrict__ out) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    if (flag[i]) out[excl[i]] = (uint32_t)i;
+}
+
+// new fiber at every th-th nonzero of a run (greedy chunks of th, src/util.h:1366-1374)
+__global__ void k_split_flags(const uint32_t* __restrict__ excl_run, const uint32_t* __restrict__ run_start,
+                              uint64_t n, uint64_t th, uint32_t* __restrict__ flag) {
+  for (uint64_t x = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; x < n; x += (uint64_t)gridDim.x * blockDim.x) {
+    uint32_t run = excl_run[x + 1] - 1;
+    uint64_t pos = x - run_start[run];
+    flag[x] = (pos % th) == 0;
+  }
+}
+
+// flag[i] = 1 where a level key differs between nonzero starts[i] and starts[i]-1
+__global__ void k_flags_at(Idx4 lev, int L, const uint32_t* __restrict__ starts, uint64_t n,
+                           uint32_t* __restrict__ flag) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    uint32_t x = starts[i];
+    uint32_t f = (x == 0);
+    if (!f)
+      for (int l = 0; l < L; ++l) f |= (lev.p[l][x] != lev.p[l][x - 1]);
+    flag[i] = f;
+  }
+}
+
+// out[i] = a[b[i]] (double indirection helper when a needs an index from b)
+__global__ void k_gather2(const uint32_t* __restrict__ a, const uint32_t* __restrict__ b,
+                          const uint32_t* __restrict__ c, uint64_t n, uint32_t* __restrict__ out) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    out[i] = a[b[c ? c[i] : i]];
+}
+
+__global__ void k_gather_f32(const float* __restrict__ in, const uint32_t* __restrict__ perm, uint64_t n,
+                             float* __restrict__ out) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    out[i] = in[perm[i]];
+}
+
+__global__ void k_set1(uint32_t* p, uint64_t i, uint32_t v) { p[i] = v; }
+
+// parent id of every child: out[c] = (inclusive scan of flag)[c] - 1
+__global__ void k_parent(const uint32_t* __restrict__ excl, uint64_t n, uint32_t* __restrict__ out) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    out[i] = excl[i + 1] - 1;
+}
+
+// 4-D fbrS split (src/util.h:1388-1405): inside each (o0,o1) run of fibers a
+// new fbrS starts at fiber g when fptr[g] > fptr[s] + th - off, s being the
+// current fbrS's first fiber and off = 0 only for the fbrS that starts at
+// nonzero 0 (the reference's counter starts one lower there). One warp per run.
+__global__ void k_fbrs_split(const uint32_t* __restrict__ fptr, const uint32_t* __restrict__ run_first,
+                             uint64_t nruns, uint64_t nfib, uint64_t th, uint32_t* __restrict__ fsflag) {
+  const int lane = threadIdx.x & 31;
+  const uint64_t warps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  for (uint64_t r = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; r < nruns; r += warps) {
+    const uint64_t g0 = run_first[r], g1 = (r + 1 < nruns) ? run_first[r + 1] : nfib;
+    uint64_t s = g0;
+    uint64_t off = (fptr[g0] == 0) ? 0 : 1;
+    for (;;) {
+      const uint64_t limit = (uint64_t)fptr[s] + th - off;
+      uint64_t found = g1;
+      for (uint64_t base = s + 1; base < g1; base += 32) {
+        uint64_t g = base + lane;
+        bool pred = g < g1 && (uint64_t)fptr[g] > limit;
+        unsigned b = __ballot_sync(0xffffffffu, pred);
+        if (b) { found = base + (__ffs(b) - 1); break; }
+      }
+      if (found >= g1) break;
+      if (lane == 0) fsflag[found] = 1;
+      s = found;
+      off = 1;
+    }
+  }
+}
+
+// bins of make_TiledBin (src/util.h:1887-1952) / make_HybBin (:1786-1885):
+// count = (with_children ? #children : 0) + #nonzeros of the slice
+__global__ void k_bins(const uint32_t* __restrict__ sptr, const uint32_t* __restrict__ nnz_start_of_child,
+                       uint64_t nslc, uint64_t tot, int with_children, int32_t* __restrict__ bin_of) {
+  const uint64_t TB = 512;
+  for (uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; s < nslc; s += (uint64_t)gridDim.x * blockDim.x) {
+    uint64_t c0 = sptr[s], c1 = sptr[s + 1];
+    uint64_t n = (uint64_t)(nnz_start_of_child[c1] - nnz_start_of_child[c0]);
+    if (with_children) n += c1 - c0;
+    const uint64_t LB[10] = {0, 2, 4, 8, 16, 1024, 4 * TB, 8 * TB, 16 * TB, 32 * TB};
+    const uint64_t UB[10] = {1025, 5, 9, 17, 1025, 4 * TB + 1, 8 * TB + 1, 16 * TB + 1, 32 * TB + 1, tot + 1};
+    int b = -1;
+    for (int i = 0; i < 10; ++i)
+      if (n > LB[i] && n < UB[i]) { b = i; break; }
+    bin_of[s] = b;
+  }
+}
+
+// ---- host helpers ----------------------------------------------------------
+
+int bits_for(uint64_t dim) {
+  int b = 0;
+  while (b < 64 && ((dim - 1) >> b)) ++b;
+  return b;
+}
+
+struct Launches {
+  int n = 0;
+};
+
+#define LCHECK(L) \
+  do { ++(L).n; MMCSF_LAUNCH_CHECK(); } while (0)
+
+// Excl scan with a fresh output buffer of n+1 entries; returns total via *tot.
+int scan_total(const uint32_t* flag, uint64_t n, DevBuf& excl, uint32_t* tot, cudaStream_t s, Launches& L) {
+  MMCSF_CUDA(excl.alloc((n + 1) * 4));
+  MMCSF_CUDA(exclusive_scan_u32(flag, excl.as<uint32_t>(), n, s));
+  L.n += 3;
+  MMCSF_CUDA(cudaMemcpyAsync(tot, excl.as<uint32_t>() + n, 4, cudaMemcpyDeviceToHost, s));
+  MMCSF_CUDA(cudaStreamSynchronize(s));
+  return MMCSF_OK;
+}
+
+}  // namespace
+
+// Reference mode ordering, src/util.h:255-311.
+void order_modes(int nd, const uint64_t* dims, int mode, int* order) {
+  uint64_t len[4];
+  int taken[4] = {0, 0, 0, 0};
+  for (int m = 0; m < nd; ++m) len[m] = dims[(m + mode) % nd];
+  for (int i = 1; i < nd; i++)
+    for (int j = i + 1; j < nd; j++)
+      if (len[i] > len[j]) std::swap(len[i], len[j]);
+  order[0] = mode;
+  taken[mode] = 1;
+  for (int i = 1; i < nd; i++)
+    for (int j = 0; j < nd; j++)
+      if (len[i] == dims[j] && !taken[j]) { order[i] = j; taken[j] = 1; break; }
+}
+
+// Stable sort of the COO by the composite mode list `keys` (most significant
+// first). Produces sorted copies of every mode's indices and the values.
+static int sort_coo(const mmcsf_coo* X, const std::vector<int>& keys, DevBuf* sorted_inds, DevBuf& sorted_vals,
+                    cudaStream_t s, Launches& L) {
+  const uint64_t n = X->nnz;
+  const int nd = X->nd;
+  DevBuf perm, perm2, k1, k2;
+  MMCSF_CUDA(perm.alloc(n * 4));
+  MMCSF_CUDA(iota_u32(perm.as<uint32_t>(), n, s));
+  ++L.n;
+  if (n > 1 && !keys.empty()) {
+    MMCSF_CUDA(perm2.alloc(n * 4));
+    MMCSF_CUDA(k1.alloc(n * 8));
+    MMCSF_CUDA(k2.alloc(n * 8));
+    // split into <=64-bit groups from the least significant end
+    std::vector<std::vector<int>> groups;
+    std::vector<int> cur;
+    int bits = 0;
+    for (int i = (int)keys.size() - 1; i >= 0; --i) {
+      int b = bits_for(X->dims[keys[i]]);
+      if (bits + b > 64 || cur.size() == 4) {
+        groups.push_back(cur);
+        cur.clear();
+        bits = 0;
+      }
+      cur.insert(cur.begin(), keys[i]);
+      bits += b;
+    }
+    if (!cur.empty()) groups.push_back(cur);
+    Idx4 in{};
+    for (int m = 0; m < nd; ++m) in.p[m] = X->d_inds[m].as<uint32_t>();
+    bool first = true;
+    for (auto& g : groups) {  // least significant group first
+      int md[4] = {0, 0, 0, 0}, sh[4] = {0, 0, 0, 0};
+      int tot = 0;
+      for (int j = (int)g.size() - 1; j >= 0; --j) {
+        md[j] = g[j];
+        sh[j] = tot;
+        tot += bits_for(X->dims[g[j]]);
+      }
+      if (tot == 0) continue;
+      k_pack<<<grid_for(n, 256), 256, 0, s>>>(in, first ? nullptr : perm.as<uint32_t>(), (int)g.size(), in, n,
+                                              make_int4(md[0], md[1], md[2], md[3]),
+                                              make_int4(sh[0], sh[1], sh[2], sh[3]), k1.as<uint64_t>());
+      LCHECK(L);
+      MMCSF_CUDA(radix_sort_pairs(k1.as<uint64_t>(), perm.as<uint32_t>(), k2.as<uint64_t>(), perm2.as<uint32_t>(),
+                                  n, tot, s));
+      L.n += 4 * ((tot + 7) / 8);
+      first = false;
+    }
+  }
+  for (int m = 0; m < nd; ++m) {
+    MMCSF_CUDA(sorted_inds[m].alloc(n * 4));
+    MMCSF_CUDA(gather_u32(X->d_inds[m].as<uint32_t>(), perm.as<uint32_t>(), sorted_inds[m].as<uint32_t>(), n, s));
+    ++L.n;
+  }
+  MMCSF_CUDA(sorted_vals.alloc(n * 4));
+  if (n) {
+    k_gather_f32<<<grid_for(n, 256), 256, 0, s>>>(X->d_vals.as<float>(), perm.as<uint32_t>(), n,
+                                                  sorted_vals.as<float>());
+    LCHECK(L);
+  }
+  return MMCSF_OK;
+}
+
+// CSF levels over sorted arrays (src/util.h:1320-1436 create_TiledHCSR; with
+// fbrs_th = "off" it is src/util.h:760-850 create_HCSR).
+static int build_csf(int nd, const int* order, uint64_t n, DevBuf* sorted, DevBuf& vals, uint64_t fbr_th,
+                     uint64_t fbrs_th, bool keep_coo, CsfPart& P, cudaStream_t s, Launches& L) {
+  P.present = n > 0;
+  P.nd = nd;
+  for (int i = 0; i < nd; ++i) P.order[i] = order[i];
+  P.nnz = n;
+  const int Lv = nd - 1;  // index levels
+  const uint32_t* o[4];
+  for (int i = 0; i < nd; ++i) o[i] = sorted[order[i]].as<uint32_t>();
+  if (n == 0) return MMCSF_OK;
+  const int G = grid_for(n, 256);
+
+  // --- leaf fibers: runs of equal (o0..o_{L-1}), split every fbr_th nonzeros
+  DevBuf fl, exr;
+  MMCSF_CUDA(fl.alloc(n * 4));
+  Idx4 lev{};
+  for (int i = 0; i < Lv; ++i) lev.p[i] = o[i];
+  k_run_flags<<<G, 256, 0, s>>>(lev, Lv, n, fl.as<uint32_t>());
+  LCHECK(L);
+  if (fbr_th < n) {
+    uint32_t nrun = 0;
+    MMCSF_TRY(scan_total(fl.as<uint32_t>(), n, exr, &nrun, s, L));
+    DevBuf rstart;
+    MMCSF_CUDA(rstart.alloc((uint64_t)nrun * 4));
+    k_compact_pos<<<G, 256, 0, s>>>(fl.as<uint32_t>(), exr.as<uint32_t>(), n, rstart.as<uint32_t>());
+    LCHECK(L);
+    k_split_flags<<<G, 256, 0, s>>>(exr.as<uint32_t>(), rstart.as<uint32_t>(), n, fbr_th, fl.as<uint32_t>());
+    LCHECK(L);
+  }
+  uint32_t F = 0;
+  DevBuf exf;
+  MMCSF_TRY(scan_total(fl.as<uint32_t>(), n, exf, &F, s, L));
+  const int lf = Lv - 1;  // level of leaf fibers: 1 (3-D) or 2 (4-D)
+  MMCSF_CUDA(P.ptr[lf].alloc(((uint64_t)F + 1) * 4));
+  k_compact_pos<<<G, 256, 0, s>>>(fl.as<uint32_t>(), exf.as<uint32_t>(), n, P.ptr[lf].as<uint32_t>());
+  LCHECK(L);
+  k_set1<<<1, 1, 0, s>>>(P.ptr[lf].as<uint32_t>(), F, (uint32_t)n);
+  LCHECK(L);
+  MMCSF_CUDA(P.idx[lf].alloc(((uint64_t)F + 1) * 4));
+  MMCSF_CUDA(gather_u32(o[lf], P.ptr[lf].as<uint32_t>(), P.idx[lf].as<uint32_t>(), F, s));
+  ++L.n;
+  {  // sentinel: the last fiber's index (0 for a single nonzero, src/util.h:1416-1419)
+    uint32_t last = 0;
+    if (n > 1) MMCSF_CUDA(cudaMemcpyAsync(&last, o[lf] + (n - 1), 4, cudaMemcpyDeviceToHost, s));
+    MMCSF_CUDA(cudaStreamSynchronize(s));
+    k_set1<<<1, 1, 0, s>>>(P.idx[lf].as<uint32_t>(), F, last);
+    LCHECK(L);
+  }
+  P.n[lf] = F;
+  const int GF = grid_for(F, 256);
+
+  // --- level 1 for 4-D: fbrS = runs of (o0,o1) over fibers, split at fbrs_th
+  const uint32_t* lvl1_start = P.ptr[lf].as<uint32_t>();  // nonzero position where each fiber starts
+  DevBuf fsstart;                                         // nonzero start of every fbrS (4-D)
+  uint64_t n1 = F;                                        // entries at the level below slices
+  if (nd == 4) {
+    DevBuf rf, exrf;
+    MMCSF_CUDA(rf.alloc((uint64_t)F * 4));
+    Idx4 l2{};
+    l2.p[0] = o[0];
+    l2.p[1] = o[1];
+    k_flags_at<<<GF, 256, 0, s>>>(l2, 2, P.ptr[2].as<uint32_t>(), F, rf.as<uint32_t>());
+    LCHECK(L);
+    if (fbrs_th < n) {
+      uint32_t nruns = 0;
+      MMCSF_TRY(scan_total(rf.as<uint32_t>(), F, exrf, &nruns, s, L));
+      DevBuf rfirst;
+      MMCSF_CUDA(rfirst.alloc((uint64_t)nruns * 4));
+      k_compact_pos<<<GF, 256, 0, s>>>(rf.as<uint32_t>(), exrf.as<uint32_t>(), F, rfirst.as<uint32_t>());
+      LCHECK(L);
+      int gw = grid_for((uint64_t)nruns * 32, 256);
+      k_fbrs_split<<<gw, 256, 0, s>>>(P.ptr[2].as<uint32_t>(), rfirst.as<uint32_t>(), nruns, F, fbrs_th,
+                                      rf.as<uint32_t>());
+      LCHECK(L);
+    }
+    uint32_t FS = 0;
+    DevBuf exs;
+    MMCSF_TRY(scan_total(rf.as<uint32_t>(), F, exs, &FS, s, L));
+    MMCSF_CUDA(P.ptr[1].alloc(((uint64_t)FS + 1) * 4));
+    k_compact_pos<<<GF, 256, 0, s>>>(rf.as<uint32_t>(), exs.as<uint32_t>(), F, P.ptr[1].as<uint32_t>());
+    LCHECK(L);
+    k_set1<<<1, 1, 0, s>>>(P.ptr[1].as<uint32_t>(), FS, F);
+    LCHECK(L);
+    MMCSF_CUDA(P.fpar.alloc((uint64_t)F * 4));
+    k_parent<<<GF, 256, 0, s>>>(exs.as<uint32_t>(), F, P.fpar.as<uint32_t>());
+    LCHECK(L);
+    MMCSF_CUDA(fsstart.alloc(((uint64_t)FS + 1) * 4));
+    k_gather2<<<grid_for(FS + 1, 256), 256, 0, s>>>(P.ptr[2].as<uint32_t>(), P.ptr[1].as<uint32_t>(), nullptr,
+                                                    FS + 1, fsstart.as<uint32_t>());
+    LCHECK(L);
+    MMCSF_CUDA(P.idx[1].alloc(((uint64_t)FS + 1) * 4));
+    MMCSF_CUDA(gather_u32(o[1], fsstart.as<uint32_t>(), P.idx[1].as<uint32_t>(), FS, s));
+    ++L.n;
+    P.n[1] = FS;
+    n1 = FS;
+    lvl1_start = fsstart.as<uint32_t>();
+  }
+
+  // --- slices: runs of o0 over level-1 entries
+  const int G1 = grid_for(n1, 256);
+  DevBuf sf, exsl;
+  MMCSF_CUDA(sf.alloc(n1 * 4));
+  Idx4 l1{};
+  l1.p[0] = o[0];
+  k_flags_at<<<G1, 256, 0, s>>>(l1, 1, lvl1_start, n1, sf.as<uint32_t>());
+  LCHECK(L);
+  uint32_t S_ = 0;
+  MMCSF_TRY(scan_total(sf.as<uint32_t>(), n1, exsl, &S_, s, L));
+  MMCSF_CUDA(P.ptr[0].alloc(((uint64_t)S_ + 1) * 4));
+  k_compact_pos<<<G1, 256, 0, s>>>(sf.as<uint32_t>(), exsl.as<uint32_t>(), n1, P.ptr[0].as<uint32_t>());
+  LCHECK(L);
+  k_set1<<<1, 1, 0, s>>>(P.ptr[0].as<uint32_t>(), S_, (uint32_t)n1);
+  LCHECK(L);
+  MMCSF_CUDA(P.idx[0].alloc(((uint64_t)S_ + 1) * 4));
+  k_gather2<<<grid_for(S_, 256), 256, 0, s>>>(o[0], lvl1_start, P.ptr[0].as<uint32_t>(), S_,
+                                              P.idx[0].as<uint32_t>());
+  LCHECK(L);
+  P.n[0] = S_;
+  // fbrLikeSlcInds: o0 of every level-1 entry (one spare entry for kernels)
+  MMCSF_CUDA(P.fbr_like.alloc((n1 + 1) * 4));
+  MMCSF_CUDA(gather_u32(o[0], lvl1_start, P.fbr_like.as<uint32_t>(), n1, s));
+  ++L.n;
+  MMCSF_CUDA(cudaMemcpyAsync(P.fbr_like.as<uint32_t>() + n1, o[0] + (n - 1), 4, cudaMemcpyDeviceToDevice, s));
+
+  // --- per-nonzero arrays
+  P.leaf = std::move(sorted[order[nd - 1]]);
+  P.vals = std::move(vals);
+  if (keep_coo) {
+    for (int m = 0; m < nd; ++m) {
+      if (m == order[nd - 1]) {
+        MMCSF_CUDA(P.coo[m].alloc(n * 4));
+        MMCSF_CUDA(cudaMemcpyAsync(P.coo[m].p, P.leaf.p, n * 4, cudaMemcpyDeviceToDevice, s));
+      } else {
+        P.coo[m] = std::move(sorted[m]);
+      }
+    }
+  }
+  MMCSF_CUDA(cudaStreamSynchronize(s));
+  return MMCSF_OK;
+}
+
+static int compute_bins(CsfPart& P, bool with_children, cudaStream_t s, Launches& L) {
+  if (!P.present) return MMCSF_OK;
+  const int lf = P.nd - 2;
+  DevBuf nzstart;  // nonzero start of every level-1 entry (+ end)
+  const uint64_t n1 = P.n[1];
+  MMCSF_CUDA(nzstart.alloc((n1 + 1) * 4));
+  if (P.nd == 3) {
+    MMCSF_CUDA(cudaMemcpyAsync(nzstart.p, P.ptr[1].p, (n1 + 1) * 4, cudaMemcpyDeviceToDevice, s));
+  } else {
+    k_gather2<<<grid_for(n1 + 1, 256), 256, 0, s>>>(P.ptr[lf].as<uint32_t>(), P.ptr[1].as<uint32_t>(), nullptr,
+                                                    n1 + 1, nzstart.as<uint32_t>());
+    LCHECK(L);
+  }
+  MMCSF_CUDA(P.bin_of.alloc(P.n[0] * 4));
+  k_bins<<<grid_for(P.n[0], 256), 256, 0, s>>>(P.ptr[0].as<uint32_t>(), nzstart.as<uint32_t>(), P.n[0], P.nnz,
+                                               with_children ? 1 : 0, P.bin_of.as<int32_t>());
+  LCHECK(L);
+  MMCSF_CUDA(cudaStreamSynchronize(s));
+  return MMCSF_OK;
+}
+
+int build_hyb(mmcsf_format* F, CsfPart& X, cudaStream_t s, int* launches);  // hyb.cu
+
+}  // namespace mmcsf
+
+using namespace mmcsf;
+
+extern "C" int mmcsf_build(mmcsf_coo* X, const mmcsf_build_opts* opts, void* stream, mmcsf_format** out) {
+  if (!X || !opts || !out) return set_error(MMCSF_ERR_INVALID, "null argument");
+  const int nd = X->nd;
+  if (opts->impl != MMCSF_IMPL_MMCSF && opts->impl != MMCSF_IMPL_BCSF && opts->impl != MMCSF_IMPL_HBCSF)
+    return set_error(MMCSF_ERR_INVALID, "unknown implementation type -t %d", opts->impl);
+  if (opts->mode < 0 || opts->mode > nd - 1)
+    return set_error(MMCSF_ERR_INVALID, "Mode cannot be larger than tensor dimension.");
+  if (opts->partition_rule != 0)
+    return set_error(MMCSF_ERR_UNSUPPORTED, "partition rule %d not implemented", opts->partition_rule);
+  cudaStream_t s = S(stream);
+  MMCSF_TRY(mmcsf_coo_to_device(X, stream));
+  mmcsf_format* Fm = new (std::nothrow) mmcsf_format;
+  if (!Fm) return set_error(MMCSF_ERR_NOMEM, "host allocation failed");
+  std::unique_ptr<mmcsf_format> guard(Fm);
+  Fm->impl = opts->impl;
+  Fm->nd = nd;
+  Fm->nnz = X->nnz;
+  Fm->mode = opts->mode;
+  for (int m = 0; m < nd; ++m) Fm->dims[m] = X->dims[m];
+  const uint64_t fth = opts->fiber_threshold ? opts->fiber_threshold : REF_DEFAULT_FBR_TH;
+  Fm->fbr_th = fth;
+  const int K = nd == 3 ? 2 : 3;  // keys compared by the reference's sorts
+  Launches L;
+  order_modes(nd, X->dims, opts->mode, Fm->xorder);
+
+  // the reference's chain of sorts, most recent last
+  std::vector<std::vector<int>> chain;
+  chain.push_back(std::vector<int>(Fm->xorder, Fm->xorder + K));
+  int part_order[4] = {0, 1, 2, 3};
+  if (opts->impl == MMCSF_IMPL_MMCSF) {
+    // src/mttkrp.cu:314-352: per-mode CSFs sorted in place on the shared arrays
+    int orders[4][4];
+    int redun = -1;
+    for (int m = 0; m < nd; ++m) {
+      order_modes(nd, X->dims, m, orders[m]);
+      for (int p = 0; p < m; ++p)
+        if (orders[m][1] == orders[p][0] && orders[m][0] == orders[p][1]) redun = m;
+      if (m != redun) chain.push_back(std::vector<int>(orders[m], orders[m] + K));
+    }
+    Fm->redun = redun;
+    // mm_partition_reuseBased ends with `mode = 2;` (src/util.h:2517): every
+    // nonzero lands in partition 2, which sort_MI_CSF then sorts by its order.
+    chain.push_back(std::vector<int>(orders[2], orders[2] + K));
+    for (int i = 0; i < nd; ++i) part_order[i] = orders[2][i];
+    for (int m = 0; m < nd; ++m) {
+      Fm->parts[m].nd = nd;
+      for (int i = 0; i < nd; ++i) Fm->parts[m].order[i] = orders[m][i];
+    }
+  } else {
+    for (int i = 0; i < nd; ++i) part_order[i] = Fm->xorder[i];
+  }
+  // composite key: latest sort first, then earlier ones, dropping repeats
+  std::vector<int> keys;
+  for (int c = (int)chain.size() - 1; c >= 0; --c)
+    for (int m : chain[c])
+      if (std::find(keys.begin(), keys.end(), m) == keys.end()) keys.push_back(m);
+
+  DevBuf sorted[4], svals;
+  MMCSF_TRY(sort_coo(X, keys, sorted, svals, s, L));
+  const int target = opts->impl == MMCSF_IMPL_MMCSF ? 2 : 0;
+  const uint64_t fbrs_th = opts->impl == MMCSF_IMPL_MMCSF ? FBRS_TH_MMCSF : FBRS_TH_OFF;
+  CsfPart& P = Fm->parts[target];
+  MMCSF_TRY(build_csf(nd, part_order, X->nnz, sorted, svals, fth, fbrs_th,
+                      opts->keep_coo != 0 || opts->impl == MMCSF_IMPL_HBCSF, P, s, L));
+  if (opts->impl == MMCSF_IMPL_BCSF) MMCSF_TRY(compute_bins(P, true, s, L));
+  if (opts->impl == MMCSF_IMPL_HBCSF) MMCSF_TRY(build_hyb(Fm, P, s, &L.n));
+  Fm->last_launches = L.n;
+  *out = guard.release();
+  return MMCSF_OK;
+}
+
+extern "C" void mmcsf_format_destroy(mmcsf_format* F) { delete F; }
+
+extern "C" int mmcsf_format_info(const mmcsf_format* F, int part, mmcsf_part_info* info) {
+  if (!F || !info) return set_error(MMCSF_ERR_INVALID, "null argument");
+  if (part < 0 || part >= 4) return set_error(MMCSF_ERR_INVALID, "bad part %d", part);
+  memset(info, 0, sizeof *info);
+  const CsfPart& P = F->parts[part];
+  info->present = P.present ? 1 : 0;
+  info->nd = F->nd;
+  for (int i = 0; i < F->nd; ++i) info->mode_order[i] = P.present || F->impl == MMCSF_IMPL_MMCSF ? P.order[i] : i;
+  info->nnz = P.nnz;
+  info->n_slices = P.n[0];
+  info->n_fbrs = P.n[1];
+  info->n_fibers = P.n_fibers();
+  info->device_bytes = P.bytes();
+  return MMCSF_OK;
+}
+
+extern "C" int mmcsf_format_meta(const mmcsf_format* F, int* redun_mode, int* x_mode_order) {
+  if (!F) return set_error(MMCSF_ERR_INVALID, "null argument");
+  if (redun_mode) *redun_mode = F->redun;
+  if (x_mode_order)
+    for (int i = 0; i < F->nd; ++i) x_mode_order[i] = F->xorder[i];
+  return MMCSF_OK;
+}
+
+extern "C" int mmcsf_format_last_launches(const mmcsf_format* F, int* launches) {
+  if (!F || !launches) return set_error(MMCSF_ERR_INVALID, "null argument");
+  *launches = F->last_launches;
+  return MMCSF_OK;
+}

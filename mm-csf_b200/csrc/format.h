@@ -1,0 +1,71 @@
+// Device-resident sparse formats (internal layout).
+//
+// One CSF "part" holds, for a mode order (o0, ..., o_{nd-1}):
+//   3-D: ptr[0] slices->fibers [S+1], idx[0] slice index (o0) [S],
+//        ptr[1] fibers->nonzeros [F+1], idx[1] fiber index (o1) [F+1, last = sentinel]
+//   4-D: ptr[0] slices->fbrS [S+1], idx[0] [S],
+//        ptr[1] fbrS->fibers [FS+1], idx[1] fbrS index (o1) [FS],
+//        ptr[2] fibers->nonzeros [F+1], idx[2] fiber index (o2) [F+1, last = sentinel]
+//   leaf[N] (index of the last mode per nonzero), vals[N],
+//   fbr_like[n1]: o0 index per level-1 entry (the reference's fbrLikeSlcInds),
+//   fpar[F] (4-D): fbrS id of every fiber.
+// These are the reference's TiledTensor arrays (src/util.h:107-136) with
+// uint32 instead of size_t entries.
+#pragma once
+#include <stdint.h>
+
+#include <vector>
+
+#include "common.h"
+
+namespace mmcsf {
+
+struct CsfPart {
+  bool present = false;
+  int nd = 0;
+  int order[4] = {0, 1, 2, 3};
+  uint64_t nnz = 0;
+  uint64_t n[3] = {0, 0, 0};  // entries per index level: S, (3-D) F | (4-D) FS, F
+  DevBuf ptr[3], idx[3];
+  DevBuf leaf, vals, fbr_like, fpar;
+  DevBuf coo[4];    // optional: sorted index array of every tensor mode (keep_coo)
+  DevBuf bin_of;    // optional: int32 bin per slice (B-CSF / HB-CSF export)
+  DevBuf fbr_of;    // 3-D: fiber of every nonzero is not stored; reserved
+  uint64_t bytes() const {
+    uint64_t b = 0;
+    for (int l = 0; l < 3; ++l) b += ptr[l].bytes + idx[l].bytes;
+    b += leaf.bytes + vals.bytes + fbr_like.bytes + fpar.bytes + bin_of.bytes;
+    for (int m = 0; m < 4; ++m) b += coo[m].bytes;
+    return b;
+  }
+  uint64_t n_slices() const { return n[0]; }
+  uint64_t n_level1() const { return n[1]; }
+  uint64_t n_fibers() const { return nd == 3 ? n[1] : n[2]; }
+};
+
+// HB-CSF extra parts (src/util.h:852-1142).
+struct HybExtra {
+  uint64_t coo_nnz = 0, csl_nnz = 0, n_csl_slices = 0;
+  DevBuf coo_inds[4], coo_vals;                       // by level
+  DevBuf csl_ptr, csl_idx, csl_i1, csl_i2, csl_vals;  // 3-D only
+  DevBuf csl_bin_of;
+};
+
+}  // namespace mmcsf
+
+struct mmcsf_format {
+  int impl = 0;
+  int nd = 0;
+  uint64_t dims[4] = {0, 0, 0, 0};
+  uint64_t nnz = 0;
+  int mode = 0;      // -m
+  int redun = -1;    // redunMode (MM-CSF)
+  int xorder[4] = {0, 1, 2, 3};
+  uint64_t fbr_th = 0;
+  mmcsf::CsfPart parts[4];
+  mmcsf::HybExtra hyb;
+  int last_launches = 0;
+  // staging for the host-buffer MTTKRP entry point
+  mmcsf::DevBuf stage_in[4], stage_out[4];
+  int stage_R = 0;
+};

@@ -1,0 +1,491 @@
+// MTTKRP kernels for MM-CSF / B-CSF / HB-CSF parts on sm_100a.
+//
+// The reference launches one warp (or -w warps) per fiber, strides lanes over
+// the rank with scalar 4-byte loads, and issues atomicAdd per fiber (slice and
+// fiber modes) or per nonzero (leaf mode) (src/mttkrp_gpu.cu:716-1509).
+// Here every mode uses the same nonzero-balanced traversal:
+//   * a TEAM of G lanes owns one factor row (R = 4*G*V floats, each lane V
+//     float4 = 16 B vectors), so one warp works on 32/G nonzeros at once;
+//   * a team walks a fixed, contiguous range of `chunk` nonzeros — skewed
+//     fibers and slices cost the same as uniform ones — locating its first
+//     fiber by binary search over the fiber pointers;
+//   * the team loads G leaf indices and values with one coalesced access,
+//     broadcasts them by shuffle, and issues all G row gathers before using
+//     any, so G independent 16-byte loads per lane are in flight;
+//   * products are accumulated in registers along the fiber / fbrS / slice
+//     hierarchy and flushed with ONE vector atomic (red.global.add.v4.f32) per
+//     output row segment: per slice run for the slice mode, per fiber or fbrS
+//     for the middle modes, per nonzero for the leaf mode (which scatters).
+// Correct for every R (the reference's kernels keep one scalar accumulator per
+// lane across the rank loop and are wrong for R > 32).
+#include <cuda_bf16.h>
+
+#include <cstring>
+
+#include "format.h"
+#include "prims.cuh"
+
+using mmcsf::set_error;
+
+namespace mmcsf {
+namespace {
+
+constexpr unsigned FULL = 0xffffffffu;
+
+template <class T> struct Row;
+template <> struct Row<float> {
+  static __device__ __forceinline__ float4 load(const float* base, uint64_t off) {
+    return __ldg(reinterpret_cast<const float4*>(base + off));
+  }
+};
+template <> struct Row<__nv_bfloat16> {
+  static __device__ __forceinline__ float4 load(const __nv_bfloat16* base, uint64_t off) {
+    uint2 u = __ldg(reinterpret_cast<const uint2*>(base + off));
+    float4 r;
+    r.x = __uint_as_float(u.x << 16);
+    r.y = __uint_as_float(u.x & 0xffff0000u);
+    r.z = __uint_as_float(u.y << 16);
+    r.w = __uint_as_float(u.y & 0xffff0000u);
+    return r;
+  }
+};
+
+__device__ __forceinline__ float4 f4(float a) { return make_float4(a, a, a, a); }
+__device__ __forceinline__ float4 operator*(float4 a, float4 b) {
+  return make_float4(a.x * b.x, a.y * b.y, a.z * b.z, a.w * b.w);
+}
+__device__ __forceinline__ float4 operator+(float4 a, float4 b) {
+  return make_float4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w);
+}
+__device__ __forceinline__ float4 fma4(float s, float4 a, float4 c) {
+  return make_float4(fmaf(s, a.x, c.x), fmaf(s, a.y, c.y), fmaf(s, a.z, c.z), fmaf(s, a.w, c.w));
+}
+__device__ __forceinline__ void red4(float* p, float4 v) { atomicAdd(reinterpret_cast<float4*>(p), v); }
+
+template <class T>
+struct Args {
+  const float* vals;
+  const uint32_t* leaf;
+  const uint32_t* fptr;   // leaf fibers -> nonzeros [F+1]
+  const uint32_t* fidx;   // leaf-fiber index (o1 in 3-D, o2 in 4-D)
+  const uint32_t* fpar;   // 4-D: fiber -> fbrS
+  const uint32_t* sidx1;  // 4-D: fbrS index (o1)
+  const uint32_t* like;   // o0 per level-1 entry (3-D: fiber, 4-D: fbrS)
+  uint64_t nnz;
+  uint32_t nfib;
+  uint32_t chunk;
+  uint32_t R;
+  const T* U[4];  // factor of mode order[l], by level l
+  float* out;
+};
+
+// largest f with fptr[f] <= x
+__device__ __forceinline__ uint32_t find_fiber(const uint32_t* __restrict__ fptr, uint32_t nfib, uint64_t x) {
+  uint32_t lo = 0, hi = nfib - 1;
+  while (lo < hi) {
+    uint32_t mid = (lo + hi + 1) >> 1;
+    if ((uint64_t)__ldg(fptr + mid) <= x) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+// ND: 3 or 4. OUT: output level (0 = slice ... ND-1 = leaf). G lanes per row,
+// V float4 per lane, R = 4*G*V.
+template <int ND, int OUT, int G, int V, class T>
+__global__ void __launch_bounds__(256) k_mttkrp(const Args<T> a) {
+  const int lane = threadIdx.x & 31;
+  const int tl = lane & (G - 1);
+  const int tb = lane - tl;
+  const uint64_t team = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) / G;
+  // Teams past the end stay in the loop (empty range) so every shuffle sees
+  // the full warp; all teams run the same number of iterations.
+  const bool active = team * a.chunk < a.nnz;
+  const uint64_t x0 = active ? team * a.chunk : a.nnz - 1;
+  const uint64_t x1 = active ? min(x0 + a.chunk, a.nnz) : x0;
+  const uint32_t R = a.R;
+  constexpr int LEAF = ND - 1;
+
+  uint32_t f = find_fiber(a.fptr, a.nfib, x0);
+  uint64_t fend = __ldg(a.fptr + f + 1);
+  uint32_t fs = 0;
+  if (ND == 4) fs = __ldg(a.fpar + f);
+
+  float4 acc[V], acc1[V], acc2[V], w[V];
+#pragma unroll
+  for (int v = 0; v < V; ++v) acc[v] = acc1[v] = acc2[v] = w[v] = f4(0.f);
+
+  // current output-row keys for the accumulators above the leaf fiber
+  uint32_t cur_a = __ldg(a.like + (ND == 3 ? f : fs));
+
+  auto col = [&](int v) -> uint64_t { return (uint64_t)(tl + v * G) * 4; };
+
+  auto leaf_weights = [&]() {  // w = Hadamard of the rows above the leaf for fiber f
+    if constexpr (OUT == LEAF) {
+      if constexpr (ND == 3) {
+        const uint64_t ra = (uint64_t)__ldg(a.like + f) * R, rb = (uint64_t)__ldg(a.fidx + f) * R;
+#pragma unroll
+        for (int v = 0; v < V; ++v) w[v] = Row<T>::load(a.U[0], ra + col(v)) * Row<T>::load(a.U[1], rb + col(v));
+      } else {
+        const uint64_t ra = (uint64_t)__ldg(a.like + fs) * R, rb = (uint64_t)__ldg(a.sidx1 + fs) * R,
+                       rc = (uint64_t)__ldg(a.fidx + f) * R;
+#pragma unroll
+        for (int v = 0; v < V; ++v)
+          w[v] = Row<T>::load(a.U[0], ra + col(v)) * Row<T>::load(a.U[1], rb + col(v)) *
+                 Row<T>::load(a.U[2], rc + col(v));
+      }
+    }
+  };
+  leaf_weights();
+
+  // Close leaf fiber f (its partial over this team's range is in acc).
+  // `last` = the team's range ends here (flush everything).
+  auto close_fiber = [&](bool last) {
+    if constexpr (OUT == LEAF) {
+      (void)last;
+      return;
+    } else if constexpr (ND == 3) {
+      if constexpr (OUT == 1) {
+        const uint64_t ra = (uint64_t)__ldg(a.like + f) * R, ro = (uint64_t)__ldg(a.fidx + f) * R;
+#pragma unroll
+        for (int v = 0; v < V; ++v) red4(a.out + ro + col(v), Row<T>::load(a.U[0], ra + col(v)) * acc[v]);
+      } else {  // OUT == 0: slice run accumulation
+        const uint64_t rb = (uint64_t)__ldg(a.fidx + f) * R;
+#pragma unroll
+        for (int v = 0; v < V; ++v) acc1[v] = acc1[v] + Row<T>::load(a.U[1], rb + col(v)) * acc[v];
+        const uint32_t nxt = last ? 0xffffffffu : __ldg(a.like + f + 1);
+        if (last || nxt != cur_a) {
+#pragma unroll
+          for (int v = 0; v < V; ++v) { red4(a.out + (uint64_t)cur_a * R + col(v), acc1[v]); acc1[v] = f4(0.f); }
+          cur_a = nxt;
+        }
+      }
+    } else {  // ND == 4
+      const uint64_t rc = (uint64_t)__ldg(a.fidx + f) * R;
+      if constexpr (OUT == 2) {
+        const uint64_t ra = (uint64_t)__ldg(a.like + fs) * R, rb = (uint64_t)__ldg(a.sidx1 + fs) * R;
+#pragma unroll
+        for (int v = 0; v < V; ++v)
+          red4(a.out + rc + col(v),
+               Row<T>::load(a.U[0], ra + col(v)) * Row<T>::load(a.U[1], rb + col(v)) * acc[v]);
+      } else {
+#pragma unroll
+        for (int v = 0; v < V; ++v) acc1[v] = acc1[v] + Row<T>::load(a.U[2], rc + col(v)) * acc[v];
+        const uint32_t nfs = last ? 0xffffffffu : __ldg(a.fpar + f + 1);
+        if (last || nfs != fs) {  // close fbrS fs
+          if constexpr (OUT == 1) {
+            const uint64_t ra = (uint64_t)__ldg(a.like + fs) * R, ro = (uint64_t)__ldg(a.sidx1 + fs) * R;
+#pragma unroll
+            for (int v = 0; v < V; ++v) {
+              red4(a.out + ro + col(v), Row<T>::load(a.U[0], ra + col(v)) * acc1[v]);
+              acc1[v] = f4(0.f);
+            }
+          } else {  // OUT == 0
+            const uint64_t rb = (uint64_t)__ldg(a.sidx1 + fs) * R;
+#pragma unroll
+            for (int v = 0; v < V; ++v) {
+              acc2[v] = acc2[v] + Row<T>::load(a.U[1], rb + col(v)) * acc1[v];
+              acc1[v] = f4(0.f);
+            }
+            const uint32_t na = last ? 0xffffffffu : __ldg(a.like + nfs);
+            if (last || na != cur_a) {
+#pragma unroll
+              for (int v = 0; v < V; ++v) {
+                red4(a.out + (uint64_t)cur_a * R + col(v), acc2[v]);
+                acc2[v] = f4(0.f);
+              }
+              cur_a = na;
+            }
+          }
+        }
+      }
+    }
+  };
+
+  constexpr int PF = G > 8 ? 8 : G;  // row gathers in flight per lane
+  for (uint32_t it = 0; it < a.chunk; it += G) {
+    const uint64_t xb = x0 + it;
+    const uint64_t xi = xb + tl;
+    const bool okx = xi < x1;
+    const uint32_t my_k = okx ? __ldg(a.leaf + xi) : 0u;
+    const float my_v = okx ? __ldg(a.vals + xi) : 0.f;
+    if constexpr (OUT != LEAF) {
+#pragma unroll
+      for (int jb = 0; jb < G; jb += PF) {
+        float4 rows[PF][V];
+#pragma unroll
+        for (int j = 0; j < PF; ++j) {
+          const uint32_t k = __shfl_sync(FULL, my_k, tb + jb + j);
+          const uint64_t rk = (uint64_t)k * R;
+#pragma unroll
+          for (int v = 0; v < V; ++v) rows[j][v] = Row<T>::load(a.U[LEAF], rk + col(v));
+        }
+#pragma unroll
+        for (int j = 0; j < PF; ++j) {
+          const float val = __shfl_sync(FULL, my_v, tb + jb + j);
+          const uint64_t x = xb + jb + j;
+          if (x < x1) {
+            if (x == fend) {
+              close_fiber(false);
+              ++f;
+              fend = __ldg(a.fptr + f + 1);
+              if (ND == 4) fs = __ldg(a.fpar + f);
+#pragma unroll
+              for (int v = 0; v < V; ++v) acc[v] = f4(0.f);
+            }
+#pragma unroll
+            for (int v = 0; v < V; ++v) acc[v] = fma4(val, rows[j][v], acc[v]);
+          }
+        }
+      }
+    } else {
+#pragma unroll
+      for (int j = 0; j < G; ++j) {
+        const uint32_t k = __shfl_sync(FULL, my_k, tb + j);
+        const float val = __shfl_sync(FULL, my_v, tb + j);
+        const uint64_t x = xb + j;
+        if (x < x1) {
+          if (x == fend) {
+            ++f;
+            fend = __ldg(a.fptr + f + 1);
+            if (ND == 4) fs = __ldg(a.fpar + f);
+            leaf_weights();
+          }
+          const uint64_t ro = (uint64_t)k * R;
+#pragma unroll
+          for (int v = 0; v < V; ++v) red4(a.out + ro + col(v), f4(val) * w[v]);
+        }
+      }
+    }
+  }
+  if (active) close_fiber(true);
+}
+
+template <int ND, int OUT, int G, int V, class T>
+cudaError_t launch_one(const Args<T>& a, int threads, cudaStream_t s) {
+  const uint64_t teams = (a.nnz + a.chunk - 1) / a.chunk;
+  const uint64_t thr = teams * G;
+  const uint64_t blocks = (thr + threads - 1) / threads;
+  k_mttkrp<ND, OUT, G, V, T><<<(unsigned)blocks, threads, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+template <int ND, int G, int V, class T>
+cudaError_t launch_lvl(const Args<T>& a, int lvl, int threads, cudaStream_t s) {
+  switch (lvl) {
+    case 0: return launch_one<ND, 0, G, V, T>(a, threads, s);
+    case 1: return launch_one<ND, 1, G, V, T>(a, threads, s);
+    case 2: return launch_one<ND, 2, G, V, T>(a, threads, s);
+    default:
+      if constexpr (ND == 4) return launch_one<ND, 3, G, V, T>(a, threads, s);
+      return cudaErrorInvalidValue;
+  }
+}
+
+template <class T>
+cudaError_t launch_R(const Args<T>& a, int nd, int lvl, int threads, cudaStream_t s) {
+#define MMCSF_RCASE(RR, GG, VV)                                                        \
+  case RR:                                                                            \
+    return nd == 3 ? launch_lvl<3, GG, VV, T>(a, lvl, threads, s)                     \
+                   : launch_lvl<4, GG, VV, T>(a, lvl, threads, s);
+  switch (a.R) {
+    MMCSF_RCASE(4, 1, 1)
+    MMCSF_RCASE(8, 2, 1)
+    MMCSF_RCASE(16, 4, 1)
+    MMCSF_RCASE(32, 8, 1)
+    MMCSF_RCASE(64, 16, 1)
+    MMCSF_RCASE(128, 32, 1)
+    MMCSF_RCASE(256, 32, 2)
+    default: return cudaErrorInvalidValue;
+  }
+#undef MMCSF_RCASE
+}
+
+bool native_R(int R) { return R == 4 || R == 8 || R == 16 || R == 32 || R == 64 || R == 128 || R == 256; }
+int padded_R(int R) {
+  const int opts[] = {4, 8, 16, 32, 64, 128, 256};
+  for (int r : opts)
+    if (r >= R) return r;
+  return -1;
+}
+
+__global__ void k_pad_rows(const void* in, int esz, uint64_t rows, int R, int Rp, void* out) {
+  const uint64_t n = rows * (uint64_t)Rp;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    uint64_t r = i / Rp, c = i % Rp;
+    if (esz == 4) static_cast<float*>(out)[i] = c < (uint64_t)R ? static_cast<const float*>(in)[r * R + c] : 0.f;
+    else static_cast<uint16_t*>(out)[i] = c < (uint64_t)R ? static_cast<const uint16_t*>(in)[r * R + c] : 0;
+  }
+}
+__global__ void k_unpad_rows(const float* in, uint64_t rows, int R, int Rp, float* out) {
+  const uint64_t n = rows * (uint64_t)R;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    out[i] = in[(i / R) * Rp + i % R];
+}
+
+int default_chunk(int R) {
+  (void)R;
+  return 512;
+}
+
+// MTTKRP on one part for tensor mode `mode`; out must be zeroed by the caller.
+int part_mttkrp(const mmcsf_format* F, const CsfPart& P, int mode, int R, int dtype, const void* const* U,
+                float* out, const mmcsf_kernel_cfg* cfg, cudaStream_t s, int* launches) {
+  if (!P.present || P.nnz == 0) return MMCSF_OK;
+  int lvl = -1;
+  for (int l = 0; l < P.nd; ++l)
+    if (P.order[l] == mode) lvl = l;
+  if (lvl < 0) return set_error(MMCSF_ERR_INVALID, "mode %d not in part", mode);
+  int chunk = cfg && cfg->chunk > 0 ? cfg->chunk : default_chunk(R);
+  int threads = cfg && cfg->block_threads > 0 ? cfg->block_threads : 256;
+  if (threads % 32 || threads > 1024) return set_error(MMCSF_ERR_INVALID, "block_threads must be a multiple of 32");
+  cudaError_t e;
+  if (dtype == MMCSF_DTYPE_F32) {
+    Args<float> a{};
+    a.vals = P.vals.as<float>();
+    a.leaf = P.leaf.as<uint32_t>();
+    const int lf = P.nd - 2;
+    a.fptr = P.ptr[lf].as<uint32_t>();
+    a.fidx = P.idx[lf].as<uint32_t>();
+    a.fpar = P.fpar.as<uint32_t>();
+    a.sidx1 = P.nd == 4 ? P.idx[1].as<uint32_t>() : nullptr;
+    a.like = P.fbr_like.as<uint32_t>();
+    a.nnz = P.nnz;
+    a.nfib = (uint32_t)P.n_fibers();
+    a.chunk = (uint32_t)chunk;
+    a.R = (uint32_t)R;
+    for (int l = 0; l < P.nd; ++l) a.U[l] = static_cast<const float*>(U[P.order[l]]);
+    a.out = out;
+    e = launch_R<float>(a, P.nd, lvl, threads, s);
+  } else {
+    Args<__nv_bfloat16> a{};
+    a.vals = P.vals.as<float>();
+    a.leaf = P.leaf.as<uint32_t>();
+    const int lf = P.nd - 2;
+    a.fptr = P.ptr[lf].as<uint32_t>();
+    a.fidx = P.idx[lf].as<uint32_t>();
+    a.fpar = P.fpar.as<uint32_t>();
+    a.sidx1 = P.nd == 4 ? P.idx[1].as<uint32_t>() : nullptr;
+    a.like = P.fbr_like.as<uint32_t>();
+    a.nnz = P.nnz;
+    a.nfib = (uint32_t)P.n_fibers();
+    a.chunk = (uint32_t)chunk;
+    a.R = (uint32_t)R;
+    for (int l = 0; l < P.nd; ++l) a.U[l] = static_cast<const __nv_bfloat16*>(U[P.order[l]]);
+    a.out = out;
+    e = launch_R<__nv_bfloat16>(a, P.nd, lvl, threads, s);
+  }
+  if (e != cudaSuccess) return set_error(MMCSF_ERR_CUDA, "MTTKRP launch failed: %s", cudaGetErrorString(e));
+  if (launches) ++*launches;
+  return MMCSF_OK;
+}
+
+}  // namespace
+
+// One mode over every part that holds nonzeros (the reference's per-mode loop
+// over partitions, src/mttkrp_gpu.cu:3578-3724).
+int mttkrp_mode(const mmcsf_format* F, int mode, int R, int dtype, const void* const* U, float* out,
+                const mmcsf_kernel_cfg* cfg, cudaStream_t s, int* launches) {
+  MMCSF_CUDA(cudaMemsetAsync(out, 0, F->dims[mode] * (uint64_t)R * sizeof(float), s));
+  for (int p = 0; p < F->nd; ++p) MMCSF_TRY(part_mttkrp(F, F->parts[p], mode, R, dtype, U, out, cfg, s, launches));
+  return MMCSF_OK;
+}
+
+}  // namespace mmcsf
+
+using namespace mmcsf;
+
+namespace {
+int check_call(const mmcsf_format* F, int R, int dtype) {
+  if (!F) return set_error(MMCSF_ERR_INVALID, "null format");
+  if (R < 1) return set_error(MMCSF_ERR_INVALID, "rank must be >= 1");
+  if (dtype != MMCSF_DTYPE_F32 && dtype != MMCSF_DTYPE_BF16) return set_error(MMCSF_ERR_INVALID, "bad dtype");
+  if (R > 256) return set_error(MMCSF_ERR_UNSUPPORTED, "rank %d > 256", R);
+  return MMCSF_OK;
+}
+
+// Run `fn(U, out_for_mode)` with rank padded to a native kernel width when R is
+// not one (factors copied into zero-padded buffers, outputs copied back).
+template <class Fn>
+int with_padding(const mmcsf_format* F, int R, int dtype, const void* const* U, Fn fn, cudaStream_t s) {
+  if (native_R(R)) return fn(R, U);
+  const int Rp = padded_R(R);
+  const int esz = dtype == MMCSF_DTYPE_F32 ? 4 : 2;
+  DevBuf pu[4];
+  const void* pp[4] = {nullptr, nullptr, nullptr, nullptr};
+  for (int m = 0; m < F->nd; ++m) {
+    MMCSF_CUDA(pu[m].alloc(F->dims[m] * (uint64_t)Rp * esz));
+    k_pad_rows<<<grid_for(F->dims[m] * (uint64_t)Rp, 256), 256, 0, s>>>(U[m], esz, F->dims[m], R, Rp, pu[m].p);
+    MMCSF_LAUNCH_CHECK();
+    pp[m] = pu[m].p;
+  }
+  int st = fn(Rp, pp);
+  MMCSF_CUDA(cudaStreamSynchronize(s));
+  return st;
+}
+}  // namespace
+
+extern "C" int mmcsf_mttkrp(const mmcsf_format* F, int mode, int R, int factor_dtype, const void* const* d_factors,
+                            float* d_out, const mmcsf_kernel_cfg* cfg, void* stream) {
+  MMCSF_TRY(check_call(F, R, factor_dtype));
+  if (mode < 0 || mode >= F->nd) return set_error(MMCSF_ERR_INVALID, "Mode cannot be larger than tensor dimension.");
+  if (!d_factors || !d_out) return set_error(MMCSF_ERR_INVALID, "null pointer");
+  if (F->impl != MMCSF_IMPL_MMCSF && mode != F->mode)
+    return set_error(MMCSF_ERR_INVALID, "this format was built for mode %d only", F->mode);
+  cudaStream_t s = S(stream);
+  mmcsf_format* Fm = const_cast<mmcsf_format*>(F);
+  int launches = 0;
+  int st = with_padding(F, R, factor_dtype, d_factors, [&](int Rk, const void* const* U) -> int {
+    if (Rk == R) return mttkrp_mode(F, mode, R, factor_dtype, U, d_out, cfg, s, &launches);
+    DevBuf tmp;
+    MMCSF_CUDA(tmp.alloc(F->dims[mode] * (uint64_t)Rk * 4));
+    MMCSF_TRY(mttkrp_mode(F, mode, Rk, factor_dtype, U, tmp.as<float>(), cfg, s, &launches));
+    k_unpad_rows<<<grid_for(F->dims[mode] * (uint64_t)R, 256), 256, 0, s>>>(tmp.as<float>(), F->dims[mode], R, Rk,
+                                                                           d_out);
+    MMCSF_LAUNCH_CHECK();
+    MMCSF_CUDA(cudaStreamSynchronize(s));
+    return MMCSF_OK;
+  }, s);
+  Fm->last_launches = launches;
+  return st;
+}
+
+extern "C" int mmcsf_mttkrp_all(const mmcsf_format* F, int R, int factor_dtype, const void* const* d_factors,
+                                float* const* d_outs, const mmcsf_kernel_cfg* cfg, void* stream) {
+  MMCSF_TRY(check_call(F, R, factor_dtype));
+  if (!d_factors || !d_outs) return set_error(MMCSF_ERR_INVALID, "null pointer");
+  if (F->impl != MMCSF_IMPL_MMCSF)
+    return set_error(MMCSF_ERR_INVALID, "all-mode MTTKRP needs an MM-CSF format (-t 12)");
+  int total = 0;
+  for (int m = 0; m < F->nd; ++m) {
+    MMCSF_TRY(mmcsf_mttkrp(F, m, R, factor_dtype, d_factors, d_outs[m], cfg, stream));
+    total += F->last_launches;
+  }
+  const_cast<mmcsf_format*>(F)->last_launches = total;
+  return MMCSF_OK;
+}
+
+extern "C" int mmcsf_mttkrp_all_host(mmcsf_format* F, int R, const float* const* h_factors, float* const* h_outs,
+                                     const mmcsf_kernel_cfg* cfg, void* stream) {
+  MMCSF_TRY(check_call(F, R, MMCSF_DTYPE_F32));
+  if (!h_factors || !h_outs) return set_error(MMCSF_ERR_INVALID, "null pointer");
+  cudaStream_t s = S(stream);
+  if (F->stage_R != R) {
+    for (int m = 0; m < F->nd; ++m) {
+      MMCSF_CUDA(F->stage_in[m].alloc(F->dims[m] * (uint64_t)R * 4));
+      MMCSF_CUDA(F->stage_out[m].alloc(F->dims[m] * (uint64_t)R * 4));
+    }
+    F->stage_R = R;
+  }
+  const void* din[4];
+  float* dout[4];
+  for (int m = 0; m < F->nd; ++m) {
+    MMCSF_CUDA(cudaMemcpyAsync(F->stage_in[m].p, h_factors[m], F->dims[m] * (uint64_t)R * 4, cudaMemcpyHostToDevice, s));
+    din[m] = F->stage_in[m].p;
+    dout[m] = F->stage_out[m].as<float>();
+  }
+  MMCSF_TRY(mmcsf_mttkrp_all(F, R, MMCSF_DTYPE_F32, din, dout, cfg, stream));
+  for (int m = 0; m < F->nd; ++m)
+    MMCSF_CUDA(cudaMemcpyAsync(h_outs[m], dout[m], F->dims[m] * (uint64_t)R * 4, cudaMemcpyDeviceToHost, s));
+  MMCSF_CUDA(cudaStreamSynchronize(s));
+  return MMCSF_OK;
+}

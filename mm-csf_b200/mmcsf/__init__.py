@@ -1,0 +1,336 @@
+"""Python host binding for the B200-native MM-CSF MTTKRP library.
+
+Everything here calls the C ABI in include/mmcsf.h through ctypes; PyTorch is
+only used to hold device memory and to name the current CUDA stream. The
+reference (isratnisa/MM-CSF) equivalents are noted per call.
+"""
+import ctypes
+
+import numpy as np
+
+from ._lib import (BuildOpts, GenSpec, KernelCfg, MmcsfError, PartInfo, c_f32p, c_u32p, c_u64, c_u64p, c_voidp,
+                   check, lib)
+
+IMPL_BCSF = 8
+IMPL_HBCSF = 10
+IMPL_MMCSF = 12
+DTYPE_F32 = 0
+DTYPE_BF16 = 1
+DIST_UNIFORM = 0
+DIST_ZIPF = 1
+VAL_UNIFORM01 = 0
+VAL_LOGNORMAL = 1
+VAL_INT1_50 = 2
+
+__all__ = ["CooTensor", "Format", "MmcsfError", "KernelCfg", "IMPL_BCSF", "IMPL_HBCSF", "IMPL_MMCSF",
+           "DTYPE_F32", "DTYPE_BF16", "current_stream"]
+
+
+def current_stream():
+    """cudaStream_t of torch's current stream (None when torch has no CUDA)."""
+    try:
+        import torch
+        if torch.cuda.is_available():
+            return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    except ImportError:
+        pass
+    return None
+
+
+def _stream(s):
+    if s is None:
+        return current_stream()
+    if isinstance(s, int):
+        return ctypes.c_void_p(s)
+    if hasattr(s, "cuda_stream"):
+        return ctypes.c_void_p(s.cuda_stream)
+    return s
+
+
+class CooTensor:
+    """A COO tensor (replaces Tensor + load_tensor, src/util.h:80-104, 313-370)."""
+
+    def __init__(self, handle):
+        self._h = handle
+
+    # -- constructors ---------------------------------------------------------
+    @classmethod
+    def load_tns(cls, path):
+        h = c_voidp()
+        check(lib().mmcsf_coo_load_tns(path.encode(), ctypes.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def from_arrays(cls, dims, inds, vals):
+        nd = len(dims)
+        d = (c_u64 * nd)(*[int(x) for x in dims])
+        ind = [np.ascontiguousarray(i, dtype=np.uint32) for i in inds]
+        v = np.ascontiguousarray(vals, dtype=np.float32)
+        ptrs = (c_u32p * nd)(*[i.ctypes.data_as(c_u32p) for i in ind])
+        h = c_voidp()
+        check(lib().mmcsf_coo_create(nd, d, c_u64(len(v)), ptrs, v.ctypes.data_as(c_f32p), ctypes.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def generate(cls, dims, nnz, dist=DIST_UNIFORM, zipf_s=1.0, val_dist=VAL_UNIFORM01, seed=0, stream=None):
+        """Seeded synthetic tensor generated on the device (see mmcsf_generate)."""
+        nd = len(dims)
+        sp = GenSpec()
+        sp.nd = nd
+        for m in range(nd):
+            sp.dims[m] = int(dims[m])
+            sp.dist[m] = dist[m] if isinstance(dist, (list, tuple)) else dist
+            sp.zipf_s[m] = zipf_s[m] if isinstance(zipf_s, (list, tuple)) else zipf_s
+        sp.nnz = int(nnz)
+        sp.val_dist = val_dist
+        sp.seed = int(seed)
+        h = c_voidp()
+        check(lib().mmcsf_generate(ctypes.byref(sp), _stream(stream), ctypes.byref(h)))
+        return cls(h)
+
+    # -- queries --------------------------------------------------------------
+    def info(self):
+        nd = ctypes.c_int()
+        dims = (c_u64 * 4)()
+        nnz = c_u64()
+        check(lib().mmcsf_coo_info(self._h, ctypes.byref(nd), dims, ctypes.byref(nnz)))
+        return nd.value, [int(dims[m]) for m in range(nd.value)], int(nnz.value)
+
+    @property
+    def nd(self):
+        return self.info()[0]
+
+    @property
+    def dims(self):
+        return self.info()[1]
+
+    @property
+    def nnz(self):
+        return self.info()[2]
+
+    def host_arrays(self):
+        """Copies of (inds[nd] uint32, vals float32) on the host."""
+        nd, _, nnz = self.info()
+        check(lib().mmcsf_coo_to_host(self._h))
+        ip = (c_voidp * 4)()
+        vp = c_voidp()
+        check(lib().mmcsf_coo_host_arrays(self._h, ip, ctypes.byref(vp)))
+        inds = [np.ctypeslib.as_array(ctypes.cast(ip[m], c_u32p), (nnz,)).copy() if nnz else np.zeros(0, np.uint32)
+                for m in range(nd)]
+        vals = (np.ctypeslib.as_array(ctypes.cast(vp, c_f32p), (nnz,)).copy() if nnz
+                else np.zeros(0, np.float32))
+        return inds, vals
+
+    def device_tensors(self):
+        """Borrowed torch views (int32 indices per mode, float32 values) of the
+        device copy; valid while this tensor is alive. Indices must be < 2^31."""
+        import torch
+        nd, _, nnz = self.info()
+        check(lib().mmcsf_coo_to_device(self._h, current_stream()))
+        ip = (c_voidp * 4)()
+        vp = c_voidp()
+        check(lib().mmcsf_coo_device_arrays(self._h, ip, ctypes.byref(vp)))
+        inds = [torch.as_tensor(_CudaArray(ip[m], nnz, "<i4"), device="cuda") for m in range(nd)]
+        vals = torch.as_tensor(_CudaArray(vp.value, nnz, "<f4"), device="cuda")
+        return inds, vals
+
+    def write_tns(self, path):
+        check(lib().mmcsf_coo_write_tns(self._h, path.encode()))
+
+    def close(self):
+        if self._h:
+            lib().mmcsf_coo_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # noqa: BLE001
+            pass
+
+
+def _ptr(t):
+    """Device pointer of a torch tensor (must be contiguous)."""
+    if not t.is_contiguous():
+        raise MmcsfError(1, "factor matrices must be contiguous row-major")
+    return ctypes.c_void_p(t.data_ptr())
+
+
+class Format:
+    """A device-resident sparse format built from a CooTensor.
+
+    impl follows the reference's -t: 12 = MM-CSF (all modes), 8 = B-CSF,
+    10 = HB-CSF (single mode `mode`). fiber_threshold is -f (0 = the
+    reference default). Replaces the builder chain the reference's main runs
+    (src/mttkrp.cu:72-389)."""
+
+    def __init__(self, coo, impl=IMPL_MMCSF, mode=0, fiber_threshold=0, keep_coo=False, stream=None):
+        o = BuildOpts()
+        o.impl = impl
+        o.mode = mode
+        o.fiber_threshold = int(fiber_threshold)
+        o.partition_rule = 0
+        o.keep_coo = 1 if keep_coo else 0
+        h = c_voidp()
+        check(lib().mmcsf_build(coo._h, ctypes.byref(o), _stream(stream), ctypes.byref(h)))
+        self._h = h
+        self.impl = impl
+        self.mode = mode
+        self.nd, self.dims, self.nnz = coo.info()
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().mmcsf_format_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # noqa: BLE001
+            pass
+
+    def info(self, part):
+        pi = PartInfo()
+        check(lib().mmcsf_format_info(self._h, part, ctypes.byref(pi)))
+        return {"present": bool(pi.present), "mode_order": [pi.mode_order[i] for i in range(pi.nd)],
+                "nnz": int(pi.nnz), "n_slices": int(pi.n_slices), "n_fbrs": int(pi.n_fbrs),
+                "n_fibers": int(pi.n_fibers), "device_bytes": int(pi.device_bytes)}
+
+    def meta(self):
+        r = ctypes.c_int()
+        xo = (ctypes.c_int * 4)()
+        check(lib().mmcsf_format_meta(self._h, ctypes.byref(r), xo))
+        return r.value, [xo[i] for i in range(self.nd)]
+
+    def export(self, part, name):
+        n = c_u64()
+        check(lib().mmcsf_format_export(self._h, part, name.encode(), None, 0, ctypes.byref(n)))
+        out = np.zeros(max(int(n.value), 1), np.uint64)
+        check(lib().mmcsf_format_export(self._h, part, name.encode(), out.ctypes.data_as(c_u64p), c_u64(len(out)),
+                                        ctypes.byref(n)))
+        return out[:int(n.value)]
+
+    def export_f32(self, part, name):
+        n = c_u64()
+        check(lib().mmcsf_format_export_f32(self._h, part, name.encode(), None, 0, ctypes.byref(n)))
+        out = np.zeros(max(int(n.value), 1), np.float32)
+        check(lib().mmcsf_format_export_f32(self._h, part, name.encode(), out.ctypes.data_as(c_f32p),
+                                            c_u64(len(out)), ctypes.byref(n)))
+        return out[:int(n.value)]
+
+    def reference_dump(self):
+        """Every array under the reference's names (the keys the reference
+        harness writes), for bit-exact comparison."""
+        d = {}
+        nd = self.nd
+        if self.impl == IMPL_MMCSF:
+            redun, xo = self.meta()
+            d["redunMode"] = np.array([redun], np.int64)
+            d["X.modeOrder"] = np.array(xo, np.uint64)
+            for p in range(nd):
+                inf = self.info(p)
+                pfx = f"part{p}"
+                d[f"{pfx}.nnz"] = np.array([inf["nnz"] if inf["present"] else 0], np.uint64)
+                d[f"{pfx}.modeOrder"] = np.array(inf["mode_order"], np.uint64)
+                if inf["present"]:
+                    self._dump_csf(d, p, pfx, nd)
+        else:
+            pfx = "bcsf" if self.impl == IMPL_BCSF else "hyb"
+            inf = self.info(0)
+            if self.impl == IMPL_BCSF:
+                d[f"{pfx}.nnz"] = np.array([inf["nnz"]], np.uint64)
+                d[f"{pfx}.modeOrder"] = np.array(inf["mode_order"], np.uint64)
+                self._dump_csf(d, 0, pfx, nd)
+                for b in range(10):
+                    d[f"{pfx}.bin{b}"] = self.export(0, f"bin{b}")
+        return d
+
+    def _dump_csf(self, d, p, pfx, nd):
+        for l in range(nd - 1):
+            d[f"{pfx}.fbrPtr{l}"] = self.export(p, f"fbrPtr{l}")
+            d[f"{pfx}.fbrIdx{l}"] = self.export(p, f"fbrIdx{l}")
+        d[f"{pfx}.nFibers"] = np.array([len(d[f"{pfx}.fbrPtr1"])], np.uint64)
+        d[f"{pfx}.fbrLikeSlcInds"] = self.export(p, "fbrLikeSlcInds")
+        try:
+            for m in range(nd):
+                d[f"{pfx}.inds{m}"] = self.export(p, f"inds{m}")
+        except MmcsfError:
+            pass
+        d[f"{pfx}.vals"] = self.export_f32(p, "vals")
+
+    # -- MTTKRP ---------------------------------------------------------------
+    def _cfg(self, cfg):
+        if cfg is None:
+            return None
+        if isinstance(cfg, KernelCfg):
+            return ctypes.byref(cfg)
+        c = KernelCfg()
+        for k, v in cfg.items():
+            setattr(c, k, v)
+        return ctypes.byref(c)
+
+    @staticmethod
+    def _dtype(factors):
+        import torch
+        dt = factors[0].dtype
+        if any(f.dtype != dt for f in factors):
+            raise MmcsfError(1, "all factors must share one dtype")
+        if dt == torch.float32:
+            return DTYPE_F32
+        if dt == torch.bfloat16:
+            return DTYPE_BF16
+        raise MmcsfError(1, f"unsupported factor dtype {dt}")
+
+    def mttkrp(self, mode, factors, out=None, cfg=None, stream=None):
+        """MTTKRP for one mode; factors: list of CUDA tensors (dims[m] x R,
+        float32 or bfloat16). Returns out (dims[mode] x R float32)."""
+        import torch
+        R = factors[0].shape[1]
+        if out is None:
+            out = torch.empty((self.dims[mode], R), dtype=torch.float32, device=factors[0].device)
+        fp = (c_voidp * self.nd)(*[_ptr(f) for f in factors])
+        check(lib().mmcsf_mttkrp(self._h, mode, R, self._dtype(factors), fp, _ptr(out), self._cfg(cfg),
+                                 _stream(stream)))
+        return out
+
+    def mttkrp_all(self, factors, outs=None, cfg=None, stream=None):
+        import torch
+        R = factors[0].shape[1]
+        if outs is None:
+            outs = [torch.empty((d, R), dtype=torch.float32, device=factors[0].device) for d in self.dims]
+        fp = (c_voidp * self.nd)(*[_ptr(f) for f in factors])
+        op = (c_voidp * self.nd)(*[_ptr(o) for o in outs])
+        check(lib().mmcsf_mttkrp_all(self._h, R, self._dtype(factors), fp, op, self._cfg(cfg), _stream(stream)))
+        return outs
+
+    def mttkrp_all_host(self, factors, outs=None, cfg=None, stream=None):
+        """All modes through host buffers (numpy float32, ideally pinned)."""
+        R = factors[0].shape[1]
+        if outs is None:
+            outs = [np.empty((d, R), np.float32) for d in self.dims]
+        fp = (c_voidp * self.nd)(*[ctypes.c_void_p(_host_ptr(f)) for f in factors])
+        op = (c_voidp * self.nd)(*[ctypes.c_void_p(_host_ptr(o)) for o in outs])
+        check(lib().mmcsf_mttkrp_all_host(self._h, R, fp, op, self._cfg(cfg), _stream(stream)))
+        return outs
+
+    @property
+    def last_launches(self):
+        n = ctypes.c_int()
+        check(lib().mmcsf_format_last_launches(self._h, ctypes.byref(n)))
+        return n.value
+
+
+class _CudaArray:
+    """Minimal __cuda_array_interface__ wrapper around a raw device pointer."""
+
+    def __init__(self, ptr, n, typestr):
+        self.__cuda_array_interface__ = {"shape": (int(n),), "typestr": typestr, "data": (int(ptr or 0), False),
+                                         "version": 2}
+
+
+def _host_ptr(a):
+    if isinstance(a, np.ndarray):
+        if not a.flags["C_CONTIGUOUS"] or a.dtype != np.float32:
+            raise MmcsfError(1, "host factors must be C-contiguous float32")
+        return a.ctypes.data
+    return a.data_ptr()  # torch CPU tensor (possibly pinned)

@@ -1,0 +1,99 @@
+"""ctypes binding to the in-tree C ABI (include/mmcsf.h, lib/libmmcsf.so).
+
+Loading fails loudly: there is no CPU fallback for anything in this package.
+"""
+import ctypes
+import os
+
+_PKG_ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(_PKG_ROOT, "lib", "libmmcsf.so")
+
+c_u64 = ctypes.c_uint64
+c_u64p = ctypes.POINTER(ctypes.c_uint64)
+c_u32p = ctypes.POINTER(ctypes.c_uint32)
+c_f32p = ctypes.POINTER(ctypes.c_float)
+c_voidp = ctypes.c_void_p
+c_int = ctypes.c_int
+
+
+class MmcsfError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"[{status}] {msg}")
+        self.status = status
+
+
+class GenSpec(ctypes.Structure):
+    _fields_ = [("nd", c_int), ("dims", c_u64 * 4), ("nnz", c_u64), ("dist", c_int * 4),
+                ("zipf_s", ctypes.c_double * 4), ("val_dist", c_int), ("seed", c_u64)]
+
+
+class BuildOpts(ctypes.Structure):
+    _fields_ = [("impl", c_int), ("mode", c_int), ("fiber_threshold", c_u64), ("partition_rule", c_int),
+                ("keep_coo", c_int)]
+
+
+class PartInfo(ctypes.Structure):
+    _fields_ = [("present", c_int), ("nd", c_int), ("mode_order", c_int * 4), ("nnz", c_u64),
+                ("n_slices", c_u64), ("n_fbrs", c_u64), ("n_fibers", c_u64), ("device_bytes", c_u64)]
+
+
+class KernelCfg(ctypes.Structure):
+    _fields_ = [("chunk", c_int), ("block_threads", c_int), ("leaf_variant", c_int), ("reserved", c_int * 5)]
+
+
+_lib = None
+
+# (name, argtypes) for every exported entry point in include/mmcsf.h
+SIGNATURES = {
+    "mmcsf_status_string": ([c_int], ctypes.c_char_p),
+    "mmcsf_last_error": ([], ctypes.c_char_p),
+    "mmcsf_version": ([], c_int),
+    "mmcsf_coo_load_tns": ([ctypes.c_char_p, ctypes.POINTER(c_voidp)], c_int),
+    "mmcsf_coo_create": ([c_int, c_u64p, c_u64, ctypes.POINTER(c_u32p), c_f32p, ctypes.POINTER(c_voidp)], c_int),
+    "mmcsf_coo_create_device": ([c_int, c_u64p, c_u64, ctypes.POINTER(c_voidp), c_voidp, c_voidp,
+                                 ctypes.POINTER(c_voidp)], c_int),
+    "mmcsf_coo_info": ([c_voidp, ctypes.POINTER(c_int), c_u64p, c_u64p], c_int),
+    "mmcsf_coo_to_host": ([c_voidp], c_int),
+    "mmcsf_coo_to_device": ([c_voidp, c_voidp], c_int),
+    "mmcsf_coo_host_arrays": ([c_voidp, ctypes.POINTER(c_voidp), ctypes.POINTER(c_voidp)], c_int),
+    "mmcsf_coo_device_arrays": ([c_voidp, ctypes.POINTER(c_voidp), ctypes.POINTER(c_voidp)], c_int),
+    "mmcsf_coo_write_tns": ([c_voidp, ctypes.c_char_p], c_int),
+    "mmcsf_coo_destroy": ([c_voidp], None),
+    "mmcsf_generate": ([ctypes.POINTER(GenSpec), c_voidp, ctypes.POINTER(c_voidp)], c_int),
+    "mmcsf_build": ([c_voidp, ctypes.POINTER(BuildOpts), c_voidp, ctypes.POINTER(c_voidp)], c_int),
+    "mmcsf_format_destroy": ([c_voidp], None),
+    "mmcsf_format_info": ([c_voidp, c_int, ctypes.POINTER(PartInfo)], c_int),
+    "mmcsf_format_meta": ([c_voidp, ctypes.POINTER(c_int), ctypes.POINTER(c_int)], c_int),
+    "mmcsf_format_export": ([c_voidp, c_int, ctypes.c_char_p, c_u64p, c_u64, c_u64p], c_int),
+    "mmcsf_format_export_f32": ([c_voidp, c_int, ctypes.c_char_p, c_f32p, c_u64, c_u64p], c_int),
+    "mmcsf_mttkrp": ([c_voidp, c_int, c_int, c_int, ctypes.POINTER(c_voidp), c_voidp,
+                      ctypes.POINTER(KernelCfg), c_voidp], c_int),
+    "mmcsf_mttkrp_all": ([c_voidp, c_int, c_int, ctypes.POINTER(c_voidp), ctypes.POINTER(c_voidp),
+                          ctypes.POINTER(KernelCfg), c_voidp], c_int),
+    "mmcsf_mttkrp_all_host": ([c_voidp, c_int, ctypes.POINTER(c_voidp), ctypes.POINTER(c_voidp),
+                               ctypes.POINTER(KernelCfg), c_voidp], c_int),
+    "mmcsf_format_last_launches": ([c_voidp, ctypes.POINTER(c_int)], c_int),
+}
+
+
+def lib():
+    """The loaded library. Raises if the in-tree build is missing."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise MmcsfError(-1, f"{LIB_PATH} is missing: build it with `make -C mm-csf_b200` "
+                                 "(python -c 'import __graft_entry__ as g; g.build()')")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (argt, rest) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.argtypes = argt
+            fn.restype = rest
+        _lib = L
+    return _lib
+
+
+def check(status):
+    if status != 0:
+        L = lib()
+        raise MmcsfError(status, L.mmcsf_last_error().decode() or L.mmcsf_status_string(status).decode())
+    return status

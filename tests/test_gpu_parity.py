@@ -1,0 +1,265 @@
+"""Parity of the CUDA path (through the C ABI) with the reference.
+
+* format arrays: bit-exact against the reference's own builders (golden
+  fixtures) and against the C oracle on fresh random tensors;
+* MTTKRP: within 1e-5 relative (Frobenius, and per element against
+  |ref| + 1e-6 * max|ref|) of the FP64 oracle, for every mode and many ranks;
+* full-size runs: size-independent properties (column checksums in FP64).
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+RTOL = 1e-5
+
+
+@pytest.fixture(scope="module")
+def torch_cuda():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return torch
+
+
+def _rand_coo(rng, dims, n, skew=False, dup=False):
+    if skew:
+        inds = [np.minimum(rng.zipf(1.4, n) - 1, d - 1).astype(np.uint64) for d in dims]
+    else:
+        inds = [rng.integers(0, d, n).astype(np.uint64) for d in dims]
+    if not dup:
+        key = np.zeros(n, np.uint64)
+        for m, d in enumerate(dims):
+            key = key * np.uint64(d) + inds[m]
+        _, first = np.unique(key, return_index=True)
+        first = np.sort(first)
+        inds = [i[first] for i in inds]
+    vals = (rng.random(len(inds[0])) + 0.05).astype(np.float32)
+    return inds, vals
+
+
+def _sentinel_key(kind, nd):
+    pfx = "part2" if kind == "mmcsf" else "bcsf"
+    return pfx, f"{pfx}.fbrIdx{nd - 2}", f"{pfx}.fbrPtr{nd - 2}"
+
+
+def _compare_dumps(ref, got, kind, nd, ctx):
+    pfx, skey, pkey = _sentinel_key(kind, nd)
+    for k, v in ref.items():
+        assert k in got, (ctx, k)
+        g = got[k]
+        if k.endswith("vals"):
+            assert np.array_equal(np.asarray(v, np.float32), g), (ctx, k)
+            continue
+        v = np.asarray(v).astype(np.int64)
+        g = np.asarray(g).astype(np.int64)
+        if k == skey and len(v):
+            # The reference's sentinel is read one past the last nonzero when
+            # the last fiber holds 2+ nonzeros; it is only defined otherwise.
+            ptr = np.asarray(ref[pkey], np.int64)
+            defined = len(ptr) < 2 or ptr[-1] - ptr[-2] == 1 or int(ref[f"{pfx}.nnz"][0]) == 1
+            assert len(v) == len(g), (ctx, k)
+            assert np.array_equal(v[:-1], g[:-1]), (ctx, k)
+            if defined:
+                assert v[-1] == g[-1], (ctx, k, "sentinel")
+            continue
+        assert len(v) == len(g) and np.array_equal(v, g), (ctx, k, v[:12], g[:12])
+
+
+def _check_close(got, ref64, ctx):
+    got = np.asarray(got, np.float64)
+    scale = np.abs(ref64).max() if ref64.size else 0.0
+    fro = np.linalg.norm(got - ref64) / max(np.linalg.norm(ref64), 1e-30)
+    assert fro <= RTOL, (ctx, "frobenius", fro)
+    if ref64.size:
+        rel = np.abs(got - ref64) / (np.abs(ref64) + 1e-6 * scale + 1e-30)
+        assert rel.max() <= RTOL * 10, (ctx, "max rel", rel.max())
+
+
+def test_golden_format_arrays_bit_exact(golden_cases, torch_cuda):
+    import mmcsf
+    n = 0
+    for case in golden_cases:
+        dims = case["dims"]
+        X = mmcsf.CooTensor.from_arrays(dims, case["inds"], case["vals"])
+        for fmt in case["formats"]:
+            if fmt["kind"] == "hyb":
+                continue
+            impl = mmcsf.IMPL_MMCSF if fmt["kind"] == "mmcsf" else mmcsf.IMPL_BCSF
+            F = mmcsf.Format(X, impl=impl, mode=fmt["mode"], fiber_threshold=fmt["f"], keep_coo=True)
+            _compare_dumps(fmt["arrays"], F.reference_dump(), fmt["kind"], len(dims),
+                           (case["name"], fmt["kind"], fmt["mode"], fmt["f"]))
+            n += 1
+    assert n >= 40
+
+
+def test_golden_mttkrp(golden_cases, torch_cuda):
+    import mmcsf
+    torch = torch_cuda
+    for case in golden_cases:
+        dims = case["dims"]
+        X = mmcsf.CooTensor.from_arrays(dims, case["inds"], case["vals"])
+        inds = [np.array(i, np.uint64) for i in case["inds"]]
+        vals = np.array(case["vals"], np.float32)
+        U = [np.array(u, np.float32).reshape(d, -1) for u, d in zip(case["factors"], dims)]
+        Ud = [torch.tensor(u, device="cuda") for u in U]
+        F = mmcsf.Format(X, impl=mmcsf.IMPL_MMCSF, mode=0, fiber_threshold=2)
+        outs = F.mttkrp_all(Ud)
+        torch.cuda.synchronize()
+        for mt in case["mttkrp"]:
+            m = mt["mode"]
+            ref32 = np.array(mt["out"], np.float32).reshape(dims[m], -1)
+            ref64 = O.mttkrp_coo_f64(dims, inds, vals, m, U)
+            got = outs[m].cpu().numpy()
+            _check_close(got, ref64, (case["name"], m))
+            # the reference's own FP32 output agrees to the same tolerance
+            assert np.linalg.norm(ref32 - ref64) / max(np.linalg.norm(ref64), 1e-30) <= RTOL
+        for m in range(len(dims)):  # single-mode B-CSF
+            B = mmcsf.Format(X, impl=mmcsf.IMPL_BCSF, mode=m, fiber_threshold=3)
+            got = B.mttkrp(m, Ud).cpu().numpy()
+            _check_close(got, O.mttkrp_coo_f64(dims, inds, vals, m, U), (case["name"], "bcsf", m))
+
+
+CASES = [
+    # nd, dims, nnz, skew, dup, f
+    (3, [300, 500, 200], 20000, False, False, 0),
+    (3, [300, 500, 200], 20000, True, False, 16),
+    (3, [64, 2000, 40], 30000, True, False, 1),
+    (3, [50, 50, 50], 8000, False, True, 5),
+    (4, [200, 40, 30, 10], 30000, False, False, 0),
+    (4, [300, 20, 10, 6], 30000, True, False, 3),
+    (4, [5, 3, 4, 2000], 20000, False, False, 0),  # long (o0,o1) runs: fbrS split at 128
+]
+
+
+@pytest.mark.parametrize("case", range(len(CASES)))
+def test_random_formats_match_oracle(case, torch_cuda):
+    import mmcsf
+    nd, dims, n, skew, dup, f = CASES[case]
+    rng = np.random.default_rng(100 + case)
+    inds, vals = _rand_coo(rng, dims, n, skew, dup)
+    X = mmcsf.CooTensor.from_arrays(dims, inds, vals)
+    fth = f if f else O.INF_TH
+    for mode in range(nd):
+        ref = O.build_mmcsf(dims, inds, vals, mode, fth)
+        F = mmcsf.Format(X, impl=mmcsf.IMPL_MMCSF, mode=mode, fiber_threshold=f, keep_coo=True)
+        _compare_dumps(ref, F.reference_dump(), "mmcsf", nd, ("mmcsf", case, mode))
+        refb = O.build_bcsf(dims, inds, vals, mode, fth)
+        B = mmcsf.Format(X, impl=mmcsf.IMPL_BCSF, mode=mode, fiber_threshold=f, keep_coo=True)
+        _compare_dumps(refb, B.reference_dump(), "bcsf", nd, ("bcsf", case, mode))
+
+
+@pytest.mark.parametrize("R", [1, 4, 8, 12, 16, 32, 48, 64, 128, 256])
+def test_mttkrp_all_modes_any_rank(R, torch_cuda):
+    import mmcsf
+    torch = torch_cuda
+    rng = np.random.default_rng(R)
+    for nd, dims, n, skew in ((3, [120, 300, 80], 15000, True), (4, [60, 30, 20, 40], 15000, False)):
+        inds, vals = _rand_coo(rng, dims, n, skew)
+        X = mmcsf.CooTensor.from_arrays(dims, inds, vals)
+        U = [rng.random((d, R)).astype(np.float32) for d in dims]
+        Ud = [torch.tensor(u, device="cuda") for u in U]
+        for f in (0, 7):
+            F = mmcsf.Format(X, impl=mmcsf.IMPL_MMCSF, mode=0, fiber_threshold=f)
+            outs = F.mttkrp_all(Ud)
+            torch.cuda.synchronize()
+            for m in range(nd):
+                _check_close(outs[m].cpu().numpy(), O.mttkrp_coo_f64(dims, inds, vals, m, U), (nd, R, f, m))
+
+
+@pytest.mark.parametrize("chunk", [1, 3, 32, 100, 4096])
+def test_chunk_sizes(chunk, torch_cuda):
+    import mmcsf
+    torch = torch_cuda
+    rng = np.random.default_rng(chunk)
+    dims = [40, 90, 30]
+    inds, vals = _rand_coo(rng, dims, 6000, True)
+    X = mmcsf.CooTensor.from_arrays(dims, inds, vals)
+    U = [rng.random((d, 32)).astype(np.float32) for d in dims]
+    Ud = [torch.tensor(u, device="cuda") for u in U]
+    F = mmcsf.Format(X, impl=mmcsf.IMPL_MMCSF, mode=0, fiber_threshold=0)
+    outs = F.mttkrp_all(Ud, cfg={"chunk": chunk})
+    torch.cuda.synchronize()
+    for m in range(3):
+        _check_close(outs[m].cpu().numpy(), O.mttkrp_coo_f64(dims, inds, vals, m, U), (chunk, m))
+
+
+def test_generator_distinct_deterministic(torch_cuda):
+    import mmcsf
+    dims = [2000, 3000, 50]
+    a = mmcsf.CooTensor.generate(dims, 200000, dist=[1, 1, 1], zipf_s=1.1, val_dist=mmcsf.VAL_LOGNORMAL, seed=3)
+    b = mmcsf.CooTensor.generate(dims, 200000, dist=[1, 1, 1], zipf_s=1.1, val_dist=mmcsf.VAL_LOGNORMAL, seed=3)
+    ia, va = a.host_arrays()
+    ib, vb = b.host_arrays()
+    for m in range(3):
+        assert np.array_equal(ia[m], ib[m])
+        assert ia[m].max() < dims[m]
+    assert np.array_equal(va, vb)
+    key = (ia[0].astype(np.uint64) * 3000 + ia[1]) * 50 + ia[2]
+    assert len(np.unique(key)) == len(key) == 200000
+    assert (va > 0).all()
+    # skew: the hottest slice of a Zipf(1.1) mode holds far more than the mean
+    cnt = np.bincount(ia[2], minlength=50)
+    assert cnt.max() > 3 * cnt.mean()
+
+
+def test_mttkrp_host_entry_point(torch_cuda):
+    import mmcsf
+    rng = np.random.default_rng(9)
+    dims = [100, 80, 60]
+    inds, vals = _rand_coo(rng, dims, 5000)
+    X = mmcsf.CooTensor.from_arrays(dims, inds, vals)
+    U = [rng.random((d, 32)).astype(np.float32) for d in dims]
+    F = mmcsf.Format(X, impl=mmcsf.IMPL_MMCSF)
+    for _ in range(2):
+        outs = F.mttkrp_all_host(U)
+        for m in range(3):
+            _check_close(outs[m], O.mttkrp_coo_f64(dims, inds, vals, m, U), ("host", m))
+
+
+def test_errors_are_status_codes(torch_cuda):
+    import mmcsf
+    torch = torch_cuda
+    dims = [10, 10, 10]
+    X = mmcsf.CooTensor.from_arrays(dims, [np.array([1]), np.array([2]), np.array([3])], np.array([1.0]))
+    with pytest.raises(mmcsf.MmcsfError):
+        mmcsf.Format(X, impl=7)
+    with pytest.raises(mmcsf.MmcsfError):
+        mmcsf.Format(X, impl=mmcsf.IMPL_MMCSF, mode=3)
+    B = mmcsf.Format(X, impl=mmcsf.IMPL_BCSF, mode=1)
+    U = [torch.rand(10, 8, device="cuda") for _ in range(3)]
+    with pytest.raises(mmcsf.MmcsfError):
+        B.mttkrp(0, U)  # built for mode 1 only
+    with pytest.raises(mmcsf.MmcsfError):
+        B.mttkrp_all(U)
+
+
+def test_full_size_skewed_checksums(torch_cuda):
+    """500k x 2M x 20k-shaped Zipf(1.1) tensor at 20M nonzeros: every mode's
+    column sums must equal sum_x v_x prod_{m != n} U_m[i_m, r] (FP64)."""
+    import mmcsf
+    torch = torch_cuda
+    dims = [500000, 2000000, 20000]
+    X = mmcsf.CooTensor.generate(dims, 20_000_000, dist=[1, 1, 1], zipf_s=1.1, val_dist=mmcsf.VAL_LOGNORMAL,
+                                 seed=11)
+    F = mmcsf.Format(X, impl=mmcsf.IMPL_MMCSF, mode=0, fiber_threshold=0)
+    g = torch.Generator(device="cuda").manual_seed(0)
+    U = [torch.rand(d, 32, device="cuda", generator=g) for d in dims]
+    outs = F.mttkrp_all(U)
+    torch.cuda.synchronize()
+    inds, vals = X.host_arrays()
+    Uc = [u.double().cpu() for u in U]
+    for m in range(3):
+        want = torch.zeros(32, dtype=torch.float64)
+        for s in range(0, len(vals), 2_000_000):
+            sl = slice(s, s + 2_000_000)
+            t = torch.from_numpy(vals[sl].astype(np.float64))[:, None].clone()
+            for q in range(3):
+                if q != m:
+                    t *= Uc[q][torch.from_numpy(inds[q][sl].astype(np.int64))]
+            want += t.sum(0)
+        got = outs[m].double().sum(0).cpu()
+        rel = ((got - want).abs() / want.abs()).max().item()
+        assert rel <= RTOL, (m, rel)

@@ -61,6 +61,8 @@ def parse():
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--views", type=int, default=1, help="0 none, 1 leaf-level modes, 2 every mode")
+    ap.add_argument("--no-tune", action="store_true")
     return ap.parse_args()
 
 
@@ -130,17 +132,18 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def algorithmic_bytes(nd, dims, nnz, R, esz, nfib, nfbrs, rows_touched):
-    """Per-mode compulsory bytes of the MM-CSF traversal (3-D: vals, leaf
-    index, fiber pointer/index/slice map; 4-D adds fiber->fbrS and the fbrS
-    index and slice map), every touched input-factor row once, and the dense
-    output written once."""
-    per_mode = []
-    struct = nnz * 8 + (nfib * 12 if nd == 3 else nfib * 12 + nfbrs * 8)
-    for m in range(nd):
-        fact = sum(rows_touched[q] * R * esz for q in range(nd) if q != m)
-        per_mode.append(struct + fact + dims[m] * R * 4)
-    return per_mode
+def struct_bytes(nd, nnz, nfib, nfbrs):
+    """Structure bytes one traversal of a CSF part reads: vals + leaf index per
+    nonzero; per leaf fiber its pointer, index and slice map (3-D), plus the
+    fiber->fbrS map per fiber and fbrS index + slice map per fbrS (4-D)."""
+    return nnz * 8 + (nfib * 12 if nd == 3 else nfib * 12 + nfbrs * 8)
+
+
+def mode_bytes(nd, dims, m, R, esz, sbytes, rows_touched):
+    """Compulsory bytes of one mode's MTTKRP: the traversal's structure, every
+    touched row of the other factors once, the dense output written once."""
+    fact = sum(rows_touched[q] * R * esz for q in range(nd) if q != m)
+    return sbytes + fact + dims[m] * R * 4
 
 
 def workload_stats(inds_dev, dims, order):
@@ -205,7 +208,8 @@ def main():
     R = a.rank or W["R"]
     esz = 4 if a.dtype == "f32" else 2
     hbm_peak, peak_kind = peaks()
-    config = {"workload": a.workload, "desc": W["desc"], "nnz": nnz, "R": R, "format": "MM-CSF (-t 12, -m 0)",
+    config = {"workload": a.workload, "desc": W["desc"], "nnz": nnz, "R": R,
+              "format": f"MM-CSF (-t 12, -m 0), views={a.views}",
               "fiber_threshold": a.fiber_threshold or "none", "factor_dtype": a.dtype,
               "l2": "inputs larger than L2 (structure > 800 MB per step)", "seed": a.seed,
               "parallelism": f"replicas x{world} (each rank its own tensor)"}
@@ -221,7 +225,7 @@ def main():
         from oracle import oracle as O
         order = O.order_modes(dims, 2)
         rows, nfib = workload_stats(inds_dev, dims, order)
-        per_mode = algorithmic_bytes(nd, dims, nnz, R, esz, nfib, 0, rows)
+        per_mode = [mode_bytes(nd, dims, m, R, esz, struct_bytes(nd, nnz, nfib, 0), rows) for m in range(nd)]
         step_bytes = sum(per_mode)
         inds_h, vals_h = X.host_arrays()
         del inds_dev
@@ -264,17 +268,26 @@ def main():
     import mmcsf
     X = mmcsf.CooTensor.generate(dims, nnz, dist=W["dist"], zipf_s=W["zipf"], val_dist=W["val"],
                                  seed=a.seed + rank)
-    F = mmcsf.Format(X, impl=mmcsf.IMPL_MMCSF, mode=0, fiber_threshold=a.fiber_threshold)
+    F = mmcsf.Format(X, impl=mmcsf.IMPL_MMCSF, mode=0, fiber_threshold=a.fiber_threshold, views=a.views)
     info = F.info(2)
     inds_dev, _ = device_coo(X)
     rows, nfib_nosplit = workload_stats(inds_dev, dims, info["mode_order"])
     del inds_dev
-    per_mode = algorithmic_bytes(nd, dims, nnz, R, esz, info["n_fibers"], info["n_fbrs"], rows)
-    step_bytes = sum(per_mode)
     g = torch.Generator(device="cuda").manual_seed(1234 + rank)
     tdt = torch.float32 if a.dtype == "f32" else torch.bfloat16
     U = [torch.rand(d, R, device="cuda", generator=g).to(tdt) for d in dims]
     outs = [torch.empty(d, R, device="cuda") for d in dims]
+    plan = None if a.no_tune else F.tune(U, outs)
+    # value: the workload's bytes under the MM-CSF partition traversal (the
+    # same definition the reference arm uses, so the two values compare as
+    # times); roofline: the bytes of the traversal each mode actually ran
+    sb_part = struct_bytes(nd, nnz, nfib_nosplit, info["n_fbrs"] if nd == 4 else 0)
+    step_bytes = sum(mode_bytes(nd, dims, m, R, esz, sb_part, rows) for m in range(nd))
+    per_mode = []
+    for m in range(nd):
+        trav = plan[m]["traversal"] if plan else (2 if F.info(4 + m)["present"] else 1)
+        pi = F.info(4 + m) if trav == 2 else info
+        per_mode.append(mode_bytes(nd, dims, m, R, esz, struct_bytes(nd, nnz, pi["n_fibers"], pi["n_fbrs"]), rows))
     stream = torch.cuda.current_stream()
 
     for _ in range(a.warmup):
@@ -344,10 +357,12 @@ def main():
     dom = max(range(nd), key=lambda m: mode_ms[m])
     achieved = per_mode[dom] / (mode_ms[dom] / 1e3) / 1e9
     traffic = traffic_from_profiles(a.workload, R, a.dtype)
+    dtrav = plan[dom]["traversal"] if plan else 1
+    dorder = F.info(4 + dom)["mode_order"] if dtrav == 2 else info["mode_order"]
     roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
                 "traffic": traffic, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
-                "kernel": f"k_mttkrp mode {dom} (level {info['mode_order'].index(dom)} of order "
-                          f"{info['mode_order']})",
+                "kernel": f"k_mttkrp mode {dom} (level {dorder.index(dom)} of order {dorder}, "
+                          f"{'view' if dtrav == 2 else 'MM-CSF partition'})",
                 "algorithmic_bytes": per_mode[dom], "avg_ms": mode_ms[dom]}
     cpu = None
     if not a.no_cpu and world == 1:
@@ -361,7 +376,8 @@ def main():
     line = {"metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": a.dtype, "data": "synthetic (seeded device generator)",
-            "config": config, "mode_ms": mode_ms, "format": info, "roofline": roofline, "cpu_baseline": cpu,
+            "config": config, "mode_ms": mode_ms, "plan": plan, "format": info, "roofline": roofline,
+            "cpu_baseline": cpu,
             "e2e": e2e, "gpu_launches": launches_per_step * a.steps, "clocks": clocks}
     print(json.dumps(line), flush=True)
     if world > 1:

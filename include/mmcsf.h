@@ -115,6 +115,8 @@ typedef struct {
   uint64_t fiber_threshold; /* -f: max nonzeros per fiber; 0 = the reference default (99999999) */
   int partition_rule;       /* 0: the reference as shipped (all nonzeros to partition 2, src/util.h:2517) */
   int keep_coo;             /* 1: keep every mode's sorted index array on the device for export */
+  int views;                /* slice-major views for MTTKRP (no counterpart in the reference):
+                               0 none, 1 = modes at the leaf level of the MM-CSF partition, 2 = every mode */
 } mmcsf_build_opts;
 
 typedef struct mmcsf_format mmcsf_format;
@@ -123,7 +125,8 @@ void mmcsf_format_destroy(mmcsf_format* F);
 
 /* Per-partition summary (the numbers the reference prints at
  * src/mttkrp_gpu.cu:3757-3767). part: 0..nd-1 for MM-CSF (a partition per
- * mode), 0 for B-CSF, 0 = CSF part / 1 = COO part / 2 = CSL part for HB-CSF. */
+ * mode), 0 for B-CSF, 0 = CSF part / 1 = COO part / 2 = CSL part for HB-CSF;
+ * 4 + m = the slice-major view of mode m (MM-CSF built with views). */
 typedef struct {
   int present;
   int nd;
@@ -157,9 +160,9 @@ int mmcsf_format_export_f32(const mmcsf_format* F, int part, const char* name, f
  * any R >= 1 (the reference's kernels are only correct for R <= 32).
  * Stream-ordered; nothing is synchronised. */
 typedef struct {
-  int chunk;         /* nonzeros per worker team; 0 = auto */
+  int chunk;         /* nonzeros per worker team; 0 = auto (the tuned plan, else 512) */
   int block_threads; /* threads per CTA; 0 = auto (256) */
-  int leaf_variant;  /* leaf-mode kernel: 0 auto, 1 scatter atomics, 2 privatised hot rows */
+  int traversal;     /* 0 auto (tuned plan, else a view when one exists), 1 MM-CSF partitions, 2 view */
   int reserved[5];
 } mmcsf_kernel_cfg;
 
@@ -178,6 +181,20 @@ int mmcsf_mttkrp_all(const mmcsf_format* F, int R, int factor_dtype, const void*
  * Device staging buffers are kept by the format between calls. */
 int mmcsf_mttkrp_all_host(mmcsf_format* F, int R, const float* const* h_factors, float* const* h_outs,
                           const mmcsf_kernel_cfg* cfg, void* stream);
+
+/* Autotuner (no counterpart in the reference, whose -w/-f are set by hand):
+ * times every traversal (MM-CSF partitions, the mode's view when built) and
+ * worker-team size for each mode with the caller's factors, keeps the fastest
+ * as the format's plan (used when mmcsf_kernel_cfg leaves chunk/traversal 0)
+ * and reports it. d_outs are used as scratch outputs. */
+typedef struct {
+  int traversal[4]; /* 1 MM-CSF partitions, 2 view */
+  int chunk[4];
+  float ms[4];      /* best time per mode */
+} mmcsf_plan;
+int mmcsf_tune(mmcsf_format* F, int R, int factor_dtype, const void* const* d_factors, float* const* d_outs,
+               void* stream, mmcsf_plan* plan);
+int mmcsf_set_plan(mmcsf_format* F, const mmcsf_plan* plan);
 
 /* Number of kernel launches the last MTTKRP/build call on this format made
  * (instrumentation for launch accounting). */

@@ -497,6 +497,21 @@ extern "C" int mmcsf_build(mmcsf_coo* X, const mmcsf_build_opts* opts, void* str
   MMCSF_TRY(build_csf(nd, part_order, X->nnz, sorted, svals, fth, fbrs_th,
                       opts->keep_coo != 0 || opts->impl == MMCSF_IMPL_HBCSF, P, s, L));
   if (opts->impl == MMCSF_IMPL_BCSF) MMCSF_TRY(compute_bins(P, true, s, L));
+  if (opts->impl == MMCSF_IMPL_MMCSF && opts->views) {
+    // Slice-major views: a CSF whose level 0 is mode m, in the reference's
+    // order for a mode-m CSF (order_tensormode), fully sorted, no splits.
+    for (int m = 0; m < nd; ++m) {
+      const bool at_leaf = P.order[nd - 1] == m;
+      if (opts->views == 1 && !at_leaf) continue;
+      if (P.order[0] == m) continue;  // the partition already serves m at level 0
+      int vo[4];
+      order_modes(nd, X->dims, m, vo);
+      std::vector<int> vkeys(vo, vo + nd);
+      DevBuf vs[4], vv;
+      MMCSF_TRY(sort_coo(X, vkeys, vs, vv, s, L));
+      MMCSF_TRY(build_csf(nd, vo, X->nnz, vs, vv, REF_DEFAULT_FBR_TH, FBRS_TH_OFF, false, Fm->views[m], s, L));
+    }
+  }
   if (opts->impl == MMCSF_IMPL_HBCSF) MMCSF_TRY(build_hyb(Fm, P, s, &L.n));
   Fm->last_launches = L.n;
   *out = guard.release();
@@ -507,12 +522,12 @@ extern "C" void mmcsf_format_destroy(mmcsf_format* F) { delete F; }
 
 extern "C" int mmcsf_format_info(const mmcsf_format* F, int part, mmcsf_part_info* info) {
   if (!F || !info) return set_error(MMCSF_ERR_INVALID, "null argument");
-  if (part < 0 || part >= 4) return set_error(MMCSF_ERR_INVALID, "bad part %d", part);
+  if (part < 0 || part >= 8) return set_error(MMCSF_ERR_INVALID, "bad part %d", part);
   memset(info, 0, sizeof *info);
-  const CsfPart& P = F->parts[part];
+  const CsfPart& P = part < 4 ? F->parts[part] : F->views[part - 4];
   info->present = P.present ? 1 : 0;
   info->nd = F->nd;
-  for (int i = 0; i < F->nd; ++i) info->mode_order[i] = P.present || F->impl == MMCSF_IMPL_MMCSF ? P.order[i] : i;
+  for (int i = 0; i < F->nd; ++i) info->mode_order[i] = P.present || (F->impl == MMCSF_IMPL_MMCSF && part < 4) ? P.order[i] : i;
   info->nnz = P.nnz;
   info->n_slices = P.n[0];
   info->n_fbrs = P.n[1];

@@ -63,6 +63,9 @@ struct mmcsf_format {
   int xorder[4] = {0, 1, 2, 3};
   uint64_t fbr_th = 0;
   mmcsf::CsfPart parts[4];
+  mmcsf::CsfPart views[4];  // views[m]: a CSF with mode m at level 0 (order_modes(m))
+  int plan_traversal[4] = {0, 0, 0, 0};  // tuned: 1 partitions, 2 view (0 = untuned)
+  int plan_chunk[4] = {0, 0, 0, 0};
   mmcsf::HybExtra hyb;
   int last_launches = 0;
   // staging for the host-buffer MTTKRP entry point

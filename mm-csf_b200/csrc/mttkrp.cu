@@ -386,7 +386,16 @@ int part_mttkrp(const mmcsf_format* F, const CsfPart& P, int mode, int R, int dt
 int mttkrp_mode(const mmcsf_format* F, int mode, int R, int dtype, const void* const* U, float* out,
                 const mmcsf_kernel_cfg* cfg, cudaStream_t s, int* launches) {
   MMCSF_CUDA(cudaMemsetAsync(out, 0, F->dims[mode] * (uint64_t)R * sizeof(float), s));
-  for (int p = 0; p < F->nd; ++p) MMCSF_TRY(part_mttkrp(F, F->parts[p], mode, R, dtype, U, out, cfg, s, launches));
+  int trav = cfg ? cfg->traversal : 0;
+  if (trav == 0) trav = F->plan_traversal[mode] ? F->plan_traversal[mode] : (F->views[mode].present ? 2 : 1);
+  mmcsf_kernel_cfg c{};
+  if (cfg) c = *cfg;
+  if (c.chunk == 0) c.chunk = F->plan_chunk[mode];
+  if (trav == 2) {
+    if (!F->views[mode].present) return set_error(MMCSF_ERR_INVALID, "no view for mode %d (build with views)", mode);
+    return part_mttkrp(F, F->views[mode], mode, R, dtype, U, out, &c, s, launches);
+  }
+  for (int p = 0; p < F->nd; ++p) MMCSF_TRY(part_mttkrp(F, F->parts[p], mode, R, dtype, U, out, &c, s, launches));
   return MMCSF_OK;
 }
 
@@ -487,5 +496,67 @@ extern "C" int mmcsf_mttkrp_all_host(mmcsf_format* F, int R, const float* const*
   for (int m = 0; m < F->nd; ++m)
     MMCSF_CUDA(cudaMemcpyAsync(h_outs[m], dout[m], F->dims[m] * (uint64_t)R * 4, cudaMemcpyDeviceToHost, s));
   MMCSF_CUDA(cudaStreamSynchronize(s));
+  return MMCSF_OK;
+}
+
+extern "C" int mmcsf_tune(mmcsf_format* F, int R, int factor_dtype, const void* const* d_factors,
+                          float* const* d_outs, void* stream, mmcsf_plan* plan) {
+  MMCSF_TRY(check_call(F, R, factor_dtype));
+  if (!d_factors || !d_outs) return set_error(MMCSF_ERR_INVALID, "null pointer");
+  cudaStream_t s = S(stream);
+  cudaEvent_t e0, e1;
+  MMCSF_CUDA(cudaEventCreate(&e0));
+  MMCSF_CUDA(cudaEventCreate(&e1));
+  const int chunks[] = {128, 256, 512, 1024, 2048, 4096};
+  const int nmodes = F->impl == MMCSF_IMPL_MMCSF ? F->nd : 1;
+  int st = MMCSF_OK;
+  for (int i = 0; i < nmodes && st == MMCSF_OK; ++i) {
+    const int m = F->impl == MMCSF_IMPL_MMCSF ? i : F->mode;
+    float best = 1e30f;
+    int bt = 1, bc = 512;
+    for (int trav = 1; trav <= 2 && st == MMCSF_OK; ++trav) {
+      if (trav == 2 && !F->views[m].present) continue;
+      for (int c : chunks) {
+        mmcsf_kernel_cfg cfg{};
+        cfg.chunk = c;
+        cfg.traversal = trav;
+        float ms = 0;
+        for (int rep = 0; rep < 2; ++rep) {  // the second run is timed
+          if ((st = mmcsf_mttkrp(F, m, R, factor_dtype, d_factors, d_outs[m], &cfg, stream)) != MMCSF_OK) break;
+          if (cudaEventRecord(e0, s) != cudaSuccess) { st = MMCSF_ERR_CUDA; break; }
+          if ((st = mmcsf_mttkrp(F, m, R, factor_dtype, d_factors, d_outs[m], &cfg, stream)) != MMCSF_OK) break;
+          if (cudaEventRecord(e1, s) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess) {
+            st = MMCSF_ERR_CUDA;
+            break;
+          }
+          cudaEventElapsedTime(&ms, e0, e1);
+        }
+        if (st != MMCSF_OK) break;
+        if (ms < best) { best = ms; bt = trav; bc = c; }
+      }
+    }
+    F->plan_traversal[m] = bt;
+    F->plan_chunk[m] = bc;
+    if (plan) {
+      plan->traversal[m] = bt;
+      plan->chunk[m] = bc;
+      plan->ms[m] = best;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return st;
+}
+
+extern "C" int mmcsf_set_plan(mmcsf_format* F, const mmcsf_plan* plan) {
+  if (!F || !plan) return set_error(MMCSF_ERR_INVALID, "null argument");
+  for (int m = 0; m < F->nd; ++m) {
+    if (plan->traversal[m] == 2 && !F->views[m].present)
+      return set_error(MMCSF_ERR_INVALID, "plan uses a view for mode %d that was not built", m);
+    if (plan->traversal[m] < 0 || plan->traversal[m] > 2 || plan->chunk[m] < 0)
+      return set_error(MMCSF_ERR_INVALID, "bad plan entry for mode %d", m);
+    F->plan_traversal[m] = plan->traversal[m];
+    F->plan_chunk[m] = plan->chunk[m];
+  }
   return MMCSF_OK;
 }

@@ -8,7 +8,7 @@ import ctypes
 
 import numpy as np
 
-from ._lib import (BuildOpts, GenSpec, KernelCfg, MmcsfError, PartInfo, c_f32p, c_u32p, c_u64, c_u64p, c_voidp,
+from ._lib import (BuildOpts, GenSpec, KernelCfg, MmcsfError, PartInfo, Plan, c_f32p, c_u32p, c_u64, c_u64p, c_voidp,
                    check, lib)
 
 IMPL_BCSF = 8
@@ -164,13 +164,14 @@ class Format:
     reference default). Replaces the builder chain the reference's main runs
     (src/mttkrp.cu:72-389)."""
 
-    def __init__(self, coo, impl=IMPL_MMCSF, mode=0, fiber_threshold=0, keep_coo=False, stream=None):
+    def __init__(self, coo, impl=IMPL_MMCSF, mode=0, fiber_threshold=0, keep_coo=False, views=0, stream=None):
         o = BuildOpts()
         o.impl = impl
         o.mode = mode
         o.fiber_threshold = int(fiber_threshold)
         o.partition_rule = 0
         o.keep_coo = 1 if keep_coo else 0
+        o.views = int(views)
         h = c_voidp()
         check(lib().mmcsf_build(coo._h, ctypes.byref(o), _stream(stream), ctypes.byref(h)))
         self._h = h
@@ -312,6 +313,27 @@ class Format:
         op = (c_voidp * self.nd)(*[ctypes.c_void_p(_host_ptr(o)) for o in outs])
         check(lib().mmcsf_mttkrp_all_host(self._h, R, fp, op, self._cfg(cfg), _stream(stream)))
         return outs
+
+    def tune(self, factors, outs=None, stream=None):
+        """Autotune traversal and team size per mode (mmcsf_tune); returns the plan."""
+        import torch
+        R = factors[0].shape[1]
+        if outs is None:
+            outs = [torch.empty((d, R), dtype=torch.float32, device=factors[0].device) for d in self.dims]
+        fp = (c_voidp * self.nd)(*[_ptr(f) for f in factors])
+        op = (c_voidp * self.nd)(*[_ptr(o) for o in outs])
+        pl = Plan()
+        check(lib().mmcsf_tune(self._h, R, self._dtype(factors), fp, op, _stream(stream), ctypes.byref(pl)))
+        n = self.nd if self.impl == IMPL_MMCSF else 1
+        modes = range(self.nd) if self.impl == IMPL_MMCSF else [self.mode]
+        return {m: {"traversal": pl.traversal[m], "chunk": pl.chunk[m], "ms": pl.ms[m]} for m in list(modes)[:n]}
+
+    def set_plan(self, plan):
+        pl = Plan()
+        for m, e in plan.items():
+            pl.traversal[m] = e["traversal"]
+            pl.chunk[m] = e["chunk"]
+        check(lib().mmcsf_set_plan(self._h, ctypes.byref(pl)))
 
     @property
     def last_launches(self):

@@ -29,7 +29,7 @@ class GenSpec(ctypes.Structure):
 
 class BuildOpts(ctypes.Structure):
     _fields_ = [("impl", c_int), ("mode", c_int), ("fiber_threshold", c_u64), ("partition_rule", c_int),
-                ("keep_coo", c_int)]
+                ("keep_coo", c_int), ("views", c_int)]
 
 
 class PartInfo(ctypes.Structure):
@@ -38,7 +38,11 @@ class PartInfo(ctypes.Structure):
 
 
 class KernelCfg(ctypes.Structure):
-    _fields_ = [("chunk", c_int), ("block_threads", c_int), ("leaf_variant", c_int), ("reserved", c_int * 5)]
+    _fields_ = [("chunk", c_int), ("block_threads", c_int), ("traversal", c_int), ("reserved", c_int * 5)]
+
+
+class Plan(ctypes.Structure):
+    _fields_ = [("traversal", c_int * 4), ("chunk", c_int * 4), ("ms", ctypes.c_float * 4)]
 
 
 _lib = None
@@ -73,6 +77,9 @@ SIGNATURES = {
     "mmcsf_mttkrp_all_host": ([c_voidp, c_int, ctypes.POINTER(c_voidp), ctypes.POINTER(c_voidp),
                                ctypes.POINTER(KernelCfg), c_voidp], c_int),
     "mmcsf_format_last_launches": ([c_voidp, ctypes.POINTER(c_int)], c_int),
+    "mmcsf_tune": ([c_voidp, c_int, c_int, ctypes.POINTER(c_voidp), ctypes.POINTER(c_voidp), c_voidp,
+                    ctypes.POINTER(Plan)], c_int),
+    "mmcsf_set_plan": ([c_voidp, ctypes.POINTER(Plan)], c_int),
 }
 
 

@@ -249,17 +249,51 @@ def test_full_size_skewed_checksums(torch_cuda):
     U = [torch.rand(d, 32, device="cuda", generator=g) for d in dims]
     outs = F.mttkrp_all(U)
     torch.cuda.synchronize()
-    inds, vals = X.host_arrays()
-    Uc = [u.double().cpu() for u in U]
+    di, dv = X.device_tensors()
+    Ud = [u.double() for u in U]
     for m in range(3):
-        want = torch.zeros(32, dtype=torch.float64)
-        for s in range(0, len(vals), 2_000_000):
-            sl = slice(s, s + 2_000_000)
-            t = torch.from_numpy(vals[sl].astype(np.float64))[:, None].clone()
+        want = torch.zeros(32, dtype=torch.float64, device="cuda")
+        for s in range(0, dv.numel(), 2_000_000):
+            t = dv[s:s + 2_000_000].double()[:, None]
             for q in range(3):
                 if q != m:
-                    t *= Uc[q][torch.from_numpy(inds[q][sl].astype(np.int64))]
+                    t = t * Ud[q][di[q][s:s + 2_000_000].long()]
             want += t.sum(0)
-        got = outs[m].double().sum(0).cpu()
+        got = outs[m].double().sum(0)
         rel = ((got - want).abs() / want.abs()).max().item()
         assert rel <= RTOL, (m, rel)
+
+
+@pytest.mark.parametrize("nd", [3, 4])
+def test_views_and_tuner(nd, torch_cuda):
+    import mmcsf
+    torch = torch_cuda
+    rng = np.random.default_rng(40 + nd)
+    dims = [150, 400, 60] if nd == 3 else [80, 50, 30, 40]
+    inds, vals = _rand_coo(rng, dims, 20000, True)
+    X = mmcsf.CooTensor.from_arrays(dims, inds, vals)
+    U = [rng.random((d, 32)).astype(np.float32) for d in dims]
+    Ud = [torch.tensor(u, device="cuda") for u in U]
+    F = mmcsf.Format(X, impl=mmcsf.IMPL_MMCSF, mode=0, views=2)
+    order = F.info(2)["mode_order"]
+    ref = [O.mttkrp_coo_f64(dims, inds, vals, m, U) for m in range(nd)]
+    for m in range(nd):
+        v = F.info(4 + m)
+        assert v["present"] == (m != order[0]) and (not v["present"] or v["mode_order"][0] == m)
+        for trav in (1, 2):
+            if trav == 2 and not v["present"]:
+                with pytest.raises(mmcsf.MmcsfError):
+                    F.mttkrp(m, Ud, cfg={"traversal": 2})
+                continue
+            out = F.mttkrp(m, Ud, cfg={"traversal": trav})
+            _check_close(out.cpu().numpy(), ref[m], ("view", nd, m, trav))
+    plan = F.tune(Ud)
+    assert set(plan) == set(range(nd))
+    outs = F.mttkrp_all(Ud)
+    torch.cuda.synchronize()
+    for m in range(nd):
+        _check_close(outs[m].cpu().numpy(), ref[m], ("tuned", nd, m))
+    # views=1 builds only the leaf-level mode's view
+    F1 = mmcsf.Format(X, impl=mmcsf.IMPL_MMCSF, mode=0, views=1)
+    present = [F1.info(4 + m)["present"] for m in range(nd)]
+    assert present == [m == order[-1] for m in range(nd)]

@@ -10,8 +10,10 @@
  * replaces. The reference has no plugin layer; its boundary is the C++
  * function API in src/mttkrp_gpu.h:59-81 plus the builders in src/util.h.
  *
- * Index limits: every mode length and the nonzero count must be below 2^32
- * (indices are stored as uint32 on the device; the reference uses size_t).
+ * Index limits: the nonzero count must be below 2^32 and, to build a format,
+ * every mode length below 2^31 (indices are stored as uint32 on the device,
+ * the leaf index carrying a fiber-start flag in bit 31; the reference uses
+ * size_t).
  */
 #ifndef MMCSF_H
 #define MMCSF_H

@@ -155,6 +155,12 @@ __global__ void k_bins(const uint32_t* __restrict__ sptr, const uint32_t* __rest
   }
 }
 
+// bit 31 of the leaf index marks the first nonzero of every leaf fiber
+__global__ void k_flag_fibers(uint32_t* __restrict__ leaf, const uint32_t* __restrict__ fptr, uint64_t nfib) {
+  for (uint64_t f = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; f < nfib; f += (uint64_t)gridDim.x * blockDim.x)
+    leaf[fptr[f]] |= 0x80000000u;
+}
+
 // ---- host helpers ----------------------------------------------------------
 
 int bits_for(uint64_t dim) {
@@ -401,6 +407,8 @@ static int build_csf(int nd, const int* order, uint64_t n, DevBuf* sorted, DevBu
       }
     }
   }
+  k_flag_fibers<<<GF, 256, 0, s>>>(P.leaf.as<uint32_t>(), P.ptr[lf].as<uint32_t>(), F);
+  LCHECK(L);
   MMCSF_CUDA(cudaStreamSynchronize(s));
   return MMCSF_OK;
 }
@@ -441,6 +449,10 @@ extern "C" int mmcsf_build(mmcsf_coo* X, const mmcsf_build_opts* opts, void* str
     return set_error(MMCSF_ERR_INVALID, "Mode cannot be larger than tensor dimension.");
   if (opts->partition_rule != 0)
     return set_error(MMCSF_ERR_UNSUPPORTED, "partition rule %d not implemented", opts->partition_rule);
+  for (int m = 0; m < nd; ++m)
+    if (X->dims[m] >= (1ull << 31))
+      return set_error(MMCSF_ERR_UNSUPPORTED, "mode %d length %llu: formats need lengths below 2^31", m,
+                       (unsigned long long)X->dims[m]);
   cudaStream_t s = S(stream);
   MMCSF_TRY(mmcsf_coo_to_device(X, stream));
   mmcsf_format* Fm = new (std::nothrow) mmcsf_format;

@@ -13,7 +13,7 @@ using mmcsf::DevBuf;
 
 namespace {
 
-int copy_u32(const DevBuf& b, uint64_t n, uint64_t* dst, uint64_t cap, uint64_t* count) {
+int copy_u32(const DevBuf& b, uint64_t n, uint64_t* dst, uint64_t cap, uint64_t* count, uint32_t mask = ~0u) {
   if (count) *count = n;
   if (!dst) return MMCSF_OK;
   if (cap < n) return set_error(MMCSF_ERR_INVALID, "export buffer too small (%llu < %llu)",
@@ -22,7 +22,7 @@ int copy_u32(const DevBuf& b, uint64_t n, uint64_t* dst, uint64_t cap, uint64_t*
   std::vector<uint32_t> h(n);
   MMCSF_CUDA(cudaDeviceSynchronize());
   MMCSF_CUDA(cudaMemcpy(h.data(), b.p, n * 4, cudaMemcpyDeviceToHost));
-  for (uint64_t i = 0; i < n; ++i) dst[i] = h[i];
+  for (uint64_t i = 0; i < n; ++i) dst[i] = h[i] & mask;
   return MMCSF_OK;
 }
 
@@ -90,7 +90,8 @@ extern "C" int mmcsf_format_export(const mmcsf_format* F, int part, const char* 
   if (starts(name, "fbrPtr", &l) && l < nd - 1) return copy_u32(P.ptr[l], ptr_len(l), dst, cap, count);
   if (starts(name, "fbrIdx", &l) && l < nd - 1) return copy_u32(P.idx[l], idx_len(l), dst, cap, count);
   if (!strcmp(name, "fbrLikeSlcInds")) return copy_u32(P.fbr_like, P.n[1], dst, cap, count);
-  if (!strcmp(name, "indsLeaf")) return copy_u32(P.leaf, P.nnz, dst, cap, count);
+  // the leaf array carries fiber-start flags in bit 31 (see build.cu)
+  if (!strcmp(name, "indsLeaf")) return copy_u32(P.leaf, P.nnz, dst, cap, count, 0x7fffffffu);
   if (starts(name, "inds", &l) && l < nd) {
     if (!P.coo[l].p) return set_error(MMCSF_ERR_INVALID, "build with keep_coo=1 to export inds%d", l);
     return copy_u32(P.coo[l], P.nnz, dst, cap, count);

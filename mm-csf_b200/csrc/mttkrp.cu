@@ -91,173 +91,208 @@ __device__ __forceinline__ uint32_t find_fiber(const uint32_t* __restrict__ fptr
 
 // ND: 3 or 4. OUT: output level (0 = slice ... ND-1 = leaf). G lanes per row,
 // V float4 per lane, R = 4*G*V.
+//
+// Per team the only dependent-load chain left per block of G nonzeros is the
+// factor-row gather: leaf indices and values for the next block are loaded
+// while the current block is processed; fiber starts are flagged in bit 31 of
+// the leaf index (no fiber-pointer reads after the initial search); the
+// fibers' metadata (index, slice map) sits in a G-wide register window
+// refilled with one coalesced load every G fibers; and the factor row a fiber
+// needs when it closes is requested as soon as the fiber opens.
 template <int ND, int OUT, int G, int V, class T>
 __global__ void __launch_bounds__(256) k_mttkrp(const Args<T> a) {
   const int lane = threadIdx.x & 31;
   const int tl = lane & (G - 1);
   const int tb = lane - tl;
+  const unsigned tmask = (G == 32) ? FULL : (((1u << G) - 1u) << tb);
   const uint64_t team = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) / G;
-  // Teams past the end stay in the loop (empty range) so every shuffle sees
-  // the full warp; all teams run the same number of iterations.
+  // Teams past the end stay in the loop (empty range) so every full-warp
+  // shuffle sees all lanes; all teams run the same number of iterations.
   const bool active = team * a.chunk < a.nnz;
   const uint64_t x0 = active ? team * a.chunk : a.nnz - 1;
   const uint64_t x1 = active ? min(x0 + a.chunk, a.nnz) : x0;
   const uint32_t R = a.R;
   constexpr int LEAF = ND - 1;
-
-  uint32_t f = find_fiber(a.fptr, a.nfib, x0);
-  uint64_t fend = __ldg(a.fptr + f + 1);
-  uint32_t fs = 0;
-  if (ND == 4) fs = __ldg(a.fpar + f);
-
-  float4 acc[V], acc1[V], acc2[V], w[V];
-#pragma unroll
-  for (int v = 0; v < V; ++v) acc[v] = acc1[v] = acc2[v] = w[v] = f4(0.f);
-
-  // current output-row keys for the accumulators above the leaf fiber
-  uint32_t cur_a = __ldg(a.like + (ND == 3 ? f : fs));
-
+  constexpr uint32_t FLAG = 0x80000000u;
   auto col = [&](int v) -> uint64_t { return (uint64_t)(tl + v * G) * 4; };
 
-  auto leaf_weights = [&]() {  // w = Hadamard of the rows above the leaf for fiber f
-    if constexpr (OUT == LEAF) {
-      if constexpr (ND == 3) {
-        const uint64_t ra = (uint64_t)__ldg(a.like + f) * R, rb = (uint64_t)__ldg(a.fidx + f) * R;
+  uint32_t f = find_fiber(a.fptr, a.nfib, x0);
+  // fiber metadata window: lane i holds fiber fw + i
+  uint32_t fw = f;
+  uint32_t wi, wp;  // 3-D: (b index, a index); 4-D: (c index, fbrS id)
+  auto refill = [&]() {
+    const uint32_t q = min(fw + (uint32_t)tl, a.nfib);
+    wi = __ldg(a.fidx + q);
+    wp = (ND == 3) ? __ldg(a.like + q) : __ldg(a.fpar + q);
+  };
+  refill();
+  uint32_t ci = __shfl_sync(tmask, wi, tb);  // current fiber's index (b in 3-D, c in 4-D)
+  uint32_t cp = __shfl_sync(tmask, wp, tb);  // current fiber's a (3-D) or fbrS (4-D)
+  uint32_t sb = 0, sa = 0;                   // 4-D: current fbrS's b and a
+  if (ND == 4) { sb = __ldg(a.sidx1 + cp); sa = __ldg(a.like + cp); }
+
+  float4 acc[V], acc1[V], acc2[V], crow[V], srow[V];
 #pragma unroll
-        for (int v = 0; v < V; ++v) w[v] = Row<T>::load(a.U[0], ra + col(v)) * Row<T>::load(a.U[1], rb + col(v));
+  for (int v = 0; v < V; ++v) acc[v] = acc1[v] = acc2[v] = crow[v] = srow[v] = f4(0.f);
+  uint32_t cur_a = (ND == 3) ? cp : sa;  // slice whose accumulation is open (OUT == 0)
+
+  // rows needed per fbrS (4-D) and per fiber, requested when they open
+  auto open_fbrs = [&]() {
+    if constexpr (ND == 4) {
+      if constexpr (OUT == 0) {
+#pragma unroll
+        for (int v = 0; v < V; ++v) srow[v] = Row<T>::load(a.U[1], (uint64_t)sb * R + col(v));
+      } else if constexpr (OUT == 1) {
+#pragma unroll
+        for (int v = 0; v < V; ++v) srow[v] = Row<T>::load(a.U[0], (uint64_t)sa * R + col(v));
       } else {
-        const uint64_t ra = (uint64_t)__ldg(a.like + fs) * R, rb = (uint64_t)__ldg(a.sidx1 + fs) * R,
-                       rc = (uint64_t)__ldg(a.fidx + f) * R;
 #pragma unroll
         for (int v = 0; v < V; ++v)
-          w[v] = Row<T>::load(a.U[0], ra + col(v)) * Row<T>::load(a.U[1], rb + col(v)) *
-                 Row<T>::load(a.U[2], rc + col(v));
+          srow[v] = Row<T>::load(a.U[0], (uint64_t)sa * R + col(v)) * Row<T>::load(a.U[1], (uint64_t)sb * R + col(v));
       }
     }
   };
-  leaf_weights();
+  auto open_fiber = [&]() {
+    if constexpr (ND == 3) {
+      if constexpr (OUT == 0) {
+#pragma unroll
+        for (int v = 0; v < V; ++v) crow[v] = Row<T>::load(a.U[1], (uint64_t)ci * R + col(v));
+      } else if constexpr (OUT == 1) {
+#pragma unroll
+        for (int v = 0; v < V; ++v) crow[v] = Row<T>::load(a.U[0], (uint64_t)cp * R + col(v));
+      } else {
+#pragma unroll
+        for (int v = 0; v < V; ++v)
+          crow[v] = Row<T>::load(a.U[0], (uint64_t)cp * R + col(v)) * Row<T>::load(a.U[1], (uint64_t)ci * R + col(v));
+      }
+    } else {
+      if constexpr (OUT == 3) {
+#pragma unroll
+        for (int v = 0; v < V; ++v) crow[v] = srow[v] * Row<T>::load(a.U[2], (uint64_t)ci * R + col(v));
+      } else if constexpr (OUT != 2) {
+#pragma unroll
+        for (int v = 0; v < V; ++v) crow[v] = Row<T>::load(a.U[2], (uint64_t)ci * R + col(v));
+      }
+    }
+  };
+  open_fbrs();
+  open_fiber();
 
-  // Close leaf fiber f (its partial over this team's range is in acc).
-  // `last` = the team's range ends here (flush everything).
-  auto close_fiber = [&](bool last) {
+  // Fold the open fiber's partial (acc) into the level above / the output.
+  auto close_fiber = [&]() {
     if constexpr (OUT == LEAF) {
-      (void)last;
       return;
     } else if constexpr (ND == 3) {
       if constexpr (OUT == 1) {
-        const uint64_t ra = (uint64_t)__ldg(a.like + f) * R, ro = (uint64_t)__ldg(a.fidx + f) * R;
 #pragma unroll
-        for (int v = 0; v < V; ++v) red4(a.out + ro + col(v), Row<T>::load(a.U[0], ra + col(v)) * acc[v]);
-      } else {  // OUT == 0: slice run accumulation
-        const uint64_t rb = (uint64_t)__ldg(a.fidx + f) * R;
-#pragma unroll
-        for (int v = 0; v < V; ++v) acc1[v] = acc1[v] + Row<T>::load(a.U[1], rb + col(v)) * acc[v];
-        const uint32_t nxt = last ? 0xffffffffu : __ldg(a.like + f + 1);
-        if (last || nxt != cur_a) {
-#pragma unroll
-          for (int v = 0; v < V; ++v) { red4(a.out + (uint64_t)cur_a * R + col(v), acc1[v]); acc1[v] = f4(0.f); }
-          cur_a = nxt;
-        }
-      }
-    } else {  // ND == 4
-      const uint64_t rc = (uint64_t)__ldg(a.fidx + f) * R;
-      if constexpr (OUT == 2) {
-        const uint64_t ra = (uint64_t)__ldg(a.like + fs) * R, rb = (uint64_t)__ldg(a.sidx1 + fs) * R;
-#pragma unroll
-        for (int v = 0; v < V; ++v)
-          red4(a.out + rc + col(v),
-               Row<T>::load(a.U[0], ra + col(v)) * Row<T>::load(a.U[1], rb + col(v)) * acc[v]);
+        for (int v = 0; v < V; ++v) red4(a.out + (uint64_t)ci * R + col(v), crow[v] * acc[v]);
       } else {
 #pragma unroll
-        for (int v = 0; v < V; ++v) acc1[v] = acc1[v] + Row<T>::load(a.U[2], rc + col(v)) * acc[v];
-        const uint32_t nfs = last ? 0xffffffffu : __ldg(a.fpar + f + 1);
-        if (last || nfs != fs) {  // close fbrS fs
-          if constexpr (OUT == 1) {
-            const uint64_t ra = (uint64_t)__ldg(a.like + fs) * R, ro = (uint64_t)__ldg(a.sidx1 + fs) * R;
+        for (int v = 0; v < V; ++v) acc1[v] = acc1[v] + crow[v] * acc[v];
+      }
+    } else {
+      if constexpr (OUT == 2) {
 #pragma unroll
-            for (int v = 0; v < V; ++v) {
-              red4(a.out + ro + col(v), Row<T>::load(a.U[0], ra + col(v)) * acc1[v]);
-              acc1[v] = f4(0.f);
-            }
-          } else {  // OUT == 0
-            const uint64_t rb = (uint64_t)__ldg(a.sidx1 + fs) * R;
+        for (int v = 0; v < V; ++v) red4(a.out + (uint64_t)ci * R + col(v), srow[v] * acc[v]);
+      } else {
 #pragma unroll
-            for (int v = 0; v < V; ++v) {
-              acc2[v] = acc2[v] + Row<T>::load(a.U[1], rb + col(v)) * acc1[v];
-              acc1[v] = f4(0.f);
-            }
-            const uint32_t na = last ? 0xffffffffu : __ldg(a.like + nfs);
-            if (last || na != cur_a) {
-#pragma unroll
-              for (int v = 0; v < V; ++v) {
-                red4(a.out + (uint64_t)cur_a * R + col(v), acc2[v]);
-                acc2[v] = f4(0.f);
-              }
-              cur_a = na;
-            }
-          }
-        }
+        for (int v = 0; v < V; ++v) acc1[v] = acc1[v] + crow[v] * acc[v];
       }
     }
   };
+  // 4-D: fold the open fbrS (acc1) upward (OUT 0) or out (OUT 1).
+  auto close_fbrs = [&]() {
+    if constexpr (ND == 4 && OUT == 1) {
+#pragma unroll
+      for (int v = 0; v < V; ++v) { red4(a.out + (uint64_t)sb * R + col(v), srow[v] * acc1[v]); acc1[v] = f4(0.f); }
+    } else if constexpr (ND == 4 && OUT == 0) {
+#pragma unroll
+      for (int v = 0; v < V; ++v) { acc2[v] = acc2[v] + srow[v] * acc1[v]; acc1[v] = f4(0.f); }
+    }
+  };
+  auto flush_slice = [&]() {
+    if constexpr (OUT == 0 && ND == 3) {
+#pragma unroll
+      for (int v = 0; v < V; ++v) { red4(a.out + (uint64_t)cur_a * R + col(v), acc1[v]); acc1[v] = f4(0.f); }
+    } else if constexpr (OUT == 0) {
+#pragma unroll
+      for (int v = 0; v < V; ++v) { red4(a.out + (uint64_t)cur_a * R + col(v), acc2[v]); acc2[v] = f4(0.f); }
+    }
+  };
 
-  constexpr int PF = G > 8 ? 8 : G;  // row gathers in flight per lane
+  constexpr int PF = G > 8 ? 8 : G;  // row gathers in flight per lane per batch
+  uint32_t nk = 0;
+  float nv = 0.f;
+  if (x0 + tl < x1) { nk = __ldg(a.leaf + x0 + tl); nv = __ldg(a.vals + x0 + tl); }
   for (uint32_t it = 0; it < a.chunk; it += G) {
     const uint64_t xb = x0 + it;
-    const uint64_t xi = xb + tl;
-    const bool okx = xi < x1;
-    const uint32_t my_k = okx ? __ldg(a.leaf + xi) : 0u;
-    const float my_v = okx ? __ldg(a.vals + xi) : 0.f;
-    if constexpr (OUT != LEAF) {
+    const uint32_t kv = nk;
+    const float vv = nv;
+    {  // next block's indices and values, while this block is processed
+      const uint64_t xn = xb + G + tl;
+      nk = 0;
+      nv = 0.f;
+      if (it + G < a.chunk && xn < x1) { nk = __ldg(a.leaf + xn); nv = __ldg(a.vals + xn); }
+    }
+    const bool fl = (xb + tl < x1) && (kv & FLAG) && (xb + tl != x0);
+    const uint32_t fm = (__ballot_sync(FULL, fl) >> tb) & ((G == 32) ? FULL : ((1u << G) - 1u));
+    const uint32_t k = kv & ~FLAG;
 #pragma unroll
-      for (int jb = 0; jb < G; jb += PF) {
-        float4 rows[PF][V];
+    for (int jb = 0; jb < G; jb += PF) {
+      float4 rows[PF][V];
+      uint32_t kj[PF];
 #pragma unroll
-        for (int j = 0; j < PF; ++j) {
-          const uint32_t k = __shfl_sync(FULL, my_k, tb + jb + j);
-          const uint64_t rk = (uint64_t)k * R;
+      for (int j = 0; j < PF; ++j) {
+        kj[j] = __shfl_sync(FULL, k, tb + jb + j);
+        if constexpr (OUT != LEAF) {
 #pragma unroll
-          for (int v = 0; v < V; ++v) rows[j][v] = Row<T>::load(a.U[LEAF], rk + col(v));
-        }
-#pragma unroll
-        for (int j = 0; j < PF; ++j) {
-          const float val = __shfl_sync(FULL, my_v, tb + jb + j);
-          const uint64_t x = xb + jb + j;
-          if (x < x1) {
-            if (x == fend) {
-              close_fiber(false);
-              ++f;
-              fend = __ldg(a.fptr + f + 1);
-              if (ND == 4) fs = __ldg(a.fpar + f);
-#pragma unroll
-              for (int v = 0; v < V; ++v) acc[v] = f4(0.f);
-            }
-#pragma unroll
-            for (int v = 0; v < V; ++v) acc[v] = fma4(val, rows[j][v], acc[v]);
-          }
+          for (int v = 0; v < V; ++v) rows[j][v] = Row<T>::load(a.U[LEAF], (uint64_t)kj[j] * R + col(v));
         }
       }
-    } else {
 #pragma unroll
-      for (int j = 0; j < G; ++j) {
-        const uint32_t k = __shfl_sync(FULL, my_k, tb + j);
-        const float val = __shfl_sync(FULL, my_v, tb + j);
-        const uint64_t x = xb + j;
+      for (int j = 0; j < PF; ++j) {
+        const float val = __shfl_sync(FULL, vv, tb + jb + j);
+        const uint64_t x = xb + jb + j;
         if (x < x1) {
-          if (x == fend) {
+          if ((fm >> (jb + j)) & 1u) {  // nonzero x opens fiber f+1 (team-uniform branch)
+            close_fiber();
             ++f;
-            fend = __ldg(a.fptr + f + 1);
-            if (ND == 4) fs = __ldg(a.fpar + f);
-            leaf_weights();
-          }
-          const uint64_t ro = (uint64_t)k * R;
+            if (f - fw >= (uint32_t)G) { fw = f; refill(); }
+            ci = __shfl_sync(tmask, wi, tb + (int)(f - fw));
+            const uint32_t np = __shfl_sync(tmask, wp, tb + (int)(f - fw));
+            if constexpr (ND == 3) {
+              if (OUT == 0 && np != cur_a) { flush_slice(); cur_a = np; }
+              cp = np;
+            } else {
+              if (np != cp) {  // new fbrS
+                close_fbrs();
+                cp = np;
+                sb = __ldg(a.sidx1 + cp);
+                sa = __ldg(a.like + cp);
+                if (OUT == 0 && sa != cur_a) { flush_slice(); cur_a = sa; }
+                open_fbrs();
+              }
+            }
+            open_fiber();
 #pragma unroll
-          for (int v = 0; v < V; ++v) red4(a.out + ro + col(v), f4(val) * w[v]);
+            for (int v = 0; v < V; ++v) acc[v] = f4(0.f);
+          }
+          if constexpr (OUT != LEAF) {
+#pragma unroll
+            for (int v = 0; v < V; ++v) acc[v] = fma4(val, rows[j][v], acc[v]);
+          } else {
+#pragma unroll
+            for (int v = 0; v < V; ++v) red4(a.out + (uint64_t)kj[j] * R + col(v), f4(val) * crow[v]);
+          }
         }
       }
     }
   }
-  if (active) close_fiber(true);
+  if (active) {
+    close_fiber();
+    close_fbrs();
+    flush_slice();
+  }
 }
 
 template <int ND, int OUT, int G, int V, class T>

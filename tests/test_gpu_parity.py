@@ -236,15 +236,23 @@ def test_errors_are_status_codes(torch_cuda):
         B.mttkrp_all(U)
 
 
-def test_full_size_skewed_checksums(torch_cuda):
+@pytest.mark.parametrize("views", [1, 0])
+def test_full_size_skewed_checksums(views, torch_cuda):
     """500k x 2M x 20k-shaped Zipf(1.1) tensor at 20M nonzeros: every mode's
-    column sums must equal sum_x v_x prod_{m != n} U_m[i_m, r] (FP64)."""
+    column sums must equal sum_x v_x prod_{m != n} U_m[i_m, r] (FP64).
+
+    With views=0 the leaf mode scatters one FP32 atomic per nonzero, as the
+    reference's kernel does (src/mttkrp_gpu.cu:1438-1472); the hottest output
+    rows then sum ~10^6 terms sequentially in FP32, whose rounding error is
+    ~1e-4 relative, so that one traversal is held to 2e-4. Every traversal
+    that reduces in registers first is held to 1e-5."""
     import mmcsf
     torch = torch_cuda
     dims = [500000, 2000000, 20000]
     X = mmcsf.CooTensor.generate(dims, 20_000_000, dist=[1, 1, 1], zipf_s=1.1, val_dist=mmcsf.VAL_LOGNORMAL,
                                  seed=11)
-    F = mmcsf.Format(X, impl=mmcsf.IMPL_MMCSF, mode=0, fiber_threshold=0)
+    F = mmcsf.Format(X, impl=mmcsf.IMPL_MMCSF, mode=0, fiber_threshold=0, views=views)
+    leaf_mode = F.info(2)["mode_order"][-1]
     g = torch.Generator(device="cuda").manual_seed(0)
     U = [torch.rand(d, 32, device="cuda", generator=g) for d in dims]
     outs = F.mttkrp_all(U)
@@ -261,7 +269,8 @@ def test_full_size_skewed_checksums(torch_cuda):
             want += t.sum(0)
         got = outs[m].double().sum(0)
         rel = ((got - want).abs() / want.abs()).max().item()
-        assert rel <= RTOL, (m, rel)
+        tol = 2e-4 if (views == 0 and m == leaf_mode) else RTOL
+        assert rel <= tol, (m, rel)
 
 
 @pytest.mark.parametrize("nd", [3, 4])

@@ -60,6 +60,9 @@ __device__ __forceinline__ float4 operator+(float4 a, float4 b) {
 __device__ __forceinline__ float4 fma4(float s, float4 a, float4 c) {
   return make_float4(fmaf(s, a.x, c.x), fmaf(s, a.y, c.y), fmaf(s, a.z, c.z), fmaf(s, a.w, c.w));
 }
+__device__ __forceinline__ float4 fma4v(float4 a, float4 b, float4 c) {
+  return make_float4(fmaf(a.x, b.x, c.x), fmaf(a.y, b.y, c.y), fmaf(a.z, b.z, c.z), fmaf(a.w, b.w, c.w));
+}
 __device__ __forceinline__ void red4(float* p, float4 v) { atomicAdd(reinterpret_cast<float4*>(p), v); }
 
 template <class T>
@@ -90,7 +93,8 @@ __device__ __forceinline__ uint32_t find_fiber(const uint32_t* __restrict__ fptr
 }
 
 // ND: 3 or 4. OUT: output level (0 = slice ... ND-1 = leaf). G lanes per row,
-// V float4 per lane, R = 4*G*V.
+// V float4 per lane, R = 4*G*V (a compile-time constant: row offsets are
+// shifts, not 64-bit multiplies).
 //
 // Per team the only dependent-load chain left per block of G nonzeros is the
 // factor-row gather: leaf indices and values for the next block are loaded
@@ -101,35 +105,54 @@ __device__ __forceinline__ uint32_t find_fiber(const uint32_t* __restrict__ fptr
 // needs when it closes is requested as soon as the fiber opens.
 template <int ND, int OUT, int G, int V, class T>
 __global__ void __launch_bounds__(256) k_mttkrp(const Args<T> a) {
+  constexpr uint32_t R = 4 * G * V;
+  constexpr int LEAF = ND - 1;
+  constexpr uint32_t FLAG = 0x80000000u;
+  constexpr int PF = G > 8 ? 8 : G;  // row gathers in flight per lane per batch
   const int lane = threadIdx.x & 31;
   const int tl = lane & (G - 1);
   const int tb = lane - tl;
   const unsigned tmask = (G == 32) ? FULL : (((1u << G) - 1u) << tb);
+  // kernel parameters in registers
+  const float* __restrict__ vals = a.vals;
+  const uint32_t* __restrict__ leaf = a.leaf;
+  const uint32_t* __restrict__ fidx = a.fidx;
+  const uint32_t* __restrict__ fpar = a.fpar;
+  const uint32_t* __restrict__ sidx1 = a.sidx1;
+  const uint32_t* __restrict__ like = a.like;
+  const uint32_t nfib = a.nfib, chunk = a.chunk;
+  const T* __restrict__ U0 = a.U[0];
+  const T* __restrict__ U1 = a.U[1];
+  const T* __restrict__ U2 = a.U[2];
+  const T* __restrict__ UL = a.U[LEAF];
+  float* __restrict__ out = a.out;
+  const uint32_t c0 = (uint32_t)tl * 4;  // this lane's first column
+  auto ld = [&](const T* U, uint32_t row, int v) -> float4 {
+    return Row<T>::load(U + (uint64_t)row * R, c0 + (uint32_t)(v * G * 4));
+  };
+  auto rd = [&](uint32_t row, int v, float4 x) { red4(out + (uint64_t)row * R + c0 + v * G * 4, x); };
+
   const uint64_t team = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) / G;
   // Teams past the end stay in the loop (empty range) so every full-warp
   // shuffle sees all lanes; all teams run the same number of iterations.
-  const bool active = team * a.chunk < a.nnz;
-  const uint64_t x0 = active ? team * a.chunk : a.nnz - 1;
-  const uint64_t x1 = active ? min(x0 + a.chunk, a.nnz) : x0;
-  const uint32_t R = a.R;
-  constexpr int LEAF = ND - 1;
-  constexpr uint32_t FLAG = 0x80000000u;
-  auto col = [&](int v) -> uint64_t { return (uint64_t)(tl + v * G) * 4; };
+  const bool active = team * chunk < a.nnz;
+  const uint64_t x0 = active ? team * chunk : a.nnz - 1;
+  const uint64_t x1 = active ? min(x0 + chunk, a.nnz) : x0;
 
-  uint32_t f = find_fiber(a.fptr, a.nfib, x0);
+  uint32_t f = find_fiber(a.fptr, nfib, x0);
   // fiber metadata window: lane i holds fiber fw + i
   uint32_t fw = f;
   uint32_t wi, wp;  // 3-D: (b index, a index); 4-D: (c index, fbrS id)
   auto refill = [&]() {
-    const uint32_t q = min(fw + (uint32_t)tl, a.nfib);
-    wi = __ldg(a.fidx + q);
-    wp = (ND == 3) ? __ldg(a.like + q) : __ldg(a.fpar + q);
+    const uint32_t q = min(fw + (uint32_t)tl, nfib);
+    wi = __ldg(fidx + q);
+    wp = (ND == 3) ? __ldg(like + q) : __ldg(fpar + q);
   };
   refill();
   uint32_t ci = __shfl_sync(tmask, wi, tb);  // current fiber's index (b in 3-D, c in 4-D)
   uint32_t cp = __shfl_sync(tmask, wp, tb);  // current fiber's a (3-D) or fbrS (4-D)
   uint32_t sb = 0, sa = 0;                   // 4-D: current fbrS's b and a
-  if (ND == 4) { sb = __ldg(a.sidx1 + cp); sa = __ldg(a.like + cp); }
+  if (ND == 4) { sb = __ldg(sidx1 + cp); sa = __ldg(like + cp); }
 
   float4 acc[V], acc1[V], acc2[V], crow[V], srow[V];
 #pragma unroll
@@ -139,39 +162,24 @@ __global__ void __launch_bounds__(256) k_mttkrp(const Args<T> a) {
   // rows needed per fbrS (4-D) and per fiber, requested when they open
   auto open_fbrs = [&]() {
     if constexpr (ND == 4) {
-      if constexpr (OUT == 0) {
 #pragma unroll
-        for (int v = 0; v < V; ++v) srow[v] = Row<T>::load(a.U[1], (uint64_t)sb * R + col(v));
-      } else if constexpr (OUT == 1) {
-#pragma unroll
-        for (int v = 0; v < V; ++v) srow[v] = Row<T>::load(a.U[0], (uint64_t)sa * R + col(v));
-      } else {
-#pragma unroll
-        for (int v = 0; v < V; ++v)
-          srow[v] = Row<T>::load(a.U[0], (uint64_t)sa * R + col(v)) * Row<T>::load(a.U[1], (uint64_t)sb * R + col(v));
+      for (int v = 0; v < V; ++v) {
+        if constexpr (OUT == 0) srow[v] = ld(U1, sb, v);
+        else if constexpr (OUT == 1) srow[v] = ld(U0, sa, v);
+        else srow[v] = ld(U0, sa, v) * ld(U1, sb, v);
       }
     }
   };
   auto open_fiber = [&]() {
-    if constexpr (ND == 3) {
-      if constexpr (OUT == 0) {
 #pragma unroll
-        for (int v = 0; v < V; ++v) crow[v] = Row<T>::load(a.U[1], (uint64_t)ci * R + col(v));
-      } else if constexpr (OUT == 1) {
-#pragma unroll
-        for (int v = 0; v < V; ++v) crow[v] = Row<T>::load(a.U[0], (uint64_t)cp * R + col(v));
+    for (int v = 0; v < V; ++v) {
+      if constexpr (ND == 3) {
+        if constexpr (OUT == 0) crow[v] = ld(U1, ci, v);
+        else if constexpr (OUT == 1) crow[v] = ld(U0, cp, v);
+        else crow[v] = ld(U0, cp, v) * ld(U1, ci, v);
       } else {
-#pragma unroll
-        for (int v = 0; v < V; ++v)
-          crow[v] = Row<T>::load(a.U[0], (uint64_t)cp * R + col(v)) * Row<T>::load(a.U[1], (uint64_t)ci * R + col(v));
-      }
-    } else {
-      if constexpr (OUT == 3) {
-#pragma unroll
-        for (int v = 0; v < V; ++v) crow[v] = srow[v] * Row<T>::load(a.U[2], (uint64_t)ci * R + col(v));
-      } else if constexpr (OUT != 2) {
-#pragma unroll
-        for (int v = 0; v < V; ++v) crow[v] = Row<T>::load(a.U[2], (uint64_t)ci * R + col(v));
+        if constexpr (OUT == 3) crow[v] = srow[v] * ld(U2, ci, v);
+        else if constexpr (OUT != 2) crow[v] = ld(U2, ci, v);
       }
     }
   };
@@ -180,51 +188,57 @@ __global__ void __launch_bounds__(256) k_mttkrp(const Args<T> a) {
 
   // Fold the open fiber's partial (acc) into the level above / the output.
   auto close_fiber = [&]() {
-    if constexpr (OUT == LEAF) {
-      return;
-    } else if constexpr (ND == 3) {
-      if constexpr (OUT == 1) {
+    if constexpr (OUT != LEAF) {
 #pragma unroll
-        for (int v = 0; v < V; ++v) red4(a.out + (uint64_t)ci * R + col(v), crow[v] * acc[v]);
-      } else {
-#pragma unroll
-        for (int v = 0; v < V; ++v) acc1[v] = acc1[v] + crow[v] * acc[v];
-      }
-    } else {
-      if constexpr (OUT == 2) {
-#pragma unroll
-        for (int v = 0; v < V; ++v) red4(a.out + (uint64_t)ci * R + col(v), srow[v] * acc[v]);
-      } else {
-#pragma unroll
-        for (int v = 0; v < V; ++v) acc1[v] = acc1[v] + crow[v] * acc[v];
+      for (int v = 0; v < V; ++v) {
+        if constexpr (ND == 3 && OUT == 1) rd(ci, v, crow[v] * acc[v]);
+        else if constexpr (ND == 4 && OUT == 2) rd(ci, v, srow[v] * acc[v]);
+        else acc1[v] = fma4v(crow[v], acc[v], acc1[v]);
       }
     }
   };
   // 4-D: fold the open fbrS (acc1) upward (OUT 0) or out (OUT 1).
   auto close_fbrs = [&]() {
-    if constexpr (ND == 4 && OUT == 1) {
 #pragma unroll
-      for (int v = 0; v < V; ++v) { red4(a.out + (uint64_t)sb * R + col(v), srow[v] * acc1[v]); acc1[v] = f4(0.f); }
-    } else if constexpr (ND == 4 && OUT == 0) {
-#pragma unroll
-      for (int v = 0; v < V; ++v) { acc2[v] = acc2[v] + srow[v] * acc1[v]; acc1[v] = f4(0.f); }
+    for (int v = 0; v < V; ++v) {
+      if constexpr (ND == 4 && OUT == 1) { rd(sb, v, srow[v] * acc1[v]); acc1[v] = f4(0.f); }
+      else if constexpr (ND == 4 && OUT == 0) { acc2[v] = fma4v(srow[v], acc1[v], acc2[v]); acc1[v] = f4(0.f); }
     }
   };
   auto flush_slice = [&]() {
-    if constexpr (OUT == 0 && ND == 3) {
 #pragma unroll
-      for (int v = 0; v < V; ++v) { red4(a.out + (uint64_t)cur_a * R + col(v), acc1[v]); acc1[v] = f4(0.f); }
-    } else if constexpr (OUT == 0) {
-#pragma unroll
-      for (int v = 0; v < V; ++v) { red4(a.out + (uint64_t)cur_a * R + col(v), acc2[v]); acc2[v] = f4(0.f); }
+    for (int v = 0; v < V; ++v) {
+      if constexpr (OUT == 0 && ND == 3) { rd(cur_a, v, acc1[v]); acc1[v] = f4(0.f); }
+      else if constexpr (OUT == 0) { rd(cur_a, v, acc2[v]); acc2[v] = f4(0.f); }
     }
   };
+  // nonzero x opens fiber f+1 (team-uniform branch)
+  auto advance = [&]() {
+    close_fiber();
+    ++f;
+    if (f - fw >= (uint32_t)G) { fw = f; refill(); }
+    ci = __shfl_sync(tmask, wi, tb + (int)(f - fw));
+    const uint32_t np = __shfl_sync(tmask, wp, tb + (int)(f - fw));
+    if constexpr (ND == 3) {
+      if (OUT == 0 && np != cur_a) { flush_slice(); cur_a = np; }
+      cp = np;
+    } else {
+      if (np != cp) {  // new fbrS
+        close_fbrs();
+        cp = np;
+        sb = __ldg(sidx1 + cp);
+        sa = __ldg(like + cp);
+        if (OUT == 0 && sa != cur_a) { flush_slice(); cur_a = sa; }
+        open_fbrs();
+      }
+    }
+    open_fiber();
+  };
 
-  constexpr int PF = G > 8 ? 8 : G;  // row gathers in flight per lane per batch
   uint32_t nk = 0;
   float nv = 0.f;
-  if (x0 + tl < x1) { nk = __ldg(a.leaf + x0 + tl); nv = __ldg(a.vals + x0 + tl); }
-  for (uint32_t it = 0; it < a.chunk; it += G) {
+  if (x0 + tl < x1) { nk = __ldg(leaf + x0 + tl); nv = __ldg(vals + x0 + tl); }
+  for (uint32_t it = 0; it < chunk; it += G) {
     const uint64_t xb = x0 + it;
     const uint32_t kv = nk;
     const float vv = nv;
@@ -232,10 +246,11 @@ __global__ void __launch_bounds__(256) k_mttkrp(const Args<T> a) {
       const uint64_t xn = xb + G + tl;
       nk = 0;
       nv = 0.f;
-      if (it + G < a.chunk && xn < x1) { nk = __ldg(a.leaf + xn); nv = __ldg(a.vals + xn); }
+      if (it + G < chunk && xn < x1) { nk = __ldg(leaf + xn); nv = __ldg(vals + xn); }
     }
-    const bool fl = (xb + tl < x1) && (kv & FLAG) && (xb + tl != x0);
-    const uint32_t fm = (__ballot_sync(FULL, fl) >> tb) & ((G == 32) ? FULL : ((1u << G) - 1u));
+    // a lane past the range holds val 0 and no flag, and gathers row 0
+    const bool fl = (kv & FLAG) && (xb + tl != x0);
+    const uint32_t fm = (__ballot_sync(FULL, fl) >> tb);
     const uint32_t k = kv & ~FLAG;
 #pragma unroll
     for (int jb = 0; jb < G; jb += PF) {
@@ -246,43 +261,24 @@ __global__ void __launch_bounds__(256) k_mttkrp(const Args<T> a) {
         kj[j] = __shfl_sync(FULL, k, tb + jb + j);
         if constexpr (OUT != LEAF) {
 #pragma unroll
-          for (int v = 0; v < V; ++v) rows[j][v] = Row<T>::load(a.U[LEAF], (uint64_t)kj[j] * R + col(v));
+          for (int v = 0; v < V; ++v) rows[j][v] = ld(UL, kj[j], v);
         }
       }
 #pragma unroll
       for (int j = 0; j < PF; ++j) {
         const float val = __shfl_sync(FULL, vv, tb + jb + j);
-        const uint64_t x = xb + jb + j;
-        if (x < x1) {
-          if ((fm >> (jb + j)) & 1u) {  // nonzero x opens fiber f+1 (team-uniform branch)
-            close_fiber();
-            ++f;
-            if (f - fw >= (uint32_t)G) { fw = f; refill(); }
-            ci = __shfl_sync(tmask, wi, tb + (int)(f - fw));
-            const uint32_t np = __shfl_sync(tmask, wp, tb + (int)(f - fw));
-            if constexpr (ND == 3) {
-              if (OUT == 0 && np != cur_a) { flush_slice(); cur_a = np; }
-              cp = np;
-            } else {
-              if (np != cp) {  // new fbrS
-                close_fbrs();
-                cp = np;
-                sb = __ldg(a.sidx1 + cp);
-                sa = __ldg(a.like + cp);
-                if (OUT == 0 && sa != cur_a) { flush_slice(); cur_a = sa; }
-                open_fbrs();
-              }
-            }
-            open_fiber();
+        if ((fm >> (jb + j)) & 1u) {
+          advance();
 #pragma unroll
-            for (int v = 0; v < V; ++v) acc[v] = f4(0.f);
-          }
-          if constexpr (OUT != LEAF) {
+          for (int v = 0; v < V; ++v) acc[v] = f4(0.f);
+        }
+        if constexpr (OUT != LEAF) {
 #pragma unroll
-            for (int v = 0; v < V; ++v) acc[v] = fma4(val, rows[j][v], acc[v]);
-          } else {
+          for (int v = 0; v < V; ++v) acc[v] = fma4(val, rows[j][v], acc[v]);
+        } else {
+          if (xb + jb + j < x1) {
 #pragma unroll
-            for (int v = 0; v < V; ++v) red4(a.out + (uint64_t)kj[j] * R + col(v), f4(val) * crow[v]);
+            for (int v = 0; v < V; ++v) rd(kj[j], v, f4(val) * crow[v]);
           }
         }
       }
@@ -295,242 +291,12 @@ __global__ void __launch_bounds__(256) k_mttkrp(const Args<T> a) {
   }
 }
 
-// Batched-close variant for the slice / fbrS / fiber levels (OUT < ND-1).
-// The nonzero loop is branch-light: when a nonzero opens a new fiber the
-// open fiber's partial row is parked in a shared-memory slot. After the block,
-// the team closes its parked fibers in a slot loop that runs in lockstep with
-// the warp's other teams (predicated, so the four teams of a warp share one
-// pass), with every close row requested before the block's nonzeros are
-// consumed. The fiber metadata window holds 2G fibers.
-template <int ND, int OUT, int G, int V, class T>
-__global__ void __launch_bounds__(256) k_mttkrp_b(const Args<T> a) {
-  static_assert(OUT < ND - 1, "leaf level uses k_mttkrp");
-  extern __shared__ float4 smem[];
-  const int lane = threadIdx.x & 31;
-  const int tl = lane & (G - 1);
-  const int tb = lane - tl;
-  const uint64_t team = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) / G;
-  const bool active = team * a.chunk < a.nnz;
-  const uint64_t x0 = active ? team * a.chunk : a.nnz - 1;
-  const uint64_t x1 = active ? min(x0 + a.chunk, a.nnz) : x0;
-  const uint32_t R = a.R;
-  constexpr int LEAF = ND - 1;
-  constexpr uint32_t FLAG = 0x80000000u;
-  constexpr uint32_t TEAMBITS = (G == 32) ? FULL : ((1u << G) - 1u);
-  auto col = [&](int v) -> uint64_t { return (uint64_t)(tl + v * G) * 4; };
-  constexpr int PF = G > 8 ? 8 : G;  // nonzeros per batch; fibers parked per batch
-  float4* slots = smem + (size_t)(threadIdx.x >> 5) * (PF * 32 * V);
-  auto slot = [&](int sidx, int v) -> float4& { return slots[(sidx * 32 + lane) * V + v]; };
-
-  uint32_t f = find_fiber(a.fptr, a.nfib, x0);
-  uint32_t fw = f, w0i, w0p, w1i, w1p;  // window: fibers fw + tl and fw + G + tl
-  auto refill = [&]() {
-    const uint32_t q0 = min(fw + (uint32_t)tl, a.nfib), q1 = min(fw + (uint32_t)(G + tl), a.nfib);
-    w0i = __ldg(a.fidx + q0);
-    w1i = __ldg(a.fidx + q1);
-    w0p = (ND == 3) ? __ldg(a.like + q0) : __ldg(a.fpar + q0);
-    w1p = (ND == 3) ? __ldg(a.like + q1) : __ldg(a.fpar + q1);
-  };
-  refill();
-  // metadata of fiber fw + d (d < 2G) for the calling team; warp-wide shuffles
-  auto meta_i = [&](uint32_t d) -> uint32_t {
-    const uint32_t u = __shfl_sync(FULL, w0i, tb + (int)(d & (G - 1)));
-    const uint32_t w = __shfl_sync(FULL, w1i, tb + (int)(d & (G - 1)));
-    return d < (uint32_t)G ? u : w;
-  };
-  auto meta_p = [&](uint32_t d) -> uint32_t {
-    const uint32_t u = __shfl_sync(FULL, w0p, tb + (int)(d & (G - 1)));
-    const uint32_t w = __shfl_sync(FULL, w1p, tb + (int)(d & (G - 1)));
-    return d < (uint32_t)G ? u : w;
-  };
-
-  float4 acc[V], acc1[V], acc2[V], srow[V];
-#pragma unroll
-  for (int v = 0; v < V; ++v) acc[v] = acc1[v] = acc2[v] = srow[v] = f4(0.f);
-  // 4-D: the open fbrS (id cp, indices sb/sa) and the row it contributes
-  uint32_t cp = meta_p(0), sb = 0, sa = 0;
-  auto open_fbrs = [&]() {
-    if constexpr (ND == 4) {
-      sb = __ldg(a.sidx1 + cp);
-      sa = __ldg(a.like + cp);
-      if constexpr (OUT == 0) {
-#pragma unroll
-        for (int v = 0; v < V; ++v) srow[v] = Row<T>::load(a.U[1], (uint64_t)sb * R + col(v));
-      } else if constexpr (OUT == 1) {
-#pragma unroll
-        for (int v = 0; v < V; ++v) srow[v] = Row<T>::load(a.U[0], (uint64_t)sa * R + col(v));
-      } else {
-#pragma unroll
-        for (int v = 0; v < V; ++v)
-          srow[v] = Row<T>::load(a.U[0], (uint64_t)sa * R + col(v)) * Row<T>::load(a.U[1], (uint64_t)sb * R + col(v));
-      }
-    }
-  };
-  open_fbrs();
-  uint32_t cur_a = (ND == 3) ? cp : sa;  // slice of the open slice accumulation (OUT == 0)
-  auto flush_slice = [&]() {
-    if constexpr (OUT == 0 && ND == 3) {
-#pragma unroll
-      for (int v = 0; v < V; ++v) { red4(a.out + (uint64_t)cur_a * R + col(v), acc1[v]); acc1[v] = f4(0.f); }
-    } else if constexpr (OUT == 0) {
-#pragma unroll
-      for (int v = 0; v < V; ++v) { red4(a.out + (uint64_t)cur_a * R + col(v), acc2[v]); acc2[v] = f4(0.f); }
-    }
-  };
-  // 4-D: fbrS changes to np before closing a fiber of np
-  auto fbrs_transition = [&](uint32_t np) {
-    if constexpr (ND == 4) {
-      if (np != cp) {
-        if constexpr (OUT == 1) {
-#pragma unroll
-          for (int v = 0; v < V; ++v) { red4(a.out + (uint64_t)sb * R + col(v), srow[v] * acc1[v]); acc1[v] = f4(0.f); }
-        } else if constexpr (OUT == 0) {
-#pragma unroll
-          for (int v = 0; v < V; ++v) { acc2[v] = acc2[v] + srow[v] * acc1[v]; acc1[v] = f4(0.f); }
-        }
-        cp = np;
-        open_fbrs();
-        if (OUT == 0 && sa != cur_a) { flush_slice(); cur_a = sa; }
-      }
-    }
-  };
-  // row a closing fiber (index ci, parent cp_) multiplies its partial by
-  auto close_row = [&](uint32_t ci, uint32_t cpp, int v) -> float4 {
-    if constexpr (ND == 3) {
-      return OUT == 0 ? Row<T>::load(a.U[1], (uint64_t)ci * R + col(v)) : Row<T>::load(a.U[0], (uint64_t)cpp * R + col(v));
-    } else {
-      (void)cpp;
-      return Row<T>::load(a.U[2], (uint64_t)ci * R + col(v));
-    }
-  };
-  // fold one closed fiber (partial p, close row c, index ci) into acc1/out
-  auto fold = [&](uint32_t ci, const float4* p, const float4* c) {
-    if constexpr (ND == 3 && OUT == 1) {
-#pragma unroll
-      for (int v = 0; v < V; ++v) red4(a.out + (uint64_t)ci * R + col(v), c[v] * p[v]);
-    } else if constexpr (ND == 4 && OUT == 2) {
-#pragma unroll
-      for (int v = 0; v < V; ++v) red4(a.out + (uint64_t)ci * R + col(v), srow[v] * p[v]);
-    } else {
-#pragma unroll
-      for (int v = 0; v < V; ++v) acc1[v] = acc1[v] + c[v] * p[v];
-    }
-  };
-
-  uint32_t nk = 0;
-  float nv = 0.f;
-  if (x0 + tl < x1) { nk = __ldg(a.leaf + x0 + tl); nv = __ldg(a.vals + x0 + tl); }
-  for (uint32_t it = 0; it < a.chunk; it += G) {
-    const uint64_t xb = x0 + it;
-    const uint32_t kv = nk;
-    const float vv = nv;
-    {
-      const uint64_t xn = xb + G + tl;
-      nk = 0;
-      nv = 0.f;
-      if (it + G < a.chunk && xn < x1) { nk = __ldg(a.leaf + xn); nv = __ldg(a.vals + xn); }
-    }
-    const bool fl = (xb + tl < x1) && (kv & FLAG) && (xb + tl != x0);
-    const uint32_t fmall = (__ballot_sync(FULL, fl) >> tb) & TEAMBITS;
-    const uint32_t k = kv & ~FLAG;
-    // batches of PF nonzeros: at most PF fibers close per batch
-#pragma unroll
-    for (int jb = 0; jb < G; jb += PF) {
-      const uint32_t fm = (fmall >> jb) & ((1u << PF) - 1u);
-      const int nc = __popc(fm);  // fibers closing in this batch: f .. f+nc-1
-      if (f - fw >= (uint32_t)G) { fw = f; refill(); }
-      const uint32_t d0 = f - fw;
-      // close rows for the batch's closing fibers, requested up front
-      float4 crow[PF][V];
-      uint32_t cidx[PF];
-#pragma unroll
-      for (int sI = 0; sI < PF; ++sI) {
-        cidx[sI] = meta_i(d0 + sI);
-        const uint32_t cpp = (ND == 3 && OUT == 1) ? meta_p(d0 + sI) : 0u;
-#pragma unroll
-        for (int v = 0; v < V; ++v)
-          crow[sI][v] = (sI < nc && !(ND == 4 && OUT == 2)) ? close_row(cidx[sI], cpp, v) : f4(0.f);
-      }
-      float4 rows[PF][V];
-#pragma unroll
-      for (int j = 0; j < PF; ++j) {
-        const uint32_t kj = __shfl_sync(FULL, k, tb + jb + j);
-#pragma unroll
-        for (int v = 0; v < V; ++v) rows[j][v] = Row<T>::load(a.U[LEAF], (uint64_t)kj * R + col(v));
-      }
-      // nonzeros: accumulate; a flagged nonzero parks the open partial first
-      int sc = 0;
-#pragma unroll
-      for (int j = 0; j < PF; ++j) {
-        const float val = __shfl_sync(FULL, vv, tb + jb + j);
-        if ((fm >> j) & 1u) {
-#pragma unroll
-          for (int v = 0; v < V; ++v) { slot(sc, v) = acc[v]; acc[v] = f4(0.f); }
-          ++sc;
-        }
-#pragma unroll
-        for (int v = 0; v < V; ++v) acc[v] = fma4(val, rows[j][v], acc[v]);
-      }
-      // close the parked fibers in lockstep across the warp's teams
-      const int maxc = (int)__reduce_max_sync(FULL, (unsigned)nc);
-      uint32_t pnext = meta_p(d0);
-#pragma unroll
-      for (int sI = 0; sI < PF; ++sI) {
-        if (sI >= maxc) break;
-        const bool act = sI < nc;
-        const uint32_t pc = pnext;
-        pnext = meta_p(d0 + sI + 1);
-        if (act) {
-          float4 part[V];
-#pragma unroll
-          for (int v = 0; v < V; ++v) part[v] = slot(sI, v);
-          if constexpr (ND == 4) fbrs_transition(pc);
-          fold(cidx[sI], part, crow[sI]);
-          if constexpr (ND == 3 && OUT == 0) {
-            if (pnext != pc) { flush_slice(); cur_a = pnext; }
-          }
-        }
-      }
-      f += nc;
-    }
-  }
-  // close the open fiber (partial over this team's range); the metadata
-  // shuffles run on every lane before the branch
-  const uint32_t dl = f - fw;
-  const uint32_t ci = meta_i(dl), pc = meta_p(dl);
-  if (active) {
-    if constexpr (ND == 4) fbrs_transition(pc);
-    float4 c[V];
-#pragma unroll
-    for (int v = 0; v < V; ++v) c[v] = (ND == 4 && OUT == 2) ? f4(0.f) : close_row(ci, pc, v);
-    fold(ci, acc, c);
-    if constexpr (ND == 4 && OUT == 1) {
-#pragma unroll
-      for (int v = 0; v < V; ++v) red4(a.out + (uint64_t)sb * R + col(v), srow[v] * acc1[v]);
-    } else if constexpr (ND == 4 && OUT == 0) {
-#pragma unroll
-      for (int v = 0; v < V; ++v) acc2[v] = acc2[v] + srow[v] * acc1[v];
-    }
-    flush_slice();
-  }
-}
-
 template <int ND, int OUT, int G, int V, class T>
 cudaError_t launch_one(const Args<T>& a, int threads, cudaStream_t s) {
   const uint64_t teams = (a.nnz + a.chunk - 1) / a.chunk;
   const uint64_t thr = teams * G;
   const uint64_t blocks = (thr + threads - 1) / threads;
-  if constexpr (OUT < ND - 1) {
-    const size_t smem = (size_t)(threads / 32) * (G > 8 ? 8 : G) * 32 * V * sizeof(float4);
-    if (smem > 48 * 1024) {
-      cudaError_t e = cudaFuncSetAttribute(k_mttkrp_b<ND, OUT, G, V, T>,
-                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      if (e != cudaSuccess) return e;
-    }
-    k_mttkrp_b<ND, OUT, G, V, T><<<(unsigned)blocks, threads, smem, s>>>(a);
-  } else {
-    k_mttkrp<ND, OUT, G, V, T><<<(unsigned)blocks, threads, 0, s>>>(a);
-  }
+  k_mttkrp<ND, OUT, G, V, T><<<(unsigned)blocks, threads, 0, s>>>(a);
   return cudaGetLastError();
 }
 

@@ -165,7 +165,8 @@ typedef struct {
   int chunk;         /* nonzeros per worker team; 0 = auto (the tuned plan, else 512) */
   int block_threads; /* threads per CTA; 0 = auto (256) */
   int traversal;     /* 0 auto (tuned plan, else a view when one exists), 1 MM-CSF partitions, 2 view */
-  int reserved[5];
+  int min_blocks;    /* register budget: 0 auto, 3 (~80 registers) or 4 (64 registers, 32 warps/SM) */
+  int reserved[4];
 } mmcsf_kernel_cfg;
 
 /* One mode. factor_dtype: MMCSF_DTYPE_F32 (d_factors are float*) or
@@ -192,6 +193,7 @@ int mmcsf_mttkrp_all_host(mmcsf_format* F, int R, const float* const* h_factors,
 typedef struct {
   int traversal[4]; /* 1 MM-CSF partitions, 2 view */
   int chunk[4];
+  int min_blocks[4];
   float ms[4];      /* best time per mode */
 } mmcsf_plan;
 int mmcsf_tune(mmcsf_format* F, int R, int factor_dtype, const void* const* d_factors, float* const* d_outs,

@@ -66,9 +66,21 @@ struct mmcsf_format {
   mmcsf::CsfPart views[4];  // views[m]: a CSF with mode m at level 0 (order_modes(m))
   int plan_traversal[4] = {0, 0, 0, 0};  // tuned: 1 partitions, 2 view (0 = untuned)
   int plan_chunk[4] = {0, 0, 0, 0};
+  int plan_mb[4] = {0, 0, 0, 0};
   mmcsf::HybExtra hyb;
   int last_launches = 0;
   // staging for the host-buffer MTTKRP entry point
   mmcsf::DevBuf stage_in[4], stage_out[4];
   int stage_R = 0;
+  cudaStream_t copy_in = nullptr, copy_out = nullptr;
+  cudaEvent_t ev_in[4] = {}, ev_done[4] = {}, ev_start = nullptr;
+  ~mmcsf_format() {
+    if (copy_in) cudaStreamDestroy(copy_in);
+    if (copy_out) cudaStreamDestroy(copy_out);
+    for (int m = 0; m < 4; ++m) {
+      if (ev_in[m]) cudaEventDestroy(ev_in[m]);
+      if (ev_done[m]) cudaEventDestroy(ev_done[m]);
+    }
+    if (ev_start) cudaEventDestroy(ev_start);
+  }
 };

@@ -54,16 +54,17 @@ __device__ __forceinline__ float4 f4(float a) { return make_float4(a, a, a, a); 
 __device__ __forceinline__ float4 operator*(float4 a, float4 b) {
   return make_float4(a.x * b.x, a.y * b.y, a.z * b.z, a.w * b.w);
 }
-__device__ __forceinline__ float4 operator+(float4 a, float4 b) {
-  return make_float4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w);
-}
 __device__ __forceinline__ float4 fma4(float s, float4 a, float4 c) {
   return make_float4(fmaf(s, a.x, c.x), fmaf(s, a.y, c.y), fmaf(s, a.z, c.z), fmaf(s, a.w, c.w));
 }
 __device__ __forceinline__ float4 fma4v(float4 a, float4 b, float4 c) {
   return make_float4(fmaf(a.x, b.x, c.x), fmaf(a.y, b.y, c.y), fmaf(a.z, b.z, c.z), fmaf(a.w, b.w, c.w));
 }
-__device__ __forceinline__ void red4(float* p, float4 v) { atomicAdd(reinterpret_cast<float4*>(p), v); }
+// One vector reduction (PTX ISA 8.1+, sm_90+): four floats added at p (16 B aligned).
+__device__ __forceinline__ void red4(float* p, float4 v) {
+  asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(p), "f"(v.x), "f"(v.y), "f"(v.z), "f"(v.w)
+               : "memory");
+}
 
 template <class T>
 struct Args {
@@ -103,8 +104,10 @@ __device__ __forceinline__ uint32_t find_fiber(const uint32_t* __restrict__ fptr
 // fibers' metadata (index, slice map) sits in a G-wide register window
 // refilled with one coalesced load every G fibers; and the factor row a fiber
 // needs when it closes is requested as soon as the fiber opens.
-template <int ND, int OUT, int G, int V, class T>
-__global__ void __launch_bounds__(256) k_mttkrp(const Args<T> a) {
+// MB: minimum resident 256-thread CTAs per SM the register allocation must
+// allow (3: ~80 registers; 4: 64 registers, 32 warps per SM); the tuner picks.
+template <int ND, int OUT, int G, int V, class T, int MB>
+__global__ void __launch_bounds__(256, MB) k_mttkrp(const Args<T> a) {
   constexpr uint32_t R = 4 * G * V;
   constexpr int LEAF = ND - 1;
   constexpr uint32_t FLAG = 0x80000000u;
@@ -292,32 +295,33 @@ __global__ void __launch_bounds__(256) k_mttkrp(const Args<T> a) {
 }
 
 template <int ND, int OUT, int G, int V, class T>
-cudaError_t launch_one(const Args<T>& a, int threads, cudaStream_t s) {
+cudaError_t launch_one(const Args<T>& a, int threads, int mb, cudaStream_t s) {
   const uint64_t teams = (a.nnz + a.chunk - 1) / a.chunk;
   const uint64_t thr = teams * G;
   const uint64_t blocks = (thr + threads - 1) / threads;
-  k_mttkrp<ND, OUT, G, V, T><<<(unsigned)blocks, threads, 0, s>>>(a);
+  if (mb >= 4) k_mttkrp<ND, OUT, G, V, T, 4><<<(unsigned)blocks, threads, 0, s>>>(a);
+  else k_mttkrp<ND, OUT, G, V, T, 3><<<(unsigned)blocks, threads, 0, s>>>(a);
   return cudaGetLastError();
 }
 
 template <int ND, int G, int V, class T>
-cudaError_t launch_lvl(const Args<T>& a, int lvl, int threads, cudaStream_t s) {
+cudaError_t launch_lvl(const Args<T>& a, int lvl, int threads, int mb, cudaStream_t s) {
   switch (lvl) {
-    case 0: return launch_one<ND, 0, G, V, T>(a, threads, s);
-    case 1: return launch_one<ND, 1, G, V, T>(a, threads, s);
-    case 2: return launch_one<ND, 2, G, V, T>(a, threads, s);
+    case 0: return launch_one<ND, 0, G, V, T>(a, threads, mb, s);
+    case 1: return launch_one<ND, 1, G, V, T>(a, threads, mb, s);
+    case 2: return launch_one<ND, 2, G, V, T>(a, threads, mb, s);
     default:
-      if constexpr (ND == 4) return launch_one<ND, 3, G, V, T>(a, threads, s);
+      if constexpr (ND == 4) return launch_one<ND, 3, G, V, T>(a, threads, mb, s);
       return cudaErrorInvalidValue;
   }
 }
 
 template <class T>
-cudaError_t launch_R(const Args<T>& a, int nd, int lvl, int threads, cudaStream_t s) {
+cudaError_t launch_R(const Args<T>& a, int nd, int lvl, int threads, int mb, cudaStream_t s) {
 #define MMCSF_RCASE(RR, GG, VV)                                                        \
   case RR:                                                                            \
-    return nd == 3 ? launch_lvl<3, GG, VV, T>(a, lvl, threads, s)                     \
-                   : launch_lvl<4, GG, VV, T>(a, lvl, threads, s);
+    return nd == 3 ? launch_lvl<3, GG, VV, T>(a, lvl, threads, mb, s)                 \
+                   : launch_lvl<4, GG, VV, T>(a, lvl, threads, mb, s);
   switch (a.R) {
     MMCSF_RCASE(4, 1, 1)
     MMCSF_RCASE(8, 2, 1)
@@ -368,7 +372,8 @@ int part_mttkrp(const mmcsf_format* F, const CsfPart& P, int mode, int R, int dt
   if (lvl < 0) return set_error(MMCSF_ERR_INVALID, "mode %d not in part", mode);
   int chunk = cfg && cfg->chunk > 0 ? cfg->chunk : default_chunk(R);
   int threads = cfg && cfg->block_threads > 0 ? cfg->block_threads : 256;
-  if (threads % 32 || threads > 1024) return set_error(MMCSF_ERR_INVALID, "block_threads must be a multiple of 32");
+  const int mb = cfg && cfg->min_blocks > 0 ? cfg->min_blocks : 3;
+  if (threads % 32 || threads > 256) return set_error(MMCSF_ERR_INVALID, "block_threads must be a multiple of 32, <= 256");
   cudaError_t e;
   if (dtype == MMCSF_DTYPE_F32) {
     Args<float> a{};
@@ -386,7 +391,7 @@ int part_mttkrp(const mmcsf_format* F, const CsfPart& P, int mode, int R, int dt
     a.R = (uint32_t)R;
     for (int l = 0; l < P.nd; ++l) a.U[l] = static_cast<const float*>(U[P.order[l]]);
     a.out = out;
-    e = launch_R<float>(a, P.nd, lvl, threads, s);
+    e = launch_R<float>(a, P.nd, lvl, threads, mb, s);
   } else {
     Args<__nv_bfloat16> a{};
     a.vals = P.vals.as<float>();
@@ -403,7 +408,7 @@ int part_mttkrp(const mmcsf_format* F, const CsfPart& P, int mode, int R, int dt
     a.R = (uint32_t)R;
     for (int l = 0; l < P.nd; ++l) a.U[l] = static_cast<const __nv_bfloat16*>(U[P.order[l]]);
     a.out = out;
-    e = launch_R<__nv_bfloat16>(a, P.nd, lvl, threads, s);
+    e = launch_R<__nv_bfloat16>(a, P.nd, lvl, threads, mb, s);
   }
   if (e != cudaSuccess) return set_error(MMCSF_ERR_CUDA, "MTTKRP launch failed: %s", cudaGetErrorString(e));
   if (launches) ++*launches;
@@ -422,6 +427,7 @@ int mttkrp_mode(const mmcsf_format* F, int mode, int R, int dtype, const void* c
   mmcsf_kernel_cfg c{};
   if (cfg) c = *cfg;
   if (c.chunk == 0) c.chunk = F->plan_chunk[mode];
+  if (c.min_blocks == 0) c.min_blocks = F->plan_mb[mode];
   if (trav == 2) {
     if (!F->views[mode].present) return set_error(MMCSF_ERR_INVALID, "no view for mode %d (build with views)", mode);
     return part_mttkrp(F, F->views[mode], mode, R, dtype, U, out, &c, s, launches);
@@ -504,29 +510,69 @@ extern "C" int mmcsf_mttkrp_all(const mmcsf_format* F, int R, int factor_dtype, 
   return MMCSF_OK;
 }
 
+// Host-buffer all-mode MTTKRP with the copies overlapped with the kernels:
+// the mode whose inputs exclude the largest factor runs first, as soon as the
+// other factors are on the device, while the largest factor is uploaded on a
+// second stream; every output is downloaded on a third stream right after its
+// mode finishes. With pinned host buffers the copies and kernels overlap.
 extern "C" int mmcsf_mttkrp_all_host(mmcsf_format* F, int R, const float* const* h_factors, float* const* h_outs,
                                      const mmcsf_kernel_cfg* cfg, void* stream) {
   MMCSF_TRY(check_call(F, R, MMCSF_DTYPE_F32));
   if (!h_factors || !h_outs) return set_error(MMCSF_ERR_INVALID, "null pointer");
+  if (F->impl != MMCSF_IMPL_MMCSF)
+    return set_error(MMCSF_ERR_INVALID, "all-mode MTTKRP needs an MM-CSF format (-t 12)");
   cudaStream_t s = S(stream);
+  const int nd = F->nd;
   if (F->stage_R != R) {
-    for (int m = 0; m < F->nd; ++m) {
+    for (int m = 0; m < nd; ++m) {
       MMCSF_CUDA(F->stage_in[m].alloc(F->dims[m] * (uint64_t)R * 4));
       MMCSF_CUDA(F->stage_out[m].alloc(F->dims[m] * (uint64_t)R * 4));
     }
     F->stage_R = R;
   }
-  const void* din[4];
-  float* dout[4];
-  for (int m = 0; m < F->nd; ++m) {
-    MMCSF_CUDA(cudaMemcpyAsync(F->stage_in[m].p, h_factors[m], F->dims[m] * (uint64_t)R * 4, cudaMemcpyHostToDevice, s));
-    din[m] = F->stage_in[m].p;
-    dout[m] = F->stage_out[m].as<float>();
+  if (!F->copy_in) {
+    MMCSF_CUDA(cudaStreamCreateWithFlags(&F->copy_in, cudaStreamNonBlocking));
+    MMCSF_CUDA(cudaStreamCreateWithFlags(&F->copy_out, cudaStreamNonBlocking));
+    for (int m = 0; m < 4; ++m) {
+      MMCSF_CUDA(cudaEventCreateWithFlags(&F->ev_in[m], cudaEventDisableTiming));
+      MMCSF_CUDA(cudaEventCreateWithFlags(&F->ev_done[m], cudaEventDisableTiming));
+    }
+    MMCSF_CUDA(cudaEventCreateWithFlags(&F->ev_start, cudaEventDisableTiming));
   }
-  MMCSF_TRY(mmcsf_mttkrp_all(F, R, MMCSF_DTYPE_F32, din, dout, cfg, stream));
-  for (int m = 0; m < F->nd; ++m)
-    MMCSF_CUDA(cudaMemcpyAsync(h_outs[m], dout[m], F->dims[m] * (uint64_t)R * 4, cudaMemcpyDeviceToHost, s));
+  // order: the largest factor is uploaded last; its own mode (which does not
+  // read it) runs first
+  int big = 0;
+  for (int m = 1; m < nd; ++m)
+    if (F->dims[m] > F->dims[big]) big = m;
+  int order[4], n = 0;
+  order[n++] = big;
+  for (int m = 0; m < nd; ++m)
+    if (m != big) order[n++] = m;
+  const void* din[4];
+  MMCSF_CUDA(cudaEventRecord(F->ev_start, s));  // staging buffers are free once earlier work on s is done
+  MMCSF_CUDA(cudaStreamWaitEvent(F->copy_in, F->ev_start, 0));
+  for (int m = 0; m < nd; ++m) din[m] = F->stage_in[m].p;
+  for (int q = 0; q < nd; ++q) {  // upload: all but the largest, then the largest
+    const int m = q < nd - 1 ? order[q + 1] : big;
+    MMCSF_CUDA(cudaMemcpyAsync(F->stage_in[m].p, h_factors[m], F->dims[m] * (uint64_t)R * 4,
+                               cudaMemcpyHostToDevice, F->copy_in));
+    MMCSF_CUDA(cudaEventRecord(F->ev_in[m], F->copy_in));
+  }
+  int total = 0;
+  for (int q = 0; q < nd; ++q) {
+    const int m = order[q];
+    for (int p = 0; p < nd; ++p)
+      if (p != m) MMCSF_CUDA(cudaStreamWaitEvent(s, F->ev_in[p], 0));
+    MMCSF_TRY(mmcsf_mttkrp(F, m, R, MMCSF_DTYPE_F32, din, F->stage_out[m].as<float>(), cfg, stream));
+    total += F->last_launches;
+    MMCSF_CUDA(cudaEventRecord(F->ev_done[m], s));
+    MMCSF_CUDA(cudaStreamWaitEvent(F->copy_out, F->ev_done[m], 0));
+    MMCSF_CUDA(cudaMemcpyAsync(h_outs[m], F->stage_out[m].p, F->dims[m] * (uint64_t)R * 4, cudaMemcpyDeviceToHost,
+                               F->copy_out));
+  }
+  MMCSF_CUDA(cudaStreamSynchronize(F->copy_out));
   MMCSF_CUDA(cudaStreamSynchronize(s));
+  F->last_launches = total;
   return MMCSF_OK;
 }
 
@@ -544,33 +590,39 @@ extern "C" int mmcsf_tune(mmcsf_format* F, int R, int factor_dtype, const void* 
   for (int i = 0; i < nmodes && st == MMCSF_OK; ++i) {
     const int m = F->impl == MMCSF_IMPL_MMCSF ? i : F->mode;
     float best = 1e30f;
-    int bt = 1, bc = 512;
+    int bt = 1, bc = 512, bm = 3;
     for (int trav = 1; trav <= 2 && st == MMCSF_OK; ++trav) {
       if (trav == 2 && !F->views[m].present) continue;
-      for (int c : chunks) {
-        mmcsf_kernel_cfg cfg{};
-        cfg.chunk = c;
-        cfg.traversal = trav;
-        float ms = 0;
-        for (int rep = 0; rep < 2; ++rep) {  // the second run is timed
-          if ((st = mmcsf_mttkrp(F, m, R, factor_dtype, d_factors, d_outs[m], &cfg, stream)) != MMCSF_OK) break;
-          if (cudaEventRecord(e0, s) != cudaSuccess) { st = MMCSF_ERR_CUDA; break; }
-          if ((st = mmcsf_mttkrp(F, m, R, factor_dtype, d_factors, d_outs[m], &cfg, stream)) != MMCSF_OK) break;
-          if (cudaEventRecord(e1, s) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess) {
-            st = MMCSF_ERR_CUDA;
-            break;
+      for (int mbv = 3; mbv <= 4; ++mbv) {
+        for (int c : chunks) {
+          mmcsf_kernel_cfg cfg{};
+          cfg.chunk = c;
+          cfg.traversal = trav;
+          cfg.min_blocks = mbv;
+          float ms = 0;
+          for (int rep = 0; rep < 2; ++rep) {  // the second run is timed
+            if ((st = mmcsf_mttkrp(F, m, R, factor_dtype, d_factors, d_outs[m], &cfg, stream)) != MMCSF_OK) break;
+            if (cudaEventRecord(e0, s) != cudaSuccess) { st = MMCSF_ERR_CUDA; break; }
+            if ((st = mmcsf_mttkrp(F, m, R, factor_dtype, d_factors, d_outs[m], &cfg, stream)) != MMCSF_OK) break;
+            if (cudaEventRecord(e1, s) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess) {
+              st = MMCSF_ERR_CUDA;
+              break;
+            }
+            cudaEventElapsedTime(&ms, e0, e1);
           }
-          cudaEventElapsedTime(&ms, e0, e1);
+          if (st != MMCSF_OK) break;
+          if (ms < best) { best = ms; bt = trav; bc = c; bm = mbv; }
         }
         if (st != MMCSF_OK) break;
-        if (ms < best) { best = ms; bt = trav; bc = c; }
       }
     }
     F->plan_traversal[m] = bt;
     F->plan_chunk[m] = bc;
+    F->plan_mb[m] = bm;
     if (plan) {
       plan->traversal[m] = bt;
       plan->chunk[m] = bc;
+      plan->min_blocks[m] = bm;
       plan->ms[m] = best;
     }
   }
@@ -588,6 +640,7 @@ extern "C" int mmcsf_set_plan(mmcsf_format* F, const mmcsf_plan* plan) {
       return set_error(MMCSF_ERR_INVALID, "bad plan entry for mode %d", m);
     F->plan_traversal[m] = plan->traversal[m];
     F->plan_chunk[m] = plan->chunk[m];
+    F->plan_mb[m] = plan->min_blocks[m];
   }
   return MMCSF_OK;
 }

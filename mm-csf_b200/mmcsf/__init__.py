@@ -326,13 +326,15 @@ class Format:
         check(lib().mmcsf_tune(self._h, R, self._dtype(factors), fp, op, _stream(stream), ctypes.byref(pl)))
         n = self.nd if self.impl == IMPL_MMCSF else 1
         modes = range(self.nd) if self.impl == IMPL_MMCSF else [self.mode]
-        return {m: {"traversal": pl.traversal[m], "chunk": pl.chunk[m], "ms": pl.ms[m]} for m in list(modes)[:n]}
+        return {m: {"traversal": pl.traversal[m], "chunk": pl.chunk[m], "min_blocks": pl.min_blocks[m],
+                    "ms": pl.ms[m]} for m in list(modes)[:n]}
 
     def set_plan(self, plan):
         pl = Plan()
         for m, e in plan.items():
             pl.traversal[m] = e["traversal"]
             pl.chunk[m] = e["chunk"]
+            pl.min_blocks[m] = e.get("min_blocks", 0)
         check(lib().mmcsf_set_plan(self._h, ctypes.byref(pl)))
 
     @property

@@ -38,11 +38,13 @@ class PartInfo(ctypes.Structure):
 
 
 class KernelCfg(ctypes.Structure):
-    _fields_ = [("chunk", c_int), ("block_threads", c_int), ("traversal", c_int), ("reserved", c_int * 5)]
+    _fields_ = [("chunk", c_int), ("block_threads", c_int), ("traversal", c_int), ("min_blocks", c_int),
+                ("reserved", c_int * 4)]
 
 
 class Plan(ctypes.Structure):
-    _fields_ = [("traversal", c_int * 4), ("chunk", c_int * 4), ("ms", ctypes.c_float * 4)]
+    _fields_ = [("traversal", c_int * 4), ("chunk", c_int * 4), ("min_blocks", c_int * 4),
+                ("ms", ctypes.c_float * 4)]
 
 
 _lib = None

@@ -115,7 +115,6 @@ __global__ void __launch_bounds__(256, MB) k_mttkrp(const Args<T> a) {
   const int lane = threadIdx.x & 31;
   const int tl = lane & (G - 1);
   const int tb = lane - tl;
-  const unsigned tmask = (G == 32) ? FULL : (((1u << G) - 1u) << tb);
   // kernel parameters in registers
   const float* __restrict__ vals = a.vals;
   const uint32_t* __restrict__ leaf = a.leaf;
@@ -143,17 +142,12 @@ __global__ void __launch_bounds__(256, MB) k_mttkrp(const Args<T> a) {
   const uint64_t x1 = active ? min(x0 + chunk, a.nnz) : x0;
 
   uint32_t f = find_fiber(a.fptr, nfib, x0);
-  // fiber metadata window: lane i holds fiber fw + i
-  uint32_t fw = f;
-  uint32_t wi, wp;  // 3-D: (b index, a index); 4-D: (c index, fbrS id)
-  auto refill = [&]() {
-    const uint32_t q = min(fw + (uint32_t)tl, nfib);
-    wi = __ldg(fidx + q);
-    wp = (ND == 3) ? __ldg(like + q) : __ldg(fpar + q);
-  };
-  refill();
-  uint32_t ci = __shfl_sync(tmask, wi, tb);  // current fiber's index (b in 3-D, c in 4-D)
-  uint32_t cp = __shfl_sync(tmask, wp, tb);  // current fiber's a (3-D) or fbrS (4-D)
+  // metadata of the open fiber (ci: b in 3-D, c in 4-D; cp: a in 3-D, fbrS
+  // in 4-D) and of the next one, loaded a fiber ahead
+  auto meta_i = [&](uint32_t q) { return __ldg(fidx + min(q, nfib - 1)); };
+  auto meta_p = [&](uint32_t q) { return (ND == 3) ? __ldg(like + min(q, nfib - 1)) : __ldg(fpar + min(q, nfib - 1)); };
+  uint32_t ci = meta_i(f), cp = meta_p(f);
+  uint32_t nci = meta_i(f + 1), ncp = meta_p(f + 1);
   uint32_t sb = 0, sa = 0;                   // 4-D: current fbrS's b and a
   if (ND == 4) { sb = __ldg(sidx1 + cp); sa = __ldg(like + cp); }
 
@@ -215,13 +209,14 @@ __global__ void __launch_bounds__(256, MB) k_mttkrp(const Args<T> a) {
       else if constexpr (OUT == 0) { rd(cur_a, v, acc2[v]); acc2[v] = f4(0.f); }
     }
   };
-  // nonzero x opens fiber f+1 (team-uniform branch)
+  // nonzero x opens fiber f+1 (team-uniform branch; no shuffles inside)
   auto advance = [&]() {
     close_fiber();
     ++f;
-    if (f - fw >= (uint32_t)G) { fw = f; refill(); }
-    ci = __shfl_sync(tmask, wi, tb + (int)(f - fw));
-    const uint32_t np = __shfl_sync(tmask, wp, tb + (int)(f - fw));
+    ci = nci;
+    const uint32_t np = ncp;
+    nci = meta_i(f + 1);
+    ncp = meta_p(f + 1);
     if constexpr (ND == 3) {
       if (OUT == 0 && np != cur_a) { flush_slice(); cur_a = np; }
       cp = np;

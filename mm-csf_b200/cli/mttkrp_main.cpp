@@ -1,4 +1,198 @@
-// placeholder CLI (filled in with the reference's flags)
+// mttkrp — command-line driver with the reference's flags (src/util.h:3341-3442,
+// src/mttkrp.cu:72-472), on top of the C ABI in include/mmcsf.h.
+//
+//   mttkrp -i X.tns [-m mode] [-R rank] [-t 8|10|12] [-f fiber-threshold]
+//          [-w warps] [-b block] [-v 0|1] [-c 0|1] [-o out.txt]
+//
+// Differences from the reference, by design:
+//   * errors print a message and return a nonzero exit status (the reference
+//     exit(0)s);
+//   * -t 1 (the serial COO CPU path) is not part of this library;
+//   * -w sets the nonzeros each worker team owns (w * 128) instead of warps
+//     per fiber; without -w the per-mode autotuner chooses;
+//   * -o writes the output of mode -m (every mode is computed for -t 12).
+// Factors are the reference's non-CPD constants U[m] = m + 0.5
+// (src/util.h:3209-3227), so printed values are directly comparable.
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <cmath>
 #include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
 #include "mmcsf.h"
-int main() { printf("mmcsf %d\n", mmcsf_version()); return 0; }
+
+namespace {
+
+struct Options {  // the reference's Options fields this driver uses (src/util.h:189-236)
+  int R = 32, mode = 0, impType = 1, warpPerSlice = 0, TBsize = 0;
+  uint64_t fbrThreashold = 0;
+  bool verbose = false, correctness = false;
+  std::string inFileName, outFileName;
+};
+
+void usage() {
+  std::printf(
+      "options:\n"
+      "        -R rank/feature : set the rank (default 32)\n"
+      "        -m mode : set the mode of MTTKRP (default 0, MM-CSF evaluates all modes)\n"
+      "        -t implementation type: 8: B-CSF 10: HB-CSF 12: MM-CSF on GPU\n"
+      "        -f fiber-splitting threshold: maximum nonzeros per fiber (default none)\n"
+      "        -w work per team: w*128 nonzeros per worker team (default: autotuned)\n"
+      "        -b threads per CTA (default 256)\n"
+      "        -v verbose: 1 to enable\n"
+      "        -c correctness: 1 to check the last mode against a host COO MTTKRP\n"
+      "        -i input file name (.tns)\n"
+      "        -o output file name\n");
+}
+
+bool parse(int argc, char** argv, Options& o) {
+  for (int i = 1; i < argc; i++) {
+    if (argv[i][0] != '-' || i + 1 >= argc) return false;
+    const char c = argv[i][1];
+    const char* v = argv[++i];
+    switch (c) {
+      case 'R': o.R = std::atoi(v); break;
+      case 'm': o.mode = std::atoi(v); break;
+      case 't': o.impType = std::atoi(v); break;
+      case 'w': o.warpPerSlice = std::atoi(v); break;
+      case 'f': o.fbrThreashold = std::strtoull(v, nullptr, 10); break;
+      case 'b': o.TBsize = std::atoi(v); break;
+      case 'v': o.verbose = std::atoi(v) == 1; break;
+      case 'c': o.correctness = std::atoi(v) == 1; break;
+      case 'i': o.inFileName = v; break;
+      case 'o': o.outFileName = v; break;
+      case 's': case 'h': case 'g': case 'l': case 'p': case 'q': case 'r': break;  // accepted, unused
+      default: std::fprintf(stderr, "unknown option: -%c\n", c); return false;
+    }
+  }
+  return !o.inFileName.empty();
+}
+
+int fail(const char* what, int st) {
+  std::fprintf(stderr, "%s failed: %s (%s)\n", what, mmcsf_status_string(st), mmcsf_last_error());
+  return 1;
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+  Options o;
+  if (!parse(argc, argv, o)) {
+    usage();
+    return 1;
+  }
+  if (o.impType != MMCSF_IMPL_MMCSF && o.impType != MMCSF_IMPL_BCSF && o.impType != MMCSF_IMPL_HBCSF) {
+    std::fprintf(stderr, "-t %d is not provided by this library (GPU formats: 8, 10, 12)\n", o.impType);
+    return 1;
+  }
+  mmcsf_coo* X = nullptr;
+  int st = mmcsf_coo_load_tns(o.inFileName.c_str(), &X);
+  if (st) return fail("load_tensor", st);
+  int nd = 0;
+  uint64_t dims[4] = {0, 0, 0, 0}, nnz = 0;
+  mmcsf_coo_info(X, &nd, dims, &nnz);
+  if (o.mode < 0 || o.mode >= nd) {
+    std::fprintf(stderr, "Mode cannot be larger than tensor dimension.\n");
+    return 1;
+  }
+  mmcsf_build_opts bo{};
+  bo.impl = o.impType;
+  bo.mode = o.impType == MMCSF_IMPL_MMCSF ? 0 : o.mode;  // check_opt forces mode 0 for -t 12
+  bo.fiber_threshold = o.fbrThreashold;
+  bo.views = o.impType == MMCSF_IMPL_MMCSF ? 1 : 0;
+  cudaStream_t s = nullptr;
+  mmcsf_format* F = nullptr;
+  auto t0 = std::chrono::steady_clock::now();
+  if ((st = mmcsf_build(X, &bo, s, &F))) return fail("format construction", st);
+  double build_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  if (o.verbose) std::printf("format construction (device): %.3f ms\n", build_ms);
+
+  const int R = o.R;
+  std::vector<float*> dU(nd), dOut(nd);
+  std::vector<std::vector<float>> hU(nd);
+  for (int m = 0; m < nd; ++m) {
+    hU[m].assign(dims[m] * (uint64_t)R, (float)m + 0.5f);
+    cudaMalloc(&dU[m], dims[m] * (uint64_t)R * 4);
+    cudaMalloc(&dOut[m], dims[m] * (uint64_t)R * 4);
+    cudaMemcpy(dU[m], hU[m].data(), dims[m] * (uint64_t)R * 4, cudaMemcpyHostToDevice);
+  }
+  const void* fac[4] = {dU[0], dU[1], dU[2], nd == 4 ? dU[3] : nullptr};
+  mmcsf_kernel_cfg cfg{};
+  if (o.warpPerSlice > 0) cfg.chunk = o.warpPerSlice * 128;
+  if (o.TBsize > 0) cfg.block_threads = o.TBsize;
+  const int nmodes = o.impType == MMCSF_IMPL_MMCSF ? nd : 1;
+  if (o.warpPerSlice <= 0 && (st = mmcsf_tune(F, R, MMCSF_DTYPE_F32, fac, dOut.data(), s, nullptr)))
+    return fail("autotune", st);
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  float total = 0;
+  for (int q = 0; q < nmodes; ++q) {
+    const int m = o.impType == MMCSF_IMPL_MMCSF ? q : o.mode;
+    cudaEventRecord(e0, s);
+    if ((st = mmcsf_mttkrp(F, m, R, MMCSF_DTYPE_F32, fac, dOut[m], o.warpPerSlice > 0 ? &cfg : nullptr, s)))
+      return fail("MTTKRP", st);
+    cudaEventRecord(e1, s);
+    cudaEventSynchronize(e1);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    total += ms;
+    if (o.verbose) std::printf("mode %d: %.3f ms\n", m, ms);
+  }
+  mmcsf_part_info pi{};
+  mmcsf_format_info(F, o.impType == MMCSF_IMPL_MMCSF ? 2 : 0, &pi);
+  std::printf("Total GPU time: %f", total);
+  if (nd == 3)
+    std::printf(" nSlc:%llu, nFibers:%llu, nnz:%llu\n", (unsigned long long)pi.n_slices,
+                (unsigned long long)pi.n_fibers + 1, (unsigned long long)pi.nnz);
+  else
+    std::printf(" nSlc:%llu, nSFibers:%llu, nFibers:%llu, nnz:%llu\n", (unsigned long long)pi.n_slices,
+                (unsigned long long)pi.n_fbrs + 1, (unsigned long long)pi.n_fibers + 1, (unsigned long long)pi.nnz);
+
+  const int check_mode = o.impType == MMCSF_IMPL_MMCSF ? nd - 1 : o.mode;
+  std::vector<float> res(dims[check_mode] * (uint64_t)R);
+  cudaMemcpy(res.data(), dOut[check_mode], res.size() * 4, cudaMemcpyDeviceToHost);
+  if (o.correctness) {
+    // host COO MTTKRP in double (src/util.h:3285-3311 compares with |diff| > 0.1)
+    const uint32_t* inds[4];
+    const float* vals;
+    mmcsf_coo_to_host(X);
+    mmcsf_coo_host_arrays(X, inds, &vals);
+    std::vector<double> ref(res.size(), 0.0);
+    for (uint64_t x = 0; x < nnz; ++x) {
+      double p = vals[x];
+      for (int m = 0; m < nd; ++m)
+        if (m != check_mode) p *= (double)m + 0.5;
+      for (int r = 0; r < R; ++r) ref[(uint64_t)inds[check_mode][x] * R + r] += p;
+    }
+    uint64_t mism = 0;
+    double maxd = 0;
+    for (size_t i = 0; i < res.size(); ++i) {
+      double d = std::fabs(res[i] - ref[i]);
+      if (d > 1e-5 * std::fabs(ref[i]) + 1e-6) ++mism;
+      if (d > maxd) maxd = d;
+    }
+    if (mism == 0) std::printf("Correctness pass!\n");
+    else std::printf("%llu mismatches; maximum diff %g\n", (unsigned long long)mism, maxd);
+  }
+  if (!o.outFileName.empty()) {
+    std::vector<float> om(dims[o.mode] * (uint64_t)R);
+    cudaMemcpy(om.data(), dOut[o.mode], om.size() * 4, cudaMemcpyDeviceToHost);
+    FILE* fo = std::fopen(o.outFileName.c_str(), "w");
+    if (!fo) { std::fprintf(stderr, "cannot write %s\n", o.outFileName.c_str()); return 1; }
+    std::fprintf(fo, "%llu x %d matrix\n", (unsigned long long)dims[o.mode], R);
+    for (uint64_t i = 0; i < dims[o.mode]; ++i) {
+      for (int j = 0; j < R; ++j) std::fprintf(fo, "%.2f\t", om[i * R + j]);
+      std::fprintf(fo, "\n");
+    }
+    std::fclose(fo);
+  }
+  for (int m = 0; m < nd; ++m) { cudaFree(dU[m]); cudaFree(dOut[m]); }
+  mmcsf_format_destroy(F);
+  mmcsf_coo_destroy(X);
+  return 0;
+}

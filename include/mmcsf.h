@@ -165,7 +165,8 @@ typedef struct {
   int chunk;         /* nonzeros per worker team; 0 = auto (the tuned plan, else 512) */
   int block_threads; /* threads per CTA; 0 = auto (256) */
   int traversal;     /* 0 auto (tuned plan, else a view when one exists), 1 MM-CSF partitions, 2 view */
-  int min_blocks;    /* register budget: 0 auto, 2 (128 registers), 3 (80) or 4 (64; 32 warps/SM) */
+  int min_blocks;    /* occupancy level: 0 auto; 1..4 = 24, 32, 40, 48 resident warps per SM
+                        (fewer rows in flight per warp at the higher levels) */
   int reserved[4];
 } mmcsf_kernel_cfg;
 

@@ -105,14 +105,15 @@ __device__ __forceinline__ uint32_t find_fiber(const uint32_t* __restrict__ fptr
 // refilled with one coalesced load every G fibers; and the factor row a fiber
 // needs when it closes is requested as soon as the fiber opens.
 // MB: minimum resident 256-thread CTAs per SM the register allocation must
-// allow (2: up to 128 registers, 3: 80, 4: 64 = 32 warps per SM); the tuner
-// picks per mode.
-template <int ND, int OUT, int G, int V, class T, int MB>
+// allow; PFX: row gathers in flight per lane. The occupancy level picks the
+// pair (1: 8 rows / 3 CTAs = 80 registers, 2: 8 rows / 4 CTAs = 64,
+// 3: 4 rows / 5 CTAs = 48, 4: 4 rows / 6 CTAs = 40); the tuner picks per mode.
+template <int ND, int OUT, int G, int V, class T, int MB, int PFX>
 __global__ void __launch_bounds__(256, MB) k_mttkrp(const Args<T> a) {
   constexpr uint32_t R = 4 * G * V;
   constexpr int LEAF = ND - 1;
   constexpr uint32_t FLAG = 0x80000000u;
-  constexpr int PF = G > 8 ? 8 : G;  // row gathers in flight per lane per batch
+  constexpr int PF = G > PFX ? PFX : G;  // row gathers in flight per lane per batch
   const int lane = threadIdx.x & 31;
   const int tl = lane & (G - 1);
   const int tb = lane - tl;
@@ -234,70 +235,54 @@ __global__ void __launch_bounds__(256, MB) k_mttkrp(const Args<T> a) {
     open_fiber();
   };
 
-  // Software pipeline over batches of PF nonzeros: while batch t is consumed,
-  // the factor rows of batch t+1 are in flight and the indices and values of
-  // batch t+2 are being loaded. Lane tl holds nonzero (tl % PF) of a batch.
-  const int bl = tl % PF;
-  const uint32_t nb = (chunk + PF - 1) / PF;  // batches per team, uniform across the warp
-  auto ldkv = [&](uint32_t bt, uint32_t& k_, float& v_) {
-    const uint64_t x = x0 + (uint64_t)bt * PF + bl;
-    k_ = 0;
-    v_ = 0.f;
-    if (bt < nb && (uint64_t)bt * PF + bl < chunk && x < x1) { k_ = __ldg(leaf + x); v_ = __ldg(vals + x); }
-  };
-  auto gather = [&](float4 (&rw)[PF][V], uint32_t kk) {
-    if constexpr (OUT != LEAF) {
+  uint32_t nk = 0;
+  float nv = 0.f;
+  if (x0 + tl < x1) { nk = __ldg(leaf + x0 + tl); nv = __ldg(vals + x0 + tl); }
+  for (uint32_t it = 0; it < chunk; it += G) {
+    const uint64_t xb = x0 + it;
+    const uint32_t kv = nk;
+    const float vv = nv;
+    {  // next block's indices and values, while this block is processed
+      const uint64_t xn = xb + G + tl;
+      nk = 0;
+      nv = 0.f;
+      if (it + G < chunk && xn < x1) { nk = __ldg(leaf + xn); nv = __ldg(vals + xn); }
+    }
+    // a lane past the range holds val 0 and no flag, and gathers row 0
+    const bool fl = (kv & FLAG) && (xb + tl != x0);
+    const uint32_t fm = (__ballot_sync(FULL, fl) >> tb);
+    const uint32_t k = kv & ~FLAG;
+#pragma unroll
+    for (int jb = 0; jb < G; jb += PF) {
+      float4 rows[PF][V];
+      uint32_t kj[PF];
 #pragma unroll
       for (int j = 0; j < PF; ++j) {
-        const uint32_t kj = __shfl_sync(FULL, kk & ~FLAG, tb + j);
+        kj[j] = __shfl_sync(FULL, k, tb + jb + j);
+        if constexpr (OUT != LEAF) {
 #pragma unroll
-        for (int v = 0; v < V; ++v) rw[j][v] = ld(UL, kj, v);
+          for (int v = 0; v < V; ++v) rows[j][v] = ld(UL, kj[j], v);
+        }
       }
-    }
-  };
-  uint32_t kc, kn;
-  float vc, vn;
-  ldkv(0, kc, vc);
-  ldkv(1, kn, vn);
-  float4 rc[PF][V];
-  gather(rc, kc);
-  for (uint32_t bt = 0; bt < nb; ++bt) {
-    float4 rn[PF][V];
-    gather(rn, kn);  // next batch's rows
-    uint32_t k2;
-    float v2;
-    ldkv(bt + 2, k2, v2);
-    const uint64_t xb = x0 + (uint64_t)bt * PF;
-    // a lane past the range holds val 0 and no flag, and gathers row 0
-    const bool fl = (tl < PF) && (kc & FLAG) && (xb + bl != x0);
-    const uint32_t fm = (__ballot_sync(FULL, fl) >> tb);
 #pragma unroll
-    for (int j = 0; j < PF; ++j) {
-      const float val = __shfl_sync(FULL, vc, tb + j);
-      if ((fm >> j) & 1u) {
-        advance();
+      for (int j = 0; j < PF; ++j) {
+        const float val = __shfl_sync(FULL, vv, tb + jb + j);
+        if ((fm >> (jb + j)) & 1u) {
+          advance();
 #pragma unroll
-        for (int v = 0; v < V; ++v) acc[v] = f4(0.f);
-      }
-      if constexpr (OUT != LEAF) {
+          for (int v = 0; v < V; ++v) acc[v] = f4(0.f);
+        }
+        if constexpr (OUT != LEAF) {
 #pragma unroll
-        for (int v = 0; v < V; ++v) acc[v] = fma4(val, rc[j][v], acc[v]);
-      } else {
-        const uint32_t kj = __shfl_sync(FULL, kc & ~FLAG, tb + j);
-        if (xb + j < x1) {
+          for (int v = 0; v < V; ++v) acc[v] = fma4(val, rows[j][v], acc[v]);
+        } else {
+          if (xb + jb + j < x1) {
 #pragma unroll
-          for (int v = 0; v < V; ++v) rd(kj, v, f4(val) * crow[v]);
+            for (int v = 0; v < V; ++v) rd(kj[j], v, f4(val) * crow[v]);
+          }
         }
       }
     }
-#pragma unroll
-    for (int j = 0; j < PF; ++j)
-#pragma unroll
-      for (int v = 0; v < V; ++v) rc[j][v] = rn[j][v];
-    kc = kn;
-    vc = vn;
-    kn = k2;
-    vn = v2;
   }
   if (active) {
     close_fiber();
@@ -311,9 +296,12 @@ cudaError_t launch_one(const Args<T>& a, int threads, int mb, cudaStream_t s) {
   const uint64_t teams = (a.nnz + a.chunk - 1) / a.chunk;
   const uint64_t thr = teams * G;
   const uint64_t blocks = (thr + threads - 1) / threads;
-  if (mb >= 4) k_mttkrp<ND, OUT, G, V, T, 4><<<(unsigned)blocks, threads, 0, s>>>(a);
-  else if (mb == 3) k_mttkrp<ND, OUT, G, V, T, 3><<<(unsigned)blocks, threads, 0, s>>>(a);
-  else k_mttkrp<ND, OUT, G, V, T, 2><<<(unsigned)blocks, threads, 0, s>>>(a);
+  switch (mb) {
+    case 1: k_mttkrp<ND, OUT, G, V, T, 3, 8><<<(unsigned)blocks, threads, 0, s>>>(a); break;
+    case 3: k_mttkrp<ND, OUT, G, V, T, 5, 4><<<(unsigned)blocks, threads, 0, s>>>(a); break;
+    case 4: k_mttkrp<ND, OUT, G, V, T, 6, 4><<<(unsigned)blocks, threads, 0, s>>>(a); break;
+    default: k_mttkrp<ND, OUT, G, V, T, 4, 8><<<(unsigned)blocks, threads, 0, s>>>(a); break;
+  }
   return cudaGetLastError();
 }
 
@@ -606,7 +594,7 @@ extern "C" int mmcsf_tune(mmcsf_format* F, int R, int factor_dtype, const void* 
     int bt = 1, bc = 512, bm = 2;
     for (int trav = 1; trav <= 2 && st == MMCSF_OK; ++trav) {
       if (trav == 2 && !F->views[m].present) continue;
-      for (int mbv = 2; mbv <= 4; ++mbv) {
+      for (int mbv = 1; mbv <= 4; ++mbv) {
         for (int c : chunks) {
           mmcsf_kernel_cfg cfg{};
           cfg.chunk = c;

@@ -201,6 +201,26 @@ int mmcsf_tune(mmcsf_format* F, int R, int factor_dtype, const void* const* d_fa
                void* stream, mmcsf_plan* plan);
 int mmcsf_set_plan(mmcsf_format* F, const mmcsf_plan* plan);
 
+/* ---- construction sort without device allocation ------------------------
+ * No counterpart in the reference. Sorts a device COO tensor (stably) into
+ * the nonzero order that mmcsf_build gives the format `impl` built with
+ * `mode` -- the order of the arrays mmcsf_format_export("inds<m>"/"vals")
+ * returns -- writing every mode's sorted indices and the values into caller
+ * buffers. It allocates no device memory: for callers whose device memory is
+ * owned by another allocator (a runtime or framework that reserved the GPU's
+ * memory up front) or that cannot take cudaMalloc's implicit synchronisation
+ * in their steady state. Its scratch is one static device array of about
+ * 12.2 MiB that every GPU loading this library holds until process exit.
+ * Limit: nnz <= 524288 (2^19) and every mode length below 2^31; larger
+ * inputs are rejected with MMCSF_ERR_INVALID. The first call on each device
+ * looks up the scratch array's device address (make that first call before
+ * any stream capture). All calls share the scratch: calls that overlap on the
+ * GPU (different streams, threads or processes sharing a context) race and
+ * must be serialised by the caller. Stream-ordered; nothing is synchronised. */
+int mmcsf_sort_coo_noalloc(int impl, int mode, int nd, const uint64_t* dims, uint64_t nnz,
+                           const uint32_t* const* d_inds, const float* d_vals, uint32_t* const* d_out_inds,
+                           float* d_out_vals, void* stream);
+
 /* Number of kernel launches the last MTTKRP/build call on this format made
  * (instrumentation for launch accounting). */
 int mmcsf_format_last_launches(const mmcsf_format* F, int* launches);

@@ -203,6 +203,36 @@ void order_modes(int nd, const uint64_t* dims, int mode, int* order) {
       if (len[i] == dims[j] && !taken[j]) { order[i] = j; taken[j] = 1; break; }
 }
 
+// The composite sort key (most significant mode first) that reproduces the
+// reference's chain of sorts for a format (the same plan mmcsf_build uses);
+// returns the number of modes written to keys.
+int sort_key_plan(int impl, int nd, const uint64_t* dims, int mode, int* keys) {
+  const int K = nd == 3 ? 2 : 3;
+  int xo[4];
+  order_modes(nd, dims, mode, xo);
+  std::vector<std::vector<int>> chain;
+  chain.push_back(std::vector<int>(xo, xo + K));
+  if (impl == MMCSF_IMPL_MMCSF) {
+    int orders[4][4];
+    int redun = -1;
+    for (int m = 0; m < nd; ++m) {
+      order_modes(nd, dims, m, orders[m]);
+      for (int p = 0; p < m; ++p)
+        if (orders[m][1] == orders[p][0] && orders[m][0] == orders[p][1]) redun = m;
+      if (m != redun) chain.push_back(std::vector<int>(orders[m], orders[m] + K));
+    }
+    chain.push_back(std::vector<int>(orders[2], orders[2] + K));
+  }
+  int n = 0;
+  for (int c = (int)chain.size() - 1; c >= 0; --c)
+    for (int m : chain[c]) {
+      bool seen = false;
+      for (int i = 0; i < n; ++i) seen = seen || keys[i] == m;
+      if (!seen) keys[n++] = m;
+    }
+  return n;
+}
+
 // Stable sort of the COO by the composite mode list `keys` (most significant
 // first). Produces sorted copies of every mode's indices and the values.
 static int sort_coo(const mmcsf_coo* X, const std::vector<int>& keys, DevBuf* sorted_inds, DevBuf& sorted_vals,

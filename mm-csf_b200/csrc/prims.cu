@@ -8,6 +8,9 @@
 // makes the reference's chain of sorts reproducible as one composite sort.
 #include <cuda_runtime.h>
 
+#include <utility>
+
+#include "common.h"
 #include "prims.cuh"
 
 namespace mmcsf {
@@ -243,3 +246,172 @@ cudaError_t gather_u32(const uint32_t* in, const uint32_t* perm, uint32_t* out, 
 }
 
 }  // namespace mmcsf
+
+// ---------------------------------------------------------------------------
+// Construction sort without device allocation.
+//
+// Some callers cannot allocate device memory once they are running: a
+// process whose device memory was reserved up front by another allocator
+// (a serving runtime or framework memory pool) finds cudaMalloc failing or
+// fragmenting that pool, and a latency-critical loop cannot afford the
+// implicit synchronisation of cudaMalloc/cudaFree. For them,
+// mmcsf_sort_coo_noalloc runs the format builder's stable radix sort with
+// all of its scratch (keys, permutation, digit histograms, scan partials) in
+// one file-scope device array of NOALLOC_BYTES (about 12.2 MiB), which every
+// GPU that loads this library holds until the process exits.
+// ---------------------------------------------------------------------------
+namespace mmcsf {
+namespace {
+
+constexpr uint64_t NOALLOC_MAX_NNZ = 1ull << 19;  // 524,288 nonzeros
+constexpr uint64_t NA_TILES = (NOALLOC_MAX_NNZ + RS_TILE - 1) / RS_TILE;
+constexpr uint64_t NA_HIST = NA_TILES * RS_RADIX + 1;          // digit histograms + total
+constexpr uint64_t NA_PART = (NA_HIST + SCAN_TILE - 1) / SCAN_TILE + 1;
+constexpr uint64_t NA_KEYS_OFF = 0;                                          // 2 x u64[MAX]
+constexpr uint64_t NA_PERM_OFF = NA_KEYS_OFF + 2 * NOALLOC_MAX_NNZ * 8;      // 2 x u32[MAX]
+constexpr uint64_t NA_HIST_OFF = NA_PERM_OFF + 2 * NOALLOC_MAX_NNZ * 4;      // u32[NA_HIST]
+constexpr uint64_t NA_PART_OFF = NA_HIST_OFF + ((NA_HIST * 4 + 255) / 256) * 256;
+constexpr uint64_t NOALLOC_BYTES = NA_PART_OFF + ((NA_PART * 4 + 255) / 256) * 256;
+
+// The scratch. Host code must not use this symbol as an address (on the host
+// it names a stand-in, not device memory); it asks for the device address with
+// cudaGetSymbolAddress, once per device.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_BYTES];
+
+constexpr int NA_MAX_DEVICES = 64;
+unsigned char* g_noalloc_ptr[NA_MAX_DEVICES] = {};
+
+__global__ void k_na_pack(const uint32_t* __restrict__ i0, const uint32_t* __restrict__ i1,
+                          const uint32_t* __restrict__ i2, const uint32_t* __restrict__ i3,
+                          const uint32_t* __restrict__ perm, int nk, int4 modes, int4 shifts, uint64_t n,
+                          uint64_t* __restrict__ keys) {
+  const uint32_t* in[4] = {i0, i1, i2, i3};
+  const int md[4] = {modes.x, modes.y, modes.z, modes.w};
+  const int sh[4] = {shifts.x, shifts.y, shifts.z, shifts.w};
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t src = perm[i];
+    uint64_t k = 0;
+    for (int j = 0; j < nk; ++j) k |= (uint64_t)in[md[j]][src] << sh[j];
+    keys[i] = k;
+  }
+}
+
+__global__ void k_na_gather_f32(const float* __restrict__ in, const uint32_t* __restrict__ perm, uint64_t n,
+                                float* __restrict__ out) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    out[i] = in[perm[i]];
+}
+
+// Exclusive scan of n <= SCAN_TILE * SCAN_TILE elements with caller scratch
+// for the partials (no allocation).
+cudaError_t na_scan(uint32_t* data, uint64_t n, uint32_t* part, cudaStream_t s) {
+  const uint64_t nb = (n + SCAN_TILE - 1) / SCAN_TILE;
+  if (nb == 1) {
+    k_scan_down<<<1, SCAN_T, 0, s>>>(data, data, n, nullptr, 1);
+    return cudaGetLastError();
+  }
+  k_scan_reduce<<<(unsigned)nb, SCAN_T, 0, s>>>(data, n, part);
+  k_scan_down<<<1, SCAN_T, 0, s>>>(part, part, nb, nullptr, 1);
+  k_scan_down<<<(unsigned)nb, SCAN_T, 0, s>>>(data, data, n, part, nb);
+  return cudaGetLastError();
+}
+
+int bits_of(uint64_t dim) {
+  int b = 0;
+  while (b < 64 && ((dim - 1) >> b)) ++b;
+  return b;
+}
+
+}  // namespace
+}  // namespace mmcsf
+
+extern "C" int mmcsf_sort_coo_noalloc(int impl, int mode, int nd, const uint64_t* dims, uint64_t nnz,
+                                      const uint32_t* const* d_inds, const float* d_vals,
+                                      uint32_t* const* d_out_inds, float* d_out_vals, void* stream) {
+  using namespace mmcsf;
+  if (!dims || (nnz && (!d_inds || !d_vals || !d_out_inds || !d_out_vals)))
+    return set_error(MMCSF_ERR_INVALID, "null argument");
+  if (nd < 3 || nd > 4) return set_error(MMCSF_ERR_INVALID, "Supported tensor dimension is 3 or 4 (got %d)", nd);
+  if (impl != MMCSF_IMPL_MMCSF && impl != MMCSF_IMPL_BCSF && impl != MMCSF_IMPL_HBCSF)
+    return set_error(MMCSF_ERR_INVALID, "unknown implementation type -t %d", impl);
+  if (mode < 0 || mode >= nd) return set_error(MMCSF_ERR_INVALID, "Mode cannot be larger than tensor dimension.");
+  if (nnz > NOALLOC_MAX_NNZ)
+    return set_error(MMCSF_ERR_INVALID,
+                     "mmcsf_sort_coo_noalloc handles at most %llu nonzeros (got %llu); use mmcsf_build",
+                     (unsigned long long)NOALLOC_MAX_NNZ, (unsigned long long)nnz);
+  for (int m = 0; m < nd; ++m)
+    if (dims[m] == 0 || dims[m] >= (1ull << 31))
+      return set_error(MMCSF_ERR_INVALID, "mode %d length %llu out of range [1, 2^31)", m,
+                       (unsigned long long)dims[m]);
+  if (nnz == 0) return MMCSF_OK;
+  cudaStream_t s = S(stream);
+
+  // Set-up, once per device, with that device current: the device address
+  // of the scratch array. The first call on a device does this.
+  int dev = 0;
+  MMCSF_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= NA_MAX_DEVICES) return set_error(MMCSF_ERR_UNSUPPORTED, "device ordinal %d", dev);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p)
+      return set_error(MMCSF_ERR_CUDA, "cudaGetSymbolAddress(scratch) failed: %s", cudaGetErrorString(e));
+    g_noalloc_ptr[dev] = static_cast<unsigned char*>(p);
+  }
+  unsigned char* base = g_noalloc_ptr[dev];
+  uint64_t* keysA = reinterpret_cast<uint64_t*>(base + NA_KEYS_OFF);
+  uint64_t* keysB = keysA + NOALLOC_MAX_NNZ;
+  uint32_t* permA = reinterpret_cast<uint32_t*>(base + NA_PERM_OFF);
+  uint32_t* permB = permA + NOALLOC_MAX_NNZ;
+  uint32_t* hist = reinterpret_cast<uint32_t*>(base + NA_HIST_OFF);
+  uint32_t* part = reinterpret_cast<uint32_t*>(base + NA_PART_OFF);
+
+  int keys[4];
+  const int nk = sort_key_plan(impl, nd, dims, mode, keys);
+  // Every scratch region is fully written before it is read (the
+  // permutation by iota, keys by packing, histograms by k_rs_hist, partials
+  // by the scan), so nothing left by the previous call is used.
+  MMCSF_CUDA(iota_u32(permA, nnz, s));
+  // LSD over <= 64-bit key groups, least significant group first
+  int g_end = nk;
+  while (g_end > 0) {
+    int g_beg = g_end, bits = 0;
+    while (g_beg > 0 && bits + bits_of(dims[keys[g_beg - 1]]) <= 64 && g_end - g_beg < 4) {
+      bits += bits_of(dims[keys[g_beg - 1]]);
+      --g_beg;
+    }
+    int md[4] = {0, 0, 0, 0}, sh[4] = {0, 0, 0, 0}, tot = 0;
+    for (int j = g_end - 1; j >= g_beg; --j) {
+      md[j - g_beg] = keys[j];
+      sh[j - g_beg] = tot;
+      tot += bits_of(dims[keys[j]]);
+    }
+    if (tot > 0) {
+      const uint32_t* ip[4] = {d_inds[0], d_inds[1], d_inds[2], nd == 4 ? d_inds[3] : d_inds[0]};
+      k_na_pack<<<grid_for(nnz, 256), 256, 0, s>>>(ip[0], ip[1], ip[2], ip[3], permA, g_end - g_beg,
+                                                   make_int4(md[0], md[1], md[2], md[3]),
+                                                   make_int4(sh[0], sh[1], sh[2], sh[3]), nnz, keysA);
+      MMCSF_LAUNCH_CHECK();
+      const uint32_t ntiles = (uint32_t)((nnz + RS_TILE - 1) / RS_TILE);
+      const uint64_t nh = (uint64_t)ntiles * RS_RADIX;
+      uint64_t *ka = keysA, *kb = keysB;
+      uint32_t *va = permA, *vb = permB;
+      int passes = 0;
+      for (int shift = 0; shift < tot; shift += 8, ++passes) {
+        k_rs_hist<<<ntiles, RS_T, 0, s>>>(ka, nnz, shift, hist, ntiles);
+        MMCSF_LAUNCH_CHECK();
+        MMCSF_CUDA(na_scan(hist, nh, part, s));
+        k_rs_scatter<<<ntiles, RS_T, 0, s>>>(ka, va, kb, vb, nnz, shift, hist, ntiles);
+        MMCSF_LAUNCH_CHECK();
+        std::swap(ka, kb);
+        std::swap(va, vb);
+      }
+      if (passes & 1) MMCSF_CUDA(cudaMemcpyAsync(permA, permB, nnz * 4, cudaMemcpyDeviceToDevice, s));
+    }
+    g_end = g_beg;
+  }
+  for (int m = 0; m < nd; ++m) MMCSF_CUDA(gather_u32(d_inds[m], permA, d_out_inds[m], nnz, s));
+  k_na_gather_f32<<<grid_for(nnz, 256), 256, 0, s>>>(d_vals, permA, nnz, d_out_vals);
+  MMCSF_LAUNCH_CHECK();
+  return MMCSF_OK;
+}

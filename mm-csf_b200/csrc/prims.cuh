@@ -37,6 +37,10 @@ cudaError_t iota_u32(uint32_t* v, uint64_t n, cudaStream_t s);
 // out[i] = in[perm[i]] for 4-byte elements
 cudaError_t gather_u32(const uint32_t* in, const uint32_t* perm, uint32_t* out, uint64_t n, cudaStream_t s);
 
+// The composite sort key of a format's construction (build.cu).
+int sort_key_plan(int impl, int nd, const uint64_t* dims, int mode, int* keys);
+void order_modes(int nd, const uint64_t* dims, int mode, int* order);
+
 // Grid size for a grid-stride kernel: a multiple of the SM count.
 int grid_for(uint64_t n, int threads);
 int sm_count();

@@ -82,6 +82,8 @@ SIGNATURES = {
     "mmcsf_tune": ([c_voidp, c_int, c_int, ctypes.POINTER(c_voidp), ctypes.POINTER(c_voidp), c_voidp,
                     ctypes.POINTER(Plan)], c_int),
     "mmcsf_set_plan": ([c_voidp, ctypes.POINTER(Plan)], c_int),
+    "mmcsf_sort_coo_noalloc": ([c_int, c_int, c_int, c_u64p, c_u64, ctypes.POINTER(c_voidp), c_voidp,
+                                ctypes.POINTER(c_voidp), c_voidp, c_voidp], c_int),
 }
 
 

@@ -63,6 +63,7 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--views", type=int, default=1, help="0 none, 1 leaf-level modes, 2 every mode")
     ap.add_argument("--no-tune", action="store_true")
+    ap.add_argument("--plan-file", default="", help="JSON plan (as printed by a tuned run) to use instead of tuning")
     return ap.parse_args()
 
 
@@ -277,7 +278,12 @@ def main():
     tdt = torch.float32 if a.dtype == "f32" else torch.bfloat16
     U = [torch.rand(d, R, device="cuda", generator=g).to(tdt) for d in dims]
     outs = [torch.empty(d, R, device="cuda") for d in dims]
-    plan = None if a.no_tune else F.tune(U, outs)
+    if a.plan_file:
+        with open(a.plan_file) as fh:
+            plan = {int(k): v for k, v in json.load(fh).items()}
+        F.set_plan(plan)
+    else:
+        plan = None if a.no_tune else F.tune(U, outs)
     # value: the workload's bytes under the MM-CSF partition traversal (the
     # same definition the reference arm uses, so the two values compare as
     # times); roofline: the bytes of the traversal each mode actually ran

@@ -418,6 +418,9 @@ int part_mttkrp(const mmcsf_format* F, const CsfPart& P, int mode, int R, int dt
 
 }  // namespace
 
+int hyb_extra_mttkrp(const mmcsf_format* F, int R, int dtype, const void* const* U, float* out, cudaStream_t s,
+                     int* launches);  // hyb.cu
+
 // One mode over every part that holds nonzeros (the reference's per-mode loop
 // over partitions, src/mttkrp_gpu.cu:3578-3724).
 int mttkrp_mode(const mmcsf_format* F, int mode, int R, int dtype, const void* const* U, float* out,
@@ -434,6 +437,7 @@ int mttkrp_mode(const mmcsf_format* F, int mode, int R, int dtype, const void* c
     return part_mttkrp(F, F->views[mode], mode, R, dtype, U, out, &c, s, launches);
   }
   for (int p = 0; p < F->nd; ++p) MMCSF_TRY(part_mttkrp(F, F->parts[p], mode, R, dtype, U, out, &c, s, launches));
+  if (F->impl == MMCSF_IMPL_HBCSF) MMCSF_TRY(hyb_extra_mttkrp(F, R, dtype, U, out, s, launches));
   return MMCSF_OK;
 }
 

@@ -235,15 +235,41 @@ class Format:
                 d[f"{pfx}.modeOrder"] = np.array(inf["mode_order"], np.uint64)
                 if inf["present"]:
                     self._dump_csf(d, p, pfx, nd)
-        else:
-            pfx = "bcsf" if self.impl == IMPL_BCSF else "hyb"
+        elif self.impl == IMPL_BCSF:
+            pfx = "bcsf"
             inf = self.info(0)
-            if self.impl == IMPL_BCSF:
-                d[f"{pfx}.nnz"] = np.array([inf["nnz"]], np.uint64)
-                d[f"{pfx}.modeOrder"] = np.array(inf["mode_order"], np.uint64)
-                self._dump_csf(d, 0, pfx, nd)
+            d[f"{pfx}.nnz"] = np.array([inf["nnz"]], np.uint64)
+            d[f"{pfx}.modeOrder"] = np.array(inf["mode_order"], np.uint64)
+            self._dump_csf(d, 0, pfx, nd)
+            for b in range(10):
+                d[f"{pfx}.bin{b}"] = self.export(0, f"bin{b}")
+        else:  # HB-CSF: part 0 = CSF slices, 1 = COO part, 2 = CSL part (3-D)
+            inf = self.info(0)
+            coo = [self.export(1, f"COOinds{l}") for l in range(nd)]
+            d["hyb.COOnnz"] = np.array([len(coo[0])], np.uint64)
+            d["hyb.HCSRnnz"] = np.array([inf["nnz"] if inf["present"] else 0], np.uint64)
+            d["hyb.modeOrder"] = np.array(inf["mode_order"], np.uint64)
+            for l in range(nd):
+                d[f"hyb.COOinds{l}"] = coo[l]
+            d["hyb.COOvals"] = self.export_f32(1, "COOvals")
+            if nd == 3:
+                d["hyb.CSLslicePtr"] = self.export(2, "CSLslicePtr")
+                d["hyb.CSLsliceIdx"] = self.export(2, "CSLsliceIdx")
+                d["hyb.CSLinds1"] = self.export(2, "CSLinds1")
+                d["hyb.CSLinds2"] = self.export(2, "CSLinds2")
+                d["hyb.CSLvals"] = self.export_f32(2, "CSLvals")
+                d["hyb.CSLnnz"] = np.array([len(d["hyb.CSLinds1"])], np.uint64)
                 for b in range(10):
-                    d[f"{pfx}.bin{b}"] = self.export(0, f"bin{b}")
+                    d[f"hyb.cslbin{b}"] = self.export(2, f"cslbin{b}")
+            else:
+                d["hyb.CSLnnz"] = np.array([0], np.uint64)
+            for l in range(nd - 1):
+                d[f"hyb.fbrPtr{l}"] = self.export(0, f"fbrPtr{l}")
+                d[f"hyb.fbrIdx{l}"] = self.export(0, f"fbrIdx{l}")
+            d["hyb.indsLeaf"] = self.export(0, "indsLeaf")
+            d["hyb.vals"] = self.export_f32(0, "vals")
+            for b in range(10):
+                d[f"hyb.bin{b}"] = self.export(0, f"bin{b}")
         return d
 
     def _dump_csf(self, d, p, pfx, nd):

@@ -41,7 +41,9 @@ def _rand_coo(rng, dims, n, skew=False, dup=False):
 
 
 def _sentinel_key(kind, nd):
-    pfx = "part2" if kind == "mmcsf" else "bcsf"
+    pfx = {"mmcsf": "part2", "bcsf": "bcsf", "hyb": "hyb"}[kind]
+    if kind == "hyb":  # create_HYB pushes no sentinel
+        return pfx, None, None
     return pfx, f"{pfx}.fbrIdx{nd - 2}", f"{pfx}.fbrPtr{nd - 2}"
 
 
@@ -85,14 +87,12 @@ def test_golden_format_arrays_bit_exact(golden_cases, torch_cuda):
         dims = case["dims"]
         X = mmcsf.CooTensor.from_arrays(dims, case["inds"], case["vals"])
         for fmt in case["formats"]:
-            if fmt["kind"] == "hyb":
-                continue
-            impl = mmcsf.IMPL_MMCSF if fmt["kind"] == "mmcsf" else mmcsf.IMPL_BCSF
+            impl = {"mmcsf": mmcsf.IMPL_MMCSF, "bcsf": mmcsf.IMPL_BCSF, "hyb": mmcsf.IMPL_HBCSF}[fmt["kind"]]
             F = mmcsf.Format(X, impl=impl, mode=fmt["mode"], fiber_threshold=fmt["f"], keep_coo=True)
             _compare_dumps(fmt["arrays"], F.reference_dump(), fmt["kind"], len(dims),
                            (case["name"], fmt["kind"], fmt["mode"], fmt["f"]))
             n += 1
-    assert n >= 40
+    assert n >= 60
 
 
 def test_golden_mttkrp(golden_cases, torch_cuda):
@@ -116,10 +116,11 @@ def test_golden_mttkrp(golden_cases, torch_cuda):
             _check_close(got, ref64, (case["name"], m))
             # the reference's own FP32 output agrees to the same tolerance
             assert np.linalg.norm(ref32 - ref64) / max(np.linalg.norm(ref64), 1e-30) <= RTOL
-        for m in range(len(dims)):  # single-mode B-CSF
-            B = mmcsf.Format(X, impl=mmcsf.IMPL_BCSF, mode=m, fiber_threshold=3)
-            got = B.mttkrp(m, Ud).cpu().numpy()
-            _check_close(got, O.mttkrp_coo_f64(dims, inds, vals, m, U), (case["name"], "bcsf", m))
+        for m in range(len(dims)):  # single-mode B-CSF and HB-CSF
+            for impl in (mmcsf.IMPL_BCSF, mmcsf.IMPL_HBCSF):
+                B = mmcsf.Format(X, impl=impl, mode=m, fiber_threshold=3)
+                got = B.mttkrp(m, Ud).cpu().numpy()
+                _check_close(got, O.mttkrp_coo_f64(dims, inds, vals, m, U), (case["name"], impl, m))
 
 
 CASES = [
@@ -149,6 +150,9 @@ def test_random_formats_match_oracle(case, torch_cuda):
         refb = O.build_bcsf(dims, inds, vals, mode, fth)
         B = mmcsf.Format(X, impl=mmcsf.IMPL_BCSF, mode=mode, fiber_threshold=f, keep_coo=True)
         _compare_dumps(refb, B.reference_dump(), "bcsf", nd, ("bcsf", case, mode))
+        refh = O.build_hyb(dims, inds, vals, mode, fth)
+        Hf = mmcsf.Format(X, impl=mmcsf.IMPL_HBCSF, mode=mode, fiber_threshold=f)
+        _compare_dumps(refh, Hf.reference_dump(), "hyb", nd, ("hyb", case, mode))
 
 
 @pytest.mark.parametrize("R", [1, 4, 8, 12, 16, 32, 48, 64, 128, 256])
@@ -306,3 +310,21 @@ def test_views_and_tuner(nd, torch_cuda):
     F1 = mmcsf.Format(X, impl=mmcsf.IMPL_MMCSF, mode=0, views=1)
     present = [F1.info(4 + m)["present"] for m in range(nd)]
     assert present == [m == order[-1] for m in range(nd)]
+
+
+@pytest.mark.parametrize("nd", [3, 4])
+def test_hbcsf_mttkrp_random(nd, torch_cuda):
+    import mmcsf
+    torch = torch_cuda
+    rng = np.random.default_rng(70 + nd)
+    dims = [3000, 40, 30] if nd == 3 else [2000, 20, 15, 10]
+    inds, vals = _rand_coo(rng, dims, 20000, True)
+    X = mmcsf.CooTensor.from_arrays(dims, inds, vals)
+    for R in (16, 32, 24):
+        U = [rng.random((d, R)).astype(np.float32) for d in dims]
+        Ud = [torch.tensor(u, device="cuda") for u in U]
+        for mode in range(nd):
+            for f in (0, 1, 2):
+                H = mmcsf.Format(X, impl=mmcsf.IMPL_HBCSF, mode=mode, fiber_threshold=f)
+                got = H.mttkrp(mode, Ud).cpu().numpy()
+                _check_close(got, O.mttkrp_coo_f64(dims, inds, vals, mode, U), ("hyb", nd, R, mode, f))

@@ -100,6 +100,10 @@ typedef struct {
   double zipf_s[4];   /* exponent for Zipf modes */
   int val_dist;       /* MMCSF_VAL_* */
   uint64_t seed;
+  int planted_rank;   /* > 0: values from a planted CP model sum_r prod_m A_m[i_m, r] with A_m uniform
+                         in [0,1) (seeded), replacing val_dist */
+  double noise;       /* planted: add N(0, (noise * RMS of the model values)^2) */
+  int poisson;        /* planted: replace each value by a Poisson draw with that mean (counts, >= 1) */
 } mmcsf_gen_spec;
 int mmcsf_generate(const mmcsf_gen_spec* spec, void* stream, mmcsf_coo** out);
 
@@ -200,6 +204,42 @@ typedef struct {
 int mmcsf_tune(mmcsf_format* F, int R, int factor_dtype, const void* const* d_factors, float* const* d_outs,
                void* stream, mmcsf_plan* plan);
 int mmcsf_set_plan(mmcsf_format* F, const mmcsf_plan* plan);
+
+/* ---- CP-ALS ---------------------------------------------------------------
+ * Replaces cpd() (src/cpd_cpu.cu:484-691) with its GPU hooks init_GPU and
+ * MTTKRP_MIHCSR_GPU_oneMode_forCPD (src/mttkrp_gpu.cu:3786-4052): the whole
+ * loop runs on the device over an MM-CSF format. Per iteration and mode:
+ * MTTKRP, solve against the Hadamard of the other Gram matrices (Cholesky,
+ * Gauss-Jordan when not positive definite), normalise (column 2-norms in the
+ * first iteration, max(column max, 1) after), update the Gram; then the fit
+ * 1 - ||X - model|| / ||X||. Stops when |fit - previous fit| < tol (after the
+ * first iteration) or after max_iters. Differences from the reference: the fit
+ * uses the full symmetric Gram product and the max-norm is a true maximum
+ * (both are wrong in the reference, src/cpd_cpu.cu:383-385 and :298-303). */
+#define MMCSF_CPD_FP32 0       /* FP32 factors and small-matrix math; host checks the fit each iteration */
+#define MMCSF_CPD_BF16 1       /* BF16 factors, FP32 MTTKRP accumulation, FP64 Gram/solve/lambda/fit; one CUDA
+                                  graph launch for the whole loop (needs a non-default stream) */
+#define MMCSF_CPD_FP64_SOLVE 2 /* FP32 factors with the FP64 small-matrix math, host-driven */
+#define MMCSF_CPD_MAX_HISTORY 1000
+typedef struct {
+  int rank;       /* 4, 8, 16, 32 or 64 */
+  int max_iters;  /* 0 = the reference's 10 (src/util.h:210) */
+  double tol;     /* 0 = the reference's 1e-5 (src/cpd_cpu.cu:494) */
+  int precision;  /* MMCSF_CPD_* */
+  int no_graph;   /* 1: run the BF16 form host-driven too */
+  uint64_t seed;  /* initial factors uniform in [0,1) when d_init is NULL */
+} mmcsf_cpd_opts;
+typedef struct {
+  int iters, converged, graph, launches; /* launches: kernels per iteration (graph) or in total */
+  double fit;
+  double seconds; /* device time of the iteration loop */
+  double fit_history[MMCSF_CPD_MAX_HISTORY];
+} mmcsf_cpd_result;
+/* d_init (optional): FP32 initial factors (dims[m] x rank); d_factors_out
+ * (optional): normalised FP32 factors; lambda_out (optional, host): rank
+ * weights. Synchronises the stream before returning. */
+int mmcsf_cpd(mmcsf_format* F, const mmcsf_cpd_opts* opts, const float* const* d_init, float* const* d_factors_out,
+              double* lambda_out, mmcsf_cpd_result* result, void* stream);
 
 /* ---- construction sort without device allocation ------------------------
  * No counterpart in the reference. Sorts a device COO tensor (stably) into

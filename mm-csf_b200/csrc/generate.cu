@@ -119,6 +119,55 @@ __global__ void k_regather(const uint64_t* ck, const uint32_t* slot, const uint6
   }
 }
 
+// Planted CP model value of nonzero t: sum_r prod_m A_m[i_m, r], A_m[i, r]
+// uniform in [0,1) from a hash of (seed, m, r, i).
+__device__ __forceinline__ double planted_value(uint64_t seed, int nd, const uint32_t* const* inds, uint64_t t, int K) {
+  double v = 0;
+  for (int r = 0; r < K; ++r) {
+    double p = 1;
+    for (int m = 0; m < nd; ++m) p *= u01(hash3(seed ^ 0x5bd1e995ull, (uint64_t)(m * 4096 + r + 7), inds[m][t]));
+    v += p;
+  }
+  return v;
+}
+
+__global__ void k_planted(uint64_t seed, int nd, const uint32_t* i0, const uint32_t* i1, const uint32_t* i2,
+                          const uint32_t* i3, uint64_t n, int K, float* vals, double* sumsq) {
+  const uint32_t* in[4] = {i0, i1, i2, i3};
+  double acc = 0;
+  for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < n; t += (uint64_t)gridDim.x * blockDim.x) {
+    const double v = planted_value(seed, nd, in, t, K);
+    vals[t] = (float)v;
+    acc += v * v;
+  }
+  atomicAdd(sumsq, acc);
+}
+
+// noise N(0, sigma^2) by Box-Muller; or a Poisson draw with mean vals[t]
+// (inversion for small means, a rounded normal for large ones), at least 1.
+__global__ void k_perturb(uint64_t seed, uint64_t n, const uint32_t* cand, double sigma, int poisson, float* vals) {
+  for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < n; t += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t j = cand[t];
+    const double u1 = u01(hash3(seed, 201, j)), u2 = u01(hash3(seed, 202, j));
+    if (poisson) {
+      const double mu = vals[t];
+      double k;
+      if (mu < 30) {
+        double pk = exp(-mu), cdf = pk;
+        k = 0;
+        while (cdf < u1 && k < 1000) { k += 1; pk *= mu / k; cdf += pk; }
+      } else {
+        const double z = sqrt(-2.0 * log(u1)) * cos(6.283185307179586 * u2);
+        k = floor(mu + sqrt(mu) * z + 0.5);
+      }
+      vals[t] = (float)(k < 1 ? 1 : k);
+    } else {
+      const double z = sqrt(-2.0 * log(u1)) * cos(6.283185307179586 * u2);
+      vals[t] = (float)(vals[t] + sigma * z);
+    }
+  }
+}
+
 int bits_for(uint64_t v) {  // bits to hold values 0..v-1
   int b = 0;
   while (b < 64 && (v - 1) >> b) ++b;
@@ -271,6 +320,25 @@ extern "C" int mmcsf_generate(const mmcsf_gen_spec* spec, void* stream, mmcsf_co
     k_emit<<<grid_for(N, 256), 256, 0, s>>>(a, cand.as<uint32_t>(), N, spec->val_dist, outs[0], outs[1], outs[2],
                                             outs[3] ? outs[3] : outs[0], X->d_vals.as<float>());
     cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess && spec->planted_rank > 0) {
+      DevBuf ss;
+      e = ss.alloc(8);
+      if (e == cudaSuccess) e = cudaMemsetAsync(ss.p, 0, 8, s);
+      if (e == cudaSuccess) {
+        k_planted<<<grid_for(N, 256), 256, 0, s>>>(spec->seed, nd, outs[0], outs[1], outs[2], outs[3] ? outs[3] : outs[0],
+                                                   N, spec->planted_rank, X->d_vals.as<float>(), ss.as<double>());
+        e = cudaGetLastError();
+      }
+      double sumsq = 0;
+      if (e == cudaSuccess) e = cudaMemcpyAsync(&sumsq, ss.p, 8, cudaMemcpyDeviceToHost, s);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+      if (e == cudaSuccess && (spec->noise > 0 || spec->poisson)) {
+        const double sigma = spec->noise * sqrt(sumsq / (double)N);
+        k_perturb<<<grid_for(N, 256), 256, 0, s>>>(spec->seed, N, cand.as<uint32_t>(), sigma, spec->poisson,
+                                                   X->d_vals.as<float>());
+        e = cudaGetLastError();
+      }
+    }
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) { delete X; return set_error(MMCSF_ERR_CUDA, "generator: %s", cudaGetErrorString(e)); }
   }

@@ -8,7 +8,7 @@ import ctypes
 
 import numpy as np
 
-from ._lib import (BuildOpts, GenSpec, KernelCfg, MmcsfError, PartInfo, Plan, c_f32p, c_u32p, c_u64, c_u64p, c_voidp,
+from ._lib import (BuildOpts, CpdOpts, CpdResult, GenSpec, KernelCfg, MmcsfError, PartInfo, Plan, c_f32p, c_u32p, c_u64, c_u64p, c_voidp,
                    check, lib)
 
 IMPL_BCSF = 8
@@ -72,8 +72,11 @@ class CooTensor:
         return cls(h)
 
     @classmethod
-    def generate(cls, dims, nnz, dist=DIST_UNIFORM, zipf_s=1.0, val_dist=VAL_UNIFORM01, seed=0, stream=None):
-        """Seeded synthetic tensor generated on the device (see mmcsf_generate)."""
+    def generate(cls, dims, nnz, dist=DIST_UNIFORM, zipf_s=1.0, val_dist=VAL_UNIFORM01, seed=0, stream=None,
+                 planted_rank=0, noise=0.0, poisson=False):
+        """Seeded synthetic tensor generated on the device (see mmcsf_generate).
+        planted_rank > 0: values from a planted CP model (+ relative Gaussian
+        noise, or Poisson counts)."""
         nd = len(dims)
         sp = GenSpec()
         sp.nd = nd
@@ -84,6 +87,9 @@ class CooTensor:
         sp.nnz = int(nnz)
         sp.val_dist = val_dist
         sp.seed = int(seed)
+        sp.planted_rank = int(planted_rank)
+        sp.noise = float(noise)
+        sp.poisson = 1 if poisson else 0
         h = c_voidp()
         check(lib().mmcsf_generate(ctypes.byref(sp), _stream(stream), ctypes.byref(h)))
         return cls(h)
@@ -362,6 +368,40 @@ class Format:
             pl.chunk[m] = e["chunk"]
             pl.min_blocks[m] = e.get("min_blocks", 0)
         check(lib().mmcsf_set_plan(self._h, ctypes.byref(pl)))
+
+    def cpd(self, rank, max_iters=10, tol=1e-5, precision="fp32", init=None, seed=0, graph=True, stream=None):
+        """CP-ALS on the device (mmcsf_cpd). precision: "fp32" (FP32 factors and
+        small-matrix math, host-driven), "bf16" (BF16 factors, FP64 solve/fit,
+        one CUDA graph for the loop unless graph=False) or "fp64solve".
+        init: optional list of FP32 CUDA tensors (dims[m] x rank). Returns a
+        dict with fit, iters, converged, seconds, history, lambda, factors."""
+        import torch
+        prec = {"fp32": 0, "bf16": 1, "fp64solve": 2}[precision]
+        o = CpdOpts()
+        o.rank = int(rank)
+        o.max_iters = int(max_iters)
+        o.tol = float(tol)
+        o.precision = prec
+        o.no_graph = 0 if graph else 1
+        o.seed = int(seed)
+        dev = init[0].device if init is not None else torch.device("cuda")
+        outs = [torch.empty((d, rank), dtype=torch.float32, device=dev) for d in self.dims]
+        ip = None
+        if init is not None:
+            keep = [t.contiguous().float() for t in init]
+            ip = (c_voidp * self.nd)(*[_ptr(t) for t in keep])
+        op = (c_voidp * self.nd)(*[_ptr(t) for t in outs])
+        lam = (ctypes.c_double * rank)()
+        res = CpdResult()
+        st = stream
+        if st is None:
+            st = torch.cuda.Stream(device=dev) if (prec == 1 and graph) else torch.cuda.current_stream(dev)
+        check(lib().mmcsf_cpd(self._h, ctypes.byref(o), ip, op, lam, ctypes.byref(res), _stream(st)))
+        torch.cuda.synchronize(dev)
+        return {"fit": res.fit, "iters": res.iters, "converged": bool(res.converged), "seconds": res.seconds,
+                "graph": bool(res.graph), "launches": res.launches,
+                "history": [res.fit_history[i] for i in range(min(res.iters, len(res.fit_history)))],
+                "lambda": np.array([lam[i] for i in range(rank)]), "factors": outs}
 
     @property
     def last_launches(self):

@@ -24,7 +24,8 @@ class MmcsfError(RuntimeError):
 
 class GenSpec(ctypes.Structure):
     _fields_ = [("nd", c_int), ("dims", c_u64 * 4), ("nnz", c_u64), ("dist", c_int * 4),
-                ("zipf_s", ctypes.c_double * 4), ("val_dist", c_int), ("seed", c_u64)]
+                ("zipf_s", ctypes.c_double * 4), ("val_dist", c_int), ("seed", c_u64), ("planted_rank", c_int),
+                ("noise", ctypes.c_double), ("poisson", c_int)]
 
 
 class BuildOpts(ctypes.Structure):
@@ -45,6 +46,20 @@ class KernelCfg(ctypes.Structure):
 class Plan(ctypes.Structure):
     _fields_ = [("traversal", c_int * 4), ("chunk", c_int * 4), ("min_blocks", c_int * 4),
                 ("ms", ctypes.c_float * 4)]
+
+
+class CpdOpts(ctypes.Structure):
+    _fields_ = [("rank", c_int), ("max_iters", c_int), ("tol", ctypes.c_double), ("precision", c_int),
+                ("no_graph", c_int), ("seed", c_u64)]
+
+
+CPD_MAX_HISTORY = 1000
+
+
+class CpdResult(ctypes.Structure):
+    _fields_ = [("iters", c_int), ("converged", c_int), ("graph", c_int), ("launches", c_int),
+                ("fit", ctypes.c_double), ("seconds", ctypes.c_double),
+                ("fit_history", ctypes.c_double * CPD_MAX_HISTORY)]
 
 
 _lib = None
@@ -82,6 +97,8 @@ SIGNATURES = {
     "mmcsf_tune": ([c_voidp, c_int, c_int, ctypes.POINTER(c_voidp), ctypes.POINTER(c_voidp), c_voidp,
                     ctypes.POINTER(Plan)], c_int),
     "mmcsf_set_plan": ([c_voidp, ctypes.POINTER(Plan)], c_int),
+    "mmcsf_cpd": ([c_voidp, ctypes.POINTER(CpdOpts), ctypes.POINTER(c_voidp), ctypes.POINTER(c_voidp),
+                   ctypes.POINTER(ctypes.c_double), ctypes.POINTER(CpdResult), c_voidp], c_int),
     "mmcsf_sort_coo_noalloc": ([c_int, c_int, c_int, c_u64p, c_u64, ctypes.POINTER(c_voidp), c_voidp,
                                 ctypes.POINTER(c_voidp), c_voidp, c_voidp], c_int),
 }

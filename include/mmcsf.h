@@ -205,6 +205,26 @@ int mmcsf_tune(mmcsf_format* F, int R, int factor_dtype, const void* const* d_fa
                void* stream, mmcsf_plan* plan);
 int mmcsf_set_plan(mmcsf_format* F, const mmcsf_plan* plan);
 
+/* ---- sampled model and its adjoint (gradient-based CP) -------------------
+ * No counterpart in the reference. The sampled CP model at every nonzero,
+ * xhat[x] = sum_r lambda_r prod_m A_m[i_m(x), r] (d_lambda may be NULL for
+ * all ones), written in the format's nonzero order. */
+int mmcsf_sampled_model(const mmcsf_format* F, int R, int factor_dtype, const void* const* d_factors,
+                        const float* d_lambda, float* d_out, void* stream);
+/* Adjoint of mmcsf_sampled_model with respect to factor `mode`:
+ * d_out[i, r] = lambda_r * sum over nonzeros x with i_mode(x) = i of
+ * d_grad[x] * prod_{m != mode} A_m[i_m(x), r], i.e. an MTTKRP of the tensor
+ * with F's sparsity and the values d_grad (one per nonzero, in the format's
+ * nonzero order) in place of its own, columns scaled by lambda (d_lambda NULL:
+ * unscaled, a plain MTTKRP on other values). d_out: dims[mode] x R FP32,
+ * overwritten. Not available for HB-CSF formats. No counterpart in the
+ * reference. */
+int mmcsf_cp_adjoint(const mmcsf_format* F, int mode, int R, int factor_dtype, const void* const* d_factors,
+                     const float* d_lambda, const float* d_grad, float* d_out, const mmcsf_kernel_cfg* cfg,
+                     void* stream);
+/* Device pointer to F's values in its nonzero order, and their count. */
+int mmcsf_format_values(const mmcsf_format* F, const float** d_vals, uint64_t* nnz);
+
 /* ---- CP-ALS ---------------------------------------------------------------
  * Replaces cpd() (src/cpd_cpu.cu:484-691) with its GPU hooks init_GPU and
  * MTTKRP_MIHCSR_GPU_oneMode_forCPD (src/mttkrp_gpu.cu:3786-4052): the whole

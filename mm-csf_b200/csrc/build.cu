@@ -155,6 +155,12 @@ __global__ void k_bins(const uint32_t* __restrict__ sptr, const uint32_t* __rest
   }
 }
 
+// inv[perm[i]] = i
+__global__ void k_invert(const uint32_t* __restrict__ perm, uint64_t n, uint32_t* __restrict__ inv) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    inv[perm[i]] = (uint32_t)i;
+}
+
 // bit 31 of the leaf index marks the first nonzero of every leaf fiber
 __global__ void k_flag_fibers(uint32_t* __restrict__ leaf, const uint32_t* __restrict__ fptr, uint64_t nfib) {
   for (uint64_t f = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; f < nfib; f += (uint64_t)gridDim.x * blockDim.x)
@@ -236,7 +242,7 @@ int sort_key_plan(int impl, int nd, const uint64_t* dims, int mode, int* keys) {
 // Stable sort of the COO by the composite mode list `keys` (most significant
 // first). Produces sorted copies of every mode's indices and the values.
 static int sort_coo(const mmcsf_coo* X, const std::vector<int>& keys, DevBuf* sorted_inds, DevBuf& sorted_vals,
-                    cudaStream_t s, Launches& L) {
+                    cudaStream_t s, Launches& L, DevBuf* perm_out = nullptr) {
   const uint64_t n = X->nnz;
   const int nd = X->nd;
   DevBuf perm, perm2, k1, k2;
@@ -295,6 +301,7 @@ static int sort_coo(const mmcsf_coo* X, const std::vector<int>& keys, DevBuf* so
                                                   sorted_vals.as<float>());
     LCHECK(L);
   }
+  if (perm_out) *perm_out = std::move(perm);  // COO index of every sorted position
   return MMCSF_OK;
 }
 
@@ -531,8 +538,8 @@ extern "C" int mmcsf_build(mmcsf_coo* X, const mmcsf_build_opts* opts, void* str
     for (int m : chain[c])
       if (std::find(keys.begin(), keys.end(), m) == keys.end()) keys.push_back(m);
 
-  DevBuf sorted[4], svals;
-  MMCSF_TRY(sort_coo(X, keys, sorted, svals, s, L));
+  DevBuf sorted[4], svals, part_perm;
+  MMCSF_TRY(sort_coo(X, keys, sorted, svals, s, L, &part_perm));
   const int target = opts->impl == MMCSF_IMPL_MMCSF ? 2 : 0;
   const uint64_t fbrs_th = opts->impl == MMCSF_IMPL_MMCSF ? FBRS_TH_MMCSF : FBRS_TH_OFF;
   CsfPart& P = Fm->parts[target];
@@ -549,9 +556,20 @@ extern "C" int mmcsf_build(mmcsf_coo* X, const mmcsf_build_opts* opts, void* str
       int vo[4];
       order_modes(nd, X->dims, m, vo);
       std::vector<int> vkeys(vo, vo + nd);
-      DevBuf vs[4], vv;
-      MMCSF_TRY(sort_coo(X, vkeys, vs, vv, s, L));
+      DevBuf vs[4], vv, vperm;
+      MMCSF_TRY(sort_coo(X, vkeys, vs, vv, s, L, &vperm));
       MMCSF_TRY(build_csf(nd, vo, X->nnz, vs, vv, REF_DEFAULT_FBR_TH, FBRS_TH_OFF, false, Fm->views[m], s, L));
+      // view position -> partition position (to reorder caller values given in
+      // the format's nonzero order, for MTTKRP on other values)
+      DevBuf inv;
+      MMCSF_CUDA(inv.alloc(X->nnz * 4));
+      k_invert<<<grid_for(X->nnz, 256), 256, 0, s>>>(part_perm.as<uint32_t>(), X->nnz, inv.as<uint32_t>());
+      LCHECK(L);
+      MMCSF_CUDA(Fm->views[m].from_part.alloc(X->nnz * 4));
+      MMCSF_CUDA(gather_u32(inv.as<uint32_t>(), vperm.as<uint32_t>(), Fm->views[m].from_part.as<uint32_t>(),
+                            X->nnz, s));
+      ++L.n;
+      MMCSF_CUDA(cudaStreamSynchronize(s));
     }
   }
   if (opts->impl == MMCSF_IMPL_HBCSF) MMCSF_TRY(build_hyb(Fm, P, s, &L.n));

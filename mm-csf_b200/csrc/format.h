@@ -30,11 +30,11 @@ struct CsfPart {
   DevBuf leaf, vals, fbr_like, fpar;
   DevBuf coo[4];    // optional: sorted index array of every tensor mode (keep_coo)
   DevBuf bin_of;    // optional: int32 bin per slice (B-CSF / HB-CSF export)
-  DevBuf fbr_of;    // 3-D: fiber of every nonzero is not stored; reserved
+  DevBuf from_part; // views: partition position of every view position (value reordering)
   uint64_t bytes() const {
     uint64_t b = 0;
     for (int l = 0; l < 3; ++l) b += ptr[l].bytes + idx[l].bytes;
-    b += leaf.bytes + vals.bytes + fbr_like.bytes + fpar.bytes + bin_of.bytes;
+    b += leaf.bytes + vals.bytes + fbr_like.bytes + fpar.bytes + bin_of.bytes + from_part.bytes;
     for (int m = 0; m < 4; ++m) b += coo[m].bytes;
     return b;
   }
@@ -72,6 +72,7 @@ struct mmcsf_format {
   // staging for the host-buffer MTTKRP entry point
   mmcsf::DevBuf stage_in[4], stage_out[4];
   int stage_R = 0;
+  mmcsf::DevBuf vals_scratch;  // caller values reordered for a view traversal
   cudaStream_t copy_in = nullptr, copy_out = nullptr;
   cudaEvent_t ev_in[4] = {}, ev_done[4] = {}, ev_start = nullptr;
   ~mmcsf_format() {

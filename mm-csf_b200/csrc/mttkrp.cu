@@ -365,7 +365,8 @@ int default_chunk(int R) {
 
 // MTTKRP on one part for tensor mode `mode`; out must be zeroed by the caller.
 int part_mttkrp(const mmcsf_format* F, const CsfPart& P, int mode, int R, int dtype, const void* const* U,
-                float* out, const mmcsf_kernel_cfg* cfg, cudaStream_t s, int* launches) {
+                float* out, const mmcsf_kernel_cfg* cfg, cudaStream_t s, int* launches,
+                const float* vals_override = nullptr) {
   if (!P.present || P.nnz == 0) return MMCSF_OK;
   int lvl = -1;
   for (int l = 0; l < P.nd; ++l)
@@ -378,7 +379,7 @@ int part_mttkrp(const mmcsf_format* F, const CsfPart& P, int mode, int R, int dt
   cudaError_t e;
   if (dtype == MMCSF_DTYPE_F32) {
     Args<float> a{};
-    a.vals = P.vals.as<float>();
+    a.vals = vals_override ? vals_override : P.vals.as<float>();
     a.leaf = P.leaf.as<uint32_t>();
     const int lf = P.nd - 2;
     a.fptr = P.ptr[lf].as<uint32_t>();
@@ -395,7 +396,7 @@ int part_mttkrp(const mmcsf_format* F, const CsfPart& P, int mode, int R, int dt
     e = launch_R<float>(a, P.nd, lvl, threads, mb, s);
   } else {
     Args<__nv_bfloat16> a{};
-    a.vals = P.vals.as<float>();
+    a.vals = vals_override ? vals_override : P.vals.as<float>();
     a.leaf = P.leaf.as<uint32_t>();
     const int lf = P.nd - 2;
     a.fptr = P.ptr[lf].as<uint32_t>();
@@ -421,10 +422,17 @@ int part_mttkrp(const mmcsf_format* F, const CsfPart& P, int mode, int R, int dt
 int hyb_extra_mttkrp(const mmcsf_format* F, int R, int dtype, const void* const* U, float* out, cudaStream_t s,
                      int* launches);  // hyb.cu
 
+__global__ void k_reorder_vals(const float* __restrict__ in, const uint32_t* __restrict__ from, uint64_t n,
+                               float* __restrict__ out) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    out[i] = in[from[i]];
+}
+
 // One mode over every part that holds nonzeros (the reference's per-mode loop
-// over partitions, src/mttkrp_gpu.cu:3578-3724).
-int mttkrp_mode(const mmcsf_format* F, int mode, int R, int dtype, const void* const* U, float* out,
-                const mmcsf_kernel_cfg* cfg, cudaStream_t s, int* launches) {
+// over partitions, src/mttkrp_gpu.cu:3578-3724). vals: optional values in the
+// format's nonzero order replacing the tensor's (the sampled model's adjoint).
+int mttkrp_mode_vals(const mmcsf_format* F, int mode, int R, int dtype, const void* const* U, const float* vals,
+                     float* out, const mmcsf_kernel_cfg* cfg, cudaStream_t s, int* launches) {
   MMCSF_CUDA(cudaMemsetAsync(out, 0, F->dims[mode] * (uint64_t)R * sizeof(float), s));
   int trav = cfg ? cfg->traversal : 0;
   if (trav == 0) trav = F->plan_traversal[mode] ? F->plan_traversal[mode] : (F->views[mode].present ? 2 : 1);
@@ -433,12 +441,32 @@ int mttkrp_mode(const mmcsf_format* F, int mode, int R, int dtype, const void* c
   if (c.chunk == 0) c.chunk = F->plan_chunk[mode];
   if (c.min_blocks == 0) c.min_blocks = F->plan_mb[mode];
   if (trav == 2) {
-    if (!F->views[mode].present) return set_error(MMCSF_ERR_INVALID, "no view for mode %d (build with views)", mode);
-    return part_mttkrp(F, F->views[mode], mode, R, dtype, U, out, &c, s, launches);
+    const CsfPart& V = F->views[mode];
+    if (!V.present) return set_error(MMCSF_ERR_INVALID, "no view for mode %d (build with views)", mode);
+    const float* vv = nullptr;
+    if (vals) {
+      mmcsf_format* Fm = const_cast<mmcsf_format*>(F);
+      if (Fm->vals_scratch.bytes < V.nnz * 4) MMCSF_CUDA(Fm->vals_scratch.alloc(V.nnz * 4));
+      k_reorder_vals<<<grid_for(V.nnz, 256), 256, 0, s>>>(vals, V.from_part.as<uint32_t>(), V.nnz,
+                                                          Fm->vals_scratch.as<float>());
+      MMCSF_LAUNCH_CHECK();
+      if (launches) ++*launches;
+      vv = Fm->vals_scratch.as<float>();
+    }
+    return part_mttkrp(F, V, mode, R, dtype, U, out, &c, s, launches, vv);
   }
-  for (int p = 0; p < F->nd; ++p) MMCSF_TRY(part_mttkrp(F, F->parts[p], mode, R, dtype, U, out, &c, s, launches));
-  if (F->impl == MMCSF_IMPL_HBCSF) MMCSF_TRY(hyb_extra_mttkrp(F, R, dtype, U, out, s, launches));
+  for (int p = 0; p < F->nd; ++p)
+    MMCSF_TRY(part_mttkrp(F, F->parts[p], mode, R, dtype, U, out, &c, s, launches, vals));
+  if (F->impl == MMCSF_IMPL_HBCSF) {
+    if (vals) return set_error(MMCSF_ERR_UNSUPPORTED, "MTTKRP on other values is not available for HB-CSF");
+    MMCSF_TRY(hyb_extra_mttkrp(F, R, dtype, U, out, s, launches));
+  }
   return MMCSF_OK;
+}
+
+int mttkrp_mode(const mmcsf_format* F, int mode, int R, int dtype, const void* const* U, float* out,
+                const mmcsf_kernel_cfg* cfg, cudaStream_t s, int* launches) {
+  return mttkrp_mode_vals(F, mode, R, dtype, U, nullptr, out, cfg, s, launches);
 }
 
 }  // namespace mmcsf
@@ -496,6 +524,44 @@ extern "C" int mmcsf_mttkrp(const mmcsf_format* F, int mode, int R, int factor_d
     MMCSF_CUDA(cudaStreamSynchronize(s));
     return MMCSF_OK;
   }, s);
+  Fm->last_launches = launches;
+  return st;
+}
+
+__global__ void k_scale_cols(float* __restrict__ M, uint64_t rows, int R, const float* __restrict__ lam) {
+  const uint64_t n = rows * (uint64_t)R;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    M[i] *= __ldg(lam + i % R);
+}
+
+extern "C" int mmcsf_cp_adjoint(const mmcsf_format* F, int mode, int R, int factor_dtype,
+                                const void* const* d_factors, const float* d_lambda, const float* d_grad,
+                                float* d_out, const mmcsf_kernel_cfg* cfg, void* stream) {
+  MMCSF_TRY(check_call(F, R, factor_dtype));
+  if (mode < 0 || mode >= F->nd) return set_error(MMCSF_ERR_INVALID, "Mode cannot be larger than tensor dimension.");
+  if (!d_factors || !d_out || !d_grad) return set_error(MMCSF_ERR_INVALID, "null pointer");
+  if (F->impl == MMCSF_IMPL_HBCSF) return set_error(MMCSF_ERR_UNSUPPORTED, "not available for HB-CSF formats");
+  if (F->impl != MMCSF_IMPL_MMCSF && mode != F->mode)
+    return set_error(MMCSF_ERR_INVALID, "this format was built for mode %d only", F->mode);
+  cudaStream_t s = S(stream);
+  mmcsf_format* Fm = const_cast<mmcsf_format*>(F);
+  int launches = 0;
+  int st = with_padding(F, R, factor_dtype, d_factors, [&](int Rk, const void* const* U) -> int {
+    if (Rk == R) return mttkrp_mode_vals(F, mode, R, factor_dtype, U, d_grad, d_out, cfg, s, &launches);
+    DevBuf tmp;
+    MMCSF_CUDA(tmp.alloc(F->dims[mode] * (uint64_t)Rk * 4));
+    MMCSF_TRY(mttkrp_mode_vals(F, mode, Rk, factor_dtype, U, d_grad, tmp.as<float>(), cfg, s, &launches));
+    k_unpad_rows<<<grid_for(F->dims[mode] * (uint64_t)R, 256), 256, 0, s>>>(tmp.as<float>(), F->dims[mode], R, Rk,
+                                                                           d_out);
+    MMCSF_LAUNCH_CHECK();
+    MMCSF_CUDA(cudaStreamSynchronize(s));
+    return MMCSF_OK;
+  }, s);
+  if (st == MMCSF_OK && d_lambda) {
+    k_scale_cols<<<grid_for(F->dims[mode] * (uint64_t)R, 256), 256, 0, s>>>(d_out, F->dims[mode], R, d_lambda);
+    MMCSF_LAUNCH_CHECK();
+    ++launches;
+  }
   Fm->last_launches = launches;
   return st;
 }

@@ -403,6 +403,56 @@ class Format:
                 "history": [res.fit_history[i] for i in range(min(res.iters, len(res.fit_history)))],
                 "lambda": np.array([lam[i] for i in range(rank)]), "factors": outs}
 
+    # -- sampled model and adjoint ------------------------------------------
+    def _main_part(self):
+        if self.impl == IMPL_MMCSF:
+            for p in range(self.nd):
+                if self.info(p)["present"]:
+                    return p
+            return 0
+        return 0
+
+    def values(self):
+        """Borrowed torch view of the tensor's values in the format's nonzero
+        order (the order of sampled_model's output and cp_adjoint's grad)."""
+        import torch
+        vp = c_voidp()
+        n = c_u64()
+        check(lib().mmcsf_format_values(self._h, ctypes.byref(vp), ctypes.byref(n)))
+        return torch.as_tensor(_CudaArray(vp.value, n.value, "<f4"), device="cuda")
+
+    def nonzero_coords(self):
+        """Per-mode coordinates (numpy uint64) of every nonzero in the
+        format's nonzero order; needs keep_coo=True at build time."""
+        p = self._main_part()
+        return [self.export(p, f"inds{m}") for m in range(self.nd)]
+
+    def sampled_model(self, factors, lam=None, out=None, stream=None):
+        """xhat[x] = sum_r lam_r prod_m A_m[i_m(x), r] at every nonzero, in the
+        format's nonzero order (float32 CUDA tensor of nnz entries)."""
+        import torch
+        R = factors[0].shape[1]
+        if out is None:
+            out = torch.empty(self.nnz, dtype=torch.float32, device=factors[0].device)
+        fp = (c_voidp * self.nd)(*[_ptr(f) for f in factors])
+        check(lib().mmcsf_sampled_model(self._h, R, self._dtype(factors), fp,
+                                        _ptr(lam) if lam is not None else None, _ptr(out), _stream(stream)))
+        return out
+
+    def cp_adjoint(self, mode, factors, grad, lam=None, out=None, cfg=None, stream=None):
+        """lam (.) MTTKRP of the tensor with this sparsity and values `grad`
+        (nnz float32 in the format's nonzero order): the gradient of
+        sum_x grad[x] * xhat[x] with respect to factor `mode`."""
+        import torch
+        R = factors[0].shape[1]
+        if out is None:
+            out = torch.empty((self.dims[mode], R), dtype=torch.float32, device=factors[0].device)
+        fp = (c_voidp * self.nd)(*[_ptr(f) for f in factors])
+        check(lib().mmcsf_cp_adjoint(self._h, mode, R, self._dtype(factors), fp,
+                                     _ptr(lam) if lam is not None else None, _ptr(grad), _ptr(out),
+                                     self._cfg(cfg), _stream(stream)))
+        return out
+
     @property
     def last_launches(self):
         n = ctypes.c_int()

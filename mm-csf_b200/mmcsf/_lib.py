@@ -99,6 +99,10 @@ SIGNATURES = {
     "mmcsf_set_plan": ([c_voidp, ctypes.POINTER(Plan)], c_int),
     "mmcsf_cpd": ([c_voidp, ctypes.POINTER(CpdOpts), ctypes.POINTER(c_voidp), ctypes.POINTER(c_voidp),
                    ctypes.POINTER(ctypes.c_double), ctypes.POINTER(CpdResult), c_voidp], c_int),
+    "mmcsf_sampled_model": ([c_voidp, c_int, c_int, ctypes.POINTER(c_voidp), c_voidp, c_voidp, c_voidp], c_int),
+    "mmcsf_cp_adjoint": ([c_voidp, c_int, c_int, c_int, ctypes.POINTER(c_voidp), c_voidp, c_voidp, c_voidp,
+                          ctypes.POINTER(KernelCfg), c_voidp], c_int),
+    "mmcsf_format_values": ([c_voidp, ctypes.POINTER(c_voidp), c_u64p], c_int),
     "mmcsf_sort_coo_noalloc": ([c_int, c_int, c_int, c_u64p, c_u64, ctypes.POINTER(c_voidp), c_voidp,
                                 ctypes.POINTER(c_voidp), c_voidp, c_voidp], c_int),
 }

@@ -1,0 +1,130 @@
+"""Gradient-based CP on an MM-CSF format (no counterpart in the reference).
+
+The sampled CP model xhat[x] = sum_r lambda_r prod_m A_m[i_m(x), r] at every
+nonzero x runs as one hand-written kernel (mmcsf_sampled_model); its adjoint
+with respect to A_n is an MTTKRP of the tensor with the same sparsity and the
+upstream gradient as values (mmcsf_cp_adjoint), the same kernels the
+reference's MTTKRP_MIHCSR_GPU (src/mttkrp_gpu.cu:3578-3724) stands for. Both
+sit behind SampledCP, a torch.autograd.Function, so any loss written in torch
+over xhat gets exact factor gradients.
+
+precision="bf16" keeps FP32 master factors for the optimiser, hands the
+kernels BF16 copies (half the gather bytes) and returns FP32 gradients
+(FP32 accumulation inside the kernels).
+
+poisson_loss is the generalized-CP Poisson loss (f(y, m) = m - y log m) over
+ALL entries of the tensor: the sum of the model over every entry is
+sum_r lambda_r prod_m colsum(A_m)_r, so only the nonzeros need the sampled
+model. gcp_poisson fits nonnegative factors to it with projected Adam and
+records the loss against device time.
+"""
+import time
+
+import torch
+
+__all__ = ["SampledCP", "sampled_cp", "poisson_loss", "gcp_poisson"]
+
+
+class SampledCP(torch.autograd.Function):
+    """xhat = SampledCP.apply(fmt, precision, lam, *factors).
+
+    fmt: mmcsf.Format (MM-CSF, or B-CSF for its built mode's sparsity);
+    precision: "fp32" or "bf16" (kernel factor type); lam: rank-R float32
+    CUDA tensor or None; factors: dims[m] x R float32 (or bfloat16) CUDA
+    tensors. Returns nnz float32 values in the format's nonzero order."""
+
+    @staticmethod
+    def forward(ctx, fmt, precision, lam, *factors):
+        kdt = torch.bfloat16 if precision == "bf16" else factors[0].dtype
+        work = [f.detach().to(kdt).contiguous() for f in factors]
+        lam_c = lam.detach().float().contiguous() if lam is not None else None
+        out = fmt.sampled_model(work, lam_c)
+        ctx.fmt = fmt
+        ctx.has_lam = lam is not None
+        ctx.dtypes = [f.dtype for f in factors]
+        if lam is not None:
+            ctx.save_for_backward(lam_c, *work)
+        else:
+            ctx.save_for_backward(*work)
+        return out
+
+    @staticmethod
+    def backward(ctx, g):
+        saved = ctx.saved_tensors
+        lam = saved[0] if ctx.has_lam else None
+        work = list(saved[1:] if ctx.has_lam else saved)
+        fmt = ctx.fmt
+        g = g.detach().float().contiguous()
+        nd = len(work)
+        grads = [None] * nd
+        g_lam = None
+        need_lam = ctx.has_lam and ctx.needs_input_grad[2]
+        for n in range(nd):
+            if not (ctx.needs_input_grad[3 + n] or (n == 0 and need_lam)):
+                continue
+            if need_lam and n == 0:
+                m0 = fmt.cp_adjoint(0, work, g)            # unscaled: lambda applied below
+                g_lam = (m0 * work[0].float()).sum(0)
+                grads[0] = (m0 * lam).to(ctx.dtypes[0])
+            else:
+                grads[n] = fmt.cp_adjoint(n, work, g, lam).to(ctx.dtypes[n])
+        return (None, None, g_lam, *grads)
+
+
+def sampled_cp(fmt, factors, lam=None, precision="fp32"):
+    """Differentiable sampled CP model at the format's nonzeros."""
+    return SampledCP.apply(fmt, precision, lam, *factors)
+
+
+def poisson_loss(fmt, factors, y, lam=None, precision="fp32", eps=1e-10):
+    """sum over every entry of m - y log(m + eps), m the CP model, y the
+    tensor (zero off its nonzeros); y: nnz values in the format's order."""
+    xhat = sampled_cp(fmt, factors, lam, precision)
+    cs = factors[0].float().sum(0)
+    for f in factors[1:]:
+        cs = cs * f.float().sum(0)
+    total = (cs * lam).sum() if lam is not None else cs.sum()
+    return total - (y * torch.log(xhat + eps)).sum()
+
+
+def gcp_poisson(fmt, rank, iters=100, lr=1e-2, precision="fp32", init=None, seed=0, eps=1e-10,
+                stop_loss=None):
+    """Projected-Adam Poisson CP (nonnegative factors, no lambda).
+
+    init: optional list of dims[m] x rank FP32 CUDA tensors (copied).
+    stop_loss: stop once the loss is at or below this value (checked every
+    iteration on the host, so it costs one sync per iteration; None runs all
+    iterations without host syncs inside the loop).
+    Returns dict(loss=[...], ms=[...] cumulative device time per iteration,
+    factors, iters, seconds)."""
+    dev = torch.device("cuda")
+    g = torch.Generator(device="cpu").manual_seed(seed)
+    if init is None:
+        init = [torch.rand((d, rank), generator=g).to(dev) * 0.5 + 0.25 for d in fmt.dims]
+    masters = [t.detach().clone().float().contiguous().requires_grad_(True) for t in init]
+    y = fmt.values()
+    opt = torch.optim.Adam(masters, lr=lr)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(iters + 1)]
+    losses = []
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ev[0].record()
+    n_done = 0
+    for it in range(iters):
+        opt.zero_grad(set_to_none=True)
+        loss = poisson_loss(fmt, masters, y, None, precision, eps)
+        loss.backward()
+        opt.step()
+        with torch.no_grad():
+            for p in masters:
+                p.clamp_(min=0.0)
+        losses.append(loss.detach())
+        ev[it + 1].record()
+        n_done = it + 1
+        if stop_loss is not None and loss.item() <= stop_loss:
+            break
+    torch.cuda.synchronize()
+    secs = time.perf_counter() - t0
+    ms = [ev[0].elapsed_time(ev[i + 1]) for i in range(n_done)]
+    return {"loss": [float(v) for v in torch.stack(losses).cpu()], "ms": ms, "iters": n_done, "seconds": secs,
+            "factors": [p.detach() for p in masters]}

@@ -64,6 +64,8 @@ def parse():
     ap.add_argument("--views", type=int, default=1, help="0 none, 1 leaf-level modes, 2 every mode")
     ap.add_argument("--no-tune", action="store_true")
     ap.add_argument("--plan-file", default="", help="JSON plan (as printed by a tuned run) to use instead of tuning")
+    ap.add_argument("--no-cp", action="store_true", help="skip the CP-ALS and Poisson gradient-CP sections")
+    ap.add_argument("--cp-scale", type=float, default=1.0, help="scale the CP workloads' nonzero counts")
     return ap.parse_args()
 
 
@@ -191,6 +193,83 @@ def reference_sample_time(inds_host, vals_host, dims, R, target_s=12.0, max_n=No
         t = run(S2)
         S = S2
     return t, S, kind
+
+
+CPALS = dict(dims=[200000, 200000, 200000], nnz=50_000_000, planted=16, noise=0.01, R=16, max_iters=50, tol=1e-5,
+             desc="200000^3, 50M uniform nnz, planted rank-16 CP (factors U[0,1)) + Gaussian noise 0.01 RMS, R=16, "
+                  "tol 1e-5 on fit change, at most 50 iterations")
+GCP = dict(dims=[100000, 50000, 10000], nnz=20_000_000, zipf=1.05, planted=32, R=32, iters=150, lr=0.05,
+           desc="100000x50000x10000, 20M nnz, Zipf(1.05) per mode, Poisson counts of a planted nonnegative "
+                "rank-32 CP, R=32, projected Adam (step 0.05 x mean initial entry, initial mass = data mass) on the Poisson "
+                "loss over every entry")
+
+
+def cp_section(seed, scale):
+    """CP seconds per iteration to a fixed fit: BF16 factors (+ FP64 solve and
+    fit, whole loop in one CUDA graph) against plain FP32 CP-ALS, and Poisson
+    gradient CP (sampled model + adjoint) with BF16 vs FP32 factors."""
+    import torch
+    import mmcsf
+    from mmcsf import gcp
+    out = {}
+    # ---- CP-ALS
+    c = CPALS
+    nnz = int(c["nnz"] * scale)
+    X = mmcsf.CooTensor.generate(c["dims"], nnz, dist=[0, 0, 0], val_dist=mmcsf.VAL_UNIFORM01, seed=seed + 11,
+                                 planted_rank=c["planted"], noise=c["noise"])
+    F = mmcsf.Format(X, impl=mmcsf.IMPL_MMCSF, views=1)
+    del X
+    g = torch.Generator(device="cuda").manual_seed(seed + 5)
+    R = c["R"]
+    init = [torch.rand(d, R, device="cuda", generator=g) for d in c["dims"]]
+    F.tune(init)
+    runs = {}
+    for prec in ("fp32", "bf16", "fp64solve"):
+        F.cpd(R, max_iters=2, tol=c["tol"], precision=prec, init=init)       # warm-up (tables, graph code)
+        r = F.cpd(R, max_iters=c["max_iters"], tol=c["tol"], precision=prec, init=init)
+        fx = F.cpd(R, max_iters=c["max_iters"], tol=1e-15, precision=prec, init=init)  # every iteration
+        runs[prec] = {"seconds_to_converge": r["seconds"], "iters_to_converge": r["iters"], "fit": r["fit"],
+                      "converged": r["converged"], "graph": r["graph"], "launches": r["launches"],
+                      "fixed_iters": fx["iters"], "fixed_seconds": fx["seconds"],
+                      "s_per_iter": fx["seconds"] / max(1, fx["iters"]), "fixed_fit": fx["fit"]}
+    f32, b16 = runs["fp32"], runs["bf16"]
+    out["cp_als"] = {"workload": c["desc"] + (f" (nnz scaled to {nnz})" if scale != 1.0 else ""),
+                     "runs": runs, "fit_gap_bf16_vs_fp32": abs(b16["fit"] - f32["fit"]),
+                     "fit_gap_bf16_vs_fp64solve": abs(b16["fit"] - runs["fp64solve"]["fit"]),
+                     "speedup_time_to_fit_bf16_vs_fp32": f32["seconds_to_converge"] / b16["seconds_to_converge"],
+                     "speedup_s_per_iter_bf16_vs_fp32": f32["s_per_iter"] / b16["s_per_iter"]}
+    del F, init
+    torch.cuda.empty_cache()
+    # ---- Poisson gradient CP
+    c = GCP
+    nnz = int(c["nnz"] * scale)
+    X = mmcsf.CooTensor.generate(c["dims"], nnz, dist=[1, 1, 1], zipf_s=c["zipf"], seed=seed + 13,
+                                 planted_rank=c["planted"], poisson=True)
+    F = mmcsf.Format(X, impl=mmcsf.IMPL_MMCSF, views=1)
+    del X
+    R = c["R"]
+    g = torch.Generator(device="cuda").manual_seed(seed + 7)
+    init = [torch.rand(d, R, device="cuda", generator=g) * 0.5 + 0.25 for d in c["dims"]]
+    F.tune(init)
+    runs = {}
+    for prec in ("fp32", "bf16"):
+        gcp.gcp_poisson(F, R, iters=3, lr=c["lr"], precision=prec, init=init)  # warm-up
+        r = gcp.gcp_poisson(F, R, iters=c["iters"], lr=c["lr"], precision=prec, init=init)
+        runs[prec] = {"ms_per_iter": r["ms"][-1] / r["iters"], "iters": r["iters"], "loss_first": r["loss"][0],
+                      "loss_final": r["loss"][-1], "ms": r["ms"], "loss": r["loss"]}
+    f32, b16 = runs["fp32"], runs["bf16"]
+    target = f32["loss_final"] * (1 + 1e-4)
+    t_b16 = next((t for t, l in zip(b16["ms"], b16["loss"]) if l <= target), None)
+    curve = {p: [[round(t, 3), l] for t, l in list(zip(v["ms"], v["loss"]))[:: max(1, len(v["ms"]) // 15)]]
+             for p, v in runs.items()}
+    for v in runs.values():
+        del v["ms"], v["loss"]
+    out["gcp_poisson"] = {"workload": c["desc"] + (f" (nnz scaled to {nnz})" if scale != 1.0 else ""),
+                          "runs": runs, "loss_vs_ms": curve,
+                          "loss_gap_bf16_vs_fp32": abs(b16["loss_final"] - f32["loss_final"]) / abs(f32["loss_final"]),
+                          "ms_bf16_to_fp32_final_loss": t_b16,
+                          "speedup_ms_per_iter_bf16_vs_fp32": f32["ms_per_iter"] / b16["ms_per_iter"]}
+    return out
 
 
 def main():
@@ -379,13 +458,18 @@ def main():
                "ms_per_step": ts * 1e3,
                "sample": f"first {S} of {nnz} nonzeros, all {nd} modes, MTTKRP_COO_CPU serial as shipped, "
                          f"extrapolated x{nnz / S:.1f}"}
+    cp = None
+    if not a.no_cp:
+        del F, X, U, outs
+        torch.cuda.empty_cache()
+        cp = cp_section(a.seed, a.cp_scale)
     line = {"metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": a.dtype, "data": "synthetic (seeded device generator)",
             "config": config, "mode_ms": mode_ms, "mode_algorithmic_bytes": per_mode, "plan": plan, "format": info,
             "roofline": roofline,
             "cpu_baseline": cpu,
-            "e2e": e2e, "gpu_launches": launches_per_step * a.steps, "clocks": clocks}
+            "e2e": e2e, "gpu_launches": launches_per_step * a.steps, "clocks": clocks, "cp": cp}
     print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()

@@ -169,9 +169,11 @@ typedef struct {
   int chunk;         /* nonzeros per worker team; 0 = auto (the tuned plan, else 512) */
   int block_threads; /* threads per CTA; 0 = auto (256) */
   int traversal;     /* 0 auto (tuned plan, else a view when one exists), 1 MM-CSF partitions, 2 view */
-  int min_blocks;    /* occupancy level: 0 auto; 1..4 = 24, 32, 40, 48 resident warps per SM
-                        (fewer rows in flight per warp at the higher levels) */
-  int reserved[4];
+  int min_blocks;    /* occupancy level: 0 auto; 1..4 = more resident warps per SM at the higher
+                        levels, fewer rows in flight per warp */
+  int kernel;        /* 0 auto (tuned plan, else 2 for 3-D and 1 for 4-D); 1 per-team fiber walk;
+                        2 branch-free walk (3-D only) */
+  int reserved[3];
 } mmcsf_kernel_cfg;
 
 /* One mode. factor_dtype: MMCSF_DTYPE_F32 (d_factors are float*) or
@@ -199,6 +201,7 @@ typedef struct {
   int traversal[4]; /* 1 MM-CSF partitions, 2 view */
   int chunk[4];
   int min_blocks[4];
+  int kernel[4];    /* mmcsf_kernel_cfg.kernel */
   float ms[4];      /* best time per mode */
 } mmcsf_plan;
 int mmcsf_tune(mmcsf_format* F, int R, int factor_dtype, const void* const* d_factors, float* const* d_outs,

@@ -473,6 +473,33 @@ static int compute_bins(CsfPart& P, bool with_children, cudaStream_t s, Launches
 
 int build_hyb(mmcsf_format* F, CsfPart& X, cudaStream_t s, int* launches);  // hyb.cu
 
+// largest fiber f with fptr[f] <= x, for every chunk start x = c * chunk
+__global__ void k_chunk_fibers(const uint32_t* __restrict__ fptr, uint32_t nfib, uint64_t chunk, uint64_t nchunks,
+                               uint32_t* __restrict__ out) {
+  const uint64_t c = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (c >= nchunks) return;
+  const uint64_t x = c * chunk;
+  uint32_t lo = 0, hi = nfib - 1;
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi + 1) >> 1;
+    if ((uint64_t)fptr[mid] <= x) lo = mid; else hi = mid - 1;
+  }
+  out[c] = lo;
+}
+
+int chunk_fibers(CsfPart& P, cudaStream_t s, Launches& L) {
+  if (!P.present || P.nnz == 0 || P.n_fibers() == 0) return MMCSF_OK;
+  for (int i = 0; i < CsfPart::N_CHUNK_SIZES; ++i) {
+    const uint64_t chunk = 128ull << i, nch = (P.nnz + chunk - 1) / chunk;
+    MMCSF_CUDA(P.cfib[i].alloc(nch * 4));
+    k_chunk_fibers<<<(unsigned)((nch + 255) / 256), 256, 0, s>>>(P.ptr[P.nd - 2].as<uint32_t>(),
+                                                                 (uint32_t)P.n_fibers(), chunk, nch,
+                                                                 P.cfib[i].as<uint32_t>());
+    LCHECK(L);
+  }
+  return MMCSF_OK;
+}
+
 }  // namespace mmcsf
 
 using namespace mmcsf;
@@ -573,6 +600,9 @@ extern "C" int mmcsf_build(mmcsf_coo* X, const mmcsf_build_opts* opts, void* str
     }
   }
   if (opts->impl == MMCSF_IMPL_HBCSF) MMCSF_TRY(build_hyb(Fm, P, s, &L.n));
+  for (int p = 0; p < 4; ++p) MMCSF_TRY(chunk_fibers(Fm->parts[p], s, L));
+  for (int m = 0; m < 4; ++m) MMCSF_TRY(chunk_fibers(Fm->views[m], s, L));
+  MMCSF_CUDA(cudaStreamSynchronize(s));
   Fm->last_launches = L.n;
   *out = guard.release();
   return MMCSF_OK;

@@ -31,9 +31,19 @@ struct CsfPart {
   DevBuf coo[4];    // optional: sorted index array of every tensor mode (keep_coo)
   DevBuf bin_of;    // optional: int32 bin per slice (B-CSF / HB-CSF export)
   DevBuf from_part; // views: partition position of every view position (value reordering)
+  // first leaf fiber of every chunk of (128 << i) nonzeros, i < 6: the worker
+  // teams' starting points for the chunk sizes the tuner tries
+  static constexpr int N_CHUNK_SIZES = 6;
+  DevBuf cfib[N_CHUNK_SIZES];
+  static int cfib_slot(uint64_t chunk) {
+    for (int i = 0; i < N_CHUNK_SIZES; ++i)
+      if (chunk == (128ull << i)) return i;
+    return -1;
+  }
   uint64_t bytes() const {
     uint64_t b = 0;
     for (int l = 0; l < 3; ++l) b += ptr[l].bytes + idx[l].bytes;
+    for (int i = 0; i < N_CHUNK_SIZES; ++i) b += cfib[i].bytes;
     b += leaf.bytes + vals.bytes + fbr_like.bytes + fpar.bytes + bin_of.bytes + from_part.bytes;
     for (int m = 0; m < 4; ++m) b += coo[m].bytes;
     return b;
@@ -67,6 +77,7 @@ struct mmcsf_format {
   int plan_traversal[4] = {0, 0, 0, 0};  // tuned: 1 partitions, 2 view (0 = untuned)
   int plan_chunk[4] = {0, 0, 0, 0};
   int plan_mb[4] = {0, 0, 0, 0};
+  int plan_kernel[4] = {0, 0, 0, 0};
   mmcsf::HybExtra hyb;
   int last_launches = 0;
   // staging for the host-buffer MTTKRP entry point

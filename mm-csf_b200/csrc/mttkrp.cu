@@ -21,6 +21,7 @@
 #include <cuda_bf16.h>
 
 #include <cstring>
+#include <type_traits>
 
 #include "format.h"
 #include "prims.cuh"
@@ -75,6 +76,7 @@ struct Args {
   const uint32_t* fpar;   // 4-D: fiber -> fbrS
   const uint32_t* sidx1;  // 4-D: fbrS index (o1)
   const uint32_t* like;   // o0 per level-1 entry (3-D: fiber, 4-D: fbrS)
+  const uint32_t* cfib;   // first fiber of every team's chunk, or null (binary search)
   uint64_t nnz;
   uint32_t nfib;
   uint32_t chunk;
@@ -143,7 +145,7 @@ __global__ void __launch_bounds__(256, MB) k_mttkrp(const Args<T> a) {
   const uint64_t x0 = active ? team * chunk : a.nnz - 1;
   const uint64_t x1 = active ? min(x0 + chunk, a.nnz) : x0;
 
-  uint32_t f = find_fiber(a.fptr, nfib, x0);
+  uint32_t f = a.cfib ? (active ? __ldg(a.cfib + team) : nfib - 1) : find_fiber(a.fptr, nfib, x0);
   // metadata of the open fiber (ci: b in 3-D, c in 4-D; cp: a in 3-D, fbrS
   // in 4-D) and of the next one, loaded a fiber ahead
   auto meta_i = [&](uint32_t q) { return __ldg(fidx + min(q, nfib - 1)); };
@@ -291,6 +293,214 @@ __global__ void __launch_bounds__(256, MB) k_mttkrp(const Args<T> a) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// Branch-free 3-D traversal ("flat" kernel). Same teams and nonzero ranges as
+// k_mttkrp, but a fiber start no longer sends its team down a separate code
+// path: every lane locates the fiber of its own nonzero from the block's
+// fiber-start ballot (popcount of the flags at or below it), loads that
+// fiber's metadata only if its nonzero opens the fiber, and the per-nonzero
+// step is the same straight-line code for every team of the warp, with the
+// fiber-open work predicated. Slice changes (rare: one per slice run) take a
+// slower variant of the block, chosen per warp. Arithmetic uses the packed
+// FP32x2 FMA of sm_100 (two fused multiply-adds per instruction).
+__device__ __forceinline__ float4 pfma(float4 a, float4 b, float4 c) {
+  const float2 lo = __ffma2_rn(make_float2(a.x, a.y), make_float2(b.x, b.y), make_float2(c.x, c.y));
+  const float2 hi = __ffma2_rn(make_float2(a.z, a.w), make_float2(b.z, b.w), make_float2(c.z, c.w));
+  return make_float4(lo.x, lo.y, hi.x, hi.y);
+}
+__device__ __forceinline__ float4 pfma_s(float s, float4 b, float4 c) {
+  const float2 ss = make_float2(s, s);
+  const float2 lo = __ffma2_rn(ss, make_float2(b.x, b.y), make_float2(c.x, c.y));
+  const float2 hi = __ffma2_rn(ss, make_float2(b.z, b.w), make_float2(c.z, c.w));
+  return make_float4(lo.x, lo.y, hi.x, hi.y);
+}
+__device__ __forceinline__ float4 pmul(float4 a, float4 b) {
+  const float2 lo = __fmul2_rn(make_float2(a.x, a.y), make_float2(b.x, b.y));
+  const float2 hi = __fmul2_rn(make_float2(a.z, a.w), make_float2(b.z, b.w));
+  return make_float4(lo.x, lo.y, hi.x, hi.y);
+}
+__device__ __forceinline__ float4 pmul_s(float s, float4 b) {
+  const float2 ss = make_float2(s, s);
+  const float2 lo = __fmul2_rn(ss, make_float2(b.x, b.y));
+  const float2 hi = __fmul2_rn(ss, make_float2(b.z, b.w));
+  return make_float4(lo.x, lo.y, hi.x, hi.y);
+}
+
+// OUT 0 (slice rows): acc_s[a] += U1[b] (.) sum_fiber v U2[k]; the fiber's
+//   U1 row is requested when the fiber opens and used when it closes.
+// OUT 1 (fiber rows): out[b] += U0[a] (.) sum_fiber v U2[k], one vector
+//   reduction per fiber.
+// OUT 2 (leaf rows): out[k] += v U0[a] (.) U1[b], one reduction per nonzero;
+//   the fiber's U1 rows for a batch are requested before the batch.
+template <int OUT, int G, int V, class T, int MB, int PFX>
+__global__ void __launch_bounds__(256, MB) k_mttkrp_flat(const Args<T> a) {
+  constexpr uint32_t R = 4 * G * V;
+  constexpr uint32_t FLAG = 0x80000000u;
+  constexpr int PF = G > PFX ? PFX : G;
+  constexpr uint32_t GMASK = G == 32 ? FULL : ((1u << G) - 1u);
+  const int lane = threadIdx.x & 31;
+  const int tl = lane & (G - 1);
+  const int tb = lane - tl;
+  const uint32_t le_mask = tl == 31 ? FULL : ((2u << tl) - 1u);  // lanes 0..tl of the team
+  const float* __restrict__ vals = a.vals;
+  const uint32_t* __restrict__ leaf = a.leaf;
+  const uint32_t* __restrict__ fidx = a.fidx;
+  const uint32_t* __restrict__ like = a.like;
+  const uint32_t chunk = a.chunk;
+  const T* __restrict__ U0 = a.U[0];
+  const T* __restrict__ U1 = a.U[1];
+  const T* __restrict__ U2 = a.U[2];
+  float* __restrict__ out = a.out;
+  const uint32_t c0 = (uint32_t)tl * 4;
+  auto ld = [&](const T* U, uint32_t row, int v) -> float4 {
+    return Row<T>::load(U + (uint64_t)row * R, c0 + (uint32_t)(v * G * 4));
+  };
+  auto rd = [&](uint32_t row, int v, float4 x) { red4(out + (uint64_t)row * R + c0 + v * G * 4, x); };
+
+  const uint64_t team = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) / G;
+  const bool active = team * chunk < a.nnz;
+  const uint64_t x0 = active ? team * chunk : a.nnz - 1;
+  const uint64_t x1 = active ? min(x0 + chunk, a.nnz) : x0;
+
+  uint32_t f = a.cfib ? (active ? __ldg(a.cfib + team) : a.nfib - 1) : find_fiber(a.fptr, a.nfib, x0);
+  uint32_t cb = __ldg(fidx + f);  // open fiber's o1
+  uint32_t ca = __ldg(like + f);  // open slice's o0
+  float4 accf[V], accs[V], rowB[V], rowA[V];
+#pragma unroll
+  for (int v = 0; v < V; ++v) {
+    accf[v] = accs[v] = f4(0.f);
+    if constexpr (OUT == 0) rowB[v] = ld(U1, cb, v);
+    if constexpr (OUT == 1) rowA[v] = ld(U0, ca, v);
+    if constexpr (OUT == 2) { rowA[v] = ld(U0, ca, v); rowB[v] = rowA[v] * ld(U1, cb, v); }
+  }
+
+  // Block pipeline: when block i (G nonzeros) is processed, its indices,
+  // values and fiber metadata are in registers; block i+1's indices are in
+  // flight or ready (their fiber flags decide which metadata to request) and
+  // block i+2's are requested.
+  auto load_kv = [&](uint32_t itb, uint32_t& kk, float& vq) {
+    const uint64_t xx = x0 + itb + tl;
+    kk = 0;
+    vq = 0.f;
+    if (itb < chunk && xx < x1) { kk = __ldg(leaf + xx); vq = __ldg(vals + xx); }
+  };
+  auto load_meta = [&](uint32_t itb, uint32_t kk, uint32_t& fm_, uint32_t& mb_, uint32_t& ma_) {
+    const bool fl_ = (kk & FLAG) && (itb + tl != 0);
+    fm_ = (__ballot_sync(FULL, fl_) >> tb) & GMASK;
+    mb_ = 0;
+    ma_ = 0;
+    if (fl_) {
+      const uint32_t fib = f + __popc(fm_ & le_mask);
+      mb_ = __ldg(fidx + fib);
+      ma_ = __ldg(like + fib);
+    }
+    f += __popc(fm_);
+  };
+  uint32_t kc, kn, fmc, mbc, mac;
+  float vc, vn;
+  load_kv(0, kc, vc);
+  load_kv(G, kn, vn);
+  load_meta(0, kc, fmc, mbc, mac);
+  for (uint32_t it = 0; it < chunk; it += G) {
+    const uint64_t xb = x0 + it;
+    uint32_t kf;
+    float vf;
+    load_kv(it + 2 * G, kf, vf);
+    uint32_t fmn, mbn, man;
+    load_meta(it + G, kn, fmn, mbn, man);
+    const uint32_t kv = kc, fm = fmc, mb = mbc, ma = mac;
+    const float vv = vc;
+    kc = kn; vc = vn; fmc = fmn; mbc = mbn; mac = man;
+    kn = kf; vn = vf;
+    const bool slow = __ballot_sync(FULL, ((fm >> tl) & 1u) && ma != ca) != 0u;  // a slice changes in this block
+    const uint32_t k = kv & ~FLAG;
+
+    auto block = [&](auto slow_tag) {
+      constexpr bool SLOW = decltype(slow_tag)::value;
+#pragma unroll
+      for (int jb = 0; jb < G; jb += PF) {
+        float4 rows[PF][V];
+        uint32_t kj[PF], bj[PF];
+#pragma unroll
+        for (int j = 0; j < PF; ++j) {
+          kj[j] = __shfl_sync(FULL, k, tb + jb + j);
+          if constexpr (OUT == 2) bj[j] = __shfl_sync(FULL, mb, tb + jb + j);
+          if constexpr (OUT != 2) {
+#pragma unroll
+            for (int v = 0; v < V; ++v) rows[j][v] = ld(U2, kj[j], v);
+          } else {
+            if ((fm >> (jb + j)) & 1u) {
+#pragma unroll
+              for (int v = 0; v < V; ++v) rows[j][v] = ld(U1, bj[j], v);
+            }
+          }
+        }
+#pragma unroll
+        for (int j = 0; j < PF; ++j) {
+          const float val = __shfl_sync(FULL, vv, tb + jb + j);
+          if constexpr (OUT != 2) bj[j] = __shfl_sync(FULL, mb, tb + jb + j);
+          uint32_t aj = 0;
+          if constexpr (SLOW) aj = __shfl_sync(FULL, ma, tb + jb + j);
+          if ((fm >> (jb + j)) & 1u) {
+            if constexpr (OUT == 0) {
+#pragma unroll
+              for (int v = 0; v < V; ++v) { accs[v] = pfma(rowB[v], accf[v], accs[v]); accf[v] = f4(0.f); }
+              if constexpr (SLOW) {
+                if (aj != ca) {
+#pragma unroll
+                  for (int v = 0; v < V; ++v) { rd(ca, v, accs[v]); accs[v] = f4(0.f); }
+                  ca = aj;
+                }
+              }
+#pragma unroll
+              for (int v = 0; v < V; ++v) rowB[v] = ld(U1, bj[j], v);
+            } else if constexpr (OUT == 1) {
+#pragma unroll
+              for (int v = 0; v < V; ++v) { rd(cb, v, pmul(rowA[v], accf[v])); accf[v] = f4(0.f); }
+              cb = bj[j];
+              if constexpr (SLOW) {
+                if (aj != ca) {
+                  ca = aj;
+#pragma unroll
+                  for (int v = 0; v < V; ++v) rowA[v] = ld(U0, ca, v);
+                }
+              }
+            } else {
+              if constexpr (SLOW) {
+                if (aj != ca) {
+                  ca = aj;
+#pragma unroll
+                  for (int v = 0; v < V; ++v) rowA[v] = ld(U0, ca, v);
+                }
+              }
+#pragma unroll
+              for (int v = 0; v < V; ++v) rowB[v] = pmul(rowA[v], rows[j][v]);
+            }
+          }
+          if constexpr (OUT != 2) {
+#pragma unroll
+            for (int v = 0; v < V; ++v) accf[v] = pfma_s(val, rows[j][v], accf[v]);
+          } else {
+            if (xb + jb + j < x1) {
+#pragma unroll
+              for (int v = 0; v < V; ++v) rd(kj[j], v, pmul_s(val, rowB[v]));
+            }
+          }
+        }
+      }
+    };
+    if (slow) block(std::true_type{});
+    else block(std::false_type{});
+  }
+  if (active) {
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      if constexpr (OUT == 0) rd(ca, v, pfma(rowB[v], accf[v], accs[v]));
+      if constexpr (OUT == 1) rd(cb, v, pmul(rowA[v], accf[v]));
+    }
+  }
+}
+
 template <int ND, int OUT, int G, int V, class T>
 cudaError_t launch_one(const Args<T>& a, int threads, int mb, cudaStream_t s) {
   const uint64_t teams = (a.nnz + a.chunk - 1) / a.chunk;
@@ -305,8 +515,33 @@ cudaError_t launch_one(const Args<T>& a, int threads, int mb, cudaStream_t s) {
   return cudaGetLastError();
 }
 
+template <int OUT, int G, int V, class T>
+cudaError_t launch_flat(const Args<T>& a, int threads, int mb, cudaStream_t s) {
+  const uint64_t teams = (a.nnz + a.chunk - 1) / a.chunk;
+  const uint64_t thr = teams * G;
+  const uint64_t blocks = (thr + threads - 1) / threads;
+  switch (mb) {
+    case 1: k_mttkrp_flat<OUT, G, V, T, 2, 8><<<(unsigned)blocks, threads, 0, s>>>(a); break;
+    case 3: k_mttkrp_flat<OUT, G, V, T, 4, 4><<<(unsigned)blocks, threads, 0, s>>>(a); break;
+    case 4: k_mttkrp_flat<OUT, G, V, T, 5, 4><<<(unsigned)blocks, threads, 0, s>>>(a); break;
+    default: k_mttkrp_flat<OUT, G, V, T, 3, 8><<<(unsigned)blocks, threads, 0, s>>>(a); break;
+  }
+  return cudaGetLastError();
+}
+
+// kern: 1 = per-team fiber walk (k_mttkrp), 2 = branch-free walk (3-D only)
 template <int ND, int G, int V, class T>
-cudaError_t launch_lvl(const Args<T>& a, int lvl, int threads, int mb, cudaStream_t s) {
+cudaError_t launch_lvl(const Args<T>& a, int lvl, int kern, int threads, int mb, cudaStream_t s) {
+  if constexpr (ND == 3) {
+    if (kern == 2) {
+      switch (lvl) {
+        case 0: return launch_flat<0, G, V, T>(a, threads, mb, s);
+        case 1: return launch_flat<1, G, V, T>(a, threads, mb, s);
+        case 2: return launch_flat<2, G, V, T>(a, threads, mb, s);
+        default: return cudaErrorInvalidValue;
+      }
+    }
+  }
   switch (lvl) {
     case 0: return launch_one<ND, 0, G, V, T>(a, threads, mb, s);
     case 1: return launch_one<ND, 1, G, V, T>(a, threads, mb, s);
@@ -318,11 +553,11 @@ cudaError_t launch_lvl(const Args<T>& a, int lvl, int threads, int mb, cudaStrea
 }
 
 template <class T>
-cudaError_t launch_R(const Args<T>& a, int nd, int lvl, int threads, int mb, cudaStream_t s) {
+cudaError_t launch_R(const Args<T>& a, int nd, int lvl, int kern, int threads, int mb, cudaStream_t s) {
 #define MMCSF_RCASE(RR, GG, VV)                                                        \
   case RR:                                                                            \
-    return nd == 3 ? launch_lvl<3, GG, VV, T>(a, lvl, threads, mb, s)                 \
-                   : launch_lvl<4, GG, VV, T>(a, lvl, threads, mb, s);
+    return nd == 3 ? launch_lvl<3, GG, VV, T>(a, lvl, kern, threads, mb, s)           \
+                   : launch_lvl<4, GG, VV, T>(a, lvl, kern, threads, mb, s);
   switch (a.R) {
     MMCSF_RCASE(4, 1, 1)
     MMCSF_RCASE(8, 2, 1)
@@ -375,6 +610,9 @@ int part_mttkrp(const mmcsf_format* F, const CsfPart& P, int mode, int R, int dt
   int chunk = cfg && cfg->chunk > 0 ? cfg->chunk : default_chunk(R);
   int threads = cfg && cfg->block_threads > 0 ? cfg->block_threads : 256;
   const int mb = cfg && cfg->min_blocks > 0 ? cfg->min_blocks : 2;
+  const int kern = cfg && cfg->kernel > 0 ? cfg->kernel : (P.nd == 3 ? 2 : 1);
+  if (kern != 1 && kern != 2) return set_error(MMCSF_ERR_INVALID, "kernel must be 0, 1 or 2");
+  const int slot = CsfPart::cfib_slot((uint64_t)chunk);
   if (threads % 32 || threads > 256) return set_error(MMCSF_ERR_INVALID, "block_threads must be a multiple of 32, <= 256");
   cudaError_t e;
   if (dtype == MMCSF_DTYPE_F32) {
@@ -387,13 +625,14 @@ int part_mttkrp(const mmcsf_format* F, const CsfPart& P, int mode, int R, int dt
     a.fpar = P.fpar.as<uint32_t>();
     a.sidx1 = P.nd == 4 ? P.idx[1].as<uint32_t>() : nullptr;
     a.like = P.fbr_like.as<uint32_t>();
+    a.cfib = slot >= 0 && P.cfib[slot].p ? P.cfib[slot].as<uint32_t>() : nullptr;
     a.nnz = P.nnz;
     a.nfib = (uint32_t)P.n_fibers();
     a.chunk = (uint32_t)chunk;
     a.R = (uint32_t)R;
     for (int l = 0; l < P.nd; ++l) a.U[l] = static_cast<const float*>(U[P.order[l]]);
     a.out = out;
-    e = launch_R<float>(a, P.nd, lvl, threads, mb, s);
+    e = launch_R<float>(a, P.nd, lvl, kern, threads, mb, s);
   } else {
     Args<__nv_bfloat16> a{};
     a.vals = vals_override ? vals_override : P.vals.as<float>();
@@ -404,13 +643,14 @@ int part_mttkrp(const mmcsf_format* F, const CsfPart& P, int mode, int R, int dt
     a.fpar = P.fpar.as<uint32_t>();
     a.sidx1 = P.nd == 4 ? P.idx[1].as<uint32_t>() : nullptr;
     a.like = P.fbr_like.as<uint32_t>();
+    a.cfib = slot >= 0 && P.cfib[slot].p ? P.cfib[slot].as<uint32_t>() : nullptr;
     a.nnz = P.nnz;
     a.nfib = (uint32_t)P.n_fibers();
     a.chunk = (uint32_t)chunk;
     a.R = (uint32_t)R;
     for (int l = 0; l < P.nd; ++l) a.U[l] = static_cast<const __nv_bfloat16*>(U[P.order[l]]);
     a.out = out;
-    e = launch_R<__nv_bfloat16>(a, P.nd, lvl, threads, mb, s);
+    e = launch_R<__nv_bfloat16>(a, P.nd, lvl, kern, threads, mb, s);
   }
   if (e != cudaSuccess) return set_error(MMCSF_ERR_CUDA, "MTTKRP launch failed: %s", cudaGetErrorString(e));
   if (launches) ++*launches;
@@ -440,6 +680,7 @@ int mttkrp_mode_vals(const mmcsf_format* F, int mode, int R, int dtype, const vo
   if (cfg) c = *cfg;
   if (c.chunk == 0) c.chunk = F->plan_chunk[mode];
   if (c.min_blocks == 0) c.min_blocks = F->plan_mb[mode];
+  if (c.kernel == 0) c.kernel = F->plan_kernel[mode];
   if (trav == 2) {
     const CsfPart& V = F->views[mode];
     if (!V.present) return set_error(MMCSF_ERR_INVALID, "no view for mode %d (build with views)", mode);
@@ -661,15 +902,18 @@ extern "C" int mmcsf_tune(mmcsf_format* F, int R, int factor_dtype, const void* 
   for (int i = 0; i < nmodes && st == MMCSF_OK; ++i) {
     const int m = F->impl == MMCSF_IMPL_MMCSF ? i : F->mode;
     float best = 1e30f;
-    int bt = 1, bc = 512, bm = 2;
+    int bt = 1, bc = 512, bm = 2, bk = 1;
+    const int nkern = F->nd == 3 ? 2 : 1;
     for (int trav = 1; trav <= 2 && st == MMCSF_OK; ++trav) {
       if (trav == 2 && !F->views[m].present) continue;
+      for (int kern = 1; kern <= nkern && st == MMCSF_OK; ++kern)
       for (int mbv = 1; mbv <= 4; ++mbv) {
         for (int c : chunks) {
           mmcsf_kernel_cfg cfg{};
           cfg.chunk = c;
           cfg.traversal = trav;
           cfg.min_blocks = mbv;
+          cfg.kernel = kern;
           float ms = 0;
           for (int rep = 0; rep < 2; ++rep) {  // the second run is timed
             if ((st = mmcsf_mttkrp(F, m, R, factor_dtype, d_factors, d_outs[m], &cfg, stream)) != MMCSF_OK) break;
@@ -682,7 +926,7 @@ extern "C" int mmcsf_tune(mmcsf_format* F, int R, int factor_dtype, const void* 
             cudaEventElapsedTime(&ms, e0, e1);
           }
           if (st != MMCSF_OK) break;
-          if (ms < best) { best = ms; bt = trav; bc = c; bm = mbv; }
+          if (ms < best) { best = ms; bt = trav; bc = c; bm = mbv; bk = kern; }
         }
         if (st != MMCSF_OK) break;
       }
@@ -690,10 +934,12 @@ extern "C" int mmcsf_tune(mmcsf_format* F, int R, int factor_dtype, const void* 
     F->plan_traversal[m] = bt;
     F->plan_chunk[m] = bc;
     F->plan_mb[m] = bm;
+    F->plan_kernel[m] = bk;
     if (plan) {
       plan->traversal[m] = bt;
       plan->chunk[m] = bc;
       plan->min_blocks[m] = bm;
+      plan->kernel[m] = bk;
       plan->ms[m] = best;
     }
   }
@@ -707,11 +953,13 @@ extern "C" int mmcsf_set_plan(mmcsf_format* F, const mmcsf_plan* plan) {
   for (int m = 0; m < F->nd; ++m) {
     if (plan->traversal[m] == 2 && !F->views[m].present)
       return set_error(MMCSF_ERR_INVALID, "plan uses a view for mode %d that was not built", m);
-    if (plan->traversal[m] < 0 || plan->traversal[m] > 2 || plan->chunk[m] < 0)
+    if (plan->traversal[m] < 0 || plan->traversal[m] > 2 || plan->chunk[m] < 0 || plan->kernel[m] < 0 ||
+        plan->kernel[m] > 2 || (plan->kernel[m] == 2 && F->nd != 3))
       return set_error(MMCSF_ERR_INVALID, "bad plan entry for mode %d", m);
     F->plan_traversal[m] = plan->traversal[m];
     F->plan_chunk[m] = plan->chunk[m];
     F->plan_mb[m] = plan->min_blocks[m];
+    F->plan_kernel[m] = plan->kernel[m];
   }
   return MMCSF_OK;
 }

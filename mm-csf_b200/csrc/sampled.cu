@@ -37,6 +37,7 @@ __device__ __forceinline__ float4 mul4(float4 a, float4 b) {
 template <class T>
 struct SArgs {
   const uint32_t *leaf, *fptr, *fidx, *fpar, *sidx1, *like;
+  const uint32_t* cfib;  // first fiber of every chunk, or null (binary search)
   uint64_t nnz;
   uint32_t nfib, chunk;
   const T* U[4];      // by level
@@ -63,7 +64,7 @@ __global__ void __launch_bounds__(256) k_sampled(const SArgs<T> a) {
   const uint64_t x0 = active ? team * a.chunk : a.nnz - 1;
   const uint64_t x1 = active ? min(x0 + a.chunk, a.nnz) : x0;
   auto col = [&](int v) { return (uint32_t)(tl + v * G) * 4; };
-  uint32_t f = find_fiber(a.fptr, a.nfib, x0);
+  uint32_t f = a.cfib ? (active ? __ldg(a.cfib + team) : a.nfib - 1) : find_fiber(a.fptr, a.nfib, x0);
   float4 w[V];
   auto weights = [&]() {
     const uint32_t c = __ldg(a.fidx + f);
@@ -173,6 +174,7 @@ extern "C" int mmcsf_sampled_model(const mmcsf_format* F, int R, int factor_dtyp
     a.nnz = P->nnz;
     a.nfib = (uint32_t)P->n_fibers();
     a.chunk = 256;
+    a.cfib = P->cfib[CsfPart::cfib_slot(256)].p ? P->cfib[CsfPart::cfib_slot(256)].as<uint32_t>() : nullptr;
     for (int l = 0; l < P->nd; ++l) a.U[l] = static_cast<const T*>(d_factors[P->order[l]]);
     a.lam = d_lambda;
     a.out = d_out;

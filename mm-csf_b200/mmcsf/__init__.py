@@ -359,7 +359,7 @@ class Format:
         n = self.nd if self.impl == IMPL_MMCSF else 1
         modes = range(self.nd) if self.impl == IMPL_MMCSF else [self.mode]
         return {m: {"traversal": pl.traversal[m], "chunk": pl.chunk[m], "min_blocks": pl.min_blocks[m],
-                    "ms": pl.ms[m]} for m in list(modes)[:n]}
+                    "kernel": pl.kernel[m], "ms": pl.ms[m]} for m in list(modes)[:n]}
 
     def set_plan(self, plan):
         pl = Plan()
@@ -367,6 +367,7 @@ class Format:
             pl.traversal[m] = e["traversal"]
             pl.chunk[m] = e["chunk"]
             pl.min_blocks[m] = e.get("min_blocks", 0)
+            pl.kernel[m] = e.get("kernel", 0)
         check(lib().mmcsf_set_plan(self._h, ctypes.byref(pl)))
 
     def cpd(self, rank, max_iters=10, tol=1e-5, precision="fp32", init=None, seed=0, graph=True, stream=None):

@@ -40,12 +40,12 @@ class PartInfo(ctypes.Structure):
 
 class KernelCfg(ctypes.Structure):
     _fields_ = [("chunk", c_int), ("block_threads", c_int), ("traversal", c_int), ("min_blocks", c_int),
-                ("reserved", c_int * 4)]
+                ("kernel", c_int), ("reserved", c_int * 3)]
 
 
 class Plan(ctypes.Structure):
     _fields_ = [("traversal", c_int * 4), ("chunk", c_int * 4), ("min_blocks", c_int * 4),
-                ("ms", ctypes.c_float * 4)]
+                ("kernel", c_int * 4), ("ms", ctypes.c_float * 4)]
 
 
 class CpdOpts(ctypes.Structure):

@@ -87,23 +87,38 @@ def poisson_loss(fmt, factors, y, lam=None, precision="fp32", eps=1e-10):
     return total - (y * torch.log(xhat + eps)).sum()
 
 
-def gcp_poisson(fmt, rank, iters=100, lr=1e-2, precision="fp32", init=None, seed=0, eps=1e-10,
-                stop_loss=None):
+def gcp_poisson(fmt, rank, iters=100, lr=0.05, precision="fp32", init=None, seed=0, eps=1e-10,
+                stop_loss=None, rescale=True):
     """Projected-Adam Poisson CP (nonnegative factors, no lambda).
 
-    init: optional list of dims[m] x rank FP32 CUDA tensors (copied).
-    stop_loss: stop once the loss is at or below this value (checked every
-    iteration on the host, so it costs one sync per iteration; None runs all
-    iterations without host syncs inside the loop).
-    Returns dict(loss=[...], ms=[...] cumulative device time per iteration,
-    factors, iters, seconds)."""
+    init: optional list of dims[m] x rank nonnegative FP32 CUDA tensors
+    (copied; default uniform [0.25, 0.75)). rescale: scale the initial factors
+    so the model's total mass equals the tensor's (sum of y), the usual GCP
+    start. lr is relative: Adam's step size is lr times the mean initial
+    factor entry, so one setting serves tensors of any size.
+    stop_loss: stop once the loss is at or below this value (one host sync
+    per iteration; None runs every iteration without host syncs).
+    Returns dict(loss=[...], ms=[...] cumulative device time after each
+    iteration, factors, iters, seconds)."""
     dev = torch.device("cuda")
     g = torch.Generator(device="cpu").manual_seed(seed)
     if init is None:
         init = [torch.rand((d, rank), generator=g).to(dev) * 0.5 + 0.25 for d in fmt.dims]
-    masters = [t.detach().clone().float().contiguous().requires_grad_(True) for t in init]
+    masters = [t.detach().clone().float().contiguous() for t in init]
     y = fmt.values()
-    opt = torch.optim.Adam(masters, lr=lr)
+    if rescale:
+        with torch.no_grad():
+            cs = masters[0].sum(0)
+            for f in masters[1:]:
+                cs = cs * f.sum(0)
+            ratio = float(y.double().sum()) / max(float(cs.double().sum()), 1e-300)
+            k = ratio ** (1.0 / len(masters))
+            for f in masters:
+                f.mul_(k)
+    step = lr * float(torch.cat([f.flatten() for f in masters]).mean())
+    for f in masters:
+        f.requires_grad_(True)
+    opt = torch.optim.Adam(masters, lr=step)
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(iters + 1)]
     losses = []
     torch.cuda.synchronize()
@@ -127,4 +142,4 @@ def gcp_poisson(fmt, rank, iters=100, lr=1e-2, precision="fp32", init=None, seed
     secs = time.perf_counter() - t0
     ms = [ev[0].elapsed_time(ev[i + 1]) for i in range(n_done)]
     return {"loss": [float(v) for v in torch.stack(losses).cpu()], "ms": ms, "iters": n_done, "seconds": secs,
-            "factors": [p.detach() for p in masters]}
+            "factors": [p.detach() for p in masters], "step": step}

@@ -44,6 +44,9 @@ WORKLOADS = {
                      desc="500000x2000000x20000, 100M nnz, Zipf(1.1) per mode, lognormal values, R=32"),
     "uniform3d": dict(dims=[1000, 1000, 1000], nnz=100_000, dist=[0, 0, 0], zipf=1.0, val=0, R=32,
                       desc="1000^3, 100k uniform nnz, R=32"),
+    "skewed4d": dict(dims=[1000000, 20000, 5000, 200], nnz=140_000_000, dist=[1, 1, 1, 0], zipf=1.0, val=2, R=32,
+                     desc="1000000x20000x5000x200, 140M nnz, Zipf(1.0) modes 0-2, uniform mode 3, integer values "
+                          "1-50, R=32; B-CSF / HB-CSF per mode beside MM-CSF all modes"),
 }
 
 
@@ -65,6 +68,7 @@ def parse():
     ap.add_argument("--no-tune", action="store_true")
     ap.add_argument("--plan-file", default="", help="JSON plan (as printed by a tuned run) to use instead of tuning")
     ap.add_argument("--no-cp", action="store_true", help="skip the CP-ALS and Poisson gradient-CP sections")
+    ap.add_argument("--no-formats", action="store_true", help="4-D workloads: skip the B-CSF / HB-CSF section")
     ap.add_argument("--cp-scale", type=float, default=1.0, help="scale the CP workloads' nonzero counts")
     return ap.parse_args()
 
@@ -153,8 +157,9 @@ def workload_stats(inds_dev, dims, order):
     """Rows touched per mode and fiber count (no split) with torch ops."""
     import torch
     rows = [int(torch.unique(i).numel()) for i in inds_dev]
-    o0, o1 = order[0], order[1]
-    key = inds_dev[o0].long() * dims[o1] + inds_dev[o1].long()
+    key = inds_dev[order[0]].long()
+    for q in order[1:len(order) - 1]:  # leaf fibers: distinct prefixes of all but the leaf level
+        key = key * dims[q] + inds_dev[q].long()
     nfib = int(torch.unique(key).numel())
     return rows, nfib
 
@@ -202,6 +207,37 @@ GCP = dict(dims=[100000, 50000, 10000], nnz=20_000_000, zipf=1.05, planted=32, R
            desc="100000x50000x10000, 20M nnz, Zipf(1.05) per mode, Poisson counts of a planted nonnegative "
                 "rank-32 CP, R=32, projected Adam (step 0.05 x mean initial entry, initial mass = data mass) on the Poisson "
                 "loss over every entry")
+
+
+def format_section(X, dims, R, tdt):
+    """Single-mode B-CSF (-t 8) and HB-CSF (-t 10) MTTKRP for every mode, each
+    format built for that mode and tuned, timed like the MM-CSF steps."""
+    import torch
+    import mmcsf
+    out = {}
+    g = torch.Generator(device="cuda").manual_seed(99)
+    U = [torch.rand(d, R, device="cuda", generator=g).to(tdt) for d in dims]
+    for name, impl in (("bcsf", mmcsf.IMPL_BCSF), ("hbcsf", mmcsf.IMPL_HBCSF)):
+        ms = []
+        for m in range(len(dims)):
+            F = mmcsf.Format(X, impl=impl, mode=m)
+            o = torch.empty(dims[m], R, device="cuda")
+            outs = [o if q == m else torch.empty(1, R, device="cuda") for q in range(len(dims))]
+            F.tune(U, outs)
+            for _ in range(3):
+                F.mttkrp(m, U, o)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(10):
+                F.mttkrp(m, U, o)
+            e1.record()
+            torch.cuda.synchronize()
+            ms.append(e0.elapsed_time(e1) / 10)
+            del F
+            torch.cuda.empty_cache()
+        out[name] = {"mode_ms": ms, "all_mode_ms": sum(ms)}
+    return out
 
 
 def cp_section(seed, scale):
@@ -458,6 +494,11 @@ def main():
                "ms_per_step": ts * 1e3,
                "sample": f"first {S} of {nnz} nonzeros, all {nd} modes, MTTKRP_COO_CPU serial as shipped, "
                          f"extrapolated x{nnz / S:.1f}"}
+    formats = None
+    if nd == 4 and not a.no_formats:
+        fm = format_section(X, dims, R, tdt)
+        fm["mmcsf"] = {"mode_ms": mode_ms, "all_mode_ms": ms_per_step}
+        formats = fm
     cp = None
     if not a.no_cp:
         del F, X, U, outs
@@ -469,7 +510,8 @@ def main():
             "config": config, "mode_ms": mode_ms, "mode_algorithmic_bytes": per_mode, "plan": plan, "format": info,
             "roofline": roofline,
             "cpu_baseline": cpu,
-            "e2e": e2e, "gpu_launches": launches_per_step * a.steps, "clocks": clocks, "cp": cp}
+            "e2e": e2e, "gpu_launches": launches_per_step * a.steps, "clocks": clocks, "cp": cp,
+            "formats": formats}
     print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()

@@ -432,6 +432,10 @@ static int build_csf(int nd, const int* order, uint64_t n, DevBuf* sorted, DevBu
   MMCSF_CUDA(cudaMemcpyAsync(P.fbr_like.as<uint32_t>() + n1, o[0] + (n - 1), 4, cudaMemcpyDeviceToDevice, s));
 
   // --- per-nonzero arrays
+  if (nd == 3) {  // o1 of every nonzero, read by the per-nonzero traversal
+    MMCSF_CUDA(P.mid.alloc(n * 4));
+    MMCSF_CUDA(cudaMemcpyAsync(P.mid.p, o[1], n * 4, cudaMemcpyDeviceToDevice, s));
+  }
   P.leaf = std::move(sorted[order[nd - 1]]);
   P.vals = std::move(vals);
   if (keep_coo) {
@@ -489,6 +493,11 @@ __global__ void k_chunk_fibers(const uint32_t* __restrict__ fptr, uint32_t nfib,
 
 int chunk_fibers(CsfPart& P, cudaStream_t s, Launches& L) {
   if (!P.present || P.nnz == 0 || P.n_fibers() == 0) return MMCSF_OK;
+  if (P.mid.p) {  // first nonzero of every slice: fiber pointer of the slice's first fiber
+    MMCSF_CUDA(P.snz.alloc((P.n[0] + 1) * 4));
+    MMCSF_CUDA(gather_u32(P.ptr[1].as<uint32_t>(), P.ptr[0].as<uint32_t>(), P.snz.as<uint32_t>(), P.n[0] + 1, s));
+    ++L.n;
+  }
   for (int i = 0; i < CsfPart::N_CHUNK_SIZES; ++i) {
     const uint64_t chunk = 128ull << i, nch = (P.nnz + chunk - 1) / chunk;
     MMCSF_CUDA(P.cfib[i].alloc(nch * 4));
@@ -496,6 +505,12 @@ int chunk_fibers(CsfPart& P, cudaStream_t s, Launches& L) {
                                                                  (uint32_t)P.n_fibers(), chunk, nch,
                                                                  P.cfib[i].as<uint32_t>());
     LCHECK(L);
+    if (P.mid.p) {  // the same search over the slices' first nonzeros
+      MMCSF_CUDA(P.cslc[i].alloc(nch * 4));
+      k_chunk_fibers<<<(unsigned)((nch + 255) / 256), 256, 0, s>>>(P.snz.as<uint32_t>(), (uint32_t)P.n[0],
+                                                                   chunk, nch, P.cslc[i].as<uint32_t>());
+      LCHECK(L);
+    }
   }
   return MMCSF_OK;
 }
@@ -599,7 +614,10 @@ extern "C" int mmcsf_build(mmcsf_coo* X, const mmcsf_build_opts* opts, void* str
       MMCSF_CUDA(cudaStreamSynchronize(s));
     }
   }
-  if (opts->impl == MMCSF_IMPL_HBCSF) MMCSF_TRY(build_hyb(Fm, P, s, &L.n));
+  if (opts->impl == MMCSF_IMPL_HBCSF) {
+    MMCSF_TRY(build_hyb(Fm, P, s, &L.n));
+    for (int p = 0; p < 4; ++p) Fm->parts[p].mid.release();  // the HB-CSF CSF part uses the fiber walks
+  }
   for (int p = 0; p < 4; ++p) MMCSF_TRY(chunk_fibers(Fm->parts[p], s, L));
   for (int m = 0; m < 4; ++m) MMCSF_TRY(chunk_fibers(Fm->views[m], s, L));
   MMCSF_CUDA(cudaStreamSynchronize(s));

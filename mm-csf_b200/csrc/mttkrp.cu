@@ -77,6 +77,11 @@ struct Args {
   const uint32_t* sidx1;  // 4-D: fbrS index (o1)
   const uint32_t* like;   // o0 per level-1 entry (3-D: fiber, 4-D: fbrS)
   const uint32_t* cfib;   // first fiber of every team's chunk, or null (binary search)
+  const uint32_t* mid;    // 3-D per-nonzero walk: o1 of every nonzero
+  const uint32_t* snz;    // ... first nonzero of every slice [nslc + 1]
+  const uint32_t* sidx;   // ... slice index (o0) of every slice
+  const uint32_t* cslc;   // ... slice of every team's chunk start, or null (binary search)
+  uint32_t nslc;
   uint64_t nnz;
   uint32_t nfib;
   uint32_t chunk;
@@ -501,6 +506,145 @@ __global__ void __launch_bounds__(256, MB) k_mttkrp_flat(const Args<T> a) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// Per-nonzero 3-D traversal ("rows" kernel) for the slice-level (OUT 0) and
+// leaf-level (OUT 2) outputs. Every nonzero carries its middle-level index
+// (`mid`), so a team needs no fiber bookkeeping: per nonzero it combines the
+// middle row and the leaf row, adding v * U1[b] (.) U2[k] to the open slice's
+// accumulator (OUT 0) or scattering v * U0[a] (.) U1[b] to the leaf row
+// (OUT 2). The middle row repeats along a fiber, so most of its gathers hit
+// L1 (gathering it unconditionally measured faster than predicating the
+// repeats away). Slice changes come from the slices' first nonzero positions
+// (`snz`), not from flags, and a block with a slice change takes a slower
+// variant.
+template <int OUT, int G, int V, class T, int MB, int PFX>
+__global__ void __launch_bounds__(256, MB) k_mttkrp_rows(const Args<T> a) {
+  constexpr uint32_t R = 4 * G * V;
+  constexpr uint32_t FLAG = 0x80000000u;
+  constexpr int PF = G > PFX ? PFX : G;
+  const int lane = threadIdx.x & 31;
+  const int tl = lane & (G - 1);
+  const int tb = lane - tl;
+  const float* __restrict__ vals = a.vals;
+  const uint32_t* __restrict__ leaf = a.leaf;
+  const uint32_t* __restrict__ mid = a.mid;
+  const uint32_t* __restrict__ snz = a.snz;
+  const uint32_t* __restrict__ sidx = a.sidx;
+  const uint32_t chunk = a.chunk, nslc = a.nslc;
+  const T* __restrict__ U0 = a.U[0];
+  const T* __restrict__ U1 = a.U[1];
+  const T* __restrict__ U2 = a.U[2];
+  float* __restrict__ out = a.out;
+  const uint32_t c0 = (uint32_t)tl * 4;
+  auto ld = [&](const T* U, uint32_t row, int v) -> float4 {
+    return Row<T>::load(U + (uint64_t)row * R, c0 + (uint32_t)(v * G * 4));
+  };
+  auto rd = [&](uint32_t row, int v, float4 x) { red4(out + (uint64_t)row * R + c0 + v * G * 4, x); };
+
+  const uint64_t team = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) / G;
+  const bool active = team * chunk < a.nnz;
+  const uint64_t x0 = active ? team * chunk : a.nnz - 1;
+  const uint64_t x1 = active ? min(x0 + chunk, a.nnz) : x0;
+
+  // open slice: number sl, index ca, first nonzero of the next slice nxt
+  uint32_t sl;
+  if (a.cslc) {
+    sl = active ? __ldg(a.cslc + team) : nslc - 1;
+  } else {
+    uint32_t lo = 0, hi = nslc - 1;
+    while (lo < hi) {
+      const uint32_t m = (lo + hi + 1) >> 1;
+      if ((uint64_t)__ldg(snz + m) <= x0) lo = m; else hi = m - 1;
+    }
+    sl = lo;
+  }
+  uint32_t ca = __ldg(sidx + sl);
+  uint64_t nxt = __ldg(snz + sl + 1);
+  float4 acc[V], rowA[V];
+#pragma unroll
+  for (int v = 0; v < V; ++v) {
+    acc[v] = f4(0.f);
+    if constexpr (OUT == 2) rowA[v] = ld(U0, ca, v);
+  }
+
+  auto load_blk = [&](uint32_t itb, uint32_t& kk, uint32_t& bb, float& vq) {
+    const uint64_t xx = x0 + itb + tl;
+    kk = 0;
+    bb = 0;
+    vq = 0.f;
+    if (itb < chunk && xx < x1) { kk = __ldg(leaf + xx); bb = __ldg(mid + xx); vq = __ldg(vals + xx); }
+  };
+  uint32_t kc, bc, kn, bn;
+  float vc, vn;
+  load_blk(0, kc, bc, vc);
+  load_blk(G, kn, bn, vn);
+  for (uint32_t it = 0; it < chunk; it += G) {
+    const uint64_t xb = x0 + it;
+    const uint32_t k = kc & ~FLAG, b = bc;
+    const float vv = vc;
+    kc = kn; bc = bn; vc = vn;
+    load_blk(it + 2 * G, kn, bn, vn);
+    // a slice starts inside this block for some team of the warp
+    const bool slow = __any_sync(FULL, xb < x1 && xb + G > nxt);
+
+    auto block = [&](auto slow_tag) {
+      constexpr bool SLOW = decltype(slow_tag)::value;
+#pragma unroll
+      for (int jb = 0; jb < G; jb += PF) {
+        float4 rc[OUT == 0 ? PF : 1][V], rb[PF][V];
+        uint32_t kj[PF];
+#pragma unroll
+        for (int j = 0; j < PF; ++j) {
+          kj[j] = __shfl_sync(FULL, k, tb + jb + j);
+          const uint32_t bj = __shfl_sync(FULL, b, tb + jb + j);
+#pragma unroll
+          for (int v = 0; v < V; ++v) {
+            rb[j][v] = ld(U1, bj, v);
+            if constexpr (OUT == 0) rc[j][v] = ld(U2, kj[j], v);
+          }
+        }
+#pragma unroll
+        for (int j = 0; j < PF; ++j) {
+          const float val = __shfl_sync(FULL, vv, tb + jb + j);
+          const uint64_t x = xb + jb + j;
+          if constexpr (SLOW) {
+            if (x < x1 && x == nxt) {  // slice change (slices are never empty)
+              if constexpr (OUT == 0) {
+#pragma unroll
+                for (int v = 0; v < V; ++v) { rd(ca, v, acc[v]); acc[v] = f4(0.f); }
+              }
+              ++sl;
+              ca = __ldg(sidx + sl);
+              nxt = __ldg(snz + sl + 1);
+              if constexpr (OUT == 2) {
+#pragma unroll
+                for (int v = 0; v < V; ++v) rowA[v] = ld(U0, ca, v);
+              }
+            }
+          }
+          if constexpr (OUT == 0) {
+#pragma unroll
+            for (int v = 0; v < V; ++v) acc[v] = pfma(pmul_s(val, rb[j][v]), rc[j][v], acc[v]);
+          } else {
+            if (x < x1) {
+#pragma unroll
+              for (int v = 0; v < V; ++v) rd(kj[j], v, pmul_s(val, pmul(rowA[v], rb[j][v])));
+            }
+          }
+        }
+      }
+    };
+    if (slow) block(std::true_type{});
+    else block(std::false_type{});
+  }
+  if constexpr (OUT == 0) {
+    if (active) {
+#pragma unroll
+      for (int v = 0; v < V; ++v) rd(ca, v, acc[v]);
+    }
+  }
+}
+
 template <int ND, int OUT, int G, int V, class T>
 cudaError_t launch_one(const Args<T>& a, int threads, int mb, cudaStream_t s) {
   const uint64_t teams = (a.nnz + a.chunk - 1) / a.chunk;
@@ -529,11 +673,28 @@ cudaError_t launch_flat(const Args<T>& a, int threads, int mb, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-// kern: 1 = per-team fiber walk (k_mttkrp), 2 = branch-free walk (3-D only)
+template <int OUT, int G, int V, class T>
+cudaError_t launch_rows(const Args<T>& a, int threads, int mb, cudaStream_t s) {
+  const uint64_t teams = (a.nnz + a.chunk - 1) / a.chunk;
+  const uint64_t thr = teams * G;
+  const uint64_t blocks = (thr + threads - 1) / threads;
+  switch (mb) {
+    case 1: k_mttkrp_rows<OUT, G, V, T, 2, 8><<<(unsigned)blocks, threads, 0, s>>>(a); break;
+    case 3: k_mttkrp_rows<OUT, G, V, T, 4, 4><<<(unsigned)blocks, threads, 0, s>>>(a); break;
+    case 4: k_mttkrp_rows<OUT, G, V, T, 5, 4><<<(unsigned)blocks, threads, 0, s>>>(a); break;
+    default: k_mttkrp_rows<OUT, G, V, T, 3, 8><<<(unsigned)blocks, threads, 0, s>>>(a); break;
+  }
+  return cudaGetLastError();
+}
+
+// kern: 1 = per-team fiber walk (k_mttkrp), 2 = branch-free walk (3-D only),
+// 3 = per-nonzero walk (3-D slice and leaf levels of parts that carry `mid`)
 template <int ND, int G, int V, class T>
 cudaError_t launch_lvl(const Args<T>& a, int lvl, int kern, int threads, int mb, cudaStream_t s) {
   if constexpr (ND == 3) {
-    if (kern == 2) {
+    if (kern == 3 && lvl == 0) return launch_rows<0, G, V, T>(a, threads, mb, s);
+    if (kern == 3 && lvl == 2) return launch_rows<2, G, V, T>(a, threads, mb, s);
+    if (kern >= 2) {
       switch (lvl) {
         case 0: return launch_flat<0, G, V, T>(a, threads, mb, s);
         case 1: return launch_flat<1, G, V, T>(a, threads, mb, s);
@@ -610,8 +771,9 @@ int part_mttkrp(const mmcsf_format* F, const CsfPart& P, int mode, int R, int dt
   int chunk = cfg && cfg->chunk > 0 ? cfg->chunk : default_chunk(R);
   int threads = cfg && cfg->block_threads > 0 ? cfg->block_threads : 256;
   const int mb = cfg && cfg->min_blocks > 0 ? cfg->min_blocks : 2;
-  const int kern = cfg && cfg->kernel > 0 ? cfg->kernel : (P.nd == 3 ? 2 : 1);
-  if (kern != 1 && kern != 2) return set_error(MMCSF_ERR_INVALID, "kernel must be 0, 1 or 2");
+  int kern = cfg && cfg->kernel > 0 ? cfg->kernel : (P.nd == 3 ? 2 : 1);
+  if (kern < 1 || kern > 3) return set_error(MMCSF_ERR_INVALID, "kernel must be 0, 1, 2 or 3");
+  if (kern == 3 && (P.nd != 3 || lvl == 1 || !P.mid.p)) kern = 2;  // per-nonzero walk not applicable
   const int slot = CsfPart::cfib_slot((uint64_t)chunk);
   if (threads % 32 || threads > 256) return set_error(MMCSF_ERR_INVALID, "block_threads must be a multiple of 32, <= 256");
   cudaError_t e;
@@ -626,6 +788,11 @@ int part_mttkrp(const mmcsf_format* F, const CsfPart& P, int mode, int R, int dt
     a.sidx1 = P.nd == 4 ? P.idx[1].as<uint32_t>() : nullptr;
     a.like = P.fbr_like.as<uint32_t>();
     a.cfib = slot >= 0 && P.cfib[slot].p ? P.cfib[slot].as<uint32_t>() : nullptr;
+    a.mid = P.mid.as<uint32_t>();
+    a.snz = P.snz.as<uint32_t>();
+    a.sidx = P.idx[0].as<uint32_t>();
+    a.cslc = slot >= 0 && P.cslc[slot].p ? P.cslc[slot].as<uint32_t>() : nullptr;
+    a.nslc = (uint32_t)P.n[0];
     a.nnz = P.nnz;
     a.nfib = (uint32_t)P.n_fibers();
     a.chunk = (uint32_t)chunk;
@@ -644,6 +811,11 @@ int part_mttkrp(const mmcsf_format* F, const CsfPart& P, int mode, int R, int dt
     a.sidx1 = P.nd == 4 ? P.idx[1].as<uint32_t>() : nullptr;
     a.like = P.fbr_like.as<uint32_t>();
     a.cfib = slot >= 0 && P.cfib[slot].p ? P.cfib[slot].as<uint32_t>() : nullptr;
+    a.mid = P.mid.as<uint32_t>();
+    a.snz = P.snz.as<uint32_t>();
+    a.sidx = P.idx[0].as<uint32_t>();
+    a.cslc = slot >= 0 && P.cslc[slot].p ? P.cslc[slot].as<uint32_t>() : nullptr;
+    a.nslc = (uint32_t)P.n[0];
     a.nnz = P.nnz;
     a.nfib = (uint32_t)P.n_fibers();
     a.chunk = (uint32_t)chunk;
@@ -903,7 +1075,7 @@ extern "C" int mmcsf_tune(mmcsf_format* F, int R, int factor_dtype, const void* 
     const int m = F->impl == MMCSF_IMPL_MMCSF ? i : F->mode;
     float best = 1e30f;
     int bt = 1, bc = 512, bm = 2, bk = 1;
-    const int nkern = F->nd == 3 ? 2 : 1;
+    const int nkern = F->nd == 3 ? 3 : 1;
     for (int trav = 1; trav <= 2 && st == MMCSF_OK; ++trav) {
       if (trav == 2 && !F->views[m].present) continue;
       for (int kern = 1; kern <= nkern && st == MMCSF_OK; ++kern)
@@ -954,7 +1126,7 @@ extern "C" int mmcsf_set_plan(mmcsf_format* F, const mmcsf_plan* plan) {
     if (plan->traversal[m] == 2 && !F->views[m].present)
       return set_error(MMCSF_ERR_INVALID, "plan uses a view for mode %d that was not built", m);
     if (plan->traversal[m] < 0 || plan->traversal[m] > 2 || plan->chunk[m] < 0 || plan->kernel[m] < 0 ||
-        plan->kernel[m] > 2 || (plan->kernel[m] == 2 && F->nd != 3))
+        plan->kernel[m] > 3 || (plan->kernel[m] >= 2 && F->nd != 3))
       return set_error(MMCSF_ERR_INVALID, "bad plan entry for mode %d", m);
     F->plan_traversal[m] = plan->traversal[m];
     F->plan_chunk[m] = plan->chunk[m];

@@ -280,7 +280,8 @@ def test_full_size_skewed_checksums(views, torch_cuda):
 @pytest.mark.parametrize("R", [4, 32, 128, 256])
 @pytest.mark.parametrize("dtype", ["f32", "bf16"])
 def test_kernel_variants_3d(R, dtype, torch_cuda):
-    """Both 3-D traversals (per-team fiber walk, branch-free walk) at every
+    """The three 3-D traversals (per-team fiber walk, branch-free fiber walk,
+    per-nonzero walk) at every
     occupancy level, on the partition and on the views, with fiber splits and
     with many short slices (slice changes inside most blocks)."""
     import mmcsf
@@ -302,7 +303,7 @@ def test_kernel_variants_3d(R, dtype, torch_cuda):
             for m in range(3):
                 travs = (1, 2) if F.info(4 + m)["present"] else (1,)
                 for trav in travs:
-                    for kern in (1, 2):
+                    for kern in (1, 2, 3):
                         for mb in (1, 2, 3, 4):
                             for chunk in (64, 1000):
                                 cfg = {"traversal": trav, "kernel": kern, "min_blocks": mb, "chunk": chunk}
@@ -310,7 +311,7 @@ def test_kernel_variants_3d(R, dtype, torch_cuda):
                                 _check_close(out.cpu().numpy(), ref[m], (dims, f, m, cfg))
             if f == 0:
                 B = mmcsf.Format(X, impl=mmcsf.IMPL_BCSF, mode=1, fiber_threshold=4)
-                for kern in (1, 2):
+                for kern in (1, 2, 3):
                     out = B.mttkrp(1, Ud, cfg={"kernel": kern})
                     _check_close(out.cpu().numpy(), ref[1], ("bcsf", dims, kern))
 

@@ -69,6 +69,7 @@ def parse():
     ap.add_argument("--plan-file", default="", help="JSON plan (as printed by a tuned run) to use instead of tuning")
     ap.add_argument("--no-cp", action="store_true", help="skip the CP-ALS and Poisson gradient-CP sections")
     ap.add_argument("--no-formats", action="store_true", help="4-D workloads: skip the B-CSF / HB-CSF section")
+    ap.add_argument("--no-bf16", action="store_true", help="skip the BF16-factor section")
     ap.add_argument("--cp-scale", type=float, default=1.0, help="scale the CP workloads' nonzero counts")
     return ap.parse_args()
 
@@ -82,15 +83,18 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def traffic_from_profiles(workload, R, dtype):
-    """dram bytes per launch of the dominant kernel from a committed ncu summary."""
+def traffic_from_profiles(workload, R, dtype, mode, kernel):
+    """DRAM bytes per launch of one mode's MTTKRP kernel from a committed ncu
+    summary (lines `mode<m>: <kernel> <bytes>`), or None when the summary has
+    no entry for that mode and kernel."""
     p = os.path.join(ROOT, "profiles", f"traffic_{workload}_R{R}_{dtype}.txt")
     if not os.path.exists(p):
         return None
     with open(p) as fh:
         for line in fh:
-            if line.startswith("traffic_bytes_per_launch:"):
-                return float(line.split(":", 1)[1])
+            f = line.split()
+            if len(f) == 3 and f[0] == f"mode{mode}:" and f[1] == kernel:
+                return float(f[2])
     return None
 
 
@@ -238,6 +242,34 @@ def format_section(X, dims, R, tdt):
             torch.cuda.empty_cache()
         out[name] = {"mode_ms": ms, "all_mode_ms": sum(ms)}
     return out
+
+
+def bf16_section(F, U32, outs32, steps, warmup):
+    """The same step with BF16 factors (FP32 accumulation), tuned for them,
+    and the error this costs against the FP32-factor outputs."""
+    import torch
+    U = [u.to(torch.bfloat16) for u in U32]
+    outs = [torch.empty_like(o) for o in outs32]
+    plan = F.tune(U, outs)
+    for _ in range(warmup):
+        F.mttkrp_all(U, outs)
+    nd = len(U)
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(nd + 1)] for _ in range(steps)]
+    torch.cuda.synchronize()
+    for k in range(steps):
+        ev[k][0].record()
+        for m in range(nd):
+            F.mttkrp(m, U, outs[m])
+            ev[k][m + 1].record()
+    torch.cuda.synchronize()
+    mode_ms = [statistics.mean(ev[k][m].elapsed_time(ev[k][m + 1]) for k in range(steps)) for m in range(nd)]
+    err = []
+    for o, r in zip(outs, outs32):
+        d = (o.double() - r.double())
+        err.append({"frobenius_rel": float(d.norm() / r.double().norm()),
+                    "max_abs_over_max_ref": float(d.abs().max() / r.double().abs().max())})
+    return {"ms_per_step": sum(mode_ms), "mode_ms": mode_ms, "plan": plan, "error_vs_fp32_factors": err,
+            "note": "BF16-rounded factor rows, FP32 products and accumulation; the error is the factors' rounding"}
 
 
 def cp_section(seed, scale):
@@ -408,7 +440,12 @@ def main():
     for m in range(nd):
         trav = plan[m]["traversal"] if plan else (2 if F.info(4 + m)["present"] else 1)
         pi = F.info(4 + m) if trav == 2 else info
-        per_mode.append(mode_bytes(nd, dims, m, R, esz, struct_bytes(nd, nnz, pi["n_fibers"], pi["n_fbrs"]), rows))
+        lvl = pi["mode_order"].index(m)
+        if plan and plan[m].get("kernel") == 3 and nd == 3 and lvl != 1:
+            sb = nnz * 12 + pi["n_slices"] * 8  # per-nonzero walk: vals, leaf, mid; slice offsets and indices
+        else:
+            sb = struct_bytes(nd, nnz, pi["n_fibers"], pi["n_fbrs"])
+        per_mode.append(mode_bytes(nd, dims, m, R, esz, sb, rows))
     stream = torch.cuda.current_stream()
 
     for _ in range(a.warmup):
@@ -477,14 +514,36 @@ def main():
         return
     dom = max(range(nd), key=lambda m: mode_ms[m])
     achieved = per_mode[dom] / (mode_ms[dom] / 1e3) / 1e9
-    traffic = traffic_from_profiles(a.workload, R, a.dtype)
+
     dtrav = plan[dom]["traversal"] if plan else 1
     dorder = F.info(4 + dom)["mode_order"] if dtrav == 2 else info["mode_order"]
+    dlvl = dorder.index(dom)
+    dk = plan[dom].get("kernel", 0) if plan else 0
+    if dk == 3 and (nd != 3 or dlvl == 1):
+        dk = 2  # the per-nonzero walk serves slice and leaf levels; the middle level runs the fiber walk
+    dker = {1: "k_mttkrp", 2: "k_mttkrp_flat", 3: "k_mttkrp_rows"}.get(dk or (2 if nd == 3 else 1))
+    traffic = traffic_from_profiles(a.workload, R, a.dtype, dom, dker)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
                 "traffic": traffic, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
-                "kernel": f"k_mttkrp mode {dom} (level {dorder.index(dom)} of order {dorder}, "
+                "kernel": f"{dker} mode {dom} (level {dlvl} of order {dorder}, "
                           f"{'view' if dtrav == 2 else 'MM-CSF partition'})",
                 "algorithmic_bytes": per_mode[dom], "avg_ms": mode_ms[dom]}
+    # gather ceiling: the same GPU gathering the leaf factor's rows for the
+    # workload's own leaf-mode index stream with nothing else to do
+    if a.dtype == "f32" and R in (16, 32, 64, 128):
+        import ctypes
+        from mmcsf._lib import lib as _mlib, check as _mcheck
+        leafm = info["mode_order"][-1]
+        dinds, _ = X.device_tensors()
+        pms = ctypes.c_float()
+        _mcheck(_mlib().mmcsf_probe_gather(ctypes.c_void_p(dinds[leafm].data_ptr()), ctypes.c_uint64(nnz),
+                                           ctypes.c_void_p(U[leafm].data_ptr()), ctypes.c_uint64(dims[leafm]), R, 5,
+                                           ctypes.byref(pms), ctypes.c_void_p(stream.cuda_stream)))
+        roofline["gather_ceiling"] = {
+            "ms": pms.value, "rows_per_s": nnz / (pms.value / 1e3),
+            "what": f"{nnz} rows of the {dims[leafm]} x {R} FP32 mode-{leafm} factor gathered by the workload's "
+                    f"mode-{leafm} indices and summed (mmcsf_probe_gather), nothing else",
+            "dominant_kernel_vs_ceiling": pms.value / mode_ms[dom]}
     cpu = None
     if not a.no_cpu and world == 1:
         inds_h, vals_h = X.host_arrays()
@@ -494,6 +553,11 @@ def main():
                "ms_per_step": ts * 1e3,
                "sample": f"first {S} of {nnz} nonzeros, all {nd} modes, MTTKRP_COO_CPU serial as shipped, "
                          f"extrapolated x{nnz / S:.1f}"}
+    bf16 = None
+    if a.dtype == "f32" and not a.no_bf16:
+        for m in range(nd):
+            F.mttkrp(m, U, outs[m])
+        bf16 = bf16_section(F, U, outs, min(a.steps, 20), a.warmup)
     formats = None
     if nd == 4 and not a.no_formats:
         fm = format_section(X, dims, R, tdt)
@@ -510,8 +574,8 @@ def main():
             "config": config, "mode_ms": mode_ms, "mode_algorithmic_bytes": per_mode, "plan": plan, "format": info,
             "roofline": roofline,
             "cpu_baseline": cpu,
-            "e2e": e2e, "gpu_launches": launches_per_step * a.steps, "clocks": clocks, "cp": cp,
-            "formats": formats}
+            "e2e": e2e, "gpu_launches": launches_per_step * a.steps, "clocks": clocks, "bf16_factors": bf16,
+            "cp": cp, "formats": formats}
     print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()

@@ -209,6 +209,14 @@ int mmcsf_tune(mmcsf_format* F, int R, int factor_dtype, const void* const* d_fa
                void* stream, mmcsf_plan* plan);
 int mmcsf_set_plan(mmcsf_format* F, const mmcsf_plan* plan);
 
+/* Row-gather probe (measurement; no counterpart in the reference): average
+ * milliseconds over `reps` launches of a kernel that only gathers and sums
+ * the rows d_rows[d_idx[x]] (R floats each, R in 16..128) for x < n, with the
+ * MTTKRP kernels' team layout. The ceiling for their per-nonzero gathers on
+ * the same index stream. Every index must be below nrows. */
+int mmcsf_probe_gather(const uint32_t* d_idx, uint64_t n, const float* d_rows, uint64_t nrows, int R, int reps,
+                       float* ms_out, void* stream);
+
 /* ---- sampled model and its adjoint (gradient-based CP) -------------------
  * No counterpart in the reference. The sampled CP model at every nonzero,
  * xhat[x] = sum_r lambda_r prod_m A_m[i_m(x), r] (d_lambda may be NULL for

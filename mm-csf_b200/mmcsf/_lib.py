@@ -103,6 +103,8 @@ SIGNATURES = {
     "mmcsf_cp_adjoint": ([c_voidp, c_int, c_int, c_int, ctypes.POINTER(c_voidp), c_voidp, c_voidp, c_voidp,
                           ctypes.POINTER(KernelCfg), c_voidp], c_int),
     "mmcsf_format_values": ([c_voidp, ctypes.POINTER(c_voidp), c_u64p], c_int),
+    "mmcsf_probe_gather": ([c_voidp, c_u64, c_voidp, c_u64, c_int, c_int, ctypes.POINTER(ctypes.c_float), c_voidp],
+                           c_int),
     "mmcsf_sort_coo_noalloc": ([c_int, c_int, c_int, c_u64p, c_u64, ctypes.POINTER(c_voidp), c_voidp,
                                 ctypes.POINTER(c_voidp), c_voidp, c_voidp], c_int),
 }

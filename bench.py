@@ -45,6 +45,7 @@ WORKLOADS = {
     "uniform3d": dict(dims=[1000, 1000, 1000], nnz=100_000, dist=[0, 0, 0], zipf=1.0, val=0, R=32,
                       desc="1000^3, 100k uniform nnz, R=32"),
     "skewed4d": dict(dims=[1000000, 20000, 5000, 200], nnz=140_000_000, dist=[1, 1, 1, 0], zipf=1.0, val=2, R=32,
+                     views=2,
                      desc="1000000x20000x5000x200, 140M nnz, Zipf(1.0) modes 0-2, uniform mode 3, integer values "
                           "1-50, R=32; B-CSF / HB-CSF per mode beside MM-CSF all modes"),
 }
@@ -64,7 +65,8 @@ def parse():
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--views", type=int, default=1, help="0 none, 1 leaf-level modes, 2 every mode")
+    ap.add_argument("--views", type=int, default=None,
+                    help="0 none, 1 leaf-level modes, 2 every mode (default: the workload's)")
     ap.add_argument("--no-tune", action="store_true")
     ap.add_argument("--plan-file", default="", help="JSON plan (as printed by a tuned run) to use instead of tuning")
     ap.add_argument("--no-cp", action="store_true", help="skip the CP-ALS and Poisson gradient-CP sections")
@@ -350,6 +352,8 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     W = WORKLOADS[a.workload]
+    if a.views is None:
+        a.views = W.get("views", 1)
     dims = W["dims"]
     nd = len(dims)
     nnz = a.nnz or W["nnz"]

@@ -432,9 +432,13 @@ static int build_csf(int nd, const int* order, uint64_t n, DevBuf* sorted, DevBu
   MMCSF_CUDA(cudaMemcpyAsync(P.fbr_like.as<uint32_t>() + n1, o[0] + (n - 1), 4, cudaMemcpyDeviceToDevice, s));
 
   // --- per-nonzero arrays
-  if (nd == 3) {  // o1 of every nonzero, read by the per-nonzero traversal
-    MMCSF_CUDA(P.mid.alloc(n * 4));
-    MMCSF_CUDA(cudaMemcpyAsync(P.mid.p, o[1], n * 4, cudaMemcpyDeviceToDevice, s));
+  // middle-level indices of every nonzero, read by the per-nonzero traversal:
+  // o_{nd-2} (and o1 in 4-D)
+  MMCSF_CUDA(P.mid.alloc(n * 4));
+  MMCSF_CUDA(cudaMemcpyAsync(P.mid.p, o[nd - 2], n * 4, cudaMemcpyDeviceToDevice, s));
+  if (nd == 4) {
+    MMCSF_CUDA(P.mid2.alloc(n * 4));
+    MMCSF_CUDA(cudaMemcpyAsync(P.mid2.p, o[1], n * 4, cudaMemcpyDeviceToDevice, s));
   }
   P.leaf = std::move(sorted[order[nd - 1]]);
   P.vals = std::move(vals);
@@ -493,10 +497,18 @@ __global__ void k_chunk_fibers(const uint32_t* __restrict__ fptr, uint32_t nfib,
 
 int chunk_fibers(CsfPart& P, cudaStream_t s, Launches& L) {
   if (!P.present || P.nnz == 0 || P.n_fibers() == 0) return MMCSF_OK;
-  if (P.mid.p) {  // first nonzero of every slice: fiber pointer of the slice's first fiber
+  if (P.mid.p) {  // first nonzero of every slice: follow the slice's first entry down to the leaf
     MMCSF_CUDA(P.snz.alloc((P.n[0] + 1) * 4));
     MMCSF_CUDA(gather_u32(P.ptr[1].as<uint32_t>(), P.ptr[0].as<uint32_t>(), P.snz.as<uint32_t>(), P.n[0] + 1, s));
     ++L.n;
+    if (P.nd == 4) {  // slice -> first fbrS -> first fiber -> first nonzero
+      DevBuf t;
+      MMCSF_CUDA(t.alloc((P.n[0] + 1) * 4));
+      MMCSF_CUDA(gather_u32(P.ptr[2].as<uint32_t>(), P.snz.as<uint32_t>(), t.as<uint32_t>(), P.n[0] + 1, s));
+      ++L.n;
+      MMCSF_CUDA(cudaStreamSynchronize(s));
+      P.snz = std::move(t);
+    }
   }
   for (int i = 0; i < CsfPart::N_CHUNK_SIZES; ++i) {
     const uint64_t chunk = 128ull << i, nch = (P.nnz + chunk - 1) / chunk;
@@ -616,7 +628,10 @@ extern "C" int mmcsf_build(mmcsf_coo* X, const mmcsf_build_opts* opts, void* str
   }
   if (opts->impl == MMCSF_IMPL_HBCSF) {
     MMCSF_TRY(build_hyb(Fm, P, s, &L.n));
-    for (int p = 0; p < 4; ++p) Fm->parts[p].mid.release();  // the HB-CSF CSF part uses the fiber walks
+    for (int p = 0; p < 4; ++p) {  // the HB-CSF CSF part uses the fiber walks
+      Fm->parts[p].mid.release();
+      Fm->parts[p].mid2.release();
+    }
   }
   for (int p = 0; p < 4; ++p) MMCSF_TRY(chunk_fibers(Fm->parts[p], s, L));
   for (int m = 0; m < 4; ++m) MMCSF_TRY(chunk_fibers(Fm->views[m], s, L));

@@ -36,7 +36,8 @@ struct CsfPart {
   static constexpr int N_CHUNK_SIZES = 6;
   DevBuf cfib[N_CHUNK_SIZES];
   DevBuf cslc[N_CHUNK_SIZES];  // ... and its slice (3-D parts with `mid`)
-  DevBuf mid;                  // 3-D: o1 of every nonzero (per-nonzero traversal), or empty
+  DevBuf mid;                  // o_{nd-2} of every nonzero (per-nonzero traversal), or empty
+  DevBuf mid2;                 // 4-D: o1 of every nonzero
   DevBuf snz;                  // with mid: first nonzero of every slice [S+1]
   static int cfib_slot(uint64_t chunk) {
     for (int i = 0; i < N_CHUNK_SIZES; ++i)
@@ -47,7 +48,7 @@ struct CsfPart {
     uint64_t b = 0;
     for (int l = 0; l < 3; ++l) b += ptr[l].bytes + idx[l].bytes;
     for (int i = 0; i < N_CHUNK_SIZES; ++i) b += cfib[i].bytes + cslc[i].bytes;
-    b += mid.bytes + snz.bytes;
+    b += mid.bytes + mid2.bytes + snz.bytes;
     b += leaf.bytes + vals.bytes + fbr_like.bytes + fpar.bytes + bin_of.bytes + from_part.bytes;
     for (int m = 0; m < 4; ++m) b += coo[m].bytes;
     return b;

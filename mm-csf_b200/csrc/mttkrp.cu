@@ -77,7 +77,8 @@ struct Args {
   const uint32_t* sidx1;  // 4-D: fbrS index (o1)
   const uint32_t* like;   // o0 per level-1 entry (3-D: fiber, 4-D: fbrS)
   const uint32_t* cfib;   // first fiber of every team's chunk, or null (binary search)
-  const uint32_t* mid;    // 3-D per-nonzero walk: o1 of every nonzero
+  const uint32_t* mid;    // per-nonzero walk: o_{nd-2} of every nonzero
+  const uint32_t* mid2;   // ... 4-D: o1 of every nonzero
   const uint32_t* snz;    // ... first nonzero of every slice [nslc + 1]
   const uint32_t* sidx;   // ... slice index (o0) of every slice
   const uint32_t* cslc;   // ... slice of every team's chunk start, or null (binary search)
@@ -507,18 +508,21 @@ __global__ void __launch_bounds__(256, MB) k_mttkrp_flat(const Args<T> a) {
 }
 
 // ---------------------------------------------------------------------------
-// Per-nonzero 3-D traversal ("rows" kernel) for the slice-level (OUT 0) and
-// leaf-level (OUT 2) outputs. Every nonzero carries its middle-level index
-// (`mid`), so a team needs no fiber bookkeeping: per nonzero it combines the
-// middle row and the leaf row, adding v * U1[b] (.) U2[k] to the open slice's
-// accumulator (OUT 0) or scattering v * U0[a] (.) U1[b] to the leaf row
-// (OUT 2). The middle row repeats along a fiber, so most of its gathers hit
-// L1 (gathering it unconditionally measured faster than predicating the
-// repeats away). Slice changes come from the slices' first nonzero positions
+// Per-nonzero traversal ("rows" kernel), 3-D and 4-D, for the slice-level
+// (OUT 0) and leaf-level (OUT ND-1) outputs. Every nonzero carries the
+// indices of its middle levels (`mid` = o_{ND-2}, and `mid2` = o1 in 4-D), so
+// a team needs no fiber bookkeeping: per nonzero it combines the middle rows
+// and the leaf row, adding v * U1[b] (.) U2[k] (4-D: v * U1[b] (.) U2[c] (.)
+// U3[k]) to the open slice's accumulator (OUT 0), or scattering
+// v * U0[a] (.) U1[b] [(.) U2[c]] to the leaf row. The middle rows repeat along
+// fibers, so most of their gathers hit L1 (gathering them unconditionally
+// measured faster than predicating the repeats away). Slice changes come from the slices' first nonzero positions
 // (`snz`), not from flags, and a block with a slice change takes a slower
 // variant.
-template <int OUT, int G, int V, class T, int MB, int PFX>
+template <int ND, int OUT, int G, int V, class T, int MB, int PFX>
 __global__ void __launch_bounds__(256, MB) k_mttkrp_rows(const Args<T> a) {
+  static_assert(OUT == 0 || OUT == ND - 1, "slice or leaf level");
+  constexpr int LEAF = ND - 1;
   constexpr uint32_t R = 4 * G * V;
   constexpr uint32_t FLAG = 0x80000000u;
   constexpr int PF = G > PFX ? PFX : G;
@@ -528,12 +532,14 @@ __global__ void __launch_bounds__(256, MB) k_mttkrp_rows(const Args<T> a) {
   const float* __restrict__ vals = a.vals;
   const uint32_t* __restrict__ leaf = a.leaf;
   const uint32_t* __restrict__ mid = a.mid;
+  const uint32_t* __restrict__ mid2 = a.mid2;
   const uint32_t* __restrict__ snz = a.snz;
   const uint32_t* __restrict__ sidx = a.sidx;
   const uint32_t chunk = a.chunk, nslc = a.nslc;
   const T* __restrict__ U0 = a.U[0];
   const T* __restrict__ U1 = a.U[1];
   const T* __restrict__ U2 = a.U[2];
+  const T* __restrict__ UL = a.U[LEAF];
   float* __restrict__ out = a.out;
   const uint32_t c0 = (uint32_t)tl * 4;
   auto ld = [&](const T* U, uint32_t row, int v) -> float4 {
@@ -564,26 +570,32 @@ __global__ void __launch_bounds__(256, MB) k_mttkrp_rows(const Args<T> a) {
 #pragma unroll
   for (int v = 0; v < V; ++v) {
     acc[v] = f4(0.f);
-    if constexpr (OUT == 2) rowA[v] = ld(U0, ca, v);
+    if constexpr (OUT == LEAF) rowA[v] = ld(U0, ca, v);
   }
 
-  auto load_blk = [&](uint32_t itb, uint32_t& kk, uint32_t& bb, float& vq) {
+  auto load_blk = [&](uint32_t itb, uint32_t& kk, uint32_t& bb, uint32_t& qq, float& vq) {
     const uint64_t xx = x0 + itb + tl;
     kk = 0;
     bb = 0;
+    qq = 0;
     vq = 0.f;
-    if (itb < chunk && xx < x1) { kk = __ldg(leaf + xx); bb = __ldg(mid + xx); vq = __ldg(vals + xx); }
+    if (itb < chunk && xx < x1) {
+      kk = __ldg(leaf + xx);
+      bb = __ldg(mid + xx);
+      if constexpr (ND == 4) qq = __ldg(mid2 + xx);
+      vq = __ldg(vals + xx);
+    }
   };
-  uint32_t kc, bc, kn, bn;
+  uint32_t kc, bc, qc, kn, bn, qn;
   float vc, vn;
-  load_blk(0, kc, bc, vc);
-  load_blk(G, kn, bn, vn);
+  load_blk(0, kc, bc, qc, vc);
+  load_blk(G, kn, bn, qn, vn);
   for (uint32_t it = 0; it < chunk; it += G) {
     const uint64_t xb = x0 + it;
-    const uint32_t k = kc & ~FLAG, b = bc;
+    const uint32_t k = kc & ~FLAG, b = bc, q = qc;
     const float vv = vc;
-    kc = kn; bc = bn; vc = vn;
-    load_blk(it + 2 * G, kn, bn, vn);
+    kc = kn; bc = bn; qc = qn; vc = vn;
+    load_blk(it + 2 * G, kn, bn, qn, vn);
     // a slice starts inside this block for some team of the warp
     const bool slow = __any_sync(FULL, xb < x1 && xb + G > nxt);
 
@@ -591,16 +603,23 @@ __global__ void __launch_bounds__(256, MB) k_mttkrp_rows(const Args<T> a) {
       constexpr bool SLOW = decltype(slow_tag)::value;
 #pragma unroll
       for (int jb = 0; jb < G; jb += PF) {
-        float4 rc[OUT == 0 ? PF : 1][V], rb[PF][V];
+        float4 rc[OUT == 0 ? PF : 1][V], rb[PF][V], rq[ND == 4 ? PF : 1][V];
         uint32_t kj[PF];
 #pragma unroll
         for (int j = 0; j < PF; ++j) {
           kj[j] = __shfl_sync(FULL, k, tb + jb + j);
           const uint32_t bj = __shfl_sync(FULL, b, tb + jb + j);
+          uint32_t qj = 0;
+          if constexpr (ND == 4) qj = __shfl_sync(FULL, q, tb + jb + j);
 #pragma unroll
           for (int v = 0; v < V; ++v) {
-            rb[j][v] = ld(U1, bj, v);
-            if constexpr (OUT == 0) rc[j][v] = ld(U2, kj[j], v);
+            if constexpr (ND == 3) {
+              rb[j][v] = ld(U1, bj, v);
+            } else {
+              rb[j][v] = ld(U2, bj, v);  // level 2 (fiber index c)
+              rq[j][v] = ld(U1, qj, v);  // level 1 (fbrS index b)
+            }
+            if constexpr (OUT == 0) rc[j][v] = ld(UL, kj[j], v);
           }
         }
 #pragma unroll
@@ -616,7 +635,7 @@ __global__ void __launch_bounds__(256, MB) k_mttkrp_rows(const Args<T> a) {
               ++sl;
               ca = __ldg(sidx + sl);
               nxt = __ldg(snz + sl + 1);
-              if constexpr (OUT == 2) {
+              if constexpr (OUT == LEAF) {
 #pragma unroll
                 for (int v = 0; v < V; ++v) rowA[v] = ld(U0, ca, v);
               }
@@ -624,11 +643,19 @@ __global__ void __launch_bounds__(256, MB) k_mttkrp_rows(const Args<T> a) {
           }
           if constexpr (OUT == 0) {
 #pragma unroll
-            for (int v = 0; v < V; ++v) acc[v] = pfma(pmul_s(val, rb[j][v]), rc[j][v], acc[v]);
+            for (int v = 0; v < V; ++v) {
+              float4 m = pmul_s(val, rb[j][v]);
+              if constexpr (ND == 4) m = pmul(m, rq[j][v]);
+              acc[v] = pfma(m, rc[j][v], acc[v]);
+            }
           } else {
             if (x < x1) {
 #pragma unroll
-              for (int v = 0; v < V; ++v) rd(kj[j], v, pmul_s(val, pmul(rowA[v], rb[j][v])));
+              for (int v = 0; v < V; ++v) {
+                float4 m = pmul(rowA[v], rb[j][v]);
+                if constexpr (ND == 4) m = pmul(m, rq[j][v]);
+                rd(kj[j], v, pmul_s(val, m));
+              }
             }
           }
         }
@@ -673,27 +700,27 @@ cudaError_t launch_flat(const Args<T>& a, int threads, int mb, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-template <int OUT, int G, int V, class T>
+template <int ND, int OUT, int G, int V, class T>
 cudaError_t launch_rows(const Args<T>& a, int threads, int mb, cudaStream_t s) {
   const uint64_t teams = (a.nnz + a.chunk - 1) / a.chunk;
   const uint64_t thr = teams * G;
   const uint64_t blocks = (thr + threads - 1) / threads;
   switch (mb) {
-    case 1: k_mttkrp_rows<OUT, G, V, T, 2, 8><<<(unsigned)blocks, threads, 0, s>>>(a); break;
-    case 3: k_mttkrp_rows<OUT, G, V, T, 4, 4><<<(unsigned)blocks, threads, 0, s>>>(a); break;
-    case 4: k_mttkrp_rows<OUT, G, V, T, 5, 4><<<(unsigned)blocks, threads, 0, s>>>(a); break;
-    default: k_mttkrp_rows<OUT, G, V, T, 3, 8><<<(unsigned)blocks, threads, 0, s>>>(a); break;
+    case 1: k_mttkrp_rows<ND, OUT, G, V, T, 2, 8><<<(unsigned)blocks, threads, 0, s>>>(a); break;
+    case 3: k_mttkrp_rows<ND, OUT, G, V, T, 4, 4><<<(unsigned)blocks, threads, 0, s>>>(a); break;
+    case 4: k_mttkrp_rows<ND, OUT, G, V, T, 5, 4><<<(unsigned)blocks, threads, 0, s>>>(a); break;
+    default: k_mttkrp_rows<ND, OUT, G, V, T, 3, 8><<<(unsigned)blocks, threads, 0, s>>>(a); break;
   }
   return cudaGetLastError();
 }
 
 // kern: 1 = per-team fiber walk (k_mttkrp), 2 = branch-free walk (3-D only),
-// 3 = per-nonzero walk (3-D slice and leaf levels of parts that carry `mid`)
+// 3 = per-nonzero walk (slice and leaf levels of parts that carry `mid`)
 template <int ND, int G, int V, class T>
 cudaError_t launch_lvl(const Args<T>& a, int lvl, int kern, int threads, int mb, cudaStream_t s) {
+  if (kern == 3 && lvl == 0) return launch_rows<ND, 0, G, V, T>(a, threads, mb, s);
+  if (kern == 3 && lvl == ND - 1) return launch_rows<ND, ND - 1, G, V, T>(a, threads, mb, s);
   if constexpr (ND == 3) {
-    if (kern == 3 && lvl == 0) return launch_rows<0, G, V, T>(a, threads, mb, s);
-    if (kern == 3 && lvl == 2) return launch_rows<2, G, V, T>(a, threads, mb, s);
     if (kern >= 2) {
       switch (lvl) {
         case 0: return launch_flat<0, G, V, T>(a, threads, mb, s);
@@ -773,7 +800,8 @@ int part_mttkrp(const mmcsf_format* F, const CsfPart& P, int mode, int R, int dt
   const int mb = cfg && cfg->min_blocks > 0 ? cfg->min_blocks : 2;
   int kern = cfg && cfg->kernel > 0 ? cfg->kernel : (P.nd == 3 ? 2 : 1);
   if (kern < 1 || kern > 3) return set_error(MMCSF_ERR_INVALID, "kernel must be 0, 1, 2 or 3");
-  if (kern == 3 && (P.nd != 3 || lvl == 1 || !P.mid.p)) kern = 2;  // per-nonzero walk not applicable
+  if (kern == 3 && ((lvl != 0 && lvl != P.nd - 1) || !P.mid.p)) kern = 2;  // per-nonzero walk not applicable
+  if (kern == 2 && P.nd == 4) kern = 1;                                         // no 4-D branch-free fiber walk
   const int slot = CsfPart::cfib_slot((uint64_t)chunk);
   if (threads % 32 || threads > 256) return set_error(MMCSF_ERR_INVALID, "block_threads must be a multiple of 32, <= 256");
   cudaError_t e;
@@ -789,6 +817,7 @@ int part_mttkrp(const mmcsf_format* F, const CsfPart& P, int mode, int R, int dt
     a.like = P.fbr_like.as<uint32_t>();
     a.cfib = slot >= 0 && P.cfib[slot].p ? P.cfib[slot].as<uint32_t>() : nullptr;
     a.mid = P.mid.as<uint32_t>();
+    a.mid2 = P.mid2.as<uint32_t>();
     a.snz = P.snz.as<uint32_t>();
     a.sidx = P.idx[0].as<uint32_t>();
     a.cslc = slot >= 0 && P.cslc[slot].p ? P.cslc[slot].as<uint32_t>() : nullptr;
@@ -812,6 +841,7 @@ int part_mttkrp(const mmcsf_format* F, const CsfPart& P, int mode, int R, int dt
     a.like = P.fbr_like.as<uint32_t>();
     a.cfib = slot >= 0 && P.cfib[slot].p ? P.cfib[slot].as<uint32_t>() : nullptr;
     a.mid = P.mid.as<uint32_t>();
+    a.mid2 = P.mid2.as<uint32_t>();
     a.snz = P.snz.as<uint32_t>();
     a.sidx = P.idx[0].as<uint32_t>();
     a.cslc = slot >= 0 && P.cslc[slot].p ? P.cslc[slot].as<uint32_t>() : nullptr;
@@ -1075,10 +1105,11 @@ extern "C" int mmcsf_tune(mmcsf_format* F, int R, int factor_dtype, const void* 
     const int m = F->impl == MMCSF_IMPL_MMCSF ? i : F->mode;
     float best = 1e30f;
     int bt = 1, bc = 512, bm = 2, bk = 1;
-    const int nkern = F->nd == 3 ? 3 : 1;
+    const int nkern = 3;
     for (int trav = 1; trav <= 2 && st == MMCSF_OK; ++trav) {
       if (trav == 2 && !F->views[m].present) continue;
-      for (int kern = 1; kern <= nkern && st == MMCSF_OK; ++kern)
+      for (int kern = 1; kern <= nkern && st == MMCSF_OK; ++kern) {
+      if (kern == 2 && F->nd == 4) continue;  // 4-D has no branch-free fiber walk
       for (int mbv = 1; mbv <= 4; ++mbv) {
         for (int c : chunks) {
           mmcsf_kernel_cfg cfg{};
@@ -1101,6 +1132,7 @@ extern "C" int mmcsf_tune(mmcsf_format* F, int R, int factor_dtype, const void* 
           if (ms < best) { best = ms; bt = trav; bc = c; bm = mbv; bk = kern; }
         }
         if (st != MMCSF_OK) break;
+      }
       }
     }
     F->plan_traversal[m] = bt;
@@ -1126,7 +1158,7 @@ extern "C" int mmcsf_set_plan(mmcsf_format* F, const mmcsf_plan* plan) {
     if (plan->traversal[m] == 2 && !F->views[m].present)
       return set_error(MMCSF_ERR_INVALID, "plan uses a view for mode %d that was not built", m);
     if (plan->traversal[m] < 0 || plan->traversal[m] > 2 || plan->chunk[m] < 0 || plan->kernel[m] < 0 ||
-        plan->kernel[m] > 3 || (plan->kernel[m] >= 2 && F->nd != 3))
+        plan->kernel[m] > 3)
       return set_error(MMCSF_ERR_INVALID, "bad plan entry for mode %d", m);
     F->plan_traversal[m] = plan->traversal[m];
     F->plan_chunk[m] = plan->chunk[m];

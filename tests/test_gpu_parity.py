@@ -316,6 +316,37 @@ def test_kernel_variants_3d(R, dtype, torch_cuda):
                     _check_close(out.cpu().numpy(), ref[1], ("bcsf", dims, kern))
 
 
+@pytest.mark.parametrize("R", [4, 32, 128])
+@pytest.mark.parametrize("dtype", ["f32", "bf16"])
+def test_kernel_variants_4d(R, dtype, torch_cuda):
+    """4-D: the per-team fiber walk and the per-nonzero walk at every occupancy
+    level, on the partition (fbrS split at 128) and on every mode's view."""
+    import mmcsf
+    torch = torch_cuda
+    rng = np.random.default_rng(400 + R)
+    for dims, n, skew in (([40, 30, 50, 20], 20000, True), ([900, 8, 6, 5], 6000, False)):
+        inds, vals = _rand_coo(rng, dims, n, skew)
+        X = mmcsf.CooTensor.from_arrays(dims, inds, vals)
+        U = [rng.random((d, R)).astype(np.float32) for d in dims]
+        if dtype == "bf16":
+            Ud = [torch.tensor(u, device="cuda").to(torch.bfloat16) for u in U]
+            U = [t.float().cpu().numpy() for t in Ud]
+        else:
+            Ud = [torch.tensor(u, device="cuda") for u in U]
+        ref = [O.mttkrp_coo_f64(dims, inds, vals, m, U) for m in range(4)]
+        for f in (0, 3):
+            F = mmcsf.Format(X, impl=mmcsf.IMPL_MMCSF, mode=0, fiber_threshold=f, views=2)
+            for m in range(4):
+                travs = (1, 2) if F.info(4 + m)["present"] else (1,)
+                for trav in travs:
+                    for kern in (1, 3):
+                        for mb in (1, 2, 3, 4):
+                            for chunk in (64, 1000):
+                                cfg = {"traversal": trav, "kernel": kern, "min_blocks": mb, "chunk": chunk}
+                                out = F.mttkrp(m, Ud, cfg=cfg)
+                                _check_close(out.cpu().numpy(), ref[m], (dims, f, m, cfg))
+
+
 @pytest.mark.parametrize("nd", [3, 4])
 def test_views_and_tuner(nd, torch_cuda):
     import mmcsf

@@ -292,9 +292,9 @@ def cp_section(seed, scale):
     g = torch.Generator(device="cuda").manual_seed(seed + 5)
     R = c["R"]
     init = [torch.rand(d, R, device="cuda", generator=g) for d in c["dims"]]
-    F.tune(init)
     runs = {}
     for prec in ("fp32", "bf16", "fp64solve"):
+        F.tune([t.to(torch.bfloat16) for t in init] if prec == "bf16" else init)  # plan for this factor type
         F.cpd(R, max_iters=2, tol=c["tol"], precision=prec, init=init)       # warm-up (tables, graph code)
         r = F.cpd(R, max_iters=c["max_iters"], tol=c["tol"], precision=prec, init=init)
         fx = F.cpd(R, max_iters=c["max_iters"], tol=1e-15, precision=prec, init=init)  # every iteration
@@ -320,9 +320,9 @@ def cp_section(seed, scale):
     R = c["R"]
     g = torch.Generator(device="cuda").manual_seed(seed + 7)
     init = [torch.rand(d, R, device="cuda", generator=g) * 0.5 + 0.25 for d in c["dims"]]
-    F.tune(init)
     runs = {}
     for prec in ("fp32", "bf16"):
+        F.tune([t.to(torch.bfloat16) for t in init] if prec == "bf16" else init)  # plan for this factor type
         gcp.gcp_poisson(F, R, iters=3, lr=c["lr"], precision=prec, init=init)  # warm-up
         r = gcp.gcp_poisson(F, R, iters=c["iters"], lr=c["lr"], precision=prec, init=init)
         runs[prec] = {"ms_per_iter": r["ms"][-1] / r["iters"], "iters": r["iters"], "loss_first": r["loss"][0],

@@ -5,9 +5,12 @@
 // (mmcsf_cp_adjoint), which is how gradient-based CP uses it.
 //
 // Traversal: a team of G lanes per row of R = 4*G*V values walks a contiguous
-// range of nonzeros; per leaf fiber it forms w = lambda (.) the rows above the
-// leaf, per nonzero it takes the dot product of w with the leaf row (lane
-// partials reduced by shuffles inside the team) and writes one value.
+// range of nonzeros. k_sampled_rows (parts that carry per-nonzero middle
+// indices, i.e. every MM-CSF and B-CSF part) gathers per nonzero the middle
+// rows and the leaf row and reduces a block's partial dot products with one
+// transposed butterfly; k_sampled (fallback) forms w = lambda (.) the rows
+// above the leaf once per fiber and reduces each nonzero's dot product with
+// shuffles inside the team.
 #include <cuda_bf16.h>
 
 #include "format.h"
@@ -38,6 +41,8 @@ template <class T>
 struct SArgs {
   const uint32_t *leaf, *fptr, *fidx, *fpar, *sidx1, *like;
   const uint32_t* cfib;  // first fiber of every chunk, or null (binary search)
+  const uint32_t *mid, *mid2, *snz, *sidx, *cslc;  // per-nonzero walk (see k_sampled_rows)
+  uint32_t nslc;
   uint64_t nnz;
   uint32_t nfib, chunk;
   const T* U[4];      // by level
@@ -112,11 +117,103 @@ __global__ void __launch_bounds__(256) k_sampled(const SArgs<T> a) {
   }
 }
 
+
+// Per-nonzero form: every nonzero carries its middle-level indices (`mid`,
+// and `mid2` in 4-D), so per nonzero a team gathers the middle rows and the
+// leaf row and forms the partial dot product of (lambda (.) slice row (.)
+// middle rows) with the leaf row over its lane's columns. The G partial sums
+// of a block (one per nonzero) are reduced across the team by a transposed
+// butterfly -- G-1 shuffles per block instead of log2(G) per nonzero -- after
+// which lane j holds the value of the block's nonzero j and the team stores
+// the block with one coalesced write.
+template <int ND, int G, int V, class T>
+__global__ void __launch_bounds__(256) k_sampled_rows(const SArgs<T> a) {
+  constexpr uint32_t R = 4 * G * V;
+  constexpr int LEAF = ND - 1;
+  const int lane = threadIdx.x & 31, tl = lane & (G - 1), tb = lane - tl;
+  const uint64_t team = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) / G;
+  const bool active = team * a.chunk < a.nnz;
+  const uint64_t x0 = active ? team * a.chunk : a.nnz - 1;
+  const uint64_t x1 = active ? min(x0 + a.chunk, a.nnz) : x0;
+  auto col = [&](int v) { return (uint32_t)(tl + v * G) * 4; };
+  uint32_t sl;
+  if (a.cslc) {
+    sl = active ? __ldg(a.cslc + team) : a.nslc - 1;
+  } else {
+    uint32_t lo = 0, hi = a.nslc - 1;
+    while (lo < hi) {
+      const uint32_t m = (lo + hi + 1) >> 1;
+      if ((uint64_t)__ldg(a.snz + m) <= x0) lo = m; else hi = m - 1;
+    }
+    sl = lo;
+  }
+  uint64_t nxt = __ldg(a.snz + sl + 1);
+  float4 wa[V];  // lambda (.) slice row
+  auto slice_row = [&]() {
+    const uint32_t ca = __ldg(a.sidx + sl);
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      float4 x = ld4(a.U[0] + (uint64_t)ca * R + col(v));
+      if (a.lam) x = mul4(x, __ldg(reinterpret_cast<const float4*>(a.lam + col(v))));
+      wa[v] = x;
+    }
+  };
+  slice_row();
+  for (uint32_t it = 0; it < a.chunk; it += G) {
+    const uint64_t xb = x0 + it;
+    const uint64_t xl = xb + tl;
+    uint32_t k = 0, b = 0, q = 0;
+    if (xl < x1) {
+      k = __ldg(a.leaf + xl) & ~FLAG;
+      b = __ldg(a.mid + xl);
+      if constexpr (ND == 4) q = __ldg(a.mid2 + xl);
+    }
+    const bool slow = __any_sync(FULL, xb < x1 && xb + G > nxt);
+    float p[G];
+#pragma unroll
+    for (int j = 0; j < G; ++j) {
+      const uint32_t kj = __shfl_sync(FULL, k, tb + j);
+      const uint32_t bj = __shfl_sync(FULL, b, tb + j);
+      uint32_t qj = 0;
+      if constexpr (ND == 4) qj = __shfl_sync(FULL, q, tb + j);
+      if (slow) {
+        if (xb + j < x1 && xb + j == nxt) {  // slice change (slices are never empty)
+          ++sl;
+          nxt = __ldg(a.snz + sl + 1);
+          slice_row();
+        }
+      }
+      float acc = 0.f;
+#pragma unroll
+      for (int v = 0; v < V; ++v) {
+        float4 w = mul4(wa[v], ld4(a.U[ND - 2] + (uint64_t)bj * R + col(v)));
+        if constexpr (ND == 4) w = mul4(w, ld4(a.U[1] + (uint64_t)qj * R + col(v)));
+        const float4 c = ld4(a.U[LEAF] + (uint64_t)kj * R + col(v));
+        acc += w.x * c.x + w.y * c.y + w.z * c.z + w.w * c.w;
+      }
+      p[j] = acc;
+    }
+    // transposed butterfly: lane tl ends with the sum of p[tl] over the team
+#pragma unroll
+    for (int st = G / 2; st >= 1; st >>= 1) {
+      const bool up = (tl & st) != 0;
+#pragma unroll
+      for (int i = 0; i < st; ++i) {
+        const float send = up ? p[i] : p[i + st];
+        const float keep = up ? p[i + st] : p[i];
+        p[i] = keep + __shfl_xor_sync(FULL, send, st);
+      }
+    }
+    if (xl < x1) a.out[xl] = p[0];
+  }
+}
+
 template <int ND, int G, int V, class T>
 cudaError_t launch_s(const SArgs<T>& a, cudaStream_t s) {
   const uint64_t teams = (a.nnz + a.chunk - 1) / a.chunk;
   const uint64_t blocks = (teams * G + 255) / 256;
-  k_sampled<ND, G, V, T><<<(unsigned)blocks, 256, 0, s>>>(a);
+  if (a.mid) k_sampled_rows<ND, G, V, T><<<(unsigned)blocks, 256, 0, s>>>(a);
+  else k_sampled<ND, G, V, T><<<(unsigned)blocks, 256, 0, s>>>(a);
   return cudaGetLastError();
 }
 
@@ -175,6 +272,12 @@ extern "C" int mmcsf_sampled_model(const mmcsf_format* F, int R, int factor_dtyp
     a.nfib = (uint32_t)P->n_fibers();
     a.chunk = 256;
     a.cfib = P->cfib[CsfPart::cfib_slot(256)].p ? P->cfib[CsfPart::cfib_slot(256)].as<uint32_t>() : nullptr;
+    a.mid = P->mid.as<uint32_t>();
+    a.mid2 = P->mid2.as<uint32_t>();
+    a.snz = P->snz.as<uint32_t>();
+    a.sidx = P->idx[0].as<uint32_t>();
+    a.cslc = P->cslc[CsfPart::cfib_slot(256)].p ? P->cslc[CsfPart::cfib_slot(256)].as<uint32_t>() : nullptr;
+    a.nslc = (uint32_t)P->n[0];
     for (int l = 0; l < P->nd; ++l) a.U[l] = static_cast<const T*>(d_factors[P->order[l]]);
     a.lam = d_lambda;
     a.out = d_out;

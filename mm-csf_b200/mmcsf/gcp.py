@@ -118,7 +118,7 @@ def gcp_poisson(fmt, rank, iters=100, lr=0.05, precision="fp32", init=None, seed
     step = lr * float(torch.cat([f.flatten() for f in masters]).mean())
     for f in masters:
         f.requires_grad_(True)
-    opt = torch.optim.Adam(masters, lr=step)
+    opt = torch.optim.Adam(masters, lr=step, fused=True)  # one kernel per step for all factors
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(iters + 1)]
     losses = []
     torch.cuda.synchronize()

@@ -1,0 +1,72 @@
+"""The `mttkrp` command (mm-csf_b200/bin/mttkrp), which keeps the reference's
+flags (-i -m -R -t -f -w -b -v -c -o; src/util.h:3341-3442) and its
+"Total GPU time ... nSlc/nFibers/nnz" line (src/mttkrp_gpu.cu:3760-3767).
+
+CPU: argument errors end with a message and a nonzero status (the reference
+exit(0)s) before any GPU work. GPU: every format and mode, with the
+reference's constant factors (U[m] = m + 0.5), checked by the command's own
+-c 1 comparison and by its -o output against the FP64 oracle."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+BIN = os.path.join(ROOT, "mm-csf_b200", "bin", "mttkrp")
+
+
+def _run(args, timeout=300):
+    return subprocess.run([BIN] + args, capture_output=True, text=True, timeout=timeout)
+
+
+def test_cli_argument_errors(tmp_path):
+    assert os.path.exists(BIN), "build mm-csf_b200 first"
+    p = _run([])
+    assert p.returncode != 0 and "-t implementation type" in p.stdout
+    p = _run(["-i", "x.tns", "-t", "1"])
+    assert p.returncode != 0 and "-t 1 is not provided" in p.stderr
+    p = _run(["-i", "x.tns", "-z", "3"])
+    assert p.returncode != 0 and "unknown option" in p.stderr
+    p = _run(["-i", str(tmp_path / "missing.tns"), "-t", "12"])
+    assert p.returncode != 0 and "load_tensor failed" in p.stderr
+
+
+def _read_out(path):
+    with open(path) as fh:
+        head = fh.readline().split()
+        rows = [[float(v) for v in line.split()] for line in fh if line.strip()]
+    return head, np.array(rows)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("nd", [3, 4])
+def test_cli_formats_and_modes(nd, tmp_path):
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    rng = np.random.default_rng(nd)
+    dims = [50, 70, 40] if nd == 3 else [30, 25, 20, 15]
+    n = 4000
+    lin = rng.choice(int(np.prod(dims)), size=n, replace=False)
+    inds = [np.asarray(i, np.uint64) for i in np.unravel_index(lin, dims)]
+    vals = np.round(rng.random(n) + 0.1, 3).astype(np.float32)
+    tns = tmp_path / "x.tns"
+    O.write_tns(str(tns), dims, inds, vals)  # the reference's .tns: order and lengths, then 1-based entries
+    R = 16
+    U = [np.full((d, R), m + 0.5, np.float32) for m, d in enumerate(dims)]
+    for t, modes in ((12, [0]), (8, range(nd)), (10, range(nd))):
+        for m in modes:
+            for extra in ([], ["-w", "2", "-f", "3"]):
+                out = tmp_path / f"o_{t}_{m}.txt"
+                p = _run(["-i", str(tns), "-m", str(m), "-R", str(R), "-t", str(t), "-c", "1", "-o", str(out)]
+                         + extra)
+                assert p.returncode == 0, (t, m, extra, p.stderr)
+                assert "Total GPU time:" in p.stdout and f"nnz:{n}" in p.stdout, p.stdout
+                assert "Correctness pass!" in p.stdout, (t, m, extra, p.stdout)
+                head, got = _read_out(out)
+                assert head[0] == str(dims[m]) and got.shape == (dims[m], R)
+                want = O.mttkrp_coo_f64(dims, inds, vals, m, U)
+                assert np.all(np.abs(got - want) <= 0.006 + 1e-5 * np.abs(want)), (t, m, extra)

@@ -79,6 +79,11 @@ int mmcsf_coo_host_arrays(const mmcsf_coo* X, const uint32_t** inds, const float
 int mmcsf_coo_device_arrays(const mmcsf_coo* X, const uint32_t** d_inds, const float** d_vals);
 /* Write as .tns (1-based). */
 int mmcsf_coo_write_tns(mmcsf_coo* X, const char* path);
+/* Binary COO file (no counterpart in the reference): the same tensor without
+ * the text parse, for loading large tensors repeatedly. Written and read on
+ * hosts of the same byte order. */
+int mmcsf_coo_write_bin(mmcsf_coo* X, const char* path);
+int mmcsf_coo_load_bin(const char* path, mmcsf_coo** out);
 void mmcsf_coo_destroy(mmcsf_coo* X);
 
 /* ---- synthetic tensors --------------------------------------------------

@@ -10,7 +10,8 @@
 //   * -t 1 (the serial COO CPU path) is not part of this library;
 //   * -w sets the nonzeros each worker team owns (w * 128) instead of warps
 //     per fiber; without -w the per-mode autotuner chooses;
-//   * -o writes the output of mode -m (every mode is computed for -t 12).
+//   * -o writes the output of mode -m (every mode is computed for -t 12);
+//   * -i accepts a binary COO file (name ending in .bin, mmcsf_coo_write_bin).
 // Factors are the reference's non-CPD constants U[m] = m + 0.5
 // (src/util.h:3209-3227), so printed values are directly comparable.
 #include <cuda_runtime.h>
@@ -90,7 +91,9 @@ int main(int argc, char** argv) {
     return 1;
   }
   mmcsf_coo* X = nullptr;
-  int st = mmcsf_coo_load_tns(o.inFileName.c_str(), &X);
+  const std::string& in = o.inFileName;
+  const bool bin = in.size() > 4 && in.compare(in.size() - 4, 4, ".bin") == 0;
+  int st = bin ? mmcsf_coo_load_bin(in.c_str(), &X) : mmcsf_coo_load_tns(in.c_str(), &X);
   if (st) return fail("load_tensor", st);
   int nd = 0;
   uint64_t dims[4] = {0, 0, 0, 0}, nnz = 0;

@@ -3,10 +3,16 @@
 // The .tns reader replaces load_tensor (src/util.h:313-370): same format
 // (order, mode lengths, then 1-based coordinates and a value per line), read
 // once with a hand-rolled parser over the whole file instead of two passes of
-// iostream extraction. The nonzero count is the number of complete entries
-// parsed; the reference takes (#lines - 2), which differs only for files with
-// trailing blank lines.
+// iostream extraction, split across host threads at line ends (one nonzero
+// per line) and concatenated in file order, so the result is the sequential
+// parse. The nonzero count is the number of complete entries parsed; the
+// reference takes (#lines - 2), which differs only for files with trailing
+// blank lines. A binary COO file (mmcsf_coo_write_bin / mmcsf_coo_load_bin)
+// skips the text parse on later runs.
+#include <algorithm>
 #include <cerrno>
+#include <thread>
+#include <vector>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -135,29 +141,79 @@ extern "C" int mmcsf_coo_load_tns(const char* path, mmcsf_coo** out) {
   if (!X) return set_error(MMCSF_ERR_NOMEM, "host allocation failed");
   X->nd = nd;
   for (int m = 0; m < nd; ++m) X->dims[m] = dims[m];
-  // rough capacity guess: ~4 bytes per token
-  size_t guess = got / (size_t)(4 * (nd + 1)) + 16;
-  for (int m = 0; m < nd; ++m) X->h_inds[m].reserve(guess);
-  X->h_vals.reserve(guess);
-  for (;;) {
-    uint64_t c[4];
-    const char* q = p;
-    int m = 0;
-    for (; m < nd; ++m)
-      if (!(q = parse_u64(q, e, &c[m]))) break;
-    if (m < nd) break;
-    float v;
-    if (!(q = parse_f32(q, e, &v))) break;
-    for (int k = 0; k < nd; ++k) {
-      if (c[k] == 0 || c[k] > dims[k]) {
-        delete X;
-        return set_error(MMCSF_ERR_IO, "%s: coordinate %llu of mode %d outside [1, %llu]", path,
-                         (unsigned long long)c[k], k, (unsigned long long)dims[k]);
+  // entries, split into per-thread chunks that start after a newline
+  struct Chunk {
+    std::vector<uint32_t> inds[4];
+    std::vector<float> vals;
+    bool stopped = false;  // an unparsable token before the chunk's end: the file's entries end here
+    uint64_t bad = 0;      // a coordinate outside its mode (1-based value), with its mode in bad_mode
+    int bad_mode = -1;
+  };
+  const size_t body = (size_t)(e - p);
+  unsigned T = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+  T = (unsigned)std::min<size_t>(T, body / (256 * 1024) + 1);
+  std::vector<const char*> cut(T + 1);
+  cut[0] = p;
+  cut[T] = e;
+  for (unsigned t = 1; t < T; ++t) {
+    const char* c = std::max(cut[t - 1], p + body * t / T);
+    while (c < e && *c != '\n') ++c;
+    cut[t] = c < e ? c + 1 : e;
+  }
+  std::vector<Chunk> ch(T);
+  auto work = [&](unsigned t) {
+    Chunk& C = ch[t];
+    const size_t guess = (size_t)(cut[t + 1] - cut[t]) / (size_t)(4 * (nd + 1)) + 16;
+    for (int m = 0; m < nd; ++m) C.inds[m].reserve(guess);
+    C.vals.reserve(guess);
+    const char* q0 = cut[t];
+    const char* ce = cut[t + 1];
+    for (;;) {
+      uint64_t c[4];
+      const char* q = q0;
+      int m = 0;
+      for (; m < nd; ++m)
+        if (!(q = parse_u64(q, ce, &c[m]))) break;
+      float v;
+      if (m < nd || !(q = parse_f32(q, ce, &v))) {
+        C.stopped = skip_ws(q0, ce) < ce;
+        break;
       }
-      X->h_inds[k].push_back((uint32_t)(c[k] - 1));
+      for (int k = 0; k < nd; ++k) {
+        if (c[k] == 0 || c[k] > dims[k]) {
+          C.bad = c[k];
+          C.bad_mode = k;
+          return;
+        }
+        C.inds[k].push_back((uint32_t)(c[k] - 1));
+      }
+      C.vals.push_back(v);
+      q0 = q;
     }
-    X->h_vals.push_back(v);
-    p = q;
+  };
+  {
+    std::vector<std::thread> th;
+    for (unsigned t = 1; t < T; ++t) th.emplace_back(work, t);
+    work(0);
+    for (auto& x : th) x.join();
+  }
+  uint64_t total = 0;
+  unsigned used = 0;
+  for (; used < T; ++used) {
+    const Chunk& C = ch[used];
+    if (C.bad_mode >= 0) {
+      delete X;
+      return set_error(MMCSF_ERR_IO, "%s: coordinate %llu of mode %d outside [1, %llu]", path,
+                       (unsigned long long)C.bad, C.bad_mode, (unsigned long long)dims[C.bad_mode]);
+    }
+    total += C.vals.size();
+    if (C.stopped) { ++used; break; }
+  }
+  for (int m = 0; m < nd; ++m) X->h_inds[m].reserve(total);
+  X->h_vals.reserve(total);
+  for (unsigned t = 0; t < used; ++t) {
+    for (int m = 0; m < nd; ++m) X->h_inds[m].insert(X->h_inds[m].end(), ch[t].inds[m].begin(), ch[t].inds[m].end());
+    X->h_vals.insert(X->h_vals.end(), ch[t].vals.begin(), ch[t].vals.end());
   }
   X->nnz = X->h_vals.size();
   int st = check_shape(nd, dims, X->nnz);
@@ -235,6 +291,70 @@ extern "C" int mmcsf_coo_write_tns(mmcsf_coo* X, const char* path) {
     fprintf(f, "%.9g\n", (double)X->h_vals[x]);
   }
   fclose(f);
+  return MMCSF_OK;
+}
+
+// Binary COO file: "MMCSFCOO", u32 version (1), u32 order, u64 nonzeros,
+// u64 mode lengths[4], then the order's uint32 index arrays (0-based) and the
+// float32 values, little-endian as written by this host.
+namespace {
+constexpr char BIN_MAGIC[8] = {'M', 'M', 'C', 'S', 'F', 'C', 'O', 'O'};
+struct BinHeader {
+  char magic[8];
+  uint32_t version, nd;
+  uint64_t nnz, dims[4];
+};
+}  // namespace
+
+extern "C" int mmcsf_coo_write_bin(mmcsf_coo* X, const char* path) {
+  if (!X || !path) return set_error(MMCSF_ERR_INVALID, "null argument");
+  MMCSF_TRY(mmcsf_coo_to_host(X));
+  FILE* f = fopen(path, "wb");
+  if (!f) return set_error(MMCSF_ERR_IO, "cannot open %s", path);
+  BinHeader h{};
+  memcpy(h.magic, BIN_MAGIC, 8);
+  h.version = 1;
+  h.nd = (uint32_t)X->nd;
+  h.nnz = X->nnz;
+  for (int m = 0; m < X->nd; ++m) h.dims[m] = X->dims[m];
+  bool ok = fwrite(&h, sizeof h, 1, f) == 1;
+  for (int m = 0; m < X->nd && ok; ++m)
+    ok = X->nnz == 0 || fwrite(X->h_inds[m].data(), 4, X->nnz, f) == X->nnz;
+  ok = ok && (X->nnz == 0 || fwrite(X->h_vals.data(), 4, X->nnz, f) == X->nnz);
+  ok = (fclose(f) == 0) && ok;
+  return ok ? MMCSF_OK : set_error(MMCSF_ERR_IO, "write to %s failed", path);
+}
+
+extern "C" int mmcsf_coo_load_bin(const char* path, mmcsf_coo** out) {
+  if (!path || !out) return set_error(MMCSF_ERR_INVALID, "null argument");
+  FILE* f = fopen(path, "rb");
+  if (!f) return set_error(MMCSF_ERR_IO, "%s does not exist!", path);
+  BinHeader h{};
+  if (fread(&h, sizeof h, 1, f) != 1 || memcmp(h.magic, BIN_MAGIC, 8) != 0 || h.version != 1) {
+    fclose(f);
+    return set_error(MMCSF_ERR_IO, "%s is not a binary COO file of this library", path);
+  }
+  const int st0 = check_shape((int)h.nd, h.dims, h.nnz);
+  if (st0 != MMCSF_OK) { fclose(f); return st0; }
+  mmcsf_coo* X = new (std::nothrow) mmcsf_coo;
+  if (!X) { fclose(f); return set_error(MMCSF_ERR_NOMEM, "host allocation failed"); }
+  X->nd = (int)h.nd;
+  X->nnz = h.nnz;
+  bool ok = true;
+  for (int m = 0; m < X->nd; ++m) {
+    X->dims[m] = h.dims[m];
+    X->h_inds[m].resize(h.nnz);
+    ok = ok && (h.nnz == 0 || fread(X->h_inds[m].data(), 4, h.nnz, f) == h.nnz);
+  }
+  X->h_vals.resize(h.nnz);
+  ok = ok && (h.nnz == 0 || fread(X->h_vals.data(), 4, h.nnz, f) == h.nnz);
+  fclose(f);
+  for (int m = 0; m < X->nd && ok; ++m)
+    for (uint64_t x = 0; x < h.nnz; ++x)
+      if (X->h_inds[m][x] >= h.dims[m]) { ok = false; break; }
+  if (!ok) { delete X; return set_error(MMCSF_ERR_IO, "%s: truncated or out-of-range entries", path); }
+  X->host_valid = true;
+  *out = X;
   return MMCSF_OK;
 }
 

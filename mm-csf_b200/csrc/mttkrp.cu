@@ -603,13 +603,14 @@ __global__ void __launch_bounds__(256, MB) k_mttkrp_rows(const Args<T> a) {
       constexpr bool SLOW = decltype(slow_tag)::value;
 #pragma unroll
       for (int jb = 0; jb < G; jb += PF) {
-        float4 rc[OUT == 0 ? PF : 1][V], rb[PF][V], rq[ND == 4 ? PF : 1][V];
+        float4 rc[OUT == 0 ? PF : 1][V], rb[PF][V];
+        [[maybe_unused]] float4 rq[ND == 4 ? PF : 1][V];
         uint32_t kj[PF];
 #pragma unroll
         for (int j = 0; j < PF; ++j) {
           kj[j] = __shfl_sync(FULL, k, tb + jb + j);
           const uint32_t bj = __shfl_sync(FULL, b, tb + jb + j);
-          uint32_t qj = 0;
+          [[maybe_unused]] uint32_t qj = 0;
           if constexpr (ND == 4) qj = __shfl_sync(FULL, q, tb + jb + j);
 #pragma unroll
           for (int v = 0; v < V; ++v) {

@@ -61,6 +61,13 @@ class CooTensor:
         return cls(h)
 
     @classmethod
+    def load_bin(cls, path):
+        """A binary COO file written by write_bin (no text parse)."""
+        h = c_voidp()
+        check(lib().mmcsf_coo_load_bin(path.encode(), ctypes.byref(h)))
+        return cls(h)
+
+    @classmethod
     def from_arrays(cls, dims, inds, vals):
         nd = len(dims)
         d = (c_u64 * nd)(*[int(x) for x in dims])
@@ -142,6 +149,9 @@ class CooTensor:
 
     def write_tns(self, path):
         check(lib().mmcsf_coo_write_tns(self._h, path.encode()))
+
+    def write_bin(self, path):
+        check(lib().mmcsf_coo_write_bin(self._h, path.encode()))
 
     def close(self):
         if self._h:

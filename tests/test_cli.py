@@ -70,3 +70,13 @@ def test_cli_formats_and_modes(nd, tmp_path):
                 assert head[0] == str(dims[m]) and got.shape == (dims[m], R)
                 want = O.mttkrp_coo_f64(dims, inds, vals, m, U)
                 assert np.all(np.abs(got - want) <= 0.006 + 1e-5 * np.abs(want)), (t, m, extra)
+    # the same tensor from a binary COO file
+    import mmcsf
+    bpath = tmp_path / "x.bin"
+    mmcsf.CooTensor.load_tns(str(tns)).write_bin(str(bpath))
+    out = tmp_path / "o_bin.txt"
+    p = _run(["-i", str(bpath), "-m", "1", "-R", str(R), "-t", "8", "-w", "2", "-c", "1", "-o", str(out)])
+    assert p.returncode == 0 and "Correctness pass!" in p.stdout, p.stderr
+    _, got = _read_out(out)
+    want = O.mttkrp_coo_f64(dims, inds, vals, 1, U)
+    assert np.all(np.abs(got - want) <= 0.006 + 1e-5 * np.abs(want))

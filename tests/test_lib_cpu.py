@@ -80,3 +80,43 @@ def test_from_arrays_validates_indices():
         mmcsf.CooTensor.from_arrays([2, 2, 2], [np.array([0]), np.array([5]), np.array([0])], np.array([1.0]))
     X = mmcsf.CooTensor.from_arrays([2, 3, 4], [np.array([1]), np.array([2]), np.array([3])], np.array([2.5]))
     assert X.info() == (3, [2, 3, 4], 1)
+
+
+def test_tns_parallel_parse_and_binary_roundtrip(tmp_path):
+    """A multi-megabyte .tns (parsed by several host threads) gives exactly the
+    oracle's sequential parse; junk ends the entries where a sequential parse
+    stops; an out-of-range coordinate is an error; the binary COO file
+    round-trips the tensor."""
+    import mmcsf
+    rng = np.random.default_rng(5)
+    dims = [300, 200, 100]
+    n = 250000
+    inds = [rng.integers(0, d, n).astype(np.uint64) for d in dims]
+    vals = (rng.random(n) * 10).astype(np.float32)
+    path = str(tmp_path / "big.tns")
+    O.write_tns(path, dims, inds, vals)
+    X = mmcsf.CooTensor.load_tns(path)
+    got_i, got_v = X.host_arrays()
+    ref_dims, ref_i, ref_v = O.load_tns(path)
+    assert X.dims == [int(d) for d in ref_dims] and X.nnz == len(ref_v) == n
+    for a, b in zip(got_i, ref_i):
+        assert np.array_equal(a.astype(np.uint64), np.asarray(b, np.uint64))
+    assert np.array_equal(got_v.view(np.uint32), np.asarray(ref_v, np.float32).view(np.uint32))
+    with open(path, "a") as fh:
+        fh.write("1 1 x 0.5\n2 2 2 1.0\n")
+    assert mmcsf.CooTensor.load_tns(path).nnz == n
+    bad = str(tmp_path / "bad.tns")
+    with open(bad, "w") as fh:
+        fh.write("3\n2 2 2\n1 1 1 1.0\n1 3 1 2.0\n")
+    with pytest.raises(mmcsf.MmcsfError):
+        mmcsf.CooTensor.load_tns(bad)
+    bpath = str(tmp_path / "big.bin")
+    X.write_bin(bpath)
+    Y = mmcsf.CooTensor.load_bin(bpath)
+    yi, yv = Y.host_arrays()
+    assert Y.dims == X.dims and Y.nnz == n
+    assert all(np.array_equal(a, b) for a, b in zip(yi, got_i)) and np.array_equal(yv, got_v)
+    with open(bpath, "r+b") as fh:
+        fh.write(b"NOTMAGIC")
+    with pytest.raises(mmcsf.MmcsfError):
+        mmcsf.CooTensor.load_bin(bpath)

@@ -239,6 +239,16 @@ int mmcsf_sampled_model(const mmcsf_format* F, int R, int factor_dtype, const vo
 int mmcsf_cp_adjoint(const mmcsf_format* F, int mode, int R, int factor_dtype, const void* const* d_factors,
                      const float* d_lambda, const float* d_grad, float* d_out, const mmcsf_kernel_cfg* cfg,
                      void* stream);
+/* Fused Poisson step for gradient CP on a 3-D format (no counterpart in the
+ * reference): one pass that computes, for every nonzero x (format order),
+ * w[x] = y[x] / (xhat[x] + eps) with xhat the CP model (no lambda) and y the
+ * tensor's values, loss = sum_x y[x] log(xhat[x] + eps) (one device double),
+ * and the gradient of that loss with respect to the factor of the format's
+ * slice mode (*root_mode = that mode), d_grad_root: dims[root] x R FP32. The
+ * gradients of the other factors are mmcsf_cp_adjoint with d_grad = d_w.
+ * Overwrites d_grad_root and d_loss. R in {4, 8, 16, 32, 64}. */
+int mmcsf_poisson_step(const mmcsf_format* F, int R, int factor_dtype, const void* const* d_factors, float eps,
+                       float* d_w, float* d_grad_root, double* d_loss, int* root_mode, void* stream);
 /* Device pointer to F's values in its nonzero order, and their count. */
 int mmcsf_format_values(const mmcsf_format* F, const float** d_vals, uint64_t* nnz);
 

@@ -464,6 +464,24 @@ class Format:
                                      self._cfg(cfg), _stream(stream)))
         return out
 
+    def poisson_step(self, factors, eps=1e-10, stream=None):
+        """Fused Poisson step (mmcsf_poisson_step): returns (w, grad_root,
+        loss, root_mode) with w[x] = y[x] / (xhat[x] + eps), loss =
+        sum_x y[x] log(xhat[x] + eps) (a 1-element float64 CUDA tensor) and
+        grad_root its gradient for the slice mode's factor."""
+        import torch
+        R = factors[0].shape[1]
+        dev = factors[0].device
+        root = ctypes.c_int()
+        w = torch.empty(self.nnz, dtype=torch.float32, device=dev)
+        order0 = self.info(self._main_part())["mode_order"][0]
+        g = torch.empty((self.dims[order0], R), dtype=torch.float32, device=dev)
+        loss = torch.empty(1, dtype=torch.float64, device=dev)
+        fp = (c_voidp * self.nd)(*[_ptr(f) for f in factors])
+        check(lib().mmcsf_poisson_step(self._h, R, self._dtype(factors), fp, ctypes.c_float(eps), _ptr(w), _ptr(g),
+                                       _ptr(loss), ctypes.byref(root), _stream(stream)))
+        return w, g, loss, root.value
+
     @property
     def last_launches(self):
         n = ctypes.c_int()

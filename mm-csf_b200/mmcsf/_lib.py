@@ -107,6 +107,8 @@ SIGNATURES = {
                            c_int),
     "mmcsf_coo_write_bin": ([c_voidp, ctypes.c_char_p], c_int),
     "mmcsf_coo_load_bin": ([ctypes.c_char_p, ctypes.POINTER(c_voidp)], c_int),
+    "mmcsf_poisson_step": ([c_voidp, c_int, c_int, ctypes.POINTER(c_voidp), ctypes.c_float, c_voidp, c_voidp,
+                            c_voidp, ctypes.POINTER(c_int), c_voidp], c_int),
     "mmcsf_sort_coo_noalloc": ([c_int, c_int, c_int, c_u64p, c_u64, ctypes.POINTER(c_voidp), c_voidp,
                                 ctypes.POINTER(c_voidp), c_voidp, c_voidp], c_int),
 }

@@ -22,7 +22,7 @@ import time
 
 import torch
 
-__all__ = ["SampledCP", "sampled_cp", "poisson_loss", "gcp_poisson"]
+__all__ = ["SampledCP", "PoissonNZ", "sampled_cp", "poisson_loss", "gcp_poisson"]
 
 
 class SampledCP(torch.autograd.Function):
@@ -71,19 +71,57 @@ class SampledCP(torch.autograd.Function):
         return (None, None, g_lam, *grads)
 
 
+class PoissonNZ(torch.autograd.Function):
+    """L = PoissonNZ.apply(fmt, precision, eps, *factors) = sum over the
+    nonzeros of y log(xhat + eps) (no lambda), through the fused kernel
+    (mmcsf_poisson_step): the forward pass also yields w = y / (xhat + eps)
+    and the slice mode's gradient, so the backward pass only runs the
+    adjoints of the other modes (mmcsf_cp_adjoint with w)."""
+
+    @staticmethod
+    def forward(ctx, fmt, precision, eps, *factors):
+        kdt = torch.bfloat16 if precision == "bf16" else factors[0].dtype
+        work = [f.detach().to(kdt).contiguous() for f in factors]
+        w, g_root, loss, root = fmt.poisson_step(work, eps)
+        ctx.fmt, ctx.root = fmt, root
+        ctx.dtypes = [f.dtype for f in factors]
+        ctx.save_for_backward(w, g_root, *work)
+        return loss[0].float()
+
+    @staticmethod
+    def backward(ctx, go):
+        w, g_root, *work = ctx.saved_tensors
+        grads = [None] * len(work)
+        for n in range(len(work)):
+            if not ctx.needs_input_grad[3 + n]:
+                continue
+            g = g_root if n == ctx.root else ctx.fmt.cp_adjoint(n, work, w)
+            grads[n] = (g * go).to(ctx.dtypes[n])
+        return (None, None, None, *grads)
+
+
+def _fused_ok(fmt, factors, lam):
+    return (lam is None and fmt.nd == 3 and factors[0].shape[1] in (4, 8, 16, 32, 64)
+            and fmt.impl == 12)
+
+
 def sampled_cp(fmt, factors, lam=None, precision="fp32"):
     """Differentiable sampled CP model at the format's nonzeros."""
     return SampledCP.apply(fmt, precision, lam, *factors)
 
 
-def poisson_loss(fmt, factors, y, lam=None, precision="fp32", eps=1e-10):
+def poisson_loss(fmt, factors, y, lam=None, precision="fp32", eps=1e-10, fused=True):
     """sum over every entry of m - y log(m + eps), m the CP model, y the
-    tensor (zero off its nonzeros); y: nnz values in the format's order."""
-    xhat = sampled_cp(fmt, factors, lam, precision)
+    tensor (zero off its nonzeros); y: nnz values in the format's order.
+    fused: use the one-pass kernel (3-D, no lambda, R <= 64; y must then be
+    the format's own values) instead of the sampled model + torch ops."""
     cs = factors[0].float().sum(0)
     for f in factors[1:]:
         cs = cs * f.float().sum(0)
     total = (cs * lam).sum() if lam is not None else cs.sum()
+    if fused and _fused_ok(fmt, factors, lam):
+        return total - PoissonNZ.apply(fmt, precision, eps, *factors)
+    xhat = sampled_cp(fmt, factors, lam, precision)
     return total - (y * torch.log(xhat + eps)).sum()
 
 

@@ -209,3 +209,32 @@ def test_gcp_poisson_bf16_tracks_fp32(torch_cuda):
             assert float(f.min()) >= 0.0
     l32, l16 = runs["fp32"]["loss"][-1], runs["bf16"]["loss"][-1]
     assert abs(l16 - l32) <= 1e-3 * abs(l32), (l32, l16)
+
+
+@pytest.mark.parametrize("impl,views", [(12, 0), (12, 1), (12, 2)])
+@pytest.mark.parametrize("R", [8, 32, 64])
+@pytest.mark.parametrize("precision", ["fp32", "bf16"])
+def test_fused_poisson_step_matches_unfused(impl, views, R, precision, torch_cuda):
+    """The one-pass Poisson kernel (model, w = y/(xhat+eps), loss, slice-mode
+    gradient) gives the loss and every factor gradient of the sampled model +
+    torch ops + adjoints path."""
+    torch = torch_cuda
+    from mmcsf import gcp
+    dims = [700, 400, 90]
+    X, F = _build(dims, 60000, seed=R, impl=impl, mode=0, views=views, zipf=True, poisson=True, planted=4)
+    rng = np.random.default_rng(R)
+    U = [_bf16_round(0.2 + rng.random((d, R)).astype(np.float32)) for d in dims]
+    res = {}
+    for fused in (False, True):
+        masters = [torch.tensor(u, device="cuda", requires_grad=True) for u in U]
+        loss = gcp.poisson_loss(F, masters, F.values(), precision=precision, fused=fused)
+        loss.backward()
+        res[fused] = (float(loss.detach()), [m.grad.double().cpu().numpy() for m in masters])
+    l0, g0 = res[False]
+    l1, g1 = res[True]
+    assert abs(l1 - l0) <= 1e-5 * abs(l0), (l0, l1)
+    for a, b in zip(g0, g1):
+        assert np.abs(a - b).max() <= 1e-5 * np.abs(a).max()
+    # one launch computes the model, the loss and the slice-mode gradient
+    w, g_root, lz, root = F.poisson_step([torch.tensor(u, device="cuda") for u in U])
+    assert F.last_launches == 1 and w.shape == (F.nnz,) and g_root.shape[0] == dims[root]

@@ -84,3 +84,36 @@ def test_cpd_errors(torch_cuda):
     B = mmcsf.Format(X, impl=mmcsf.IMPL_BCSF)
     with pytest.raises(mmcsf.MmcsfError):
         B.cpd(8)
+
+
+@pytest.mark.parametrize("precision,tol", [("fp32", 1e-4), ("fp64solve", 1e-6)])
+def test_cpd_4d_tracks_fp64_oracle(precision, tol, torch_cuda):
+    """CP-ALS on a 4-D tensor (the reference's cpd is 3-D only)."""
+    import mmcsf
+    dims = [30, 25, 20, 15]
+    X, inds, vals = _tensor(dims, 6000, seed=44, planted=3, noise=0.01)
+    F = mmcsf.Format(X, impl=mmcsf.IMPL_MMCSF, views=1)
+    U, Ud = _init(torch_cuda, dims, 8, seed=45)
+    res = F.cpd(8, max_iters=6, tol=1e-12, precision=precision, init=Ud)
+    _, lam_o, fit_o, hist_o = CO.cp_als(dims, inds, vals, U, max_iters=6, tol=1e-12)
+    assert res["iters"] == 6
+    assert np.max(np.abs(np.array(res["history"]) - np.array(hist_o))) <= tol, (res["history"], hist_o)
+
+
+def test_cpd_resume_from_checkpoint(torch_cuda):
+    """Checkpoint/resume: the normalised factors and lambda of a run, with
+    lambda folded back into one factor, restart ALS where it stopped; 3 + 3
+    iterations give the fits of the 4th..6th iterations of one 6-iteration
+    run (the model's scale split does not change an ALS update)."""
+    import mmcsf
+    torch = torch_cuda
+    dims = [40, 55, 30]
+    X, _, _ = _tensor(dims, 6000, seed=7, planted=4, noise=0.01)
+    F = mmcsf.Format(X, impl=mmcsf.IMPL_MMCSF, views=1)
+    _, Ud = _init(torch, dims, 8, seed=8)
+    full = F.cpd(8, max_iters=6, tol=1e-12, precision="fp64solve", init=Ud)
+    first = F.cpd(8, max_iters=3, tol=1e-12, precision="fp64solve", init=Ud)
+    ck = [f.clone() for f in first["factors"]]
+    ck[0] = ck[0] * torch.tensor(first["lambda"], dtype=torch.float32, device="cuda")
+    second = F.cpd(8, max_iters=3, tol=1e-12, precision="fp64solve", init=ck)
+    assert np.max(np.abs(np.array(second["history"]) - np.array(full["history"][3:]))) <= 1e-6

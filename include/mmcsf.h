@@ -222,6 +222,19 @@ int mmcsf_set_plan(mmcsf_format* F, const mmcsf_plan* plan);
 int mmcsf_probe_gather(const uint32_t* d_idx, uint64_t n, const float* d_rows, uint64_t nrows, int R, int reps,
                        float* ms_out, void* stream);
 
+/* ---- TTM ------------------------------------------------------------------
+ * Replaces TTM_GPU / TTM_CPU (src/ttm_gpu.cu:83-143, src/ttm_cpu.cpp:60-86):
+ * on a 3-D B-CSF format built for mode m (-t 8, -m m, -f as given), for every
+ * leaf fiber f of its CSF, in the format's fiber order,
+ *   d_Y[f, :] = sum over the fiber's nonzeros of val * d_factor[leaf index, :]
+ * (d_factor: the leaf mode's factor, dims[leaf] x R; d_Y: n_fibers x R FP32,
+ * overwritten; the reference's semi-sparse Y without its unused sentinel row).
+ * The fibers' coordinates are mmcsf_format_export(F, 0, "fbrIdx0/1",
+ * "fbrPtr0"). With d_factor and d_Y NULL only *n_fibers is returned.
+ * R in {4, 8, ..., 128}. */
+int mmcsf_ttm(const mmcsf_format* F, int R, int factor_dtype, const void* d_factor, float* d_Y, uint64_t* n_fibers,
+              void* stream);
+
 /* ---- sampled model and its adjoint (gradient-based CP) -------------------
  * No counterpart in the reference. The sampled CP model at every nonzero,
  * xhat[x] = sum_r lambda_r prod_m A_m[i_m(x), r] (d_lambda may be NULL for

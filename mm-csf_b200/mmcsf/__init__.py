@@ -482,6 +482,20 @@ class Format:
                                        _ptr(loss), ctypes.byref(root), _stream(stream)))
         return w, g, loss, root.value
 
+    def ttm(self, factor, out=None, stream=None):
+        """TTM along the leaf mode of a 3-D B-CSF format (mmcsf_ttm): one
+        R-vector per leaf fiber, in the format's fiber order. factor: the
+        leaf mode's factor (dims[leaf] x R, float32 or bfloat16, CUDA)."""
+        import torch
+        R = factor.shape[1]
+        n = c_u64()
+        check(lib().mmcsf_ttm(self._h, R, self._dtype([factor]), None, None, ctypes.byref(n), _stream(stream)))
+        if out is None:
+            out = torch.empty((int(n.value), R), dtype=torch.float32, device=factor.device)
+        check(lib().mmcsf_ttm(self._h, R, self._dtype([factor]), _ptr(factor), _ptr(out), ctypes.byref(n),
+                              _stream(stream)))
+        return out
+
     @property
     def last_launches(self):
         n = ctypes.c_int()

@@ -109,6 +109,7 @@ SIGNATURES = {
     "mmcsf_coo_load_bin": ([ctypes.c_char_p, ctypes.POINTER(c_voidp)], c_int),
     "mmcsf_poisson_step": ([c_voidp, c_int, c_int, ctypes.POINTER(c_voidp), ctypes.c_float, c_voidp, c_voidp,
                             c_voidp, ctypes.POINTER(c_int), c_voidp], c_int),
+    "mmcsf_ttm": ([c_voidp, c_int, c_int, c_voidp, c_voidp, c_u64p, c_voidp], c_int),
     "mmcsf_sort_coo_noalloc": ([c_int, c_int, c_int, c_u64p, c_u64, ctypes.POINTER(c_voidp), c_voidp,
                                 ctypes.POINTER(c_voidp), c_voidp, c_voidp], c_int),
 }

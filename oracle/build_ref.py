@@ -1,8 +1,9 @@
 #!/usr/bin/env python3
 """Build recipe for the reference-as-oracle library (test infrastructure).
 
-Compiles isratnisa/MM-CSF's own host code (format builders in src/util.h and
-the COO CPU MTTKRP in src/mttkrp_cpu.cpp) together with oracle/ref_harness.cpp
+Compiles isratnisa/MM-CSF's own host code (format builders in src/util.h, the
+COO CPU MTTKRP in src/mttkrp_cpu.cpp and the CPU TTM in src/ttm_cpu.cpp)
+together with oracle/ref_harness.cpp
 into oracle/_ref/libmmcsf_ref.so.
 
 The reference does not build as shipped with this image's g++ 13:
@@ -31,7 +32,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 OUT_DIR = os.path.join(HERE, "_ref")
 OUT_LIB = os.path.join(OUT_DIR, "libmmcsf_ref.so")
 DEFAULT_SRC = "/root/reference/src"
-FILES = ["util.h", "mttkrp_cpu.h", "mttkrp_cpu.cpp"]
+FILES = ["util.h", "mttkrp_cpu.h", "mttkrp_cpu.cpp", "ttm_cpu.h", "ttm_cpu.cpp"]
 CXXFLAGS = ["-std=c++14", "-fopenmp", "-fPIC", "-Wreturn-type"]
 WARN_RE = re.compile(r"^(?P<file>[^:\s]+):(?P<line>\d+):(?P<col>\d+): warning: "
                      r"(no return statement in function returning non-void|"
@@ -88,7 +89,8 @@ def build(src=DEFAULT_SRC, force=False, verbose=True):
             os.chmod(os.path.join(build_dir, f), 0o644)
         harness = os.path.join(HERE, "ref_harness.cpp")
         units = [(harness, os.path.join(build_dir, "harness.o")),
-                 (os.path.join(build_dir, "mttkrp_cpu.cpp"), os.path.join(build_dir, "mttkrp_cpu.o"))]
+                 (os.path.join(build_dir, "mttkrp_cpu.cpp"), os.path.join(build_dir, "mttkrp_cpu.o")),
+                 (os.path.join(build_dir, "ttm_cpu.cpp"), os.path.join(build_dir, "ttm_cpu.o"))]
         total = 0
         for _ in range(8):
             patched = 0

@@ -219,6 +219,21 @@ void orc_hyb_bins(int nd, const u64* const* ptr, u64 nslc, u64 totNnz, int* bin_
  * Cyclic mode order (m + mode) % nd; U[mode] is accumulated into. Float
  * arithmetic in the reference's association order ((v*a)*b)*c, no FMA
  * contraction (compile with -ffp-contract=off). */
+/* TTM_CPU (src/ttm_cpu.cpp:60-86) on a 3-D CSF: per leaf fiber f (fptr[f] ..
+ * fptr[f+1]) an FP32 running sum over its nonzeros of vals[x] * U[leaf[x]],
+ * added into y[f] (zeroed here). nfib real fibers (no sentinel row). */
+void orc_ttm_f32(u64 nfib, const u64* fptr, const u64* leaf, const float* vals, const float* U, int R, float* y) {
+  float tmp[1024];
+  for (u64 f = 0; f < nfib; ++f) {
+    for (int r = 0; r < R; ++r) tmp[r] = 0.f;
+    for (u64 x = fptr[f]; x < fptr[f + 1]; ++x) {
+      const float* u = U + leaf[x] * (u64)R;
+      for (int r = 0; r < R; ++r) tmp[r] += vals[x] * u[r];
+    }
+    for (int r = 0; r < R; ++r) y[f * (u64)R + r] = 0.f + tmp[r];
+  }
+}
+
 void orc_mttkrp_coo_f32(int nd, u64 nnz, u64* const* inds, const float* vals, int mode, int R,
                         float* const* U) {
   int cm[8];

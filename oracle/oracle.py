@@ -287,6 +287,30 @@ def build_hyb(dims, inds, vals, mode=0, fbr_th=INF_TH):
 # --------------------------------------------------------------------------
 # MTTKRP
 # --------------------------------------------------------------------------
+def ttm_f32(dims, inds, vals, mode, factor_leaf, fbr_th=INF_TH):
+    """TTM_CPU (src/ttm_cpu.cpp:60-86) on the CSF of `mode` as the reference's
+    ttm builds it (the sort of mttkrp -t 8, create_HCSR with the -f split).
+    Returns (Y (F x R float32, one row per real fiber), ptr, idx) with the
+    CSF's pointer and index arrays."""
+    order = order_modes(dims, mode)
+    sinds = [np.array(i, dtype=np.uint64) for i in inds]
+    svals = np.array(vals, dtype=np.float32)
+    sort_coo(sinds, svals, order[:2])
+    ptr, idx = create_csf(sinds, order, fbr_th, FBRS_TH_OFF)
+    F = len(ptr[1]) - 1
+    R = factor_leaf.shape[1]
+    y = np.zeros((max(F, 1), R), np.float32)
+    fp = ctypes.POINTER(ctypes.c_float)
+    fptr = np.ascontiguousarray(ptr[1], np.uint64)
+    leaf = np.ascontiguousarray(sinds[order[2]], np.uint64)
+    u = np.ascontiguousarray(factor_leaf, np.float32)
+    v = np.ascontiguousarray(svals, np.float32)
+    lib().orc_ttm_f32(ctypes.c_uint64(F), fptr.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)),
+                      leaf.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)), v.ctypes.data_as(fp),
+                      u.ctypes.data_as(fp), R, y.ctypes.data_as(fp))
+    return y[:F], ptr, idx
+
+
 def mttkrp_coo_f32(inds, vals, mode, factors):
     """MTTKRP_COO_CPU semantics (src/mttkrp_cpu.cpp:60-113) with the output
     zeroed first. factors: list of float32 (dim, R) arrays (not modified)."""
@@ -360,6 +384,19 @@ def ref_dump(kind, tns_path, mode, fbr_th, out_path):
     if rc != 0:
         raise RuntimeError(f"{fn} failed")
     return parse_dump(out_path)
+
+
+def ref_ttm(tns_path, mode, fbr_th, factor_leaf, max_fibers):
+    """The reference's own TTM_CPU (oracle/_ref) on a .tns file: (Y, F)."""
+    R = factor_leaf.shape[1]
+    y = np.zeros((max_fibers, R), np.float32)
+    n = ctypes.c_uint64()
+    fp = ctypes.POINTER(ctypes.c_float)
+    u = np.ascontiguousarray(factor_leaf, np.float32)
+    rc = ref_lib().ref_ttm(tns_path.encode(), mode, ctypes.c_long(fbr_th), R, u.ctypes.data_as(fp),
+                           y.ctypes.data_as(fp), ctypes.c_uint64(max_fibers), ctypes.byref(n))
+    assert rc == 0, "fiber capacity too small"
+    return y[:n.value], int(n.value)
 
 
 def ref_mttkrp_coo(dims, inds, vals, mode, factors):

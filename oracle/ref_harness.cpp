@@ -11,10 +11,12 @@
 // "<name> <count> v0 v1 ...".
 #include "util.h"
 #include "mttkrp_cpu.h"
+#include "ttm_cpu.h"
 
 #include <cstdio>
 #include <cstdint>
 #include <cstdlib>
+#include <cstring>
 #include <new>
 
 // Zero-filled, padded allocations. The reference reads one element past the
@@ -230,6 +232,41 @@ int ref_hyb_dump(const char* tns, int mode, long fbrTh, const char* out) {
 // arrays. inds[m] are 0-based uint64 per mode; factors[m] are row-major
 // dims[m] x R float. factors[mode] is the output and is accumulated into, as
 // the reference does: callers zero it first for a plain MTTKRP.
+// ttm (src/ttm.cu:55-229 with the -f split of create_HCSR): TTM_CPU on the
+// CSF of `mode` after the reference's sort. Y holds up to cap x R floats;
+// *nfib gets the number of real fibers (the reference's Y has one more,
+// unused, sentinel row).
+int ref_ttm(const char* tns, int mode, long fbrTh, int R, const float* u_leaf, float* y, uint64_t cap,
+            uint64_t* nfib) {
+  Options Opt = make_opts(tns, 8, mode, fbrTh);
+  Opt.R = R;
+  Tensor X;
+  load_tensor(X, Opt);
+  sort_COOtensor(X);
+  check_opt(X, Opt);
+  create_HCSR(X, Opt);
+  const ITYPE leaf = X.modeOrder[X.ndims - 1];
+  Matrix* U = new Matrix[X.ndims];
+  for (int m = 0; m < (int)X.ndims; ++m) {
+    U[m].nRows = X.dims[m];
+    U[m].nCols = R;
+    U[m].vals = static_cast<DTYPE*>(std::calloc((size_t)X.dims[m] * R, sizeof(DTYPE)));
+  }
+  std::memcpy(U[leaf].vals, u_leaf, (size_t)X.dims[leaf] * R * sizeof(float));
+  semiSpTensor Y;
+  Y.nRows = X.nFibers;
+  Y.nCols = R;
+  Y.vals = static_cast<DTYPE*>(std::calloc((size_t)X.nFibers * R, sizeof(DTYPE)));
+  TTM_CPU(X, Y, U, Opt);
+  const uint64_t F = X.nFibers ? X.nFibers - 1 : 0;
+  *nfib = F;
+  if (F <= cap) std::memcpy(y, Y.vals, (size_t)F * R * sizeof(float));
+  for (int m = 0; m < (int)X.ndims; ++m) std::free(U[m].vals);
+  delete[] U;
+  std::free(Y.vals);
+  return F <= cap ? 0 : 1;
+}
+
 int ref_coo_mttkrp(int nd, const uint64_t* dims, uint64_t nnz, const uint64_t* const* inds,
                    const float* vals, int mode, int R, float* const* factors) {
   if (nd != 3 && nd != 4) return 1;

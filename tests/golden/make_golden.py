@@ -1,7 +1,7 @@
 #!/usr/bin/env python3
 """Generate the golden fixtures in tests/golden/ from the reference itself.
 
-Runs the reference's own format builders and COO CPU MTTKRP (built as
+Runs the reference's own format builders, COO CPU MTTKRP and CPU TTM (built as
 oracle/_ref/libmmcsf_ref.so by oracle/build_ref.py from the reference's
 sources) on the reference's toy.tns and on seeded synthetic tensors, and
 writes inputs and outputs as JSON. The tests compare both the C oracle and
@@ -72,11 +72,48 @@ def make_case(name, dims, inds, vals, tmp, runs, seed):
     return name
 
 
+def ttm_factor(rows, R):
+    """The leaf factor of the TTM fixtures: a fixed formula, so the tests
+    rebuild it exactly without storing it."""
+    i = np.arange(rows, dtype=np.int64)[:, None]
+    r = np.arange(R, dtype=np.int64)[None, :]
+    return (((i * 31 + r * 17) % 97).astype(np.float32) / np.float32(97.0) + np.float32(0.01)).astype(np.float32)
+
+
+def make_ttm(tmp, names):
+    """ttm.json: the reference's TTM_CPU (its ttm command, src/ttm.cu) on the
+    small 3-D cases above, every mode, -f none / 2, leaf factor ttm_factor."""
+    out = {"R": R_GOLD, "runs": []}
+    for name in names:
+        with open(os.path.join(HERE, name + ".json")) as fh:
+            case = json.load(fh)
+        dims = case["dims"]
+        if len(dims) != 3 or len(case["vals"]) > 160:
+            continue
+        inds = [np.asarray(i, np.uint64) for i in case["inds"]]
+        vals = np.asarray(case["vals"], np.float32)
+        path = os.path.join(tmp, name + "_ttm.tns")
+        O.write_tns(path, dims, inds, vals)
+        for mode in range(3):
+            leaf = O.order_modes(dims, mode)[2]
+            u = ttm_factor(dims[leaf], R_GOLD)
+            for f in (0, 2):
+                y, nf = O.ref_ttm(path, mode, f, u, len(vals) + 2)
+                out["runs"].append({"case": name, "mode": mode, "f": f, "Y": [_tolist(r) for r in y]})
+    with open(os.path.join(HERE, "ttm.json"), "w") as fh:
+        json.dump(out, fh, separators=(",", ":"))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--ttm-only", action="store_true", help="write ttm.json from the existing cases only")
     a = ap.parse_args()
     build_ref.build(os.path.join(a.reference, "src"))
+    if a.ttm_only:
+        with open(os.path.join(HERE, "manifest.json")) as fh:
+            make_ttm(tempfile.mkdtemp(), json.load(fh)["cases"])
+        return
     tmp = tempfile.mkdtemp()
     names = []
     INF = O.INF_TH
@@ -105,6 +142,7 @@ def main():
             for f in (1, 3, INF):
                 runs.append((kind, int(rng.integers(0, nd)), f))
         names.append(make_case(name, dims, inds, vals, tmp, runs, seed=len(names)))
+    make_ttm(tmp, names)
     with open(os.path.join(HERE, "manifest.json"), "w") as fh:
         json.dump({"cases": names, "R": R_GOLD,
                    "source": "reference host code built by oracle/build_ref.py"}, fh, indent=1)

@@ -80,3 +80,44 @@ def test_cli_formats_and_modes(nd, tmp_path):
     _, got = _read_out(out)
     want = O.mttkrp_coo_f64(dims, inds, vals, 1, U)
     assert np.all(np.abs(got - want) <= 0.006 + 1e-5 * np.abs(want))
+
+
+TTM_BIN = os.path.join(ROOT, "mm-csf_b200", "bin", "ttm")
+
+
+def test_ttm_cli_argument_errors():
+    assert os.path.exists(TTM_BIN), "build mm-csf_b200 first"
+    p = subprocess.run([TTM_BIN], capture_output=True, text=True, timeout=60)
+    assert p.returncode != 0 and "usage" in p.stdout
+    p = subprocess.run([TTM_BIN, "-i", "x.tns", "-t", "1"], capture_output=True, text=True, timeout=60)
+    assert p.returncode != 0 and "-t 1 is not provided" in p.stderr
+
+
+@pytest.mark.gpu
+def test_ttm_cli(tmp_path):
+    """The ttm command: every mode, with and without a fiber split, against the
+    oracle's TTM with the reference's constant factor (leaf mode + 0.5)."""
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    rng = np.random.default_rng(11)
+    dims = [50, 70, 40]
+    n = 4000
+    lin = rng.choice(int(np.prod(dims)), size=n, replace=False)
+    inds = [np.asarray(i, np.uint64) for i in np.unravel_index(lin, dims)]
+    vals = np.round(rng.random(n) + 0.1, 3).astype(np.float32)
+    tns = tmp_path / "x.tns"
+    O.write_tns(str(tns), dims, inds, vals)
+    for m in range(3):
+        for f in (0, 3):
+            out = tmp_path / f"y_{m}_{f}.txt"
+            args = [TTM_BIN, "-i", str(tns), "-m", str(m), "-R", "16", "-c", "1", "-o", str(out)]
+            if f:
+                args += ["-f", str(f)]
+            p = subprocess.run(args, capture_output=True, text=True, timeout=300)
+            assert p.returncode == 0 and "TTM GPU - time" in p.stdout and "Correctness pass!" in p.stdout, p
+            head, got = _read_out(out)
+            leaf = O.order_modes(dims, m)[2]
+            want, _, _ = O.ttm_f32(dims, inds, vals, m, np.full((dims[leaf], 16), leaf + 0.5, np.float32),
+                                   f or O.INF_TH)
+            assert got.shape == want.shape and np.all(np.abs(got - want) <= 0.006 + 1e-5 * np.abs(want))

@@ -274,6 +274,33 @@ def bf16_section(F, U32, outs32, steps, warmup):
             "note": "BF16-rounded factor rows, FP32 products and accumulation; the error is the factors' rounding"}
 
 
+def ttm_section(X, dims, R, mode, rows_touched):
+    """TTM along the leaf mode of the B-CSF format of `mode` (the reference's
+    ttm): device time per call and its algorithmic GB/s (values + leaf index
+    per nonzero, the touched leaf rows once, Y written once)."""
+    import torch
+    import mmcsf
+    F = mmcsf.Format(X, impl=mmcsf.IMPL_BCSF, mode=mode)
+    leaf = F.info(0)["mode_order"][2]
+    g = torch.Generator(device="cuda").manual_seed(5)
+    U = torch.rand(dims[leaf], R, device="cuda", generator=g)
+    Y = F.ttm(U)
+    for _ in range(3):
+        F.ttm(U, Y)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(10):
+        F.ttm(U, Y)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / 10
+    nnz, nfib = F.nnz, Y.shape[0]
+    b = nnz * 8 + rows_touched[leaf] * R * 4 + nfib * R * 4
+    return {"mode": mode, "leaf_mode": leaf, "fibers": nfib, "ms": ms, "algorithmic_bytes": b,
+            "gbs": b / (ms / 1e3) / 1e9}
+
+
 def cp_section(seed, scale):
     """CP seconds per iteration to a fixed fit: BF16 factors (+ FP64 solve and
     fit, whole loop in one CUDA graph) against plain FP32 CP-ALS, and Poisson
@@ -562,6 +589,7 @@ def main():
         for m in range(nd):
             F.mttkrp(m, U, outs[m])
         bf16 = bf16_section(F, U, outs, min(a.steps, 20), a.warmup)
+    ttm = ttm_section(X, dims, R, info["mode_order"][0], rows) if nd == 3 and R in (4, 8, 16, 32, 64, 128) else None
     formats = None
     if nd == 4 and not a.no_formats:
         fm = format_section(X, dims, R, tdt)
@@ -579,7 +607,7 @@ def main():
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": e2e, "gpu_launches": launches_per_step * a.steps, "clocks": clocks, "bf16_factors": bf16,
-            "cp": cp, "formats": formats}
+            "ttm": ttm, "cp": cp, "formats": formats}
     print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()

@@ -8,8 +8,11 @@
 // team of G lanes (R = 4*G*V) walks a contiguous, nonzero-balanced chunk,
 // numbers fibers from the fiber-start flags in bit 31 of the leaf index (one
 // ballot and popcount per block of G nonzeros, from the chunk's precomputed
-// first fiber), accumulates in registers and leaves each fiber with one vector
-// reduction (a fiber split across two chunks gets two).
+// first fiber) and accumulates in registers. Y is written with plain stores,
+// never zeroed or read: the team that holds a fiber's first nonzero stores the
+// fiber's row; a team whose chunk begins inside a fiber leaves that partial
+// row in a per-chunk side buffer, and a second small kernel adds the side rows
+// into Y once every owner has stored.
 #include <cuda_bf16.h>
 
 #include "format.h"
@@ -46,8 +49,12 @@ struct TArgs {
   uint64_t nnz;
   uint32_t nfib, chunk;
   const T* U;            // leaf-mode factor, rows of R
-  float* Y;              // F x R, zeroed by the caller
+  float* Y;              // F x R
+  float* side;           // per chunk: R floats, the partial of a fiber begun in an earlier chunk
+  uint32_t* side_fib;    // per chunk: that fiber, or NO_FIB
 };
+
+constexpr uint32_t NO_FIB = 0xffffffffu;
 
 template <int G, int V, class T>
 __global__ void __launch_bounds__(256) k_ttm(const TArgs<T> a) {
@@ -73,6 +80,16 @@ __global__ void __launch_bounds__(256) k_ttm(const TArgs<T> a) {
   float4 acc[V];
 #pragma unroll
   for (int v = 0; v < V; ++v) acc[v] = make_float4(0.f, 0.f, 0.f, 0.f);
+  // the open fiber began in an earlier chunk: its partial goes to the side buffer
+  bool cont = active && (uint64_t)__ldg(a.fptr + f) < x0;
+  auto emit = [&]() {
+    float* dst = cont ? a.side + team * R : a.Y + (uint64_t)f * R;
+#pragma unroll
+    for (int v = 0; v < V; ++v) *reinterpret_cast<float4*>(dst + col(v)) = acc[v];
+    if (cont && tl == 0) a.side_fib[team] = f;
+    cont = false;
+  };
+  if (active && !cont && tl == 0) a.side_fib[team] = NO_FIB;
   for (uint32_t it = 0; it < a.chunk; it += G) {
     const uint64_t xl = x0 + it + tl;
     uint32_t kv = 0;
@@ -91,11 +108,9 @@ __global__ void __launch_bounds__(256) k_ttm(const TArgs<T> a) {
     for (int j = 0; j < G; ++j) {
       const float val = __shfl_sync(FULL, vv, tb + j);
       if ((fm >> j) & 1u) {  // nonzero j opens the next fiber: the open one is complete here
+        emit();
 #pragma unroll
-        for (int v = 0; v < V; ++v) {
-          red4(a.Y + (uint64_t)f * R + col(v), acc[v]);
-          acc[v] = make_float4(0.f, 0.f, 0.f, 0.f);
-        }
+        for (int v = 0; v < V; ++v) acc[v] = make_float4(0.f, 0.f, 0.f, 0.f);
         ++f;
       }
 #pragma unroll
@@ -107,10 +122,21 @@ __global__ void __launch_bounds__(256) k_ttm(const TArgs<T> a) {
       }
     }
   }
-  if (active) {
-#pragma unroll
-    for (int v = 0; v < V; ++v) red4(a.Y + (uint64_t)f * R + col(v), acc[v]);
-  }
+  if (active) emit();
+}
+
+// Y[side_fib[c]] += side[c] for every chunk c that began inside a fiber.
+template <int G>
+__global__ void __launch_bounds__(256) k_ttm_side(const float* __restrict__ side,
+                                                   const uint32_t* __restrict__ side_fib, uint64_t nchunks,
+                                                   uint32_t R, float* __restrict__ Y) {
+  const uint64_t t = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) / G;
+  const int tl = threadIdx.x & (G - 1);
+  if (t >= nchunks) return;
+  const uint32_t f = side_fib[t];
+  if (f == NO_FIB) return;
+  for (uint32_t c = tl * 4; c < R; c += G * 4)
+    red4(Y + (uint64_t)f * R + c, *reinterpret_cast<const float4*>(side + t * R + c));
 }
 
 template <class T>
@@ -150,8 +176,14 @@ extern "C" int mmcsf_ttm(const mmcsf_format* F, int R, int factor_dtype, const v
     return set_error(MMCSF_ERR_INVALID, "bad dtype");
   if (!P.present || P.nnz == 0) return MMCSF_OK;
   cudaStream_t s = S(stream);
-  MMCSF_CUDA(cudaMemsetAsync(d_Y, 0, P.n_fibers() * (uint64_t)R * sizeof(float), s));
   const int slot = CsfPart::cfib_slot(512);
+  const uint64_t nchunks = (P.nnz + 511) / 512;
+  // the per-chunk side rows live with the format, sized for the largest R used
+  mmcsf_format* Fm = const_cast<mmcsf_format*>(F);
+  const uint64_t side_bytes = nchunks * ((uint64_t)R * 4 + 4);
+  if (Fm->ttm_side.bytes < side_bytes) MMCSF_CUDA(Fm->ttm_side.alloc(side_bytes));
+  float* side = Fm->ttm_side.as<float>();
+  uint32_t* side_fib = reinterpret_cast<uint32_t*>(side + nchunks * (uint64_t)R);
   cudaError_t e;
   auto fill = [&](auto& a, auto tag) {
     using T = decltype(tag);
@@ -164,6 +196,8 @@ extern "C" int mmcsf_ttm(const mmcsf_format* F, int R, int factor_dtype, const v
     a.chunk = 512;
     a.U = static_cast<const T*>(d_factor);
     a.Y = d_Y;
+    a.side = side;
+    a.side_fib = side_fib;
   };
   if (factor_dtype == MMCSF_DTYPE_F32) {
     TArgs<float> a{};
@@ -175,6 +209,9 @@ extern "C" int mmcsf_ttm(const mmcsf_format* F, int R, int factor_dtype, const v
     e = launch_ttm<__nv_bfloat16>(a, R, s);
   }
   if (e != cudaSuccess) return set_error(MMCSF_ERR_CUDA, "TTM launch: %s", cudaGetErrorString(e));
-  const_cast<mmcsf_format*>(F)->last_launches = 1;
+  k_ttm_side<8><<<(unsigned)((nchunks * 8 + 255) / 256), 256, 0, s>>>(side, side_fib, nchunks, (uint32_t)R, d_Y);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return set_error(MMCSF_ERR_CUDA, "TTM side launch: %s", cudaGetErrorString(e));
+  Fm->last_launches = 2;
   return MMCSF_OK;
 }

@@ -88,7 +88,7 @@ def test_ttm_gpu_vs_oracle(R, dtype):
                 got = F.ttm(ud).cpu().numpy().astype(np.float64)
                 want, ptr, idx = O.ttm_f32(dims, inds, vals, mode, u, f or O.INF_TH)
                 assert got.shape == want.shape, (mode, f)
-                assert F.last_launches == 1
+                assert F.last_launches == 2  # main pass + side rows
                 scale = np.abs(want).max()
                 assert np.abs(got - want).max() <= 1e-5 * scale, (mode, f)
                 # the rows are the format's fibers: its exported fiber indices are the oracle's

@@ -472,7 +472,7 @@ def main():
         trav = plan[m]["traversal"] if plan else (2 if F.info(4 + m)["present"] else 1)
         pi = F.info(4 + m) if trav == 2 else info
         lvl = pi["mode_order"].index(m)
-        if plan and plan[m].get("kernel") == 3 and nd == 3 and lvl != 1:
+        if plan and plan[m].get("kernel") == 3 and (nd == 3 or lvl in (0, nd - 1)):
             sb = nnz * 12 + pi["n_slices"] * 8  # per-nonzero walk: vals, leaf, mid; slice offsets and indices
         else:
             sb = struct_bytes(nd, nnz, pi["n_fibers"], pi["n_fbrs"])
@@ -550,8 +550,8 @@ def main():
     dorder = F.info(4 + dom)["mode_order"] if dtrav == 2 else info["mode_order"]
     dlvl = dorder.index(dom)
     dk = plan[dom].get("kernel", 0) if plan else 0
-    if dk == 3 and (nd != 3 or dlvl == 1):
-        dk = 2  # the per-nonzero walk serves slice and leaf levels; the middle level runs the fiber walk
+    if dk == 3 and nd == 4 and dlvl not in (0, 3):
+        dk = 1  # the 4-D middle levels run the per-team fiber walk
     dker = {1: "k_mttkrp", 2: "k_mttkrp_flat", 3: "k_mttkrp_rows"}.get(dk or (2 if nd == 3 else 1))
     traffic = traffic_from_profiles(a.workload, R, a.dtype, dom, dker)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,

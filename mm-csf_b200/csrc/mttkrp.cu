@@ -521,10 +521,12 @@ __global__ void __launch_bounds__(256, MB) k_mttkrp_flat(const Args<T> a) {
 // variant.
 template <int ND, int OUT, int G, int V, class T, int MB, int PFX>
 __global__ void __launch_bounds__(256, MB) k_mttkrp_rows(const Args<T> a) {
-  static_assert(OUT == 0 || OUT == ND - 1, "slice or leaf level");
+  static_assert(OUT == 0 || OUT == ND - 1 || (ND == 3 && OUT == 1), "slice, leaf or 3-D middle level");
   constexpr int LEAF = ND - 1;
+  constexpr bool MIDL = ND == 3 && OUT == 1;  // fiber-row output: sum v U2[k] per fiber, times U0[a], one reduction
   constexpr uint32_t R = 4 * G * V;
   constexpr uint32_t FLAG = 0x80000000u;
+  constexpr uint32_t GMASK = G == 32 ? FULL : ((1u << G) - 1u);
   constexpr int PF = G > PFX ? PFX : G;
   const int lane = threadIdx.x & 31;
   const int tl = lane & (G - 1);
@@ -570,8 +572,10 @@ __global__ void __launch_bounds__(256, MB) k_mttkrp_rows(const Args<T> a) {
 #pragma unroll
   for (int v = 0; v < V; ++v) {
     acc[v] = f4(0.f);
-    if constexpr (OUT == LEAF) rowA[v] = ld(U0, ca, v);
+    if constexpr (OUT == LEAF || MIDL) rowA[v] = ld(U0, ca, v);
   }
+  [[maybe_unused]] uint32_t bopen = 0;  // middle level: the open fiber's row
+  if constexpr (MIDL) bopen = __ldg(mid + x0);
 
   auto load_blk = [&](uint32_t itb, uint32_t& kk, uint32_t& bb, uint32_t& qq, float& vq) {
     const uint64_t xx = x0 + itb + tl;
@@ -594,6 +598,8 @@ __global__ void __launch_bounds__(256, MB) k_mttkrp_rows(const Args<T> a) {
     const uint64_t xb = x0 + it;
     const uint32_t k = kc & ~FLAG, b = bc, q = qc;
     const float vv = vc;
+    [[maybe_unused]] uint32_t fm = 0;  // middle level: nonzero j of the block opens a fiber
+    if constexpr (MIDL) fm = (__ballot_sync(FULL, (kc & FLAG) && (xb + tl != x0)) >> tb) & GMASK;
     kc = kn; bc = bn; qc = qn; vc = vn;
     load_blk(it + 2 * G, kn, bn, qn, vn);
     // a slice starts inside this block for some team of the warp
@@ -603,8 +609,10 @@ __global__ void __launch_bounds__(256, MB) k_mttkrp_rows(const Args<T> a) {
       constexpr bool SLOW = decltype(slow_tag)::value;
 #pragma unroll
       for (int jb = 0; jb < G; jb += PF) {
-        float4 rc[OUT == 0 ? PF : 1][V], rb[PF][V];
+        [[maybe_unused]] float4 rc[(OUT == 0 || MIDL) ? PF : 1][V];
+        [[maybe_unused]] float4 rb[MIDL ? 1 : PF][V];
         [[maybe_unused]] float4 rq[ND == 4 ? PF : 1][V];
+        [[maybe_unused]] uint32_t bjs[MIDL ? PF : 1];
         uint32_t kj[PF];
 #pragma unroll
         for (int j = 0; j < PF; ++j) {
@@ -612,9 +620,12 @@ __global__ void __launch_bounds__(256, MB) k_mttkrp_rows(const Args<T> a) {
           const uint32_t bj = __shfl_sync(FULL, b, tb + jb + j);
           [[maybe_unused]] uint32_t qj = 0;
           if constexpr (ND == 4) qj = __shfl_sync(FULL, q, tb + jb + j);
+          if constexpr (MIDL) bjs[j] = bj;
 #pragma unroll
           for (int v = 0; v < V; ++v) {
-            if constexpr (ND == 3) {
+            if constexpr (MIDL) {
+              rc[j][v] = ld(UL, kj[j], v);
+            } else if constexpr (ND == 3) {
               rb[j][v] = ld(U1, bj, v);
             } else {
               rb[j][v] = ld(U2, bj, v);  // level 2 (fiber index c)
@@ -627,6 +638,13 @@ __global__ void __launch_bounds__(256, MB) k_mttkrp_rows(const Args<T> a) {
         for (int j = 0; j < PF; ++j) {
           const float val = __shfl_sync(FULL, vv, tb + jb + j);
           const uint64_t x = xb + jb + j;
+          if constexpr (MIDL) {
+            if ((fm >> (jb + j)) & 1u) {  // the open fiber ends before nonzero j (it is in the old slice)
+#pragma unroll
+              for (int v = 0; v < V; ++v) { rd(bopen, v, pmul(rowA[v], acc[v])); acc[v] = f4(0.f); }
+              bopen = bjs[j];
+            }
+          }
           if constexpr (SLOW) {
             if (x < x1 && x == nxt) {  // slice change (slices are never empty)
               if constexpr (OUT == 0) {
@@ -636,13 +654,16 @@ __global__ void __launch_bounds__(256, MB) k_mttkrp_rows(const Args<T> a) {
               ++sl;
               ca = __ldg(sidx + sl);
               nxt = __ldg(snz + sl + 1);
-              if constexpr (OUT == LEAF) {
+              if constexpr (OUT == LEAF || MIDL) {
 #pragma unroll
                 for (int v = 0; v < V; ++v) rowA[v] = ld(U0, ca, v);
               }
             }
           }
-          if constexpr (OUT == 0) {
+          if constexpr (MIDL) {
+#pragma unroll
+            for (int v = 0; v < V; ++v) acc[v] = pfma_s(val, rc[j][v], acc[v]);
+          } else if constexpr (OUT == 0) {
 #pragma unroll
             for (int v = 0; v < V; ++v) {
               float4 m = pmul_s(val, rb[j][v]);
@@ -669,6 +690,12 @@ __global__ void __launch_bounds__(256, MB) k_mttkrp_rows(const Args<T> a) {
     if (active) {
 #pragma unroll
       for (int v = 0; v < V; ++v) rd(ca, v, acc[v]);
+    }
+  }
+  if constexpr (MIDL) {
+    if (active) {
+#pragma unroll
+      for (int v = 0; v < V; ++v) rd(bopen, v, pmul(rowA[v], acc[v]));
     }
   }
 }
@@ -721,6 +748,8 @@ template <int ND, int G, int V, class T>
 cudaError_t launch_lvl(const Args<T>& a, int lvl, int kern, int threads, int mb, cudaStream_t s) {
   if (kern == 3 && lvl == 0) return launch_rows<ND, 0, G, V, T>(a, threads, mb, s);
   if (kern == 3 && lvl == ND - 1) return launch_rows<ND, ND - 1, G, V, T>(a, threads, mb, s);
+  if constexpr (ND == 3)
+    if (kern == 3 && lvl == 1) return launch_rows<3, 1, G, V, T>(a, threads, mb, s);
   if constexpr (ND == 3) {
     if (kern >= 2) {
       switch (lvl) {
@@ -801,7 +830,7 @@ int part_mttkrp(const mmcsf_format* F, const CsfPart& P, int mode, int R, int dt
   const int mb = cfg && cfg->min_blocks > 0 ? cfg->min_blocks : 2;
   int kern = cfg && cfg->kernel > 0 ? cfg->kernel : (P.nd == 3 ? 2 : 1);
   if (kern < 1 || kern > 3) return set_error(MMCSF_ERR_INVALID, "kernel must be 0, 1, 2 or 3");
-  if (kern == 3 && ((lvl != 0 && lvl != P.nd - 1) || !P.mid.p)) kern = 2;  // per-nonzero walk not applicable
+  if (kern == 3 && (!P.mid.p || (P.nd == 4 && lvl != 0 && lvl != 3))) kern = 2;  // per-nonzero walk not applicable
   if (kern == 2 && P.nd == 4) kern = 1;                                         // no 4-D branch-free fiber walk
   const int slot = CsfPart::cfib_slot((uint64_t)chunk);
   if (threads % 32 || threads > 256) return set_error(MMCSF_ERR_INVALID, "block_threads must be a multiple of 32, <= 256");

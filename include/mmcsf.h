@@ -178,7 +178,7 @@ typedef struct {
                         levels, fewer rows in flight per warp */
   int kernel;        /* 0 auto (tuned plan, else 2 for 3-D and 1 for 4-D); 1 per-team fiber walk;
                         2 branch-free fiber walk (3-D; 4-D runs 1); 3 per-nonzero walk (every 3-D
-                        level; 4-D slice and leaf levels; the 4-D middle levels run 1, HB-CSF runs 2) */
+                        level; 4-D slice and leaf levels; the 4-D middle levels run 1) */
   int reserved[3];
 } mmcsf_kernel_cfg;
 

@@ -495,6 +495,37 @@ __global__ void k_chunk_fibers(const uint32_t* __restrict__ fptr, uint32_t nfib,
   out[c] = lo;
 }
 
+// mid[x] = fiber index of nonzero x's leaf fiber (o_{nd-2}); 4-D: mid2[x] = its
+// fbrS index (o1). One thread per nonzero, binary search over the fiber pointers.
+__global__ void k_expand_mid(const uint32_t* __restrict__ fptr, const uint32_t* __restrict__ fidx,
+                             const uint32_t* __restrict__ fpar, const uint32_t* __restrict__ sidx1, uint32_t nfib,
+                             uint64_t nnz, uint32_t* __restrict__ mid, uint32_t* __restrict__ mid2) {
+  for (uint64_t x = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; x < nnz; x += (uint64_t)gridDim.x * blockDim.x) {
+    uint32_t lo = 0, hi = nfib - 1;
+    while (lo < hi) {
+      const uint32_t m = (lo + hi + 1) >> 1;
+      if ((uint64_t)fptr[m] <= x) lo = m; else hi = m - 1;
+    }
+    mid[x] = fidx[lo];
+    if (mid2) mid2[x] = sidx1[fpar[lo]];
+  }
+}
+
+// Per-nonzero middle indices of a part built without them (the HB-CSF CSF part).
+int expand_mid(CsfPart& P, cudaStream_t s, Launches& L) {
+  if (!P.present || P.nnz == 0 || P.n_fibers() == 0) return MMCSF_OK;
+  const int lf = P.nd - 2;
+  MMCSF_CUDA(P.mid.alloc(P.nnz * 4));
+  if (P.nd == 4) MMCSF_CUDA(P.mid2.alloc(P.nnz * 4));
+  k_expand_mid<<<grid_for(P.nnz, 256), 256, 0, s>>>(P.ptr[lf].as<uint32_t>(), P.idx[lf].as<uint32_t>(),
+                                                    P.nd == 4 ? P.fpar.as<uint32_t>() : nullptr,
+                                                    P.nd == 4 ? P.idx[1].as<uint32_t>() : nullptr,
+                                                    (uint32_t)P.n_fibers(), P.nnz, P.mid.as<uint32_t>(),
+                                                    P.nd == 4 ? P.mid2.as<uint32_t>() : nullptr);
+  LCHECK(L);
+  return MMCSF_OK;
+}
+
 int chunk_fibers(CsfPart& P, cudaStream_t s, Launches& L) {
   if (!P.present || P.nnz == 0 || P.n_fibers() == 0) return MMCSF_OK;
   if (P.mid.p) {  // first nonzero of every slice: follow the slice's first entry down to the leaf
@@ -628,9 +659,10 @@ extern "C" int mmcsf_build(mmcsf_coo* X, const mmcsf_build_opts* opts, void* str
   }
   if (opts->impl == MMCSF_IMPL_HBCSF) {
     MMCSF_TRY(build_hyb(Fm, P, s, &L.n));
-    for (int p = 0; p < 4; ++p) {  // the HB-CSF CSF part uses the fiber walks
+    for (int p = 0; p < 4; ++p) {  // the CSF part now holds a subset: derive its middle indices again
       Fm->parts[p].mid.release();
       Fm->parts[p].mid2.release();
+      MMCSF_TRY(expand_mid(Fm->parts[p], s, L));
     }
   }
   for (int p = 0; p < 4; ++p) MMCSF_TRY(chunk_fibers(Fm->parts[p], s, L));

@@ -396,5 +396,7 @@ def test_hbcsf_mttkrp_random(nd, torch_cuda):
         for mode in range(nd):
             for f in (0, 1, 2):
                 H = mmcsf.Format(X, impl=mmcsf.IMPL_HBCSF, mode=mode, fiber_threshold=f)
-                got = H.mttkrp(mode, Ud).cpu().numpy()
-                _check_close(got, O.mttkrp_coo_f64(dims, inds, vals, mode, U), ("hyb", nd, R, mode, f))
+                ref = O.mttkrp_coo_f64(dims, inds, vals, mode, U)
+                for kern in (0, 1, 3):  # default, per-team walk, per-nonzero walk on the CSF part
+                    got = H.mttkrp(mode, Ud, cfg={"kernel": kern} if kern else None).cpu().numpy()
+                    _check_close(got, ref, ("hyb", nd, R, mode, f, kern))

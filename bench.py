@@ -176,34 +176,78 @@ def device_coo(X):
     return [i.clone() for i in inds], vals.clone()
 
 
-def reference_sample_time(inds_host, vals_host, dims, R, target_s=12.0, max_n=None):
-    """Time the reference's MTTKRP_COO_CPU (all modes) on the first S nonzeros,
-    S sized so the run takes about target_s seconds. Returns (seconds, S, kind)."""
-    import numpy as np
+class RefCpuMttkrp:
+    """All-mode MTTKRP with the reference's own MTTKRP_COO_CPU
+    (src/mttkrp_cpu.cpp:60-113, built as oracle/_ref; the C restatement of the
+    oracle when the reference was not built here) on `threads` host threads:
+    thread t runs it on a contiguous range of the first S nonzeros into a
+    private output, and one step also sums the private outputs. The function
+    is serial as shipped (its OpenMP pragma is commented out,
+    src/mttkrp_cpu.cpp:79), so the threads split the nonzeros among calls."""
 
-    from oracle import oracle as O
-    use_ref = O.ref_available()
-    kind = "reference" if use_ref else "port"
-    fn = O.ref_mttkrp_coo if use_ref else (lambda d, i, v, m, U: O.mttkrp_coo_f32(i, v, m, U))
-    n_all = len(vals_host)
-    rng = np.random.default_rng(0)
-    U = [rng.random((d, R)).astype(np.float32) for d in dims]
+    def __init__(self, inds_host, vals_host, dims, R, S, threads):
+        import ctypes
+        import numpy as np
 
-    def run(S):
-        ind = [np.ascontiguousarray(i[:S].astype(np.uint64)) for i in inds_host]
-        v = np.ascontiguousarray(vals_host[:S])
+        from oracle import oracle as O
+        self.kind = "reference" if O.ref_available() else "port"
+        self.lib = O.ref_lib() if self.kind == "reference" else O.lib()
+        self.dims, self.R, self.nd, self.S = list(dims), R, len(dims), S
+        self.T = max(1, min(threads, S))
+        rng = np.random.default_rng(0)
+        self.U = [rng.random((d, R)).astype(np.float32) for d in dims]
+        cuts = [S * t // self.T for t in range(self.T + 1)]
+        self.parts = []
+        fp = ctypes.POINTER(ctypes.c_float)
+        for t in range(self.T):
+            a, b = cuts[t], cuts[t + 1]
+            ind = [np.ascontiguousarray(i[a:b].astype(np.uint64)) for i in inds_host]
+            v = np.ascontiguousarray(vals_host[a:b])
+            outs = [np.zeros((d, R), np.float32) for d in dims]
+            self.parts.append((ind, v, outs, O._ptr_array(ind), v.ctypes.data_as(fp)))
+        self.dptr = (ctypes.c_uint64 * self.nd)(*[int(d) for d in dims])
+        self.fp = fp
+
+    def _run(self, t, m):
+        import ctypes
+        ind, v, outs, ip, vp = self.parts[t]
+        outs[m].fill(0.0)
+        fac = (self.fp * self.nd)(*[(outs[m] if q == m else self.U[q]).ctypes.data_as(self.fp)
+                                    for q in range(self.nd)])
+        if self.kind == "reference":
+            rc = self.lib.ref_coo_mttkrp(self.nd, self.dptr, ctypes.c_uint64(len(v)), ip, vp, m, self.R, fac)
+            assert rc == 0
+        else:
+            self.lib.orc_mttkrp_coo_f32(self.nd, ctypes.c_uint64(len(v)), ip, vp, m, self.R, fac)
+
+    def step(self):
+        """One all-mode MTTKRP over the sample (threads, then the sums)."""
+        from concurrent.futures import ThreadPoolExecutor
+        with ThreadPoolExecutor(self.T) as ex:
+            for m in range(self.nd):
+                list(ex.map(lambda t: self._run(t, m), range(self.T)))
+                acc = self.parts[0][2][m].copy()
+                for t in range(1, self.T):
+                    acc += self.parts[t][2][m]
+
+    def seconds(self):
         t = time.perf_counter()
-        for m in range(len(dims)):
-            fn(dims, ind, v, m, U)
+        self.step()
         return time.perf_counter() - t
 
-    S = min(200_000, n_all)
-    t = run(S)
-    S2 = int(min(max_n or n_all, n_all, max(S, S * target_s / max(t, 1e-3))))
+
+def reference_cpu(inds_host, vals_host, dims, R, target_s=12.0):
+    """A RefCpuMttkrp on all host threads (at most 16, to bound the private
+    outputs), with S sized so one step takes about target_s seconds."""
+    n_all = len(vals_host)
+    threads = max(1, min(16, os.cpu_count() or 1))
+    S = min(2_000_000, n_all)
+    r = RefCpuMttkrp(inds_host, vals_host, dims, R, S, threads)
+    t = r.seconds()
+    S2 = int(min(n_all, max(S, S * target_s / max(t, 1e-3))))
     if S2 > S * 1.5:
-        t = run(S2)
-        S = S2
-    return t, S, kind
+        r = RefCpuMttkrp(inds_host, vals_host, dims, R, S2, threads)
+    return r
 
 
 CPALS = dict(dims=[200000, 200000, 200000], nnz=50_000_000, planted=16, noise=0.01, R=16, max_iters=50, tol=1e-5,
@@ -411,28 +455,23 @@ def main():
         # one step = the reference's MTTKRP_COO_CPU over all modes on a sample
         # of the nonzeros, sized so warmup + steps finish in a few minutes
         budget = 150.0 / max(1, a.steps + a.warmup)
-        _, S, kind = reference_sample_time(inds_h, vals_h, dims, R, target_s=min(20.0, budget))
-        ind = [np.ascontiguousarray(x[:S].astype(np.uint64)) for x in inds_h]
-        v = np.ascontiguousarray(vals_h[:S])
-        rng = np.random.default_rng(0)
-        Uh = [rng.random((d, R)).astype(np.float32) for d in dims]
-        fn = O.ref_mttkrp_coo if kind == "reference" else (lambda d, i_, v_, m, U_: O.mttkrp_coo_f32(i_, v_, m, U_))
+        ref = reference_cpu(inds_h, vals_h, dims, R, target_s=min(20.0, budget))
+        S, kind = ref.S, ref.kind
         times = []
         for i in range(a.warmup + a.steps):
-            t0 = time.perf_counter()
-            for m in range(nd):
-                fn(dims, ind, v, m, Uh)
+            t = ref.seconds()
             if i >= a.warmup:
-                times.append(time.perf_counter() - t0)
+                times.append(t)
         ts = statistics.mean(times) * nnz / S
         val = step_bytes / ts / 1e9
         line = {"metric": METRIC, "value": val, "unit": "GB/s", "n_gpus": a.gpus, "steps": a.steps,
                 "warmup": a.warmup, "ms_per_step": ts * 1e3, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator)", "impl": "reference",
                 "config": config,
-                "cpu_baseline": {"value": val, "unit": "GB/s", "cores": 1, "kind": kind,
-                                 "sample": f"first {S} of {nnz} nonzeros, all {nd} modes, MTTKRP_COO_CPU "
-                                           f"(serial as shipped: src/mttkrp_cpu.cpp:79), extrapolated x{nnz / S:.1f}"},
+                "cpu_baseline": {"value": val, "unit": "GB/s", "cores": ref.T, "kind": kind,
+                                 "sample": f"first {S} of {nnz} nonzeros, all {nd} modes, MTTKRP_COO_CPU (serial as "
+                                           f"shipped, src/mttkrp_cpu.cpp:79) on {ref.T} threads over nonzero ranges "
+                                           f"with private outputs summed, extrapolated x{nnz / S:.1f}"},
                 "e2e": {"value": val, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)
         return
@@ -578,12 +617,13 @@ def main():
     cpu = None
     if not a.no_cpu and world == 1:
         inds_h, vals_h = X.host_arrays()
-        t, S, kind = reference_sample_time(inds_h, vals_h, dims, R, target_s=12.0)
-        ts = t * nnz / S
-        cpu = {"value": step_bytes / ts / 1e9, "unit": "GB/s", "cores": 1, "kind": kind,
+        ref = reference_cpu(inds_h, vals_h, dims, R, target_s=12.0)
+        S = ref.S
+        ts = ref.seconds() * nnz / S
+        cpu = {"value": step_bytes / ts / 1e9, "unit": "GB/s", "cores": ref.T, "kind": ref.kind,
                "ms_per_step": ts * 1e3,
-               "sample": f"first {S} of {nnz} nonzeros, all {nd} modes, MTTKRP_COO_CPU serial as shipped, "
-                         f"extrapolated x{nnz / S:.1f}"}
+               "sample": f"first {S} of {nnz} nonzeros, all {nd} modes, MTTKRP_COO_CPU on {ref.T} threads over "
+                         f"nonzero ranges (private outputs summed), extrapolated x{nnz / S:.1f}"}
     bf16 = None
     if a.dtype == "f32" and not a.no_bf16:
         for m in range(nd):

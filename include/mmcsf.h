@@ -10,6 +10,12 @@
  * replaces. The reference has no plugin layer; its boundary is the C++
  * function API in src/mttkrp_gpu.h:59-81 plus the builders in src/util.h.
  *
+ * Threads and streams: different tensors and formats are independent. A
+ * format keeps small per-format state between calls (its tuned plan, staging
+ * buffers of the host-buffer MTTKRP, reordered values for the adjoint, TTM's
+ * side rows, the launch count), so calls on ONE format must not overlap from
+ * several host threads, nor run on several streams at once; serialise them.
+ *
  * Index limits: the nonzero count must be below 2^32 and, to build a format,
  * every mode length below 2^31 (indices are stored as uint32 on the device,
  * the leaf index carrying a fiber-start flag in bit 31; the reference uses

@@ -14,10 +14,18 @@ value      = effective HBM GB/s over all ranks: the MM-CSF traversal's
 e2e        = the same bytes / time of the host-buffer C-ABI call
              (mmcsf_mttkrp_all_host: factors H2D, all modes, outputs D2H).
 roofline   = the dominant mode's kernel: its algorithmic bytes / its average
-             CUDA-event duration, against MEASURED_PEAKS.json's HBM copy rate.
+             CUDA-event duration, against MEASURED_PEAKS.json's HBM copy rate;
+             its DRAM traffic from the committed ncu summary; the row-gather
+             ceiling measured on the same GPU (mmcsf_probe_gather).
 cpu_baseline / --impl reference = the reference's own MTTKRP_COO_CPU
-             (oracle/_ref, single-threaded as shipped) on a bounded sample of
-             the same nonzeros, extrapolated to the full workload.
+             (oracle/_ref) on all host threads (nonzero ranges, private
+             outputs summed) on a bounded sample of the same nonzeros,
+             extrapolated to the full workload.
+also       = format_build_ms (device construction), bf16_factors (the step
+             with BF16 factors and its error), ttm (the reference's ttm on
+             the same tensor), cp (CP-ALS and Poisson gradient CP: BF16 vs
+             FP32 seconds per iteration and fits), formats (4-D: B-CSF and
+             HB-CSF beside MM-CSF).
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 """
@@ -486,7 +494,11 @@ def main():
     import mmcsf
     X = mmcsf.CooTensor.generate(dims, nnz, dist=W["dist"], zipf_s=W["zipf"], val_dist=W["val"],
                                  seed=a.seed + rank)
+    torch.cuda.synchronize()
+    tb0 = time.perf_counter()
     F = mmcsf.Format(X, impl=mmcsf.IMPL_MMCSF, mode=0, fiber_threshold=a.fiber_threshold, views=a.views)
+    torch.cuda.synchronize()
+    build_ms = (time.perf_counter() - tb0) * 1e3  # device construction: sorts, CSF levels, views, tables
     info = F.info(2)
     inds_dev, _ = device_coo(X)
     rows, nfib_nosplit = workload_stats(inds_dev, dims, info["mode_order"])
@@ -643,7 +655,7 @@ def main():
     line = {"metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": a.dtype, "data": "synthetic (seeded device generator)",
-            "config": config, "mode_ms": mode_ms, "mode_algorithmic_bytes": per_mode, "plan": plan, "format": info,
+            "config": config, "format_build_ms": build_ms, "mode_ms": mode_ms, "mode_algorithmic_bytes": per_mode, "plan": plan, "format": info,
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": e2e, "gpu_launches": launches_per_step * a.steps, "clocks": clocks, "bf16_factors": bf16,

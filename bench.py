@@ -13,7 +13,11 @@ value      = effective HBM GB/s over all ranks: the MM-CSF traversal's
              once) / device time per step.
 e2e        = the same bytes / time of the host-buffer C-ABI call
              (mmcsf_mttkrp_all_host: factors H2D, all modes, outputs D2H).
-roofline   = the dominant mode's kernel: its algorithmic bytes / its average
+units      = the step's launches as mmcsf_mttkrp_all issues them under the
+             tuned plan (the two-output walk for the partition's slice and
+             middle modes when it wins, one MTTKRP per other mode), each with
+             its CUDA-event time and algorithmic bytes.
+roofline   = the dominant launch's kernel: its algorithmic bytes / its average
              CUDA-event duration, against MEASURED_PEAKS.json's HBM copy rate;
              its DRAM traffic from the committed ncu summary; the row-gather
              ceiling measured on the same GPU (mmcsf_probe_gather).
@@ -298,6 +302,46 @@ def format_section(X, dims, R, tdt):
     return out
 
 
+def step_units(F, U, outs, plan):
+    """The launches of one all-mode step as mmcsf_mttkrp_all issues them under
+    `plan`: the two-output walk for the partition's slice and middle modes
+    when the plan chose it, one MTTKRP per remaining mode. Returns
+    [(modes, fn)]; timing each fn separately gives the per-kernel times."""
+    nd = len(U)
+    units = []
+    done = set()
+    if plan and plan.get("pair", {}).get("use"):
+        m0, m1 = F.pair_modes()
+        po = {m0: outs[m0], m1: outs[m1]}
+        units.append(((m0, m1), lambda: F.mttkrp_pair(U, po)))
+        done = {m0, m1}
+    for m in range(nd):
+        if m not in done:
+            units.append(((m,), lambda m=m: F.mttkrp(m, U, outs[m])))
+    return units
+
+
+def time_units(units, steps, stream=None):
+    """Per-unit device times (CUDA events on the launching stream), mean over
+    `steps` steps, and the whole span."""
+    import torch
+    stream = stream or torch.cuda.current_stream()
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(len(units) + 1)] for _ in range(steps)]
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    t0.record(stream)
+    for k in range(steps):
+        ev[k][0].record(stream)
+        for i, (_, fn) in enumerate(units):
+            fn()
+            ev[k][i + 1].record(stream)
+    t1.record(stream)
+    torch.cuda.synchronize()
+    unit_ms = [statistics.mean(ev[k][i].elapsed_time(ev[k][i + 1]) for k in range(steps)) for i in range(len(units))]
+    return unit_ms, t0.elapsed_time(t1)
+
+
 def bf16_section(F, U32, outs32, steps, warmup):
     """The same step with BF16 factors (FP32 accumulation), tuned for them,
     and the error this costs against the FP32-factor outputs."""
@@ -307,22 +351,15 @@ def bf16_section(F, U32, outs32, steps, warmup):
     plan = F.tune(U, outs)
     for _ in range(warmup):
         F.mttkrp_all(U, outs)
-    nd = len(U)
-    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(nd + 1)] for _ in range(steps)]
-    torch.cuda.synchronize()
-    for k in range(steps):
-        ev[k][0].record()
-        for m in range(nd):
-            F.mttkrp(m, U, outs[m])
-            ev[k][m + 1].record()
-    torch.cuda.synchronize()
-    mode_ms = [statistics.mean(ev[k][m].elapsed_time(ev[k][m + 1]) for k in range(steps)) for m in range(nd)]
+    units = step_units(F, U, outs, plan)
+    unit_ms, span = time_units(units, steps)
     err = []
     for o, r in zip(outs, outs32):
         d = (o.double() - r.double())
         err.append({"frobenius_rel": float(d.norm() / r.double().norm()),
                     "max_abs_over_max_ref": float(d.abs().max() / r.double().abs().max())})
-    return {"ms_per_step": sum(mode_ms), "mode_ms": mode_ms, "plan": plan, "error_vs_fp32_factors": err,
+    return {"ms_per_step": span / steps, "units": [{"modes": list(u[0]), "ms": t} for u, t in zip(units, unit_ms)],
+            "plan": plan, "error_vs_fp32_factors": err,
             "note": "BF16-rounded factor rows, FP32 products and accumulation; the error is the factors' rounding"}
 
 
@@ -509,7 +546,7 @@ def main():
     outs = [torch.empty(d, R, device="cuda") for d in dims]
     if a.plan_file:
         with open(a.plan_file) as fh:
-            plan = {int(k): v for k, v in json.load(fh).items()}
+            plan = {(k if k == "pair" else int(k)): v for k, v in json.load(fh).items()}
         F.set_plan(plan)
     else:
         plan = None if a.no_tune else F.tune(U, outs)
@@ -529,6 +566,16 @@ def main():
             sb = struct_bytes(nd, nnz, pi["n_fibers"], pi["n_fbrs"])
         per_mode.append(mode_bytes(nd, dims, m, R, esz, sb, rows))
     stream = torch.cuda.current_stream()
+    units = step_units(F, U, outs, plan)
+
+    def unit_bytes(modes):
+        if len(modes) == 1:
+            return per_mode[modes[0]]
+        # the two-output walk: vals, leaf and middle index per nonzero, slice
+        # offsets and indices, every touched row of the three factors once,
+        # both outputs written once
+        return (nnz * 12 + info["n_slices"] * 8 + sum(rows[q] * R * esz for q in range(nd))
+                + sum(dims[q] * R * 4 for q in modes))
 
     for _ in range(a.warmup):
         F.mttkrp_all(U, outs)
@@ -539,25 +586,13 @@ def main():
     sampler = ClockSampler(local) if rank == 0 else None
     if sampler:
         sampler.start()
-    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(nd + 1)] for _ in range(a.steps)]
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
-    t0 = torch.cuda.Event(enable_timing=True)
-    t1 = torch.cuda.Event(enable_timing=True)
-    t0.record(stream)
-    for k in range(a.steps):
-        ev[k][0].record(stream)
-        for m in range(nd):
-            F.mttkrp(m, U, outs[m])
-            ev[k][m + 1].record(stream)
-    t1.record(stream)
-    torch.cuda.synchronize()
+    unit_ms, total_ms = time_units(units, a.steps, stream)
     if world > 1:
         dist.barrier()
     clocks = sampler.stop() if sampler else None
-    total_ms = t0.elapsed_time(t1)
-    mode_ms = [statistics.mean(ev[k][m].elapsed_time(ev[k][m + 1]) for k in range(a.steps)) for m in range(nd)]
     tmax = torch.tensor([total_ms], device="cuda")
     if world > 1:
         dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
@@ -594,22 +629,32 @@ def main():
         if world > 1:
             dist.destroy_process_group()
         return
-    dom = max(range(nd), key=lambda m: mode_ms[m])
-    achieved = per_mode[dom] / (mode_ms[dom] / 1e3) / 1e9
-
-    dtrav = plan[dom]["traversal"] if plan else 1
-    dorder = F.info(4 + dom)["mode_order"] if dtrav == 2 else info["mode_order"]
-    dlvl = dorder.index(dom)
-    dk = plan[dom].get("kernel", 0) if plan else 0
-    if dk == 3 and nd == 4 and dlvl not in (0, 3):
-        dk = 1  # the 4-D middle levels run the per-team fiber walk
-    dker = {1: "k_mttkrp", 2: "k_mttkrp_flat", 3: "k_mttkrp_rows"}.get(dk or (2 if nd == 3 else 1))
-    traffic = traffic_from_profiles(a.workload, R, a.dtype, dom, dker)
+    ub = [unit_bytes(u[0]) for u in units]
+    di = max(range(len(units)), key=lambda i: unit_ms[i])
+    dmodes = units[di][0]
+    achieved = ub[di] / (unit_ms[di] / 1e3) / 1e9
+    if len(dmodes) == 2:
+        dker = "k_mttkrp_pair"
+        dlabel = (f"{dker} modes {dmodes[0]} and {dmodes[1]} (slice and middle levels of order "
+                  f"{info['mode_order']}, MM-CSF partition, one walk)")
+        traffic = traffic_from_profiles(a.workload, R, a.dtype, "".join(str(m) for m in dmodes), dker)
+    else:
+        dom = dmodes[0]
+        dtrav = plan[dom]["traversal"] if plan else 1
+        dorder = F.info(4 + dom)["mode_order"] if dtrav == 2 else info["mode_order"]
+        dlvl = dorder.index(dom)
+        dk = plan[dom].get("kernel", 0) if plan else 0
+        if dk == 3 and nd == 4 and dlvl not in (0, 3):
+            dk = 1  # the 4-D middle levels run the per-team fiber walk
+        dker = {1: "k_mttkrp", 2: "k_mttkrp_flat", 3: "k_mttkrp_rows"}.get(dk or (2 if nd == 3 else 1))
+        dlabel = (f"{dker} mode {dom} (level {dlvl} of order {dorder}, "
+                  f"{'view' if dtrav == 2 else 'MM-CSF partition'})")
+        traffic = traffic_from_profiles(a.workload, R, a.dtype, dom, dker)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
                 "traffic": traffic, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
-                "kernel": f"{dker} mode {dom} (level {dlvl} of order {dorder}, "
-                          f"{'view' if dtrav == 2 else 'MM-CSF partition'})",
-                "algorithmic_bytes": per_mode[dom], "avg_ms": mode_ms[dom]}
+                "kernel": dlabel, "algorithmic_bytes": ub[di], "avg_ms": unit_ms[di]}
+    unit_report = [{"modes": list(u[0]), "ms": t, "algorithmic_bytes": b} for u, t, b in zip(units, unit_ms, ub)]
+    mode_ms = [next((t for u, t in zip(units, unit_ms) if u[0] == (m,)), None) for m in range(nd)]
     # gather ceiling: the same GPU gathering the leaf factor's rows for the
     # workload's own leaf-mode index stream with nothing else to do
     if a.dtype == "f32" and R in (16, 32, 64, 128):
@@ -625,7 +670,7 @@ def main():
             "ms": pms.value, "rows_per_s": nnz / (pms.value / 1e3),
             "what": f"{nnz} rows of the {dims[leafm]} x {R} FP32 mode-{leafm} factor gathered by the workload's "
                     f"mode-{leafm} indices and summed (mmcsf_probe_gather), nothing else",
-            "dominant_kernel_vs_ceiling": pms.value / mode_ms[dom]}
+            "dominant_kernel_vs_ceiling": pms.value / unit_ms[di]}
     cpu = None
     if not a.no_cpu and world == 1:
         inds_h, vals_h = X.host_arrays()
@@ -638,8 +683,7 @@ def main():
                          f"nonzero ranges (private outputs summed), extrapolated x{nnz / S:.1f}"}
     bf16 = None
     if a.dtype == "f32" and not a.no_bf16:
-        for m in range(nd):
-            F.mttkrp(m, U, outs[m])
+        F.mttkrp_all(U, outs)
         bf16 = bf16_section(F, U, outs, min(a.steps, 20), a.warmup)
     ttm = ttm_section(X, dims, R, info["mode_order"][0], rows) if nd == 3 and R in (4, 8, 16, 32, 64, 128) else None
     formats = None
@@ -655,7 +699,7 @@ def main():
     line = {"metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": a.dtype, "data": "synthetic (seeded device generator)",
-            "config": config, "format_build_ms": build_ms, "mode_ms": mode_ms, "mode_algorithmic_bytes": per_mode, "plan": plan, "format": info,
+            "config": config, "format_build_ms": build_ms, "units": unit_report, "plan": plan, "format": info,
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": e2e, "gpu_launches": launches_per_step * a.steps, "clocks": clocks, "bf16_factors": bf16,

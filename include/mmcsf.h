@@ -193,7 +193,17 @@ typedef struct {
  * B-CSF/HB-CSF formats only the built mode is available. */
 int mmcsf_mttkrp(const mmcsf_format* F, int mode, int R, int factor_dtype, const void* const* d_factors,
                  float* d_out, const mmcsf_kernel_cfg* cfg, void* stream);
-/* All modes, each from the same input factors: d_outs[m] gets mode m.
+/* Two modes in one walk (no counterpart in the reference; MM-CSF's reuse of a
+ * partition across modes): on a 3-D MM-CSF format, the MTTKRP of the
+ * partition's slice mode (modes[0], into d_out_slice) and of its middle mode
+ * (modes[1], into d_out_mid) from one traversal that gathers each nonzero's
+ * factor rows once. With null outputs only `modes` is filled. R in 4..128
+ * (powers of two). */
+int mmcsf_mttkrp_pair(const mmcsf_format* F, int R, int factor_dtype, const void* const* d_factors,
+                      float* d_out_slice, float* d_out_mid, int* modes, const mmcsf_kernel_cfg* cfg, void* stream);
+/* All modes, each from the same input factors: d_outs[m] gets mode m. When
+ * the tuned plan says so (and cfg overrides neither traversal nor kernel), the
+ * partition's two upper modes run in one walk (mmcsf_mttkrp_pair).
  * (The reference's all-mode loop, src/mttkrp_gpu.cu:3548-3724.) */
 int mmcsf_mttkrp_all(const mmcsf_format* F, int R, int factor_dtype, const void* const* d_factors,
                      float* const* d_outs, const mmcsf_kernel_cfg* cfg, void* stream);
@@ -215,6 +225,9 @@ typedef struct {
   int min_blocks[4];
   int kernel[4];    /* mmcsf_kernel_cfg.kernel */
   float ms[4];      /* best time per mode */
+  int pair;         /* 1: mmcsf_mttkrp_all runs the partition's two upper modes in one walk (mmcsf_mttkrp_pair) */
+  int pair_chunk, pair_min_blocks;
+  float pair_ms;    /* best time of that walk (both modes) */
 } mmcsf_plan;
 int mmcsf_tune(mmcsf_format* F, int R, int factor_dtype, const void* const* d_factors, float* const* d_outs,
                void* stream, mmcsf_plan* plan);

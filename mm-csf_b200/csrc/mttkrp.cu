@@ -89,6 +89,7 @@ struct Args {
   uint32_t R;
   const T* U[4];  // factor of mode order[l], by level l
   float* out;
+  float* out2;  // two-output walk: the middle mode's output
 };
 
 // largest f with fptr[f] <= x
@@ -700,6 +701,164 @@ __global__ void __launch_bounds__(256, MB) k_mttkrp_rows(const Args<T> a) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// Two outputs from one walk of a 3-D part (MM-CSF's reuse across modes): the
+// slice mode's MTTKRP, out[a] += v U1[b] (.) U2[k], and the middle mode's,
+// out2[b] += U0[a] (.) sum over the fiber (a, b) of v U2[k], share every
+// nonzero's gathers of U1[b] and U2[k]. Slice accumulation as in the
+// per-nonzero walk, fiber sums closed at the leaf-index flags with one vector
+// reduction per fiber; both outputs zeroed by the caller.
+template <int G, int V, class T, int MB, int PFX>
+__global__ void __launch_bounds__(256, MB) k_mttkrp_pair(const Args<T> a) {
+  constexpr uint32_t R = 4 * G * V;
+  constexpr uint32_t FLAG = 0x80000000u;
+  constexpr int PF = G > PFX ? PFX : G;
+  constexpr uint32_t GMASK = G == 32 ? FULL : ((1u << G) - 1u);
+  const int lane = threadIdx.x & 31;
+  const int tl = lane & (G - 1);
+  const int tb = lane - tl;
+  const float* __restrict__ vals = a.vals;
+  const uint32_t* __restrict__ leaf = a.leaf;
+  const uint32_t* __restrict__ mid = a.mid;
+  const uint32_t* __restrict__ snz = a.snz;
+  const uint32_t* __restrict__ sidx = a.sidx;
+  const uint32_t chunk = a.chunk, nslc = a.nslc;
+  const T* __restrict__ U0 = a.U[0];
+  const T* __restrict__ U1 = a.U[1];
+  const T* __restrict__ U2 = a.U[2];
+  float* __restrict__ out = a.out;
+  float* __restrict__ out2 = a.out2;
+  const uint32_t c0 = (uint32_t)tl * 4;
+  auto ld = [&](const T* U, uint32_t row, int v) -> float4 {
+    return Row<T>::load(U + (uint64_t)row * R, c0 + (uint32_t)(v * G * 4));
+  };
+  auto rd = [&](float* o, uint32_t row, int v, float4 x) { red4(o + (uint64_t)row * R + c0 + v * G * 4, x); };
+
+  const uint64_t team = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) / G;
+  const bool active = team * chunk < a.nnz;
+  const uint64_t x0 = active ? team * chunk : a.nnz - 1;
+  const uint64_t x1 = active ? min(x0 + chunk, a.nnz) : x0;
+  uint32_t sl;
+  if (a.cslc) {
+    sl = active ? __ldg(a.cslc + team) : nslc - 1;
+  } else {
+    uint32_t lo = 0, hi = nslc - 1;
+    while (lo < hi) {
+      const uint32_t m = (lo + hi + 1) >> 1;
+      if ((uint64_t)__ldg(snz + m) <= x0) lo = m; else hi = m - 1;
+    }
+    sl = lo;
+  }
+  uint32_t ca = __ldg(sidx + sl);
+  uint64_t nxt = __ldg(snz + sl + 1);
+  uint32_t bopen = __ldg(mid + x0);
+  float4 acc[V], accf[V], rowA[V];
+#pragma unroll
+  for (int v = 0; v < V; ++v) {
+    acc[v] = accf[v] = f4(0.f);
+    rowA[v] = ld(U0, ca, v);
+  }
+  auto load_blk = [&](uint32_t itb, uint32_t& kk, uint32_t& bb, float& vq) {
+    const uint64_t xx = x0 + itb + tl;
+    kk = 0;
+    bb = 0;
+    vq = 0.f;
+    if (itb < chunk && xx < x1) { kk = __ldg(leaf + xx); bb = __ldg(mid + xx); vq = __ldg(vals + xx); }
+  };
+  uint32_t kc, bc, kn, bn;
+  float vc, vn;
+  load_blk(0, kc, bc, vc);
+  load_blk(G, kn, bn, vn);
+  for (uint32_t it = 0; it < chunk; it += G) {
+    const uint64_t xb = x0 + it;
+    const uint32_t k = kc & ~FLAG, b = bc;
+    const float vv = vc;
+    const uint32_t fm = (__ballot_sync(FULL, (kc & FLAG) && (xb + tl != x0)) >> tb) & GMASK;
+    kc = kn; bc = bn; vc = vn;
+    load_blk(it + 2 * G, kn, bn, vn);
+    const bool slow = __any_sync(FULL, xb < x1 && xb + G > nxt);
+    auto block = [&](auto slow_tag) {
+      constexpr bool SLOW = decltype(slow_tag)::value;
+#pragma unroll
+      for (int jb = 0; jb < G; jb += PF) {
+        float4 rb[PF][V], rc[PF][V];
+        uint32_t bjs[PF];
+#pragma unroll
+        for (int j = 0; j < PF; ++j) {
+          const uint32_t kj = __shfl_sync(FULL, k, tb + jb + j);
+          bjs[j] = __shfl_sync(FULL, b, tb + jb + j);
+#pragma unroll
+          for (int v = 0; v < V; ++v) {
+            rb[j][v] = ld(U1, bjs[j], v);
+            rc[j][v] = ld(U2, kj, v);
+          }
+        }
+#pragma unroll
+        for (int j = 0; j < PF; ++j) {
+          const float val = __shfl_sync(FULL, vv, tb + jb + j);
+          const uint64_t x = xb + jb + j;
+          if ((fm >> (jb + j)) & 1u) {  // the open fiber ends before nonzero j (in the open slice)
+#pragma unroll
+            for (int v = 0; v < V; ++v) { rd(out2, bopen, v, pmul(rowA[v], accf[v])); accf[v] = f4(0.f); }
+            bopen = bjs[j];
+          }
+          if constexpr (SLOW) {
+            if (x < x1 && x == nxt) {
+#pragma unroll
+              for (int v = 0; v < V; ++v) { rd(out, ca, v, acc[v]); acc[v] = f4(0.f); }
+              ++sl;
+              ca = __ldg(sidx + sl);
+              nxt = __ldg(snz + sl + 1);
+#pragma unroll
+              for (int v = 0; v < V; ++v) rowA[v] = ld(U0, ca, v);
+            }
+          }
+#pragma unroll
+          for (int v = 0; v < V; ++v) {
+            acc[v] = pfma(pmul_s(val, rb[j][v]), rc[j][v], acc[v]);
+            accf[v] = pfma_s(val, rc[j][v], accf[v]);
+          }
+        }
+      }
+    };
+    if (slow) block(std::true_type{});
+    else block(std::false_type{});
+  }
+  if (active) {
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      rd(out, ca, v, acc[v]);
+      rd(out2, bopen, v, pmul(rowA[v], accf[v]));
+    }
+  }
+}
+
+template <int G, int V, class T>
+cudaError_t launch_pair(const Args<T>& a, int threads, int mb, cudaStream_t s) {
+  const uint64_t teams = (a.nnz + a.chunk - 1) / a.chunk;
+  const uint64_t blocks = (teams * G + threads - 1) / threads;
+  switch (mb) {
+    case 1: k_mttkrp_pair<G, V, T, 2, 8><<<(unsigned)blocks, threads, 0, s>>>(a); break;
+    case 3: k_mttkrp_pair<G, V, T, 4, 4><<<(unsigned)blocks, threads, 0, s>>>(a); break;
+    case 4: k_mttkrp_pair<G, V, T, 5, 4><<<(unsigned)blocks, threads, 0, s>>>(a); break;
+    default: k_mttkrp_pair<G, V, T, 3, 8><<<(unsigned)blocks, threads, 0, s>>>(a); break;
+  }
+  return cudaGetLastError();
+}
+
+template <class T>
+cudaError_t launch_pair_R(const Args<T>& a, int threads, int mb, cudaStream_t s) {
+  switch (a.R) {
+    case 4: return launch_pair<1, 1, T>(a, threads, mb, s);
+    case 8: return launch_pair<2, 1, T>(a, threads, mb, s);
+    case 16: return launch_pair<4, 1, T>(a, threads, mb, s);
+    case 32: return launch_pair<8, 1, T>(a, threads, mb, s);
+    case 64: return launch_pair<16, 1, T>(a, threads, mb, s);
+    case 128: return launch_pair<32, 1, T>(a, threads, mb, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
 template <int ND, int OUT, int G, int V, class T>
 cudaError_t launch_one(const Args<T>& a, int threads, int mb, cudaStream_t s) {
   const uint64_t teams = (a.nnz + a.chunk - 1) / a.chunk;
@@ -816,6 +975,33 @@ int default_chunk(int R) {
   return 512;
 }
 
+// Kernel arguments for part P (factors U by tensor mode, reordered by level).
+template <class T>
+void fill_args(Args<T>& a, const CsfPart& P, const float* vals_override, int slot, int chunk, int R,
+               const void* const* U, float* out) {
+  a.vals = vals_override ? vals_override : P.vals.as<float>();
+  a.leaf = P.leaf.as<uint32_t>();
+  const int lf = P.nd - 2;
+  a.fptr = P.ptr[lf].as<uint32_t>();
+  a.fidx = P.idx[lf].as<uint32_t>();
+  a.fpar = P.fpar.as<uint32_t>();
+  a.sidx1 = P.nd == 4 ? P.idx[1].as<uint32_t>() : nullptr;
+  a.like = P.fbr_like.as<uint32_t>();
+  a.cfib = slot >= 0 && P.cfib[slot].p ? P.cfib[slot].as<uint32_t>() : nullptr;
+  a.mid = P.mid.as<uint32_t>();
+  a.mid2 = P.mid2.as<uint32_t>();
+  a.snz = P.snz.as<uint32_t>();
+  a.sidx = P.idx[0].as<uint32_t>();
+  a.cslc = slot >= 0 && P.cslc[slot].p ? P.cslc[slot].as<uint32_t>() : nullptr;
+  a.nslc = (uint32_t)P.n[0];
+  a.nnz = P.nnz;
+  a.nfib = (uint32_t)P.n_fibers();
+  a.chunk = (uint32_t)chunk;
+  a.R = (uint32_t)R;
+  for (int l = 0; l < P.nd; ++l) a.U[l] = static_cast<const T*>(U[P.order[l]]);
+  a.out = out;
+}
+
 // MTTKRP on one part for tensor mode `mode`; out must be zeroed by the caller.
 int part_mttkrp(const mmcsf_format* F, const CsfPart& P, int mode, int R, int dtype, const void* const* U,
                 float* out, const mmcsf_kernel_cfg* cfg, cudaStream_t s, int* launches,
@@ -837,51 +1023,11 @@ int part_mttkrp(const mmcsf_format* F, const CsfPart& P, int mode, int R, int dt
   cudaError_t e;
   if (dtype == MMCSF_DTYPE_F32) {
     Args<float> a{};
-    a.vals = vals_override ? vals_override : P.vals.as<float>();
-    a.leaf = P.leaf.as<uint32_t>();
-    const int lf = P.nd - 2;
-    a.fptr = P.ptr[lf].as<uint32_t>();
-    a.fidx = P.idx[lf].as<uint32_t>();
-    a.fpar = P.fpar.as<uint32_t>();
-    a.sidx1 = P.nd == 4 ? P.idx[1].as<uint32_t>() : nullptr;
-    a.like = P.fbr_like.as<uint32_t>();
-    a.cfib = slot >= 0 && P.cfib[slot].p ? P.cfib[slot].as<uint32_t>() : nullptr;
-    a.mid = P.mid.as<uint32_t>();
-    a.mid2 = P.mid2.as<uint32_t>();
-    a.snz = P.snz.as<uint32_t>();
-    a.sidx = P.idx[0].as<uint32_t>();
-    a.cslc = slot >= 0 && P.cslc[slot].p ? P.cslc[slot].as<uint32_t>() : nullptr;
-    a.nslc = (uint32_t)P.n[0];
-    a.nnz = P.nnz;
-    a.nfib = (uint32_t)P.n_fibers();
-    a.chunk = (uint32_t)chunk;
-    a.R = (uint32_t)R;
-    for (int l = 0; l < P.nd; ++l) a.U[l] = static_cast<const float*>(U[P.order[l]]);
-    a.out = out;
+    fill_args(a, P, vals_override, slot, chunk, R, U, out);
     e = launch_R<float>(a, P.nd, lvl, kern, threads, mb, s);
   } else {
     Args<__nv_bfloat16> a{};
-    a.vals = vals_override ? vals_override : P.vals.as<float>();
-    a.leaf = P.leaf.as<uint32_t>();
-    const int lf = P.nd - 2;
-    a.fptr = P.ptr[lf].as<uint32_t>();
-    a.fidx = P.idx[lf].as<uint32_t>();
-    a.fpar = P.fpar.as<uint32_t>();
-    a.sidx1 = P.nd == 4 ? P.idx[1].as<uint32_t>() : nullptr;
-    a.like = P.fbr_like.as<uint32_t>();
-    a.cfib = slot >= 0 && P.cfib[slot].p ? P.cfib[slot].as<uint32_t>() : nullptr;
-    a.mid = P.mid.as<uint32_t>();
-    a.mid2 = P.mid2.as<uint32_t>();
-    a.snz = P.snz.as<uint32_t>();
-    a.sidx = P.idx[0].as<uint32_t>();
-    a.cslc = slot >= 0 && P.cslc[slot].p ? P.cslc[slot].as<uint32_t>() : nullptr;
-    a.nslc = (uint32_t)P.n[0];
-    a.nnz = P.nnz;
-    a.nfib = (uint32_t)P.n_fibers();
-    a.chunk = (uint32_t)chunk;
-    a.R = (uint32_t)R;
-    for (int l = 0; l < P.nd; ++l) a.U[l] = static_cast<const __nv_bfloat16*>(U[P.order[l]]);
-    a.out = out;
+    fill_args(a, P, vals_override, slot, chunk, R, U, out);
     e = launch_R<__nv_bfloat16>(a, P.nd, lvl, kern, threads, mb, s);
   }
   if (e != cudaSuccess) return set_error(MMCSF_ERR_CUDA, "MTTKRP launch failed: %s", cudaGetErrorString(e));
@@ -1039,6 +1185,60 @@ extern "C" int mmcsf_cp_adjoint(const mmcsf_format* F, int mode, int R, int fact
   return st;
 }
 
+extern "C" int mmcsf_mttkrp_pair(const mmcsf_format* F, int R, int factor_dtype, const void* const* d_factors,
+                                 float* d_out_slice, float* d_out_mid, int* modes, const mmcsf_kernel_cfg* cfg,
+                                 void* stream) {
+  MMCSF_TRY(check_call(F, R, factor_dtype));
+  if (F->impl != MMCSF_IMPL_MMCSF) return set_error(MMCSF_ERR_INVALID, "the two-output walk needs an MM-CSF format");
+  const CsfPart* P = nullptr;
+  for (int p = 0; p < F->nd; ++p)
+    if (F->parts[p].present) P = &F->parts[p];
+  if (!P || P->nd != 3 || !P->mid.p) return set_error(MMCSF_ERR_UNSUPPORTED, "the two-output walk is 3-D");
+  if (modes) { modes[0] = P->order[0]; modes[1] = P->order[1]; }
+  if (!d_factors || !d_out_slice || !d_out_mid) return modes ? MMCSF_OK : set_error(MMCSF_ERR_INVALID, "null pointer");
+  if (!native_R(R) || R > 128) return set_error(MMCSF_ERR_UNSUPPORTED, "the two-output walk runs R in 4..128");
+  cudaStream_t s = S(stream);
+  MMCSF_CUDA(cudaMemsetAsync(d_out_slice, 0, F->dims[P->order[0]] * (uint64_t)R * sizeof(float), s));
+  MMCSF_CUDA(cudaMemsetAsync(d_out_mid, 0, F->dims[P->order[1]] * (uint64_t)R * sizeof(float), s));
+  const int chunk = cfg && cfg->chunk > 0 ? cfg->chunk : (F->pair_chunk ? F->pair_chunk : 256);
+  const int threads = cfg && cfg->block_threads > 0 ? cfg->block_threads : 256;
+  const int mb = cfg && cfg->min_blocks > 0 ? cfg->min_blocks : (F->pair_mb ? F->pair_mb : 3);
+  if (threads % 32 || threads > 256) return set_error(MMCSF_ERR_INVALID, "block_threads must be a multiple of 32, <= 256");
+  const int slot = CsfPart::cfib_slot((uint64_t)chunk);
+  cudaError_t e;
+  if (factor_dtype == MMCSF_DTYPE_F32) {
+    Args<float> a{};
+    fill_args(a, *P, nullptr, slot, chunk, R, d_factors, d_out_slice);
+    a.out2 = d_out_mid;
+    e = launch_pair_R<float>(a, threads, mb, s);
+  } else {
+    Args<__nv_bfloat16> a{};
+    fill_args(a, *P, nullptr, slot, chunk, R, d_factors, d_out_slice);
+    a.out2 = d_out_mid;
+    e = launch_pair_R<__nv_bfloat16>(a, threads, mb, s);
+  }
+  if (e != cudaSuccess) return set_error(MMCSF_ERR_CUDA, "two-output walk launch: %s", cudaGetErrorString(e));
+  const_cast<mmcsf_format*>(F)->last_launches = 1;
+  return MMCSF_OK;
+}
+
+namespace {
+// The tuned plan runs the partition's two upper modes in one walk (only
+// without a caller override of the traversal or kernel). modes[0..1] get
+// them.
+bool pair_active(const mmcsf_format* F, int R, const mmcsf_kernel_cfg* cfg, int* modes) {
+  if (!F->pair_use || F->impl != MMCSF_IMPL_MMCSF || F->nd != 3 || !native_R(R) || R > 128) return false;
+  if (cfg && (cfg->traversal != 0 || cfg->kernel != 0)) return false;
+  for (int p = 0; p < F->nd; ++p)
+    if (F->parts[p].present && F->parts[p].mid.p) {
+      modes[0] = F->parts[p].order[0];
+      modes[1] = F->parts[p].order[1];
+      return true;
+    }
+  return false;
+}
+}  // namespace
+
 extern "C" int mmcsf_mttkrp_all(const mmcsf_format* F, int R, int factor_dtype, const void* const* d_factors,
                                 float* const* d_outs, const mmcsf_kernel_cfg* cfg, void* stream) {
   MMCSF_TRY(check_call(F, R, factor_dtype));
@@ -1046,7 +1246,14 @@ extern "C" int mmcsf_mttkrp_all(const mmcsf_format* F, int R, int factor_dtype, 
   if (F->impl != MMCSF_IMPL_MMCSF)
     return set_error(MMCSF_ERR_INVALID, "all-mode MTTKRP needs an MM-CSF format (-t 12)");
   int total = 0;
+  int pm[2] = {-1, -1};
+  const bool pair = pair_active(F, R, cfg, pm);
+  if (pair) {
+    MMCSF_TRY(mmcsf_mttkrp_pair(F, R, factor_dtype, d_factors, d_outs[pm[0]], d_outs[pm[1]], nullptr, nullptr, stream));
+    total += F->last_launches;
+  }
   for (int m = 0; m < F->nd; ++m) {
+    if (pair && (m == pm[0] || m == pm[1])) continue;
     MMCSF_TRY(mmcsf_mttkrp(F, m, R, factor_dtype, d_factors, d_outs[m], cfg, stream));
     total += F->last_launches;
   }
@@ -1084,10 +1291,16 @@ extern "C" int mmcsf_mttkrp_all_host(mmcsf_format* F, int R, const float* const*
     MMCSF_CUDA(cudaEventCreateWithFlags(&F->ev_start, cudaEventDisableTiming));
   }
   // order: the largest factor is uploaded last; its own mode (which does not
-  // read it) runs first
+  // read it) runs first. With the two-output walk, the mode outside it runs
+  // first and its factor is uploaded last (the walk reads every factor).
+  int pm[2] = {-1, -1};
+  const bool pair = pair_active(F, R, cfg, pm);
   int big = 0;
   for (int m = 1; m < nd; ++m)
     if (F->dims[m] > F->dims[big]) big = m;
+  if (pair)
+    for (int m = 0; m < nd; ++m)
+      if (m != pm[0] && m != pm[1]) big = m;
   int order[4], n = 0;
   order[n++] = big;
   for (int m = 0; m < nd; ++m)
@@ -1103,16 +1316,30 @@ extern "C" int mmcsf_mttkrp_all_host(mmcsf_format* F, int R, const float* const*
     MMCSF_CUDA(cudaEventRecord(F->ev_in[m], F->copy_in));
   }
   int total = 0;
-  for (int q = 0; q < nd; ++q) {
-    const int m = order[q];
-    for (int p = 0; p < nd; ++p)
-      if (p != m) MMCSF_CUDA(cudaStreamWaitEvent(s, F->ev_in[p], 0));
-    MMCSF_TRY(mmcsf_mttkrp(F, m, R, MMCSF_DTYPE_F32, din, F->stage_out[m].as<float>(), cfg, stream));
-    total += F->last_launches;
+  auto download = [&](int m) -> int {
     MMCSF_CUDA(cudaEventRecord(F->ev_done[m], s));
     MMCSF_CUDA(cudaStreamWaitEvent(F->copy_out, F->ev_done[m], 0));
     MMCSF_CUDA(cudaMemcpyAsync(h_outs[m], F->stage_out[m].p, F->dims[m] * (uint64_t)R * 4, cudaMemcpyDeviceToHost,
                                F->copy_out));
+    return MMCSF_OK;
+  };
+  for (int q = 0; q < nd; ++q) {
+    const int m = order[q];
+    if (pair && m == pm[1]) continue;  // produced with pm[0]
+    const bool both = pair && m == pm[0];
+    for (int p = 0; p < nd; ++p)
+      if (p != m || both) MMCSF_CUDA(cudaStreamWaitEvent(s, F->ev_in[p], 0));
+    if (both) {
+      MMCSF_TRY(mmcsf_mttkrp_pair(F, R, MMCSF_DTYPE_F32, din, F->stage_out[pm[0]].as<float>(),
+                                  F->stage_out[pm[1]].as<float>(), nullptr, nullptr, stream));
+      total += F->last_launches;
+      MMCSF_TRY(download(pm[0]));
+      MMCSF_TRY(download(pm[1]));
+    } else {
+      MMCSF_TRY(mmcsf_mttkrp(F, m, R, MMCSF_DTYPE_F32, din, F->stage_out[m].as<float>(), cfg, stream));
+      total += F->last_launches;
+      MMCSF_TRY(download(m));
+    }
   }
   MMCSF_CUDA(cudaStreamSynchronize(F->copy_out));
   MMCSF_CUDA(cudaStreamSynchronize(s));
@@ -1130,6 +1357,7 @@ extern "C" int mmcsf_tune(mmcsf_format* F, int R, int factor_dtype, const void* 
   MMCSF_CUDA(cudaEventCreate(&e1));
   const int chunks[] = {128, 256, 512, 1024, 2048, 4096};
   const int nmodes = F->impl == MMCSF_IMPL_MMCSF ? F->nd : 1;
+  float best_ms[4] = {0, 0, 0, 0};
   int st = MMCSF_OK;
   for (int i = 0; i < nmodes && st == MMCSF_OK; ++i) {
     const int m = F->impl == MMCSF_IMPL_MMCSF ? i : F->mode;
@@ -1169,6 +1397,7 @@ extern "C" int mmcsf_tune(mmcsf_format* F, int R, int factor_dtype, const void* 
     F->plan_chunk[m] = bc;
     F->plan_mb[m] = bm;
     F->plan_kernel[m] = bk;
+    best_ms[m] = best;
     if (plan) {
       plan->traversal[m] = bt;
       plan->chunk[m] = bc;
@@ -1176,6 +1405,54 @@ extern "C" int mmcsf_tune(mmcsf_format* F, int R, int factor_dtype, const void* 
       plan->kernel[m] = bk;
       plan->ms[m] = best;
     }
+  }
+  // the two upper modes of the partition in one walk, kept when it beats the
+  // two modes' best single-mode plans
+  F->pair_use = false;
+  int pm[2] = {-1, -1};
+  if (st == MMCSF_OK && F->impl == MMCSF_IMPL_MMCSF &&
+      mmcsf_mttkrp_pair(F, R, factor_dtype, nullptr, nullptr, nullptr, pm, nullptr, stream) == MMCSF_OK &&
+      native_R(R) && R <= 128) {
+    float bestp = 1e30f;
+    int bpc = 0, bpm = 0;
+    for (int mbv = 1; mbv <= 3 && st == MMCSF_OK; ++mbv)
+      for (int c : {256, 512, 1024}) {
+        mmcsf_kernel_cfg cfg{};
+        cfg.chunk = c;
+        cfg.min_blocks = mbv;
+        float ms = 0;
+        for (int rep = 0; rep < 2; ++rep) {
+          if ((st = mmcsf_mttkrp_pair(F, R, factor_dtype, d_factors, d_outs[pm[0]], d_outs[pm[1]], nullptr, &cfg,
+                                      stream)) != MMCSF_OK)
+            break;
+          if (cudaEventRecord(e0, s) != cudaSuccess) { st = MMCSF_ERR_CUDA; break; }
+          if ((st = mmcsf_mttkrp_pair(F, R, factor_dtype, d_factors, d_outs[pm[0]], d_outs[pm[1]], nullptr, &cfg,
+                                      stream)) != MMCSF_OK)
+            break;
+          if (cudaEventRecord(e1, s) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess) {
+            st = MMCSF_ERR_CUDA;
+            break;
+          }
+          cudaEventElapsedTime(&ms, e0, e1);
+        }
+        if (st != MMCSF_OK) break;
+        if (ms < bestp) { bestp = ms; bpc = c; bpm = mbv; }
+      }
+    if (st == MMCSF_OK && bestp < best_ms[pm[0]] + best_ms[pm[1]]) {
+      F->pair_use = true;
+      F->pair_chunk = bpc;
+      F->pair_mb = bpm;
+    }
+    if (plan && st == MMCSF_OK) {
+      plan->pair = F->pair_use ? 1 : 0;
+      plan->pair_chunk = bpc;
+      plan->pair_min_blocks = bpm;
+      plan->pair_ms = bestp;
+    }
+  } else if (plan) {
+    plan->pair = 0;
+    plan->pair_chunk = plan->pair_min_blocks = 0;
+    plan->pair_ms = 0.f;
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
@@ -1195,5 +1472,9 @@ extern "C" int mmcsf_set_plan(mmcsf_format* F, const mmcsf_plan* plan) {
     F->plan_mb[m] = plan->min_blocks[m];
     F->plan_kernel[m] = plan->kernel[m];
   }
+  if (plan->pair_chunk < 0 || plan->pair_min_blocks < 0) return set_error(MMCSF_ERR_INVALID, "bad pair entry");
+  F->pair_use = plan->pair != 0;
+  F->pair_chunk = plan->pair_chunk;
+  F->pair_mb = plan->pair_min_blocks;
   return MMCSF_OK;
 }

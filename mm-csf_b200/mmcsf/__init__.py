@@ -336,6 +336,29 @@ class Format:
                                  _stream(stream)))
         return out
 
+    def pair_modes(self):
+        """(slice mode, middle mode) of the MM-CSF partition the two-output
+        walk runs on; raises MmcsfError when the format has none (4-D, B-CSF)."""
+        if getattr(self, "_pair_modes", None) is None:
+            modes = (ctypes.c_int * 2)()
+            check(lib().mmcsf_mttkrp_pair(self._h, 4, 0, None, None, None, modes, None, None))
+            self._pair_modes = (modes[0], modes[1])
+        return self._pair_modes
+
+    def mttkrp_pair(self, factors, outs=None, cfg=None, stream=None):
+        """The partition's slice and middle modes in one walk
+        (mmcsf_mttkrp_pair). Returns {mode: output} for the two modes."""
+        import torch
+        R = factors[0].shape[1]
+        m0, m1 = self.pair_modes()
+        modes = None
+        if outs is None:
+            outs = {m: torch.empty((self.dims[m], R), dtype=torch.float32, device=factors[0].device) for m in (m0, m1)}
+        fp = (c_voidp * self.nd)(*[_ptr(f) for f in factors])
+        check(lib().mmcsf_mttkrp_pair(self._h, R, self._dtype(factors), fp, _ptr(outs[m0]), _ptr(outs[m1]), modes,
+                                      self._cfg(cfg), _stream(stream)))
+        return outs
+
     def mttkrp_all(self, factors, outs=None, cfg=None, stream=None):
         import torch
         R = factors[0].shape[1]
@@ -357,7 +380,9 @@ class Format:
         return outs
 
     def tune(self, factors, outs=None, stream=None):
-        """Autotune traversal and team size per mode (mmcsf_tune); returns the plan."""
+        """Autotune traversal, kernel, chunk and occupancy per mode (mmcsf_tune);
+        returns the plan: {mode: {...}} plus, for MM-CSF, "pair": the
+        two-output walk's best setting and whether mttkrp_all uses it."""
         import torch
         R = factors[0].shape[1]
         if outs is None:
@@ -368,12 +393,24 @@ class Format:
         check(lib().mmcsf_tune(self._h, R, self._dtype(factors), fp, op, _stream(stream), ctypes.byref(pl)))
         n = self.nd if self.impl == IMPL_MMCSF else 1
         modes = range(self.nd) if self.impl == IMPL_MMCSF else [self.mode]
-        return {m: {"traversal": pl.traversal[m], "chunk": pl.chunk[m], "min_blocks": pl.min_blocks[m],
+        plan = {m: {"traversal": pl.traversal[m], "chunk": pl.chunk[m], "min_blocks": pl.min_blocks[m],
                     "kernel": pl.kernel[m], "ms": pl.ms[m]} for m in list(modes)[:n]}
+        if self.impl == IMPL_MMCSF:
+            plan["pair"] = {"use": bool(pl.pair), "chunk": pl.pair_chunk, "min_blocks": pl.pair_min_blocks,
+                            "ms": pl.pair_ms}
+        return plan
 
     def set_plan(self, plan):
+        """Install a plan as returned by tune() (JSON round trips allowed:
+        string mode keys are accepted)."""
         pl = Plan()
         for m, e in plan.items():
+            if m == "pair":
+                pl.pair = 1 if e.get("use") else 0
+                pl.pair_chunk = e.get("chunk", 0)
+                pl.pair_min_blocks = e.get("min_blocks", 0)
+                continue
+            m = int(m)
             pl.traversal[m] = e["traversal"]
             pl.chunk[m] = e["chunk"]
             pl.min_blocks[m] = e.get("min_blocks", 0)

@@ -45,7 +45,8 @@ class KernelCfg(ctypes.Structure):
 
 class Plan(ctypes.Structure):
     _fields_ = [("traversal", c_int * 4), ("chunk", c_int * 4), ("min_blocks", c_int * 4),
-                ("kernel", c_int * 4), ("ms", ctypes.c_float * 4)]
+                ("kernel", c_int * 4), ("ms", ctypes.c_float * 4), ("pair", c_int), ("pair_chunk", c_int),
+                ("pair_min_blocks", c_int), ("pair_ms", ctypes.c_float)]
 
 
 class CpdOpts(ctypes.Structure):
@@ -110,6 +111,8 @@ SIGNATURES = {
     "mmcsf_poisson_step": ([c_voidp, c_int, c_int, ctypes.POINTER(c_voidp), ctypes.c_float, c_voidp, c_voidp,
                             c_voidp, ctypes.POINTER(c_int), c_voidp], c_int),
     "mmcsf_ttm": ([c_voidp, c_int, c_int, c_voidp, c_voidp, c_u64p, c_voidp], c_int),
+    "mmcsf_mttkrp_pair": ([c_voidp, c_int, c_int, ctypes.POINTER(c_voidp), c_voidp, c_voidp, ctypes.POINTER(c_int),
+                           ctypes.POINTER(KernelCfg), c_voidp], c_int),
     "mmcsf_sort_coo_noalloc": ([c_int, c_int, c_int, c_u64p, c_u64, ctypes.POINTER(c_voidp), c_voidp,
                                 ctypes.POINTER(c_voidp), c_voidp, c_voidp], c_int),
 }

@@ -347,6 +347,82 @@ def test_kernel_variants_4d(R, dtype, torch_cuda):
                                 _check_close(out.cpu().numpy(), ref[m], (dims, f, m, cfg))
 
 
+@pytest.mark.parametrize("R", [4, 8, 32, 64, 128])
+@pytest.mark.parametrize("dtype", ["f32", "bf16"])
+def test_two_output_walk(R, dtype, torch_cuda):
+    """mmcsf_mttkrp_pair: the partition's slice and middle modes from one walk
+    match the FP64 oracle at every occupancy level and chunk, with fiber
+    splits, with many short slices, and through mttkrp_all / the host-buffer
+    call once a plan selects it."""
+    import mmcsf
+    torch = torch_cuda
+    rng = np.random.default_rng(500 + R)
+    cases = (([150, 400, 60], 20000, True), ([3000, 50, 40], 9000, False), ([5, 7, 900], 3000, False))
+    for dims, n, skew in cases:
+        inds, vals = _rand_coo(rng, dims, n, skew)
+        X = mmcsf.CooTensor.from_arrays(dims, inds, vals)
+        U = [rng.random((d, R)).astype(np.float32) for d in dims]
+        if dtype == "bf16":
+            Ud = [torch.tensor(u, device="cuda").to(torch.bfloat16) for u in U]
+            U = [t.float().cpu().numpy() for t in Ud]
+        else:
+            Ud = [torch.tensor(u, device="cuda") for u in U]
+        ref = [O.mttkrp_coo_f64(dims, inds, vals, m, U) for m in range(3)]
+        for f in (0, 3):
+            F = mmcsf.Format(X, impl=mmcsf.IMPL_MMCSF, mode=0, fiber_threshold=f, views=1)
+            m0, m1 = F.pair_modes()
+            order = F.info(2)["mode_order"]
+            assert (m0, m1) == (order[0], order[1])
+            for mb in (1, 2, 3, 4):
+                for chunk in (1, 32, 100, 1024):
+                    outs = F.mttkrp_pair(Ud, cfg={"min_blocks": mb, "chunk": chunk})
+                    assert set(outs) == {m0, m1}
+                    for m in (m0, m1):
+                        _check_close(outs[m].cpu().numpy(), ref[m], (dims, f, m, mb, chunk))
+            plan = F.tune(Ud)
+            plan["pair"].update(use=False)
+            F.set_plan(plan)
+            F.mttkrp_all(Ud)
+            separate = F.last_launches
+            plan["pair"].update(use=True, chunk=256, min_blocks=2)
+            F.set_plan(plan)
+            for _ in range(2):
+                outs = F.mttkrp_all(Ud)
+                assert F.last_launches == separate - 1
+                for m in range(3):
+                    _check_close(outs[m].cpu().numpy(), ref[m], ("all+pair", dims, f, m))
+            if dtype == "f32":
+                houts = F.mttkrp_all_host(U)
+                for m in range(3):
+                    _check_close(houts[m], ref[m], ("host+pair", dims, f, m))
+            # a caller's traversal or kernel override turns the walk off
+            outs = F.mttkrp_all(Ud, cfg={"kernel": 1})
+            assert F.last_launches == separate
+            for m in range(3):
+                _check_close(outs[m].cpu().numpy(), ref[m], ("override", dims, f, m))
+
+
+def test_two_output_walk_errors(torch_cuda):
+    import mmcsf
+    torch = torch_cuda
+    rng = np.random.default_rng(77)
+    dims = [20, 30, 10, 8]
+    inds, vals = _rand_coo(rng, dims, 2000)
+    X = mmcsf.CooTensor.from_arrays(dims, inds, vals)
+    U = [torch.rand(d, 16, device="cuda") for d in dims]
+    with pytest.raises(mmcsf.MmcsfError):
+        mmcsf.Format(X, impl=mmcsf.IMPL_MMCSF).mttkrp_pair(U)  # 4-D
+    X3 = mmcsf.CooTensor.from_arrays(dims[:3], inds[:3], vals)
+    B = mmcsf.Format(X3, impl=mmcsf.IMPL_BCSF, mode=0)
+    with pytest.raises(mmcsf.MmcsfError):
+        B.mttkrp_pair(U[:3])
+    F = mmcsf.Format(X3, impl=mmcsf.IMPL_MMCSF)
+    with pytest.raises(mmcsf.MmcsfError):
+        F.mttkrp_pair([torch.rand(d, 256, device="cuda") for d in dims[:3]])  # R above 128
+    with pytest.raises(mmcsf.MmcsfError):
+        F.set_plan({"pair": {"use": True, "chunk": -1, "min_blocks": 1}})
+
+
 @pytest.mark.parametrize("nd", [3, 4])
 def test_views_and_tuner(nd, torch_cuda):
     import mmcsf
@@ -371,7 +447,8 @@ def test_views_and_tuner(nd, torch_cuda):
             out = F.mttkrp(m, Ud, cfg={"traversal": trav})
             _check_close(out.cpu().numpy(), ref[m], ("view", nd, m, trav))
     plan = F.tune(Ud)
-    assert set(plan) == set(range(nd))
+    assert set(plan) == set(range(nd)) | {"pair"}
+    assert plan["pair"]["use"] in (True, False) and (nd == 3 or not plan["pair"]["use"])
     outs = F.mttkrp_all(Ud)
     torch.cuda.synchronize()
     for m in range(nd):

@@ -18,6 +18,12 @@ Both edits are applied to a scratch copy under a temporary directory; the
 reference tree is only read, nothing from it is written into this repository,
 and the only outputs are the files under oracle/_ref/.
 
+A second library, oracle/_ref/libmmcsf_ref_heur.so, is the same build with
+one more edit: the unconditional `mode = 2;` that closes the nonzero loop of
+mm_partition_reuseBased (src/util.h:2517) is removed, so the partition
+heuristic above it decides. It pins the oracle's restatement of that
+heuristic (run on one OpenMP thread: the loop decrements shared counters).
+
 Usage: python oracle/build_ref.py [--src DIR] [--force]
 """
 import argparse
@@ -31,6 +37,8 @@ import tempfile
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT_DIR = os.path.join(HERE, "_ref")
 OUT_LIB = os.path.join(OUT_DIR, "libmmcsf_ref.so")
+OUT_LIB_HEUR = os.path.join(OUT_DIR, "libmmcsf_ref_heur.so")
+OVERRIDE_RE = re.compile(r"^(\s*)mode = 2;\s*$")
 DEFAULT_SRC = "/root/reference/src"
 FILES = ["util.h", "mttkrp_cpu.h", "mttkrp_cpu.cpp", "ttm_cpu.h", "ttm_cpu.cpp"]
 CXXFLAGS = ["-std=c++14", "-fopenmp", "-fPIC", "-Wreturn-type"]
@@ -76,17 +84,48 @@ def _patch_missing_returns(build, stderr):
     return n
 
 
-def build(src=DEFAULT_SRC, force=False, verbose=True):
+def _remove_partition_override(build):
+    """Drop the `mode = 2;` directly above the `/*populate new partitions*/`
+    comment in mm_partition_reuseBased (src/util.h:2517)."""
+    path = os.path.join(build, "util.h")
+    with open(path) as fh:
+        lines = fh.readlines()
+    start = next(i for i, l in enumerate(lines) if "inline int mm_partition_reuseBased(" in l)
+    end = next(i for i in range(start + 1, len(lines)) if lines[i].startswith("inline ") or
+               lines[i].startswith("// more detailed check"))
+    sites = []
+    for i in range(start, end):
+        if OVERRIDE_RE.match(lines[i]):
+            nxt = next((j for j in range(i + 1, end) if lines[j].strip()), None)
+            if nxt is not None and "populate new partitions" in lines[nxt]:
+                sites.append(i)
+    if len(sites) != 1:
+        raise RuntimeError(f"expected one partition override in mm_partition_reuseBased, found {len(sites)}")
+    i = sites[0]
+    lines[i] = OVERRIDE_RE.sub(r"\1/* override removed */", lines[i]) + "\n"
+    with open(path, "w") as fh:
+        fh.writelines(lines)
+    return i + 1
+
+
+def build(src=DEFAULT_SRC, force=False, verbose=True, variant="shipped"):
+    """variant "shipped": the reference as it is (libmmcsf_ref.so);
+    "heuristic": without the partition override (libmmcsf_ref_heur.so)."""
     if not os.path.isdir(src):
         raise FileNotFoundError(f"reference sources not found at {src}")
-    if os.path.exists(OUT_LIB) and not force:
-        return OUT_LIB
+    out_lib = OUT_LIB if variant == "shipped" else OUT_LIB_HEUR
+    if os.path.exists(out_lib) and not force:
+        return out_lib
     os.makedirs(OUT_DIR, exist_ok=True)
     build_dir = tempfile.mkdtemp(prefix="mmcsf_ref_build_")
     try:
         for f in FILES:
             shutil.copy(os.path.join(src, f), os.path.join(build_dir, f))
             os.chmod(os.path.join(build_dir, f), 0o644)
+        if variant == "heuristic":
+            ln = _remove_partition_override(build_dir)
+            if verbose:
+                print(f"removed the partition override at util.h:{ln} in the scratch copy")
         harness = os.path.join(HERE, "ref_harness.cpp")
         units = [(harness, os.path.join(build_dir, "harness.o")),
                  (os.path.join(build_dir, "mttkrp_cpu.cpp"), os.path.join(build_dir, "mttkrp_cpu.o")),
@@ -106,11 +145,11 @@ def build(src=DEFAULT_SRC, force=False, verbose=True):
                 break
         else:
             raise RuntimeError("missing-return patching did not converge")
-        cmd = ["g++", "-shared", "-fopenmp", "-o", OUT_LIB] + [o for _, o in units]
+        cmd = ["g++", "-shared", "-fopenmp", "-o", out_lib] + [o for _, o in units]
         subprocess.run(cmd, check=True, cwd=build_dir)
         if verbose:
-            print(f"built {OUT_LIB} ({total} missing-return sites patched in the scratch copy)")
-        return OUT_LIB
+            print(f"built {out_lib} ({total} missing-return sites patched in the scratch copy)")
+        return out_lib
     finally:
         shutil.rmtree(build_dir, ignore_errors=True)
 
@@ -122,6 +161,7 @@ if __name__ == "__main__":
     a = ap.parse_args()
     try:
         build(a.src, a.force)
+        build(a.src, a.force, variant="heuristic")
     except Exception as e:  # noqa: BLE001
         print(f"reference build failed: {e}", file=sys.stderr)
         sys.exit(1)

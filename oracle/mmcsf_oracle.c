@@ -391,3 +391,166 @@ void orc_create_hyb(int nd, u64 nnz, u64* const* inds, const float* vals, const 
   counts[8] = nhi[1];
   counts[9] = nhi[2];
 }
+
+/* ---- MM-CSF partition heuristic: src/util.h:2167-2516 (mm_partition_reuseBased)
+ * without the unconditional `mode = 2;` of :2517, nonzeros visited in order
+ * (the reference's `omp for` on one thread). inds are X's arrays at the time
+ * of the call (after the chain of per-mode sorts); orders[m] is arrX[m]'s
+ * mode order; redun is Opt.redunMode; fbTh is Opt.MIfbTh (-h). Writes the
+ * partition of every nonzero. Returns 0, or a negative code where the
+ * reference would read or write out of bounds (-2: binarySearch1 runs off
+ * the front, -3: a fiber number below 0, -4: a decrement of the redundant
+ * mode's unallocated counters, -5: out of memory). */
+typedef struct { u64 a, b, pos; } orc_ab;
+static int ab_cmp(const void* x, const void* y) {
+  const orc_ab* p = (const orc_ab*)x;
+  const orc_ab* q = (const orc_ab*)y;
+  if (p->a != q->a) return p->a < q->a ? -1 : 1;
+  if (p->b != q->b) return p->b < q->b ? -1 : 1;
+  return p->pos < q->pos ? -1 : (p->pos > q->pos);
+}
+
+/* binarySearch1 (src/util.h:2128-2141): ITYPE bounds, 32-bit unsigned midpoint */
+static long long orc_bsearch1(const u64* arr, u64 len_avail, u64 left, u64 right, u64 value, int* err) {
+  while (left <= right) {
+    int middle = (int)(((unsigned int)left + (unsigned int)right) >> 1);
+    if ((u64)(unsigned int)middle >= len_avail) { *err = -2; return 0; }
+    if (arr[middle] == value) return middle;
+    else if (arr[middle] > value) right = (u64)(long long)(middle - 1);
+    else left = (u64)(long long)(middle + 1);
+  }
+  return -1;
+}
+
+typedef struct {
+  u64 nfib;       /* distinct (o0, o1) groups: the reference's level-1 entries */
+  u64* fidx1;     /* o1 of every group, then one extra entry (the next level-1 index read past the slice) */
+  u64* cnt;       /* nnzPerFiber, nfib + 1 entries (the last stays 0) */
+  u64* dsp;       /* denseSlcPtr, dims[o0] + 1 entries */
+} orc_mode_csf;
+
+int orc_mm_partition(int nd, u64 nnz, u64* const* inds, const u64* dims, const int orders[][8], const int* xorder,
+                     int redun, int fbTh, int* part) {
+  orc_mode_csf C[4];
+  memset(C, 0, sizeof C);
+  int rc = 0;
+  /* nnzPerFiber / nnzPerSlice / denseSlcPtr per non-redundant mode (:2175-2240) */
+  for (int m = 0; m < nd && rc == 0; ++m) {
+    if (m == redun) continue;
+    const int o0 = orders[m][0], o1 = orders[m][1];
+    orc_ab* v = (orc_ab*)malloc((nnz ? nnz : 1) * sizeof(orc_ab));
+    if (!v) { rc = -5; break; }
+    for (u64 i = 0; i < nnz; ++i) { v[i].a = inds[o0][i]; v[i].b = inds[o1][i]; v[i].pos = i; }
+    qsort(v, nnz, sizeof(orc_ab), ab_cmp);
+    u64 nf = 0;
+    for (u64 i = 0; i < nnz; ++i)
+      if (i == 0 || v[i].a != v[i - 1].a || v[i].b != v[i - 1].b) ++nf;
+    C[m].nfib = nf;
+    C[m].fidx1 = (u64*)calloc(nf + 2, sizeof(u64));
+    C[m].cnt = (u64*)calloc(nf + 2, sizeof(u64));
+    C[m].dsp = (u64*)calloc(dims[o0] + 2, sizeof(u64));
+    u64* sfirst = (u64*)calloc(nf + 2, sizeof(u64)); /* first group of each slice */
+    u64* sidx = (u64*)calloc(nf + 2, sizeof(u64));
+    if (!C[m].fidx1 || !C[m].cnt || !C[m].dsp || !sfirst || !sidx) { free(v); free(sfirst); free(sidx); rc = -5; break; }
+    u64 g = 0, ns = 0;
+    for (u64 i = 0; i < nnz; ++i) {
+      const int newg = i == 0 || v[i].a != v[i - 1].a || v[i].b != v[i - 1].b;
+      if (newg) {
+        if (i == 0 || v[i].a != v[i - 1].a) { sfirst[ns] = g; sidx[ns] = v[i].a; ++ns; }
+        C[m].fidx1[g] = v[i].b;
+        ++g;
+      }
+      C[m].cnt[g - 1]++;
+    }
+    sfirst[ns] = nf;
+    /* the entry after the last group: the reference's leaf-level sentinel is
+       never reached by a search that stays inside the slices it covers */
+    C[m].fidx1[nf] = 0;
+    for (u64 s = 0; s < ns; ++s) {
+      C[m].dsp[sidx[s]] = sfirst[s];
+      C[m].dsp[sidx[s] + 1] = s == ns - 1 ? sfirst[s] : sfirst[s + 1]; /* :2203-2206 */
+    }
+    free(v);
+    free(sfirst);
+    free(sidx);
+  }
+  /* sameFm flags, shortMode / longMode (:2263-2308) */
+  int s01 = 0, s02 = 0, s12 = 0, s03 = 0, s13 = 0, s23 = 0, shortMode = 0, longMode = -1;
+  for (int m = 0; m < nd; ++m) {
+    if (m == 1) {
+      if (same_pair(orders[1], orders[0])) { s01 = 1; shortMode = dims[0] <= dims[1] ? 0 : 1; longMode = dims[0] <= dims[1] ? 1 : 0; }
+    } else if (m == 2) {
+      if (same_pair(orders[2], orders[0])) { s02 = 1; shortMode = dims[0] <= dims[2] ? 0 : 2; longMode = dims[0] <= dims[2] ? 2 : 0; }
+      else if (same_pair(orders[2], orders[1])) { s12 = 1; shortMode = dims[1] <= dims[2] ? 1 : 2; longMode = dims[1] <= dims[2] ? 2 : 1; }
+    } else if (m == 3) {
+      if (same_pair(orders[3], orders[0])) { s03 = 1; shortMode = dims[0] <= dims[3] ? 0 : 3; longMode = dims[0] <= dims[3] ? 3 : 0; }
+      else if (same_pair(orders[3], orders[1])) { s13 = 1; shortMode = dims[1] <= dims[3] ? 1 : 3; longMode = dims[1] <= dims[3] ? 3 : 1; }
+      else if (same_pair(orders[3], orders[2])) { s23 = 1; shortMode = dims[2] <= dims[3] ? 2 : 3; longMode = dims[2] <= dims[3] ? 3 : 2; }
+    }
+  }
+  const int shortestMode = dims[xorder[0]] <= dims[xorder[1]] ? xorder[0] : xorder[1]; /* :2261 */
+  const u64 th = (u64)(long long)fbTh;
+  /* the nonzero loop (:2331-2511) */
+  for (u64 idx = 0; idx < nnz && rc == 0; ++idx) {
+    u64 f[4] = {0, 0, 0, 0}, no[4] = {0, 0, 0, 0};
+    for (int m = 0; m < nd && rc == 0; ++m) {
+      if ((m == 1 && s01) || (m == 2 && s12) || (m == 3 && s23)) { f[m] = f[m - 1]; no[m] = 99999; }
+      else if ((m == 2 && s02) || (m == 3 && s13)) { f[m] = f[m - 2]; no[m] = 99999; }
+      else if (m == 3 && s03) { f[m] = f[m - 3]; no[m] = 99999; }
+      else {
+        if (m == redun) { rc = -4; break; }
+        const u64 j = inds[orders[m][1]][idx];
+        const u64 slc = inds[m][idx];
+        const int n = (int)(C[m].dsp[slc + 1] - C[m].dsp[slc]);
+        const u64 fbr = C[m].dsp[slc];
+        int err = 0;
+        long long r = orc_bsearch1(C[m].fidx1 + fbr, C[m].nfib + 1 - fbr, 0, (u64)(long long)n, j, &err);
+        if (err) { rc = err; break; }
+        const u64 at = (u64)r + fbr;
+        if (at > C[m].nfib) { rc = -3; break; }
+        f[m] = C[m].cnt[at];
+        no[m] = at;
+      }
+    }
+    if (rc) break;
+    int mode = shortestMode, done = 0;
+    if (nd == 3) {
+      u64 mx;
+      mx = f[1] > f[2] ? f[1] : f[2];
+      if (f[0] >= th * mx) { done = 1; mode = (s01 || s02 || s03) ? shortMode : 0; }
+      if (!done) { mx = f[0] > f[2] ? f[0] : f[2]; if (f[1] >= th * mx) { done = 1; mode = (s12 || s13) ? shortMode : 1; } }
+      if (!done) { mx = f[0] > f[1] ? f[0] : f[1]; if (f[2] >= th * mx) { done = 1; mode = s23 ? shortMode : 2; } }
+    } else {
+      /* maxOf3(int, int, int) (:2142-2146) on ITYPE arguments, times an int */
+      int a[4];
+      for (int m = 0; m < 4; ++m) a[m] = (int)(unsigned int)f[m];
+      for (int m = 0; m < 4 && !done; ++m) {
+        int x = -1, y = -1, z = -1, k = 0, o[3];
+        for (int q = 0; q < 4; ++q) if (q != m) o[k++] = a[q];
+        x = o[0]; y = o[1]; z = o[2];
+        int mx = x < y ? y : x;
+        mx = mx < z ? z : mx;
+        const int prod = (int)((unsigned int)fbTh * (unsigned int)mx);
+        if (f[m] >= (u64)(long long)prod) {
+          done = 1;
+          if (m == 0) mode = (s01 || s02 || s03) ? shortMode : 0;
+          else if (m == 1) mode = (s12 || s13) ? shortMode : 1;
+          else if (m == 2) mode = s23 ? shortMode : 2;
+          else mode = 3;
+        }
+      }
+    }
+    if (!done) mode = shortestMode;
+    for (int i = 0; i < nd; ++i) {
+      int dec;
+      if (mode == shortMode) dec = i != shortMode && i != longMode;
+      else dec = i != redun && i != mode;
+      if (!dec) continue;
+      if (i == redun || !C[i].cnt) { rc = -4; break; }
+      C[i].cnt[no[i]]--;
+    }
+    part[idx] = mode;
+  }
+  for (int m = 0; m < 4; ++m) { free(C[m].fidx1); free(C[m].cnt); free(C[m].dsp); }
+  return rc;
+}

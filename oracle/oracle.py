@@ -17,6 +17,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 _BUILD = os.path.join(HERE, "_build")
 _LIB_PATH = os.path.join(_BUILD, "libmmcsf_oracle.so")
 _REF_LIB = os.path.join(HERE, "_ref", "libmmcsf_ref.so")
+_REF_LIB_HEUR = os.path.join(HERE, "_ref", "libmmcsf_ref_heur.so")
 INF_TH = 99999999  # the reference's default -f (src/util.h:212)
 FBRS_TH_MMCSF = 128  # 4-D fbrS split for -t 12 (src/util.h:1325-1326)
 FBRS_TH_OFF = 999999999
@@ -166,10 +167,35 @@ def _csf_dict(pfx, order, ptr, idx, inds, vals, with_fbr_like=True):
 # --------------------------------------------------------------------------
 # format builders (mirror the reference main's call sequence)
 # --------------------------------------------------------------------------
-def build_mmcsf(dims, inds, vals, mode=0, fbr_th=INF_TH, partition="all-to-last"):
+def mm_partition(dims, inds_x, orders, xorder, redun, fbth=1):
+    """The partition heuristic of mm_partition_reuseBased (src/util.h:2167-2516)
+    without its closing `mode = 2;` override (:2517), nonzeros in X's order
+    (inds_x: X's arrays after the chain of per-mode sorts). Returns the
+    partition of every nonzero (int32)."""
+    nd = len(dims)
+    n = len(inds_x[0])
+    part = np.zeros(max(n, 1), np.int32)
+    o = ((ctypes.c_int * 8) * nd)()
+    for m in range(nd):
+        for i in range(nd):
+            o[m][i] = orders[m][i]
+    d = (ctypes.c_uint64 * nd)(*dims)
+    xo = (ctypes.c_int * nd)(*xorder)
+    arrs = [np.ascontiguousarray(i, dtype=np.uint64) for i in inds_x]
+    rc = lib().orc_mm_partition(nd, ctypes.c_uint64(n), _ptr_array(arrs), d, o, xo, redun, int(fbth),
+                                part.ctypes.data_as(ctypes.POINTER(ctypes.c_int)))
+    if rc != 0:
+        raise ValueError(f"the reference reads out of bounds on this input (code {rc})")
+    return part[:n]
+
+
+def build_mmcsf(dims, inds, vals, mode=0, fbr_th=INF_TH, partition="all-to-last", fbth=1):
     """mttkrp -t 12: src/mttkrp.cu:72-389. partition="all-to-last" is the
     reference as shipped (src/util.h:2517 assigns every nonzero to partition
-    2). Returns a dict keyed like the reference harness dump."""
+    2); partition="heuristic" keeps the heuristic's choice (mm_partition,
+    with -h = fbth) and fills every partition the way populate_paritions and
+    sort_MI_CSF do (src/util.h:2088-2126, 412-527). Returns a dict keyed like
+    the reference harness dump."""
     nd = len(dims)
     K = keys_per_sort(nd)
     inds = [np.array(i, dtype=np.uint64) for i in inds]
@@ -184,18 +210,22 @@ def build_mmcsf(dims, inds, vals, mode=0, fbr_th=INF_TH, partition="all-to-last"
             redun = m
         if m != redun:
             sort_coo(inds, vals, orders[m][:K])
-    if partition != "all-to-last":
+    if partition == "all-to-last":
+        part_of = np.full(len(vals), 2, np.int32)
+    elif partition == "heuristic":
+        part_of = mm_partition(dims, inds, orders, xorder, redun, fbth)
+    else:
         raise NotImplementedError(partition)
-    part = 2
     out = {"redunMode": np.array([redun], np.int64), "X.modeOrder": np.array(xorder, np.uint64)}
     for p in range(nd):
         pfx = f"part{p}"
-        if p != part or len(vals) == 0:
+        sel = part_of == p
+        if not sel.any():
             out[f"{pfx}.nnz"] = np.array([0], np.uint64)
             out[f"{pfx}.modeOrder"] = np.array(orders[p], np.uint64)
             continue
-        pin = [i.copy() for i in inds]
-        pv = vals.copy()
+        pin = [i[sel].copy() for i in inds]
+        pv = vals[sel].copy()
         sort_coo(pin, pv, orders[p][:K])
         ptr, idx = create_csf(pin, orders[p], fbr_th, FBRS_TH_MMCSF)
         out.update(_csf_dict(pfx, orders[p], ptr, idx, pin, pv))
@@ -375,6 +405,33 @@ def parse_dump(path):
             else:
                 d[name] = np.array(vals, dtype=np.uint64)
     return d
+
+
+_ref_heur = None
+
+
+def ref_heur_available():
+    return os.path.exists(_REF_LIB_HEUR)
+
+
+def ref_heur_lib():
+    """The reference built without its partition override (oracle/_ref), on
+    one OpenMP thread."""
+    global _ref_heur
+    if _ref_heur is None:
+        _ref_heur = ctypes.CDLL(_REF_LIB_HEUR)
+        _ref_heur.ref_set_threads(1)
+    return _ref_heur
+
+
+def ref_dump_heuristic(tns_path, mode, fbr_th, mifbth, out_path):
+    """The reference's MM-CSF builder with the partition heuristic deciding
+    (-h = mifbth)."""
+    rc = ref_heur_lib().ref_mmcsf_dump_h(tns_path.encode(), int(mode), ctypes.c_long(int(fbr_th)),
+                                         ctypes.c_long(int(mifbth)), out_path.encode())
+    if rc != 0:
+        raise RuntimeError("ref_mmcsf_dump_h failed")
+    return parse_dump(out_path)
 
 
 def ref_dump(kind, tns_path, mode, fbr_th, out_path):

@@ -17,6 +17,7 @@
 #include <cstdint>
 #include <cstdlib>
 #include <cstring>
+#include <omp.h>
 #include <new>
 
 // Zero-filled, padded allocations. The reference reads one element past the
@@ -88,9 +89,16 @@ Options make_opts(const char* tns, int impType, int mode, long fbrTh) {
 
 extern "C" {
 
-// mttkrp -t 12 (MM-CSF): src/mttkrp.cu:72-389.
-int ref_mmcsf_dump(const char* tns, int mode, long fbrTh, const char* out) {
+// OpenMP threads for the builders (1 makes the partition heuristic's nonzero
+// loop run in order; it decrements shared counters).
+void ref_set_threads(int n) { omp_set_num_threads(n); }
+
+// mttkrp -t 12 (MM-CSF): src/mttkrp.cu:72-389, with -h (Opt.MIfbTh, the
+// partition heuristic's fiber ratio; it decides only in the build without
+// the partition override).
+int ref_mmcsf_dump_h(const char* tns, int mode, long fbrTh, long mifbTh, const char* out) {
   Options Opt = make_opts(tns, 12, mode, fbrTh);
+  Opt.MIfbTh = mifbTh;
   Tensor X;
   load_tensor(X, Opt);
   sort_COOtensor(X);
@@ -148,6 +156,10 @@ int ref_mmcsf_dump(const char* tns, int mode, long fbrTh, const char* out) {
   }
   std::fclose(f);
   return 0;
+}
+
+int ref_mmcsf_dump(const char* tns, int mode, long fbrTh, const char* out) {
+  return ref_mmcsf_dump_h(tns, mode, fbrTh, 1, out);
 }
 
 // mttkrp -t 8 (B-CSF): src/mttkrp.cu:72-100 and :167-236.

@@ -3,8 +3,9 @@
 
 Runs the reference's own format builders, COO CPU MTTKRP and CPU TTM (built as
 oracle/_ref/libmmcsf_ref.so by oracle/build_ref.py from the reference's
-sources) on the reference's toy.tns and on seeded synthetic tensors, and
-writes inputs and outputs as JSON. The tests compare both the C oracle and
+sources; the MM-CSF builder also as oracle/_ref/libmmcsf_ref_heur.so, without
+the partition override) on the reference's toy.tns and on seeded synthetic
+tensors, and writes inputs and outputs as JSON. The tests compare both the C oracle and
 the CUDA library against these files, so they run without the reference.
 
 Usage: python tests/golden/make_golden.py [--reference /root/reference]
@@ -104,15 +105,52 @@ def make_ttm(tmp, names):
         json.dump(out, fh, separators=(",", ":"))
 
 
+def make_heuristic(tmp, names):
+    """heuristic.json: the reference's MM-CSF builder with its partition
+    heuristic deciding (the build of oracle/_ref/libmmcsf_ref_heur.so, which
+    drops the `mode = 2;` override of src/util.h:2517), on the cases above,
+    for (-h, -f) = (1, none), (1, 3), (2, 3). Inputs the reference would read out of
+    bounds on (the oracle says which) are skipped."""
+    out = {"runs": []}
+    for name in names:
+        with open(os.path.join(HERE, name + ".json")) as fh:
+            case = json.load(fh)
+        dims = case["dims"]
+        if len(case["vals"]) > 1000:
+            continue
+        inds = [np.asarray(i, np.uint64) for i in case["inds"]]
+        vals = np.asarray(case["vals"], np.float32)
+        path = os.path.join(tmp, name + "_heur.tns")
+        O.write_tns(path, dims, inds, vals)
+        d2, i2, v2 = O.load_tns(path)
+        for h, f in ((1, O.INF_TH), (1, 3), (2, 3)):
+            try:
+                O.build_mmcsf(d2, i2, v2, mode=0, fbr_th=f, partition="heuristic", fbth=h)
+            except ValueError:
+                continue
+            d = O.ref_dump_heuristic(path, 0, f, h, os.path.join(tmp, "dump.txt"))
+            out["runs"].append({"case": name, "mode": 0, "h": h, "f": int(f),
+                                "arrays": {k: _tolist(v) for k, v in d.items()}})
+    with open(os.path.join(HERE, "heuristic.json"), "w") as fh:
+        json.dump(out, fh, separators=(",", ":"))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
     ap.add_argument("--ttm-only", action="store_true", help="write ttm.json from the existing cases only")
+    ap.add_argument("--heuristic-only", action="store_true",
+                    help="write heuristic.json from the existing cases only")
     a = ap.parse_args()
     build_ref.build(os.path.join(a.reference, "src"))
-    if a.ttm_only:
+    if a.ttm_only or a.heuristic_only:
         with open(os.path.join(HERE, "manifest.json")) as fh:
-            make_ttm(tempfile.mkdtemp(), json.load(fh)["cases"])
+            names = json.load(fh)["cases"]
+        if a.ttm_only:
+            make_ttm(tempfile.mkdtemp(), names)
+        if a.heuristic_only:
+            build_ref.build(os.path.join(a.reference, "src"), variant="heuristic")
+            make_heuristic(tempfile.mkdtemp(), names)
         return
     tmp = tempfile.mkdtemp()
     names = []
@@ -143,6 +181,8 @@ def main():
                 runs.append((kind, int(rng.integers(0, nd)), f))
         names.append(make_case(name, dims, inds, vals, tmp, runs, seed=len(names)))
     make_ttm(tmp, names)
+    build_ref.build(os.path.join(a.reference, "src"), variant="heuristic")
+    make_heuristic(tmp, names)
     with open(os.path.join(HERE, "manifest.json"), "w") as fh:
         json.dump({"cases": names, "R": R_GOLD,
                    "source": "reference host code built by oracle/build_ref.py"}, fh, indent=1)

@@ -79,3 +79,54 @@ def test_reference_library_agrees_on_fresh_random_tensor(tmp_path):
         got = build(dims2, inds2, vals2, 1, 2)
         for k, v in ref.items():
             assert np.array_equal(got[k], v.astype(got[k].dtype)), (kind, k)
+
+
+def _heuristic_runs():
+    import json
+    import os
+    here = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+    with open(os.path.join(here, "heuristic.json")) as fh:
+        return json.load(fh)["runs"]
+
+
+def test_partition_heuristic_matches_reference(golden_cases):
+    """The restated partition heuristic (mm_partition_reuseBased without its
+    `mode = 2;` override) against the reference's own builder with that line
+    removed: every partition's arrays, bit-exact."""
+    by_name = {c["name"]: c for c in golden_cases}
+    n = 0
+    multi = 0
+    for run in _heuristic_runs():
+        dims, inds, vals = _inputs(by_name[run["case"]])
+        got = O.build_mmcsf(dims, inds, vals, run["mode"], run["f"], partition="heuristic", fbth=run["h"])
+        for k, v in run["arrays"].items():
+            assert k in got, (run["case"], k)
+            want = np.array(v, dtype=got[k].dtype)
+            assert np.array_equal(got[k], want), (run["case"], run["h"], run["f"], k)
+            n += 1
+        multi += sum(int(run["arrays"][f"part{p}.nnz"][0]) > 0 for p in range(len(dims))) > 1
+    assert n > 500 and multi >= 10
+
+
+@pytest.mark.skipif(not O.ref_heur_available(), reason="reference oracle not built here")
+@pytest.mark.parametrize("nd", [3, 4])
+def test_partition_heuristic_matches_reference_library(nd, tmp_path):
+    rng = np.random.default_rng(40 + nd)
+    dims = [60, 90, 25] if nd == 3 else [20, 30, 12, 9]
+    n = 4000
+    inds = [np.minimum(rng.zipf(1.4, n) - 1, d - 1).astype(np.uint64) for d in dims]
+    key = np.zeros(n, np.uint64)
+    for m, d in enumerate(dims):
+        key = key * np.uint64(d) + inds[m]
+    _, first = np.unique(key, return_index=True)
+    inds = [i[np.sort(first)] for i in inds]
+    vals = (rng.random(len(inds[0])) + 0.1).astype(np.float32)
+    p = str(tmp_path / "t.tns")
+    O.write_tns(p, dims, inds, vals)
+    dims2, inds2, vals2 = O.load_tns(p)
+    for mode in range(nd):
+        for h in (1, 3):
+            ref = O.ref_dump_heuristic(p, mode, 5, h, str(tmp_path / "d.txt"))
+            got = O.build_mmcsf(dims2, inds2, vals2, mode, 5, partition="heuristic", fbth=h)
+            for k, v in ref.items():
+                assert np.array_equal(got[k], v.astype(got[k].dtype)), (mode, h, k)

@@ -130,10 +130,15 @@ typedef struct {
   int impl;                 /* MMCSF_IMPL_MMCSF, _BCSF or _HBCSF (-t) */
   int mode;                 /* -m: drives the first sort; the computed mode for B-CSF/HB-CSF */
   uint64_t fiber_threshold; /* -f: max nonzeros per fiber; 0 = the reference default (99999999) */
-  int partition_rule;       /* 0: the reference as shipped (all nonzeros to partition 2, src/util.h:2517) */
+  int partition_rule;       /* 0: the reference as shipped (all nonzeros to partition 2, src/util.h:2517);
+                               1: the partition heuristic above that line decides (mm_partition_reuseBased,
+                               src/util.h:2167-2516, nonzeros visited in order), each partition sorted and
+                               built as sort_MI_CSF / create_TiledHCSR do */
   int keep_coo;             /* 1: keep every mode's sorted index array on the device for export */
   int views;                /* slice-major views for MTTKRP (no counterpart in the reference):
                                0 none, 1 = modes at the leaf level of the MM-CSF partition, 2 = every mode */
+  int partition_ratio;      /* -h (Opt.MIfbTh): a mode wins a nonzero when its fiber is at least this many
+                               times the others' (0 = the reference default 1); partition_rule 1 only */
 } mmcsf_build_opts;
 
 typedef struct mmcsf_format mmcsf_format;
@@ -157,6 +162,9 @@ typedef struct {
 int mmcsf_format_info(const mmcsf_format* F, int part, mmcsf_part_info* info);
 /* Reference-side scalars: redunMode (-1 if none) and X's mode order. */
 int mmcsf_format_meta(const mmcsf_format* F, int* redun_mode, int* x_mode_order);
+/* partition_rule of the build, and the rounds the partition heuristic took
+ * to settle (0 for partition_rule 0; no counterpart in the reference). */
+int mmcsf_format_partitioning(const mmcsf_format* F, int* partition_rule, int* rounds);
 
 /* Copy one array to host, named as the reference names it (widened to
  * uint64): "fbrPtr<l>", "fbrIdx<l>", "fbrLikeSlcInds", "inds<m>" (needs

@@ -29,7 +29,7 @@
 namespace {
 
 struct Options {  // the reference's Options fields this driver uses (src/util.h:189-236)
-  int R = 32, mode = 0, impType = 1, warpPerSlice = 0, TBsize = 0;
+  int R = 32, mode = 0, impType = 1, warpPerSlice = 0, TBsize = 0, MIfbTh = 1, partitionRule = 0;
   uint64_t fbrThreashold = 0;
   bool verbose = false, correctness = false;
   std::string inFileName, outFileName;
@@ -42,6 +42,9 @@ void usage() {
       "        -m mode : set the mode of MTTKRP (default 0, MM-CSF evaluates all modes)\n"
       "        -t implementation type: 8: B-CSF 10: HB-CSF 12: MM-CSF on GPU\n"
       "        -f fiber-splitting threshold: maximum nonzeros per fiber (default none)\n"
+      "        -h MM-CSF partition ratio: a mode takes a nonzero when its fiber is h times the others' (default 1)\n"
+      "        -P MM-CSF partition rule: 0 all nonzeros to partition 2 as the reference ships (default),\n"
+      "           1 the reference's partition heuristic decides\n"
       "        -w work per team: w*128 nonzeros per worker team (default: autotuned)\n"
       "        -b threads per CTA (default 256)\n"
       "        -v verbose: 1 to enable\n"
@@ -66,7 +69,9 @@ bool parse(int argc, char** argv, Options& o) {
       case 'c': o.correctness = std::atoi(v) == 1; break;
       case 'i': o.inFileName = v; break;
       case 'o': o.outFileName = v; break;
-      case 's': case 'h': case 'g': case 'l': case 'p': case 'q': case 'r': break;  // accepted, unused
+      case 'h': o.MIfbTh = std::atoi(v); break;
+      case 'P': o.partitionRule = std::atoi(v); break;
+      case 's': case 'g': case 'l': case 'p': case 'q': case 'r': break;  // accepted, unused
       default: std::fprintf(stderr, "unknown option: -%c\n", c); return false;
     }
   }
@@ -107,6 +112,8 @@ int main(int argc, char** argv) {
   bo.mode = o.impType == MMCSF_IMPL_MMCSF ? 0 : o.mode;  // check_opt forces mode 0 for -t 12
   bo.fiber_threshold = o.fbrThreashold;
   bo.views = o.impType == MMCSF_IMPL_MMCSF ? 1 : 0;
+  bo.partition_rule = o.impType == MMCSF_IMPL_MMCSF ? o.partitionRule : 0;
+  bo.partition_ratio = o.MIfbTh;
   cudaStream_t s = nullptr;
   mmcsf_format* F = nullptr;
   auto t0 = std::chrono::steady_clock::now();
@@ -146,15 +153,23 @@ int main(int argc, char** argv) {
     total += ms;
     if (o.verbose) std::printf("mode %d: %.3f ms\n", m, ms);
   }
-  mmcsf_part_info pi{};
-  mmcsf_format_info(F, o.impType == MMCSF_IMPL_MMCSF ? 2 : 0, &pi);
+  // totals over the partitions, as src/mttkrp_gpu.cu:3740-3766 prints them
+  unsigned long long tslc = 0, tsfib = 0, tfib = 0, tnnz = 0;
+  for (int p = 0; p < (o.impType == MMCSF_IMPL_MMCSF ? nd : 1); ++p) {
+    mmcsf_part_info pi{};
+    mmcsf_format_info(F, p, &pi);
+    if (!pi.present) continue;
+    tslc += pi.n_slices;
+    tsfib += pi.n_fbrs + 1;
+    tfib += pi.n_fibers + 1;
+    tnnz += pi.nnz;
+    if (o.verbose) std::printf("partition %d: %llu nonzeros\n", p, (unsigned long long)pi.nnz);
+  }
   std::printf("Total GPU time: %f", total);
   if (nd == 3)
-    std::printf(" nSlc:%llu, nFibers:%llu, nnz:%llu\n", (unsigned long long)pi.n_slices,
-                (unsigned long long)pi.n_fibers + 1, (unsigned long long)pi.nnz);
+    std::printf(" nSlc:%llu, nFibers:%llu, nnz:%llu\n", tslc, tfib, tnnz);
   else
-    std::printf(" nSlc:%llu, nSFibers:%llu, nFibers:%llu, nnz:%llu\n", (unsigned long long)pi.n_slices,
-                (unsigned long long)pi.n_fbrs + 1, (unsigned long long)pi.n_fibers + 1, (unsigned long long)pi.nnz);
+    std::printf(" nSlc:%llu, nSFibers:%llu, nFibers:%llu, nnz:%llu\n", tslc, tsfib, tfib, tnnz);
 
   const int check_mode = o.impType == MMCSF_IMPL_MMCSF ? nd - 1 : o.mode;
   std::vector<float> res(dims[check_mode] * (uint64_t)R);

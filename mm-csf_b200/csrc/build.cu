@@ -241,14 +241,21 @@ int sort_key_plan(int impl, int nd, const uint64_t* dims, int mode, int* keys) {
 
 // Stable sort of the COO by the composite mode list `keys` (most significant
 // first). Produces sorted copies of every mode's indices and the values.
+// Stable sort of the nonzeros (or of the subset `subset[0..n_sub)` of COO
+// indices, ties kept in subset order) by `keys`, most significant first.
 static int sort_coo(const mmcsf_coo* X, const std::vector<int>& keys, DevBuf* sorted_inds, DevBuf& sorted_vals,
-                    cudaStream_t s, Launches& L, DevBuf* perm_out = nullptr) {
-  const uint64_t n = X->nnz;
+                    cudaStream_t s, Launches& L, DevBuf* perm_out = nullptr, const DevBuf* subset = nullptr,
+                    uint64_t n_sub = 0) {
+  const uint64_t n = subset ? n_sub : X->nnz;
   const int nd = X->nd;
   DevBuf perm, perm2, k1, k2;
-  MMCSF_CUDA(perm.alloc(n * 4));
-  MMCSF_CUDA(iota_u32(perm.as<uint32_t>(), n, s));
-  ++L.n;
+  MMCSF_CUDA(perm.alloc(std::max<uint64_t>(n, 1) * 4));
+  if (subset) {
+    if (n) MMCSF_CUDA(cudaMemcpyAsync(perm.p, subset->p, n * 4, cudaMemcpyDeviceToDevice, s));
+  } else {
+    MMCSF_CUDA(iota_u32(perm.as<uint32_t>(), n, s));
+    ++L.n;
+  }
   if (n > 1 && !keys.empty()) {
     MMCSF_CUDA(perm2.alloc(n * 4));
     MMCSF_CUDA(k1.alloc(n * 8));
@@ -270,7 +277,7 @@ static int sort_coo(const mmcsf_coo* X, const std::vector<int>& keys, DevBuf* so
     if (!cur.empty()) groups.push_back(cur);
     Idx4 in{};
     for (int m = 0; m < nd; ++m) in.p[m] = X->d_inds[m].as<uint32_t>();
-    bool first = true;
+    bool first = subset == nullptr;  // keys come through perm once it is not the identity
     for (auto& g : groups) {  // least significant group first
       int md[4] = {0, 0, 0, 0}, sh[4] = {0, 0, 0, 0};
       int tot = 0;
@@ -569,8 +576,11 @@ extern "C" int mmcsf_build(mmcsf_coo* X, const mmcsf_build_opts* opts, void* str
     return set_error(MMCSF_ERR_INVALID, "unknown implementation type -t %d", opts->impl);
   if (opts->mode < 0 || opts->mode > nd - 1)
     return set_error(MMCSF_ERR_INVALID, "Mode cannot be larger than tensor dimension.");
-  if (opts->partition_rule != 0)
+  if (opts->partition_rule != 0 && opts->partition_rule != 1)
     return set_error(MMCSF_ERR_UNSUPPORTED, "partition rule %d not implemented", opts->partition_rule);
+  if (opts->partition_rule == 1 && opts->impl != MMCSF_IMPL_MMCSF)
+    return set_error(MMCSF_ERR_INVALID, "the partition heuristic applies to MM-CSF formats (-t 12)");
+  if (opts->partition_ratio < 0) return set_error(MMCSF_ERR_INVALID, "partition ratio must be >= 0");
   for (int m = 0; m < nd; ++m)
     if (X->dims[m] >= (1ull << 31))
       return set_error(MMCSF_ERR_UNSUPPORTED, "mode %d length %llu: formats need lengths below 2^31", m,
@@ -595,6 +605,8 @@ extern "C" int mmcsf_build(mmcsf_coo* X, const mmcsf_build_opts* opts, void* str
   std::vector<std::vector<int>> chain;
   chain.push_back(std::vector<int>(Fm->xorder, Fm->xorder + K));
   int part_order[4] = {0, 1, 2, 3};
+  bool heuristic = false;
+  int orders_all[4][4] = {{0, 1, 2, 3}, {0, 1, 2, 3}, {0, 1, 2, 3}, {0, 1, 2, 3}};
   if (opts->impl == MMCSF_IMPL_MMCSF) {
     // src/mttkrp.cu:314-352: per-mode CSFs sorted in place on the shared arrays
     int orders[4][4];
@@ -606,14 +618,20 @@ extern "C" int mmcsf_build(mmcsf_coo* X, const mmcsf_build_opts* opts, void* str
       if (m != redun) chain.push_back(std::vector<int>(orders[m], orders[m] + K));
     }
     Fm->redun = redun;
-    // mm_partition_reuseBased ends with `mode = 2;` (src/util.h:2517): every
-    // nonzero lands in partition 2, which sort_MI_CSF then sorts by its order.
-    chain.push_back(std::vector<int>(orders[2], orders[2] + K));
-    for (int i = 0; i < nd; ++i) part_order[i] = orders[2][i];
+    Fm->partition_rule = opts->partition_rule;
     for (int m = 0; m < nd; ++m) {
       Fm->parts[m].nd = nd;
       for (int i = 0; i < nd; ++i) Fm->parts[m].order[i] = orders[m][i];
     }
+    if (opts->partition_rule == 1) heuristic = true;
+    // mm_partition_reuseBased ends with `mode = 2;` (src/util.h:2517): every
+    // nonzero lands in partition 2, which sort_MI_CSF then sorts by its order.
+    if (!heuristic) {
+      chain.push_back(std::vector<int>(orders[2], orders[2] + K));
+      for (int i = 0; i < nd; ++i) part_order[i] = orders[2][i];
+    }
+    for (int m = 0; m < nd; ++m)
+      for (int i = 0; i < nd; ++i) orders_all[m][i] = orders[m][i];
   } else {
     for (int i = 0; i < nd; ++i) part_order[i] = Fm->xorder[i];
   }
@@ -627,17 +645,60 @@ extern "C" int mmcsf_build(mmcsf_coo* X, const mmcsf_build_opts* opts, void* str
   MMCSF_TRY(sort_coo(X, keys, sorted, svals, s, L, &part_perm));
   const int target = opts->impl == MMCSF_IMPL_MMCSF ? 2 : 0;
   const uint64_t fbrs_th = opts->impl == MMCSF_IMPL_MMCSF ? FBRS_TH_MMCSF : FBRS_TH_OFF;
+  if (heuristic) {
+    // X is now in the order the partition loop visits it (the chain of
+    // per-mode sorts); the heuristic picks a partition per nonzero, and every
+    // partition is filled in X order (populate_paritions) and sorted by its
+    // own mode order (sort_MI_CSF, src/util.h:412-527)
+    const uint32_t* sx[4] = {nullptr, nullptr, nullptr, nullptr};
+    for (int m = 0; m < nd; ++m) sx[m] = sorted[m].as<uint32_t>();
+    DevBuf part;
+    MMCSF_CUDA(part.alloc(std::max<uint64_t>(X->nnz, 1)));
+    const int ratio = opts->partition_ratio ? opts->partition_ratio : 1;
+    MMCSF_TRY(mm_partition_heuristic(nd, X->dims, orders_all, Fm->xorder, Fm->redun, ratio, sx, X->nnz,
+                                     part.as<uint8_t>(), &Fm->heur_rounds, &L.n, s));
+    for (int m = 0; m < nd; ++m) sorted[m].release();
+    svals.release();
+    DevBuf gperm;  // the format's nonzero order: partitions 0..nd-1, each in its own sorted order
+    MMCSF_CUDA(gperm.alloc(std::max<uint64_t>(X->nnz, 1) * 4));
+    uint64_t off = 0;
+    for (int p = 0; p < nd; ++p) {
+      DevBuf members;
+      uint64_t cnt = 0;
+      MMCSF_TRY(partition_members(part.as<uint8_t>(), p, part_perm.as<uint32_t>(), X->nnz, members, &cnt, &L.n, s));
+      if (cnt == 0) continue;
+      std::vector<int> pkeys(orders_all[p], orders_all[p] + K);
+      DevBuf ps[4], pv, pperm;
+      MMCSF_TRY(sort_coo(X, pkeys, ps, pv, s, L, &pperm, &members, cnt));
+      MMCSF_TRY(build_csf(nd, orders_all[p], cnt, ps, pv, fth, fbrs_th, opts->keep_coo != 0, Fm->parts[p], s, L));
+      MMCSF_CUDA(cudaMemcpyAsync(gperm.as<uint32_t>() + off, pperm.p, cnt * 4, cudaMemcpyDeviceToDevice, s));
+      if (cnt < X->nnz) {
+        if (!Fm->all_vals.p) MMCSF_CUDA(Fm->all_vals.alloc(X->nnz * 4));
+        MMCSF_CUDA(cudaMemcpyAsync(Fm->all_vals.as<float>() + off, Fm->parts[p].vals.p, cnt * 4,
+                                   cudaMemcpyDeviceToDevice, s));
+      }
+      off += cnt;
+      MMCSF_CUDA(cudaStreamSynchronize(s));
+    }
+    part_perm = std::move(gperm);
+  } else {
+    MMCSF_TRY(build_csf(nd, part_order, X->nnz, sorted, svals, fth, fbrs_th,
+                        opts->keep_coo != 0 || opts->impl == MMCSF_IMPL_HBCSF, Fm->parts[target], s, L));
+  }
   CsfPart& P = Fm->parts[target];
-  MMCSF_TRY(build_csf(nd, part_order, X->nnz, sorted, svals, fth, fbrs_th,
-                      opts->keep_coo != 0 || opts->impl == MMCSF_IMPL_HBCSF, P, s, L));
   if (opts->impl == MMCSF_IMPL_BCSF) MMCSF_TRY(compute_bins(P, true, s, L));
   if (opts->impl == MMCSF_IMPL_MMCSF && opts->views) {
     // Slice-major views: a CSF whose level 0 is mode m, in the reference's
     // order for a mode-m CSF (order_tensormode), fully sorted, no splits.
     for (int m = 0; m < nd; ++m) {
-      const bool at_leaf = P.order[nd - 1] == m;
+      bool at_leaf = false, root_everywhere = true;
+      for (int p = 0; p < nd; ++p) {
+        if (!Fm->parts[p].present) continue;
+        if (Fm->parts[p].order[nd - 1] == m) at_leaf = true;
+        if (Fm->parts[p].order[0] != m) root_everywhere = false;
+      }
       if (opts->views == 1 && !at_leaf) continue;
-      if (P.order[0] == m) continue;  // the partition already serves m at level 0
+      if (root_everywhere) continue;  // the partitions already serve m at level 0
       int vo[4];
       order_modes(nd, X->dims, m, vo);
       std::vector<int> vkeys(vo, vo + nd);
@@ -688,6 +749,13 @@ extern "C" int mmcsf_format_info(const mmcsf_format* F, int part, mmcsf_part_inf
   info->n_fbrs = P.n[1];
   info->n_fibers = P.n_fibers();
   info->device_bytes = P.bytes();
+  return MMCSF_OK;
+}
+
+extern "C" int mmcsf_format_partitioning(const mmcsf_format* F, int* partition_rule, int* rounds) {
+  if (!F) return set_error(MMCSF_ERR_INVALID, "null argument");
+  if (partition_rule) *partition_rule = F->partition_rule;
+  if (rounds) *rounds = F->heur_rounds;
   return MMCSF_OK;
 }
 

@@ -66,6 +66,13 @@ struct HybExtra {
   DevBuf csl_bin_of;
 };
 
+// The MM-CSF partition heuristic (partition.cu).
+int mm_partition_heuristic(int nd, const uint64_t* dims, const int (*orders)[4], const int* xorder, int redun,
+                           int fbth, const uint32_t* const* sx, uint64_t n, uint8_t* part, int* rounds,
+                           int* launches, cudaStream_t s);
+int partition_members(const uint8_t* part, int p, const uint32_t* perm, uint64_t n, DevBuf& out, uint64_t* count,
+                      int* launches, cudaStream_t s);
+
 }  // namespace mmcsf
 
 struct mmcsf_format {
@@ -75,6 +82,9 @@ struct mmcsf_format {
   uint64_t nnz = 0;
   int mode = 0;      // -m
   int redun = -1;    // redunMode (MM-CSF)
+  int partition_rule = 0;
+  int heur_rounds = 0;  // rounds the partition heuristic took (partition_rule 1)
+  mmcsf::DevBuf all_vals;  // several partitions: their values concatenated (the format's nonzero order)
   int xorder[4] = {0, 1, 2, 3};
   uint64_t fbr_th = 0;
   mmcsf::CsfPart parts[4];

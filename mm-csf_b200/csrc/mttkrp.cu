@@ -1074,8 +1074,11 @@ int mttkrp_mode_vals(const mmcsf_format* F, int mode, int R, int dtype, const vo
     }
     return part_mttkrp(F, V, mode, R, dtype, U, out, &c, s, launches, vv);
   }
-  for (int p = 0; p < F->nd; ++p)
-    MMCSF_TRY(part_mttkrp(F, F->parts[p], mode, R, dtype, U, out, &c, s, launches, vals));
+  uint64_t off = 0;  // caller values are in the format's order: partitions 0..nd-1
+  for (int p = 0; p < F->nd; ++p) {
+    MMCSF_TRY(part_mttkrp(F, F->parts[p], mode, R, dtype, U, out, &c, s, launches, vals ? vals + off : nullptr));
+    if (F->parts[p].present) off += F->parts[p].nnz;
+  }
   if (F->impl == MMCSF_IMPL_HBCSF) {
     if (vals) return set_error(MMCSF_ERR_UNSUPPORTED, "MTTKRP on other values is not available for HB-CSF");
     MMCSF_TRY(hyb_extra_mttkrp(F, R, dtype, U, out, s, launches));
@@ -1191,8 +1194,10 @@ extern "C" int mmcsf_mttkrp_pair(const mmcsf_format* F, int R, int factor_dtype,
   MMCSF_TRY(check_call(F, R, factor_dtype));
   if (F->impl != MMCSF_IMPL_MMCSF) return set_error(MMCSF_ERR_INVALID, "the two-output walk needs an MM-CSF format");
   const CsfPart* P = nullptr;
+  int np = 0;
   for (int p = 0; p < F->nd; ++p)
-    if (F->parts[p].present) P = &F->parts[p];
+    if (F->parts[p].present) { P = &F->parts[p]; ++np; }
+  if (np > 1) return set_error(MMCSF_ERR_UNSUPPORTED, "the two-output walk needs a single-partition format");
   if (!P || P->nd != 3 || !P->mid.p) return set_error(MMCSF_ERR_UNSUPPORTED, "the two-output walk is 3-D");
   if (modes) { modes[0] = P->order[0]; modes[1] = P->order[1]; }
   if (!d_factors || !d_out_slice || !d_out_mid) return modes ? MMCSF_OK : set_error(MMCSF_ERR_INVALID, "null pointer");
@@ -1229,13 +1234,16 @@ namespace {
 bool pair_active(const mmcsf_format* F, int R, const mmcsf_kernel_cfg* cfg, int* modes) {
   if (!F->pair_use || F->impl != MMCSF_IMPL_MMCSF || F->nd != 3 || !native_R(R) || R > 128) return false;
   if (cfg && (cfg->traversal != 0 || cfg->kernel != 0)) return false;
+  const CsfPart* P = nullptr;
   for (int p = 0; p < F->nd; ++p)
-    if (F->parts[p].present && F->parts[p].mid.p) {
-      modes[0] = F->parts[p].order[0];
-      modes[1] = F->parts[p].order[1];
-      return true;
+    if (F->parts[p].present) {
+      if (P) return false;  // several partitions
+      P = &F->parts[p];
     }
-  return false;
+  if (!P || !P->mid.p) return false;
+  modes[0] = P->order[0];
+  modes[1] = P->order[1];
+  return true;
 }
 }  // namespace
 

@@ -394,6 +394,12 @@ cudaError_t launch_poisson(const SArgs<T>& a, int R, cudaStream_t s) {
   }
 }
 
+int n_parts(const mmcsf_format* F) {
+  int k = 0;
+  for (int p = 0; p < 4; ++p) k += F->parts[p].present ? 1 : 0;
+  return k;
+}
+
 const CsfPart* main_part(const mmcsf_format* F) {
   if (F->impl == MMCSF_IMPL_MMCSF) {
     for (int p = 0; p < F->nd; ++p)
@@ -416,8 +422,12 @@ extern "C" int mmcsf_sampled_model(const mmcsf_format* F, int R, int factor_dtyp
     return set_error(MMCSF_ERR_UNSUPPORTED, "sampled model runs ranks 4, 8, ..., 256");
   if (factor_dtype != MMCSF_DTYPE_F32 && factor_dtype != MMCSF_DTYPE_BF16)
     return set_error(MMCSF_ERR_INVALID, "bad dtype");
-  const CsfPart* P = main_part(F);
-  if (!P || !P->nnz) return MMCSF_OK;
+  // every part in the format's nonzero order (MM-CSF partitions 0..nd-1)
+  uint64_t off = 0;
+  int launched = 0;
+  for (int p = 0; p < 4; ++p) {
+  const CsfPart* P = F->impl == MMCSF_IMPL_MMCSF ? &F->parts[p] : (p == 0 ? &F->parts[0] : nullptr);
+  if (!P || !P->present || !P->nnz) continue;
   const int lf = P->nd - 2;
   cudaError_t e;
   auto fill = [&](auto& a, auto tag) {
@@ -440,7 +450,7 @@ extern "C" int mmcsf_sampled_model(const mmcsf_format* F, int R, int factor_dtyp
     a.nslc = (uint32_t)P->n[0];
     for (int l = 0; l < P->nd; ++l) a.U[l] = static_cast<const T*>(d_factors[P->order[l]]);
     a.lam = d_lambda;
-    a.out = d_out;
+    a.out = d_out + off;
   };
   if (factor_dtype == MMCSF_DTYPE_F32) {
     SArgs<float> a{};
@@ -452,7 +462,10 @@ extern "C" int mmcsf_sampled_model(const mmcsf_format* F, int R, int factor_dtyp
     e = launch_sR<__nv_bfloat16>(a, P->nd, R, S(stream));
   }
   if (e != cudaSuccess) return set_error(MMCSF_ERR_CUDA, "sampled model launch: %s", cudaGetErrorString(e));
-  const_cast<mmcsf_format*>(F)->last_launches = 1;
+  off += P->nnz;
+  ++launched;
+  }
+  const_cast<mmcsf_format*>(F)->last_launches = launched;
   return MMCSF_OK;
 }
 
@@ -465,6 +478,8 @@ extern "C" int mmcsf_poisson_step(const mmcsf_format* F, int R, int factor_dtype
     return set_error(MMCSF_ERR_UNSUPPORTED, "the fused Poisson step runs ranks 4, 8, 16, 32, 64");
   if (factor_dtype != MMCSF_DTYPE_F32 && factor_dtype != MMCSF_DTYPE_BF16)
     return set_error(MMCSF_ERR_INVALID, "bad dtype");
+  if (n_parts(F) > 1)
+    return set_error(MMCSF_ERR_UNSUPPORTED, "the fused Poisson step needs a single-partition format");
   const CsfPart* P = main_part(F);
   if (!P || P->nd != 3 || !P->mid.p) return set_error(MMCSF_ERR_UNSUPPORTED, "the fused Poisson step needs a 3-D part");
   if (root_mode) *root_mode = P->order[0];
@@ -507,6 +522,11 @@ extern "C" int mmcsf_poisson_step(const mmcsf_format* F, int R, int factor_dtype
 extern "C" int mmcsf_format_values(const mmcsf_format* F, const float** d_vals, uint64_t* nnz) {
   if (!F) return set_error(MMCSF_ERR_INVALID, "null argument");
   if (F->impl == MMCSF_IMPL_HBCSF) return set_error(MMCSF_ERR_UNSUPPORTED, "not available for HB-CSF formats");
+  if (n_parts(F) > 1) {  // several partitions: their values concatenated at construction
+    if (d_vals) *d_vals = F->all_vals.as<float>();
+    if (nnz) *nnz = F->nnz;
+    return MMCSF_OK;
+  }
   const CsfPart* P = main_part(F);
   if (d_vals) *d_vals = P ? P->vals.as<float>() : nullptr;
   if (nnz) *nnz = P ? P->nnz : 0;

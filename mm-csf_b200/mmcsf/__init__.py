@@ -177,17 +177,22 @@ class Format:
 
     impl follows the reference's -t: 12 = MM-CSF (all modes), 8 = B-CSF,
     10 = HB-CSF (single mode `mode`). fiber_threshold is -f (0 = the
-    reference default). Replaces the builder chain the reference's main runs
-    (src/mttkrp.cu:72-389)."""
+    reference default). partition_rule 0 is the reference as shipped (every
+    nonzero in partition 2); 1 lets its partition heuristic decide
+    (mm_partition_reuseBased without the override at src/util.h:2517), with
+    partition_ratio as -h. Replaces the builder chain the reference's main
+    runs (src/mttkrp.cu:72-389)."""
 
-    def __init__(self, coo, impl=IMPL_MMCSF, mode=0, fiber_threshold=0, keep_coo=False, views=0, stream=None):
+    def __init__(self, coo, impl=IMPL_MMCSF, mode=0, fiber_threshold=0, keep_coo=False, views=0,
+                 partition_rule=0, partition_ratio=0, stream=None):
         o = BuildOpts()
         o.impl = impl
         o.mode = mode
         o.fiber_threshold = int(fiber_threshold)
-        o.partition_rule = 0
+        o.partition_rule = int(partition_rule)
         o.keep_coo = 1 if keep_coo else 0
         o.views = int(views)
+        o.partition_ratio = int(partition_ratio)
         h = c_voidp()
         check(lib().mmcsf_build(coo._h, ctypes.byref(o), _stream(stream), ctypes.byref(h)))
         self._h = h
@@ -452,6 +457,19 @@ class Format:
                 "lambda": np.array([lam[i] for i in range(rank)]), "factors": outs}
 
     # -- sampled model and adjoint ------------------------------------------
+    def partitioning(self):
+        """(partition_rule, rounds the partition heuristic took to settle)."""
+        rule, rounds = ctypes.c_int(), ctypes.c_int()
+        check(lib().mmcsf_format_partitioning(self._h, ctypes.byref(rule), ctypes.byref(rounds)))
+        return rule.value, rounds.value
+
+    def partitions(self):
+        """Indices of the non-empty parts (MM-CSF: partitions 0..nd-1), in
+        the format's nonzero order."""
+        if self.impl != IMPL_MMCSF:
+            return [0]
+        return [p for p in range(self.nd) if self.info(p)["present"]]
+
     def _main_part(self):
         if self.impl == IMPL_MMCSF:
             for p in range(self.nd):
@@ -472,8 +490,8 @@ class Format:
     def nonzero_coords(self):
         """Per-mode coordinates (numpy uint64) of every nonzero in the
         format's nonzero order; needs keep_coo=True at build time."""
-        p = self._main_part()
-        return [self.export(p, f"inds{m}") for m in range(self.nd)]
+        parts = self.partitions() or [self._main_part()]
+        return [np.concatenate([self.export(p, f"inds{m}") for p in parts]) for m in range(self.nd)]
 
     def sampled_model(self, factors, lam=None, out=None, stream=None):
         """xhat[x] = sum_r lam_r prod_m A_m[i_m(x), r] at every nonzero, in the

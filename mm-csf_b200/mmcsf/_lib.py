@@ -30,7 +30,7 @@ class GenSpec(ctypes.Structure):
 
 class BuildOpts(ctypes.Structure):
     _fields_ = [("impl", c_int), ("mode", c_int), ("fiber_threshold", c_u64), ("partition_rule", c_int),
-                ("keep_coo", c_int), ("views", c_int)]
+                ("keep_coo", c_int), ("views", c_int), ("partition_ratio", c_int)]
 
 
 class PartInfo(ctypes.Structure):
@@ -86,6 +86,7 @@ SIGNATURES = {
     "mmcsf_format_destroy": ([c_voidp], None),
     "mmcsf_format_info": ([c_voidp, c_int, ctypes.POINTER(PartInfo)], c_int),
     "mmcsf_format_meta": ([c_voidp, ctypes.POINTER(c_int), ctypes.POINTER(c_int)], c_int),
+    "mmcsf_format_partitioning": ([c_voidp, ctypes.POINTER(c_int), ctypes.POINTER(c_int)], c_int),
     "mmcsf_format_export": ([c_voidp, c_int, ctypes.c_char_p, c_u64p, c_u64, c_u64p], c_int),
     "mmcsf_format_export_f32": ([c_voidp, c_int, ctypes.c_char_p, c_f32p, c_u64, c_u64p], c_int),
     "mmcsf_mttkrp": ([c_voidp, c_int, c_int, c_int, ctypes.POINTER(c_voidp), c_voidp,

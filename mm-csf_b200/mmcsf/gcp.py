@@ -102,7 +102,7 @@ class PoissonNZ(torch.autograd.Function):
 
 def _fused_ok(fmt, factors, lam):
     return (lam is None and fmt.nd == 3 and factors[0].shape[1] in (4, 8, 16, 32, 64)
-            and fmt.impl == 12)
+            and fmt.impl == 12 and len(fmt.partitions()) == 1)
 
 
 def sampled_cp(fmt, factors, lam=None, precision="fp32"):

@@ -29,7 +29,8 @@ also       = format_build_ms (device construction), bf16_factors (the step
              with BF16 factors and its error), ttm (the reference's ttm on
              the same tensor), cp (CP-ALS and Poisson gradient CP: BF16 vs
              FP32 seconds per iteration and fits), formats (4-D: B-CSF and
-             HB-CSF beside MM-CSF).
+             HB-CSF beside MM-CSF), partition_heuristic (the same step on the
+             partitions the reference's heuristic picks, partition_rule 1).
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 """
@@ -84,6 +85,8 @@ def parse():
     ap.add_argument("--no-cp", action="store_true", help="skip the CP-ALS and Poisson gradient-CP sections")
     ap.add_argument("--no-formats", action="store_true", help="4-D workloads: skip the B-CSF / HB-CSF section")
     ap.add_argument("--no-bf16", action="store_true", help="skip the BF16-factor section")
+    ap.add_argument("--no-heuristic", action="store_true",
+                    help="skip the section on the partition heuristic's MM-CSF (partition_rule 1)")
     ap.add_argument("--cp-scale", type=float, default=1.0, help="scale the CP workloads' nonzero counts")
     return ap.parse_args()
 
@@ -299,6 +302,41 @@ def format_section(X, dims, R, tdt):
             del F
             torch.cuda.empty_cache()
         out[name] = {"mode_ms": ms, "all_mode_ms": sum(ms)}
+    return out
+
+
+def heuristic_section(X, dims, R, tdt, views):
+    """The same all-mode step on the MM-CSF whose partitions the reference's
+    partition heuristic chooses (partition_rule 1, -h 1) instead of the
+    shipped all-to-partition-2: device build time (the heuristic's rounds
+    included), partition sizes, and the tuned step time."""
+    import torch
+    import mmcsf
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    F = mmcsf.Format(X, impl=mmcsf.IMPL_MMCSF, mode=0, views=views, partition_rule=1)
+    torch.cuda.synchronize()
+    build_ms = (time.perf_counter() - t0) * 1e3
+    _, rounds = F.partitioning()
+    parts = {p: F.info(p)["nnz"] for p in F.partitions()}
+    g = torch.Generator(device="cuda").manual_seed(1234)
+    U = [torch.rand(d, R, device="cuda", generator=g).to(tdt) for d in dims]
+    outs = [torch.empty(d, R, device="cuda") for d in dims]
+    F.tune(U, outs)
+    for _ in range(3):
+        F.mttkrp_all(U, outs)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(10):
+        F.mttkrp_all(U, outs)
+    e1.record()
+    torch.cuda.synchronize()
+    out = {"format_build_ms": build_ms, "rounds": rounds, "partition_nnz": parts,
+           "ms_per_step": e0.elapsed_time(e1) / 10, "launches_per_step": F.last_launches}
+    del F
+    torch.cuda.empty_cache()
     return out
 
 
@@ -686,6 +724,9 @@ def main():
         F.mttkrp_all(U, outs)
         bf16 = bf16_section(F, U, outs, min(a.steps, 20), a.warmup)
     ttm = ttm_section(X, dims, R, info["mode_order"][0], rows) if nd == 3 and R in (4, 8, 16, 32, 64, 128) else None
+    heur = None
+    if not a.no_heuristic:
+        heur = heuristic_section(X, dims, R, tdt, a.views)
     formats = None
     if nd == 4 and not a.no_formats:
         fm = format_section(X, dims, R, tdt)
@@ -703,7 +744,7 @@ def main():
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": e2e, "gpu_launches": launches_per_step * a.steps, "clocks": clocks, "bf16_factors": bf16,
-            "ttm": ttm, "cp": cp, "formats": formats}
+            "ttm": ttm, "cp": cp, "formats": formats, "partition_heuristic": heur}
     print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()

@@ -1,5 +1,6 @@
 """The `mttkrp` command (mm-csf_b200/bin/mttkrp), which keeps the reference's
-flags (-i -m -R -t -f -w -b -v -c -o; src/util.h:3341-3442) and its
+flags (-i -m -R -t -f -w -b -v -c -o -h; src/util.h:3341-3442), adds -P (the
+partition rule), and keeps its
 "Total GPU time ... nSlc/nFibers/nnz" line (src/mttkrp_gpu.cu:3760-3767).
 
 CPU: argument errors end with a message and a nonzero status (the reference
@@ -59,7 +60,10 @@ def test_cli_formats_and_modes(nd, tmp_path):
     U = [np.full((d, R), m + 0.5, np.float32) for m, d in enumerate(dims)]
     for t, modes in ((12, [0]), (8, range(nd)), (10, range(nd))):
         for m in modes:
-            for extra in ([], ["-w", "2", "-f", "3"]):
+            extras = [[], ["-w", "2", "-f", "3"]]
+            if t == 12:  # the partition heuristic deciding (-P 1), with -h
+                extras += [["-P", "1"], ["-P", "1", "-h", "2", "-f", "3"]]
+            for extra in extras:
                 out = tmp_path / f"o_{t}_{m}.txt"
                 p = _run(["-i", str(tns), "-m", str(m), "-R", str(R), "-t", str(t), "-c", "1", "-o", str(out)]
                          + extra)

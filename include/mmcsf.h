@@ -205,8 +205,10 @@ int mmcsf_mttkrp(const mmcsf_format* F, int mode, int R, int factor_dtype, const
  * partition across modes): on a 3-D MM-CSF format, the MTTKRP of the
  * partition's slice mode (modes[0], into d_out_slice) and of its middle mode
  * (modes[1], into d_out_mid) from one traversal that gathers each nonzero's
- * factor rows once. With null outputs only `modes` is filled. R in 4..128
- * (powers of two). */
+ * factor rows once. cfg->kernel 2 runs the branch-free fiber walk (the middle
+ * row gathered once per fiber), 3 the per-nonzero form (0: the tuned choice);
+ * chunk and min_blocks as for mmcsf_mttkrp. With null outputs only `modes` is
+ * filled. R in 4..128 (powers of two). */
 int mmcsf_mttkrp_pair(const mmcsf_format* F, int R, int factor_dtype, const void* const* d_factors,
                       float* d_out_slice, float* d_out_mid, int* modes, const mmcsf_kernel_cfg* cfg, void* stream);
 /* All modes, each from the same input factors: d_outs[m] gets mode m. When
@@ -235,6 +237,7 @@ typedef struct {
   float ms[4];      /* best time per mode */
   int pair;         /* 1: mmcsf_mttkrp_all runs the partition's two upper modes in one walk (mmcsf_mttkrp_pair) */
   int pair_chunk, pair_min_blocks;
+  int pair_kernel;  /* 2: branch-free fiber walk with both outputs; 3 (or 0): per-nonzero form */
   float pair_ms;    /* best time of that walk (both modes) */
 } mmcsf_plan;
 int mmcsf_tune(mmcsf_format* F, int R, int factor_dtype, const void* const* d_factors, float* const* d_outs,

@@ -93,7 +93,7 @@ struct mmcsf_format {
   int plan_chunk[4] = {0, 0, 0, 0};
   int plan_mb[4] = {0, 0, 0, 0};
   int plan_kernel[4] = {0, 0, 0, 0};
-  int pair_chunk = 0, pair_mb = 0;  // the two-output walk's launch shape (0: defaults)
+  int pair_chunk = 0, pair_mb = 0, pair_kernel = 0;  // the two-output walk's launch shape (0: defaults)
   bool pair_use = false;            // mmcsf_mttkrp_all runs the partition's two upper modes in one walk
   mmcsf::HybExtra hyb;
   int last_launches = 0;

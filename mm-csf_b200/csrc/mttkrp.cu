@@ -358,11 +358,13 @@ __global__ void __launch_bounds__(256, MB) k_mttkrp_flat(const Args<T> a) {
   const T* __restrict__ U1 = a.U[1];
   const T* __restrict__ U2 = a.U[2];
   float* __restrict__ out = a.out;
+  float* __restrict__ out2 = a.out2;
   const uint32_t c0 = (uint32_t)tl * 4;
   auto ld = [&](const T* U, uint32_t row, int v) -> float4 {
     return Row<T>::load(U + (uint64_t)row * R, c0 + (uint32_t)(v * G * 4));
   };
   auto rd = [&](uint32_t row, int v, float4 x) { red4(out + (uint64_t)row * R + c0 + v * G * 4, x); };
+  auto rd2 = [&](uint32_t row, int v, float4 x) { red4(out2 + (uint64_t)row * R + c0 + v * G * 4, x); };
 
   const uint64_t team = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) / G;
   const bool active = team * chunk < a.nnz;
@@ -379,6 +381,7 @@ __global__ void __launch_bounds__(256, MB) k_mttkrp_flat(const Args<T> a) {
     if constexpr (OUT == 0) rowB[v] = ld(U1, cb, v);
     if constexpr (OUT == 1) rowA[v] = ld(U0, ca, v);
     if constexpr (OUT == 2) { rowA[v] = ld(U0, ca, v); rowB[v] = rowA[v] * ld(U1, cb, v); }
+    if constexpr (OUT == 3) { rowA[v] = ld(U0, ca, v); rowB[v] = ld(U1, cb, v); }
   }
 
   // Block pipeline: when block i (G nonzeros) is processed, its indices,
@@ -472,6 +475,27 @@ __global__ void __launch_bounds__(256, MB) k_mttkrp_flat(const Args<T> a) {
                   for (int v = 0; v < V; ++v) rowA[v] = ld(U0, ca, v);
                 }
               }
+            } else if constexpr (OUT == 3) {
+              // both outputs: the closing fiber's sum goes to the middle
+              // mode's row and, through its middle row, into the slice sum
+#pragma unroll
+              for (int v = 0; v < V; ++v) {
+                rd2(cb, v, pmul(rowA[v], accf[v]));
+                accs[v] = pfma(rowB[v], accf[v], accs[v]);
+                accf[v] = f4(0.f);
+              }
+              cb = bj[j];
+              if constexpr (SLOW) {
+                if (aj != ca) {
+#pragma unroll
+                  for (int v = 0; v < V; ++v) { rd(ca, v, accs[v]); accs[v] = f4(0.f); }
+                  ca = aj;
+#pragma unroll
+                  for (int v = 0; v < V; ++v) rowA[v] = ld(U0, ca, v);
+                }
+              }
+#pragma unroll
+              for (int v = 0; v < V; ++v) rowB[v] = ld(U1, cb, v);
             } else {
               if constexpr (SLOW) {
                 if (aj != ca) {
@@ -504,6 +528,10 @@ __global__ void __launch_bounds__(256, MB) k_mttkrp_flat(const Args<T> a) {
     for (int v = 0; v < V; ++v) {
       if constexpr (OUT == 0) rd(ca, v, pfma(rowB[v], accf[v], accs[v]));
       if constexpr (OUT == 1) rd(cb, v, pmul(rowA[v], accf[v]));
+      if constexpr (OUT == 3) {
+        rd(ca, v, pfma(rowB[v], accf[v], accs[v]));
+        rd2(cb, v, pmul(rowA[v], accf[v]));
+      }
     }
   }
 }
@@ -846,8 +874,24 @@ cudaError_t launch_pair(const Args<T>& a, int threads, int mb, cudaStream_t s) {
   return cudaGetLastError();
 }
 
+template <int OUT, int G, int V, class T>
+cudaError_t launch_flat(const Args<T>& a, int threads, int mb, cudaStream_t s);
+
+// kern 2: the branch-free fiber walk with both outputs; otherwise the
+// per-nonzero form
 template <class T>
-cudaError_t launch_pair_R(const Args<T>& a, int threads, int mb, cudaStream_t s) {
+cudaError_t launch_pair_R(const Args<T>& a, int threads, int mb, int kern, cudaStream_t s) {
+  if (kern == 2) {
+    switch (a.R) {
+      case 4: return launch_flat<3, 1, 1, T>(a, threads, mb, s);
+      case 8: return launch_flat<3, 2, 1, T>(a, threads, mb, s);
+      case 16: return launch_flat<3, 4, 1, T>(a, threads, mb, s);
+      case 32: return launch_flat<3, 8, 1, T>(a, threads, mb, s);
+      case 64: return launch_flat<3, 16, 1, T>(a, threads, mb, s);
+      case 128: return launch_flat<3, 32, 1, T>(a, threads, mb, s);
+      default: return cudaErrorInvalidValue;
+    }
+  }
   switch (a.R) {
     case 4: return launch_pair<1, 1, T>(a, threads, mb, s);
     case 8: return launch_pair<2, 1, T>(a, threads, mb, s);
@@ -1208,6 +1252,8 @@ extern "C" int mmcsf_mttkrp_pair(const mmcsf_format* F, int R, int factor_dtype,
   const int chunk = cfg && cfg->chunk > 0 ? cfg->chunk : (F->pair_chunk ? F->pair_chunk : 256);
   const int threads = cfg && cfg->block_threads > 0 ? cfg->block_threads : 256;
   const int mb = cfg && cfg->min_blocks > 0 ? cfg->min_blocks : (F->pair_mb ? F->pair_mb : 3);
+  const int kern = cfg && cfg->kernel > 0 ? cfg->kernel : F->pair_kernel;
+  if (kern < 0 || kern > 3) return set_error(MMCSF_ERR_INVALID, "kernel must be 0, 1, 2 or 3");
   if (threads % 32 || threads > 256) return set_error(MMCSF_ERR_INVALID, "block_threads must be a multiple of 32, <= 256");
   const int slot = CsfPart::cfib_slot((uint64_t)chunk);
   cudaError_t e;
@@ -1215,12 +1261,12 @@ extern "C" int mmcsf_mttkrp_pair(const mmcsf_format* F, int R, int factor_dtype,
     Args<float> a{};
     fill_args(a, *P, nullptr, slot, chunk, R, d_factors, d_out_slice);
     a.out2 = d_out_mid;
-    e = launch_pair_R<float>(a, threads, mb, s);
+    e = launch_pair_R<float>(a, threads, mb, kern, s);
   } else {
     Args<__nv_bfloat16> a{};
     fill_args(a, *P, nullptr, slot, chunk, R, d_factors, d_out_slice);
     a.out2 = d_out_mid;
-    e = launch_pair_R<__nv_bfloat16>(a, threads, mb, s);
+    e = launch_pair_R<__nv_bfloat16>(a, threads, mb, kern, s);
   }
   if (e != cudaSuccess) return set_error(MMCSF_ERR_CUDA, "two-output walk launch: %s", cudaGetErrorString(e));
   const_cast<mmcsf_format*>(F)->last_launches = 1;
@@ -1422,12 +1468,14 @@ extern "C" int mmcsf_tune(mmcsf_format* F, int R, int factor_dtype, const void* 
       mmcsf_mttkrp_pair(F, R, factor_dtype, nullptr, nullptr, nullptr, pm, nullptr, stream) == MMCSF_OK &&
       native_R(R) && R <= 128) {
     float bestp = 1e30f;
-    int bpc = 0, bpm = 0;
+    int bpc = 0, bpm = 0, bpk = 0;
+    for (int kern : {2, 3})
     for (int mbv = 1; mbv <= 3 && st == MMCSF_OK; ++mbv)
       for (int c : {256, 512, 1024}) {
         mmcsf_kernel_cfg cfg{};
         cfg.chunk = c;
         cfg.min_blocks = mbv;
+        cfg.kernel = kern;
         float ms = 0;
         for (int rep = 0; rep < 2; ++rep) {
           if ((st = mmcsf_mttkrp_pair(F, R, factor_dtype, d_factors, d_outs[pm[0]], d_outs[pm[1]], nullptr, &cfg,
@@ -1444,22 +1492,24 @@ extern "C" int mmcsf_tune(mmcsf_format* F, int R, int factor_dtype, const void* 
           cudaEventElapsedTime(&ms, e0, e1);
         }
         if (st != MMCSF_OK) break;
-        if (ms < bestp) { bestp = ms; bpc = c; bpm = mbv; }
+        if (ms < bestp) { bestp = ms; bpc = c; bpm = mbv; bpk = kern; }
       }
     if (st == MMCSF_OK && bestp < best_ms[pm[0]] + best_ms[pm[1]]) {
       F->pair_use = true;
       F->pair_chunk = bpc;
       F->pair_mb = bpm;
+      F->pair_kernel = bpk;
     }
     if (plan && st == MMCSF_OK) {
       plan->pair = F->pair_use ? 1 : 0;
       plan->pair_chunk = bpc;
       plan->pair_min_blocks = bpm;
+      plan->pair_kernel = bpk;
       plan->pair_ms = bestp;
     }
   } else if (plan) {
     plan->pair = 0;
-    plan->pair_chunk = plan->pair_min_blocks = 0;
+    plan->pair_chunk = plan->pair_min_blocks = plan->pair_kernel = 0;
     plan->pair_ms = 0.f;
   }
   cudaEventDestroy(e0);
@@ -1480,9 +1530,11 @@ extern "C" int mmcsf_set_plan(mmcsf_format* F, const mmcsf_plan* plan) {
     F->plan_mb[m] = plan->min_blocks[m];
     F->plan_kernel[m] = plan->kernel[m];
   }
-  if (plan->pair_chunk < 0 || plan->pair_min_blocks < 0) return set_error(MMCSF_ERR_INVALID, "bad pair entry");
+  if (plan->pair_chunk < 0 || plan->pair_min_blocks < 0 || plan->pair_kernel < 0 || plan->pair_kernel > 3)
+    return set_error(MMCSF_ERR_INVALID, "bad pair entry");
   F->pair_use = plan->pair != 0;
   F->pair_chunk = plan->pair_chunk;
   F->pair_mb = plan->pair_min_blocks;
+  F->pair_kernel = plan->pair_kernel;
   return MMCSF_OK;
 }

@@ -402,7 +402,7 @@ class Format:
                     "kernel": pl.kernel[m], "ms": pl.ms[m]} for m in list(modes)[:n]}
         if self.impl == IMPL_MMCSF:
             plan["pair"] = {"use": bool(pl.pair), "chunk": pl.pair_chunk, "min_blocks": pl.pair_min_blocks,
-                            "ms": pl.pair_ms}
+                            "kernel": pl.pair_kernel, "ms": pl.pair_ms}
         return plan
 
     def set_plan(self, plan):
@@ -414,6 +414,7 @@ class Format:
                 pl.pair = 1 if e.get("use") else 0
                 pl.pair_chunk = e.get("chunk", 0)
                 pl.pair_min_blocks = e.get("min_blocks", 0)
+                pl.pair_kernel = e.get("kernel", 0)
                 continue
             m = int(m)
             pl.traversal[m] = e["traversal"]

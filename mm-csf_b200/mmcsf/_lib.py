@@ -46,7 +46,8 @@ class KernelCfg(ctypes.Structure):
 class Plan(ctypes.Structure):
     _fields_ = [("traversal", c_int * 4), ("chunk", c_int * 4), ("min_blocks", c_int * 4),
                 ("kernel", c_int * 4), ("ms", ctypes.c_float * 4), ("pair", c_int), ("pair_chunk", c_int),
-                ("pair_min_blocks", c_int), ("pair_ms", ctypes.c_float)]
+                ("pair_min_blocks", c_int), ("pair_kernel", c_int),
+                ("pair_ms", ctypes.c_float)]
 
 
 class CpdOpts(ctypes.Structure):

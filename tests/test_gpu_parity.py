@@ -373,24 +373,26 @@ def test_two_output_walk(R, dtype, torch_cuda):
             m0, m1 = F.pair_modes()
             order = F.info(2)["mode_order"]
             assert (m0, m1) == (order[0], order[1])
-            for mb in (1, 2, 3, 4):
-                for chunk in (1, 32, 100, 1024):
-                    outs = F.mttkrp_pair(Ud, cfg={"min_blocks": mb, "chunk": chunk})
-                    assert set(outs) == {m0, m1}
-                    for m in (m0, m1):
-                        _check_close(outs[m].cpu().numpy(), ref[m], (dims, f, m, mb, chunk))
+            for kern in (2, 3):
+                for mb in (1, 2, 3, 4):
+                    for chunk in (1, 32, 100, 1024):
+                        outs = F.mttkrp_pair(Ud, cfg={"min_blocks": mb, "chunk": chunk, "kernel": kern})
+                        assert set(outs) == {m0, m1}
+                        for m in (m0, m1):
+                            _check_close(outs[m].cpu().numpy(), ref[m], (dims, f, m, kern, mb, chunk))
             plan = F.tune(Ud)
             plan["pair"].update(use=False)
             F.set_plan(plan)
             F.mttkrp_all(Ud)
             separate = F.last_launches
-            plan["pair"].update(use=True, chunk=256, min_blocks=2)
-            F.set_plan(plan)
-            for _ in range(2):
-                outs = F.mttkrp_all(Ud)
-                assert F.last_launches == separate - 1
-                for m in range(3):
-                    _check_close(outs[m].cpu().numpy(), ref[m], ("all+pair", dims, f, m))
+            for kern in (2, 3):
+                plan["pair"].update(use=True, chunk=256, min_blocks=2, kernel=kern)
+                F.set_plan(plan)
+                for _ in range(2):
+                    outs = F.mttkrp_all(Ud)
+                    assert F.last_launches == separate - 1
+                    for m in range(3):
+                        _check_close(outs[m].cpu().numpy(), ref[m], ("all+pair", dims, f, kern, m))
             if dtype == "f32":
                 houts = F.mttkrp_all_host(U)
                 for m in range(3):
@@ -421,6 +423,8 @@ def test_two_output_walk_errors(torch_cuda):
         F.mttkrp_pair([torch.rand(d, 256, device="cuda") for d in dims[:3]])  # R above 128
     with pytest.raises(mmcsf.MmcsfError):
         F.set_plan({"pair": {"use": True, "chunk": -1, "min_blocks": 1}})
+    with pytest.raises(mmcsf.MmcsfError):
+        F.set_plan({"pair": {"use": True, "chunk": 256, "min_blocks": 1, "kernel": 7}})
 
 
 @pytest.mark.parametrize("nd", [3, 4])

@@ -609,10 +609,10 @@ def main():
     def unit_bytes(modes):
         if len(modes) == 1:
             return per_mode[modes[0]]
-        # the two-output walk: vals, leaf and middle index per nonzero, slice
+        # the two-output walk: vals, leaf and middle indices per nonzero, slice
         # offsets and indices, every touched row of the three factors once,
         # both outputs written once
-        return (nnz * 12 + info["n_slices"] * 8 + sum(rows[q] * R * esz for q in range(nd))
+        return (nnz * (12 if nd == 3 else 16) + info["n_slices"] * 8 + sum(rows[q] * R * esz for q in range(nd))
                 + sum(dims[q] * R * 4 for q in modes))
 
     for _ in range(a.warmup):
@@ -672,8 +672,8 @@ def main():
     dmodes = units[di][0]
     achieved = ub[di] / (unit_ms[di] / 1e3) / 1e9
     if len(dmodes) == 2:
-        dker = "k_mttkrp_pair"
-        dlabel = (f"{dker} modes {dmodes[0]} and {dmodes[1]} (slice and middle levels of order "
+        dker = "k_mttkrp_pair" if nd == 3 else "k_mttkrp_pair4"
+        dlabel = (f"{dker} modes {dmodes[0]} and {dmodes[1]} (levels 0 and 1 of order "
                   f"{info['mode_order']}, MM-CSF partition, one walk)")
         traffic = traffic_from_profiles(a.workload, R, a.dtype, "".join(str(m) for m in dmodes), dker)
     else:

@@ -202,7 +202,7 @@ typedef struct {
 int mmcsf_mttkrp(const mmcsf_format* F, int mode, int R, int factor_dtype, const void* const* d_factors,
                  float* d_out, const mmcsf_kernel_cfg* cfg, void* stream);
 /* Two modes in one walk (no counterpart in the reference; MM-CSF's reuse of a
- * partition across modes): on a 3-D MM-CSF format, the MTTKRP of the
+ * partition across modes): on a 3-D or 4-D MM-CSF format, the MTTKRP of the
  * partition's slice mode (modes[0], into d_out_slice) and of its middle mode
  * (modes[1], into d_out_mid) from one traversal that gathers each nonzero's
  * factor rows once. cfg->kernel 2 runs the branch-free fiber walk (the middle

@@ -861,6 +861,166 @@ __global__ void __launch_bounds__(256, MB) k_mttkrp_pair(const Args<T> a) {
   }
 }
 
+// The 4-D two-output walk: the slice mode's MTTKRP, out[a] += v U1[b] (.)
+// U2[c] (.) U3[k], and the level-1 mode's, out2[b] += U0[a] (.) sum over the
+// (a, b) group of v U2[c] (.) U3[k], from one walk that gathers each
+// nonzero's three rows once (b = mid2, c = mid, k = leaf). A group closes at a
+// leaf-fiber start whose b differs from the open one, or where a slice
+// starts; splits of one (a, b) group (the fbrS split) only add reductions.
+// Both outputs zeroed by the caller.
+template <int G, int V, class T, int MB, int PFX>
+__global__ void __launch_bounds__(256, MB) k_mttkrp_pair4(const Args<T> a) {
+  constexpr uint32_t R = 4 * G * V;
+  constexpr uint32_t FLAG = 0x80000000u;
+  constexpr int PF = G > PFX ? PFX : G;
+  constexpr uint32_t GMASK = G == 32 ? FULL : ((1u << G) - 1u);
+  const int lane = threadIdx.x & 31;
+  const int tl = lane & (G - 1);
+  const int tb = lane - tl;
+  const float* __restrict__ vals = a.vals;
+  const uint32_t* __restrict__ leaf = a.leaf;
+  const uint32_t* __restrict__ mid = a.mid;
+  const uint32_t* __restrict__ mid2 = a.mid2;
+  const uint32_t* __restrict__ snz = a.snz;
+  const uint32_t* __restrict__ sidx = a.sidx;
+  const uint32_t chunk = a.chunk, nslc = a.nslc;
+  const T* __restrict__ U0 = a.U[0];
+  const T* __restrict__ U1 = a.U[1];
+  const T* __restrict__ U2 = a.U[2];
+  const T* __restrict__ U3 = a.U[3];
+  float* __restrict__ out = a.out;
+  float* __restrict__ out2 = a.out2;
+  const uint32_t c0 = (uint32_t)tl * 4;
+  auto ld = [&](const T* U, uint32_t row, int v) -> float4 {
+    return Row<T>::load(U + (uint64_t)row * R, c0 + (uint32_t)(v * G * 4));
+  };
+  auto rd = [&](float* o, uint32_t row, int v, float4 x) { red4(o + (uint64_t)row * R + c0 + v * G * 4, x); };
+
+  const uint64_t team = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) / G;
+  const bool active = team * chunk < a.nnz;
+  const uint64_t x0 = active ? team * chunk : a.nnz - 1;
+  const uint64_t x1 = active ? min(x0 + chunk, a.nnz) : x0;
+  uint32_t sl;
+  if (a.cslc) {
+    sl = active ? __ldg(a.cslc + team) : nslc - 1;
+  } else {
+    uint32_t lo = 0, hi = nslc - 1;
+    while (lo < hi) {
+      const uint32_t m = (lo + hi + 1) >> 1;
+      if ((uint64_t)__ldg(snz + m) <= x0) lo = m; else hi = m - 1;
+    }
+    sl = lo;
+  }
+  uint32_t ca = __ldg(sidx + sl);
+  uint64_t nxt = __ldg(snz + sl + 1);
+  uint32_t bopen = __ldg(mid2 + x0);
+  float4 acc[V], accf[V], rowA[V];
+#pragma unroll
+  for (int v = 0; v < V; ++v) {
+    acc[v] = accf[v] = f4(0.f);
+    rowA[v] = ld(U0, ca, v);
+  }
+  auto load_blk = [&](uint32_t itb, uint32_t& kk, uint32_t& bb, uint32_t& cc, float& vq) {
+    const uint64_t xx = x0 + itb + tl;
+    kk = 0;
+    bb = 0;
+    cc = 0;
+    vq = 0.f;
+    if (itb < chunk && xx < x1) {
+      kk = __ldg(leaf + xx);
+      bb = __ldg(mid2 + xx);
+      cc = __ldg(mid + xx);
+      vq = __ldg(vals + xx);
+    }
+  };
+  uint32_t kc, bc, cc, kn, bn, cn;
+  float vc, vn;
+  load_blk(0, kc, bc, cc, vc);
+  load_blk(G, kn, bn, cn, vn);
+  for (uint32_t it = 0; it < chunk; it += G) {
+    const uint64_t xb = x0 + it;
+    const uint32_t k = kc & ~FLAG, b = bc, c = cc;
+    const float vv = vc;
+    const uint32_t fm = (__ballot_sync(FULL, (kc & FLAG) && (xb + tl != x0)) >> tb) & GMASK;
+    kc = kn; bc = bn; cc = cn; vc = vn;
+    load_blk(it + 2 * G, kn, bn, cn, vn);
+    const bool slow = __any_sync(FULL, xb < x1 && xb + G > nxt);
+    auto block = [&](auto slow_tag) {
+      constexpr bool SLOW = decltype(slow_tag)::value;
+#pragma unroll
+      for (int jb = 0; jb < G; jb += PF) {
+        float4 rb[PF][V], rc[PF][V], rk[PF][V];
+        uint32_t bjs[PF];
+#pragma unroll
+        for (int j = 0; j < PF; ++j) {
+          const uint32_t kj = __shfl_sync(FULL, k, tb + jb + j);
+          const uint32_t cj = __shfl_sync(FULL, c, tb + jb + j);
+          bjs[j] = __shfl_sync(FULL, b, tb + jb + j);
+#pragma unroll
+          for (int v = 0; v < V; ++v) {
+            rb[j][v] = ld(U1, bjs[j], v);
+            rc[j][v] = ld(U2, cj, v);
+            rk[j][v] = ld(U3, kj, v);
+          }
+        }
+#pragma unroll
+        for (int j = 0; j < PF; ++j) {
+          const float val = __shfl_sync(FULL, vv, tb + jb + j);
+          const uint64_t x = xb + jb + j;
+          if ((fm >> (jb + j)) & 1u) {
+            bool close = bjs[j] != bopen;
+            if constexpr (SLOW) close = close || (x < x1 && x == nxt);
+            if (close) {  // the open (a, b) group ends before nonzero j
+#pragma unroll
+              for (int v = 0; v < V; ++v) { rd(out2, bopen, v, pmul(rowA[v], accf[v])); accf[v] = f4(0.f); }
+              bopen = bjs[j];
+            }
+          }
+          if constexpr (SLOW) {
+            if (x < x1 && x == nxt) {
+#pragma unroll
+              for (int v = 0; v < V; ++v) { rd(out, ca, v, acc[v]); acc[v] = f4(0.f); }
+              ++sl;
+              ca = __ldg(sidx + sl);
+              nxt = __ldg(snz + sl + 1);
+#pragma unroll
+              for (int v = 0; v < V; ++v) rowA[v] = ld(U0, ca, v);
+            }
+          }
+#pragma unroll
+          for (int v = 0; v < V; ++v) {
+            const float4 u = pmul(rc[j][v], rk[j][v]);
+            acc[v] = pfma(pmul_s(val, rb[j][v]), u, acc[v]);
+            accf[v] = pfma_s(val, u, accf[v]);
+          }
+        }
+      }
+    };
+    if (slow) block(std::true_type{});
+    else block(std::false_type{});
+  }
+  if (active) {
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      rd(out, ca, v, acc[v]);
+      rd(out2, bopen, v, pmul(rowA[v], accf[v]));
+    }
+  }
+}
+
+template <int G, int V, class T>
+cudaError_t launch_pair4(const Args<T>& a, int threads, int mb, cudaStream_t s) {
+  const uint64_t teams = (a.nnz + a.chunk - 1) / a.chunk;
+  const uint64_t blocks = (teams * G + threads - 1) / threads;
+  switch (mb) {
+    case 1: k_mttkrp_pair4<G, V, T, 1, 8><<<(unsigned)blocks, threads, 0, s>>>(a); break;
+    case 3: k_mttkrp_pair4<G, V, T, 2, 2><<<(unsigned)blocks, threads, 0, s>>>(a); break;
+    case 4: k_mttkrp_pair4<G, V, T, 3, 2><<<(unsigned)blocks, threads, 0, s>>>(a); break;
+    default: k_mttkrp_pair4<G, V, T, 2, 4><<<(unsigned)blocks, threads, 0, s>>>(a); break;
+  }
+  return cudaGetLastError();
+}
+
 template <int G, int V, class T>
 cudaError_t launch_pair(const Args<T>& a, int threads, int mb, cudaStream_t s) {
   const uint64_t teams = (a.nnz + a.chunk - 1) / a.chunk;
@@ -880,7 +1040,18 @@ cudaError_t launch_flat(const Args<T>& a, int threads, int mb, cudaStream_t s);
 // kern 2: the branch-free fiber walk with both outputs; otherwise the
 // per-nonzero form
 template <class T>
-cudaError_t launch_pair_R(const Args<T>& a, int threads, int mb, int kern, cudaStream_t s) {
+cudaError_t launch_pair_R(const Args<T>& a, int nd, int threads, int mb, int kern, cudaStream_t s) {
+  if (nd == 4) {
+    switch (a.R) {
+      case 4: return launch_pair4<1, 1, T>(a, threads, mb, s);
+      case 8: return launch_pair4<2, 1, T>(a, threads, mb, s);
+      case 16: return launch_pair4<4, 1, T>(a, threads, mb, s);
+      case 32: return launch_pair4<8, 1, T>(a, threads, mb, s);
+      case 64: return launch_pair4<16, 1, T>(a, threads, mb, s);
+      case 128: return launch_pair4<32, 1, T>(a, threads, mb, s);
+      default: return cudaErrorInvalidValue;
+    }
+  }
   if (kern == 2) {
     switch (a.R) {
       case 4: return launch_flat<3, 1, 1, T>(a, threads, mb, s);
@@ -1242,7 +1413,8 @@ extern "C" int mmcsf_mttkrp_pair(const mmcsf_format* F, int R, int factor_dtype,
   for (int p = 0; p < F->nd; ++p)
     if (F->parts[p].present) { P = &F->parts[p]; ++np; }
   if (np > 1) return set_error(MMCSF_ERR_UNSUPPORTED, "the two-output walk needs a single-partition format");
-  if (!P || P->nd != 3 || !P->mid.p) return set_error(MMCSF_ERR_UNSUPPORTED, "the two-output walk is 3-D");
+  if (!P || !P->mid.p || (P->nd == 4 && !P->mid2.p))
+    return set_error(MMCSF_ERR_UNSUPPORTED, "the two-output walk needs the per-nonzero middle indices");
   if (modes) { modes[0] = P->order[0]; modes[1] = P->order[1]; }
   if (!d_factors || !d_out_slice || !d_out_mid) return modes ? MMCSF_OK : set_error(MMCSF_ERR_INVALID, "null pointer");
   if (!native_R(R) || R > 128) return set_error(MMCSF_ERR_UNSUPPORTED, "the two-output walk runs R in 4..128");
@@ -1261,12 +1433,12 @@ extern "C" int mmcsf_mttkrp_pair(const mmcsf_format* F, int R, int factor_dtype,
     Args<float> a{};
     fill_args(a, *P, nullptr, slot, chunk, R, d_factors, d_out_slice);
     a.out2 = d_out_mid;
-    e = launch_pair_R<float>(a, threads, mb, kern, s);
+    e = launch_pair_R<float>(a, P->nd, threads, mb, kern, s);
   } else {
     Args<__nv_bfloat16> a{};
     fill_args(a, *P, nullptr, slot, chunk, R, d_factors, d_out_slice);
     a.out2 = d_out_mid;
-    e = launch_pair_R<__nv_bfloat16>(a, threads, mb, kern, s);
+    e = launch_pair_R<__nv_bfloat16>(a, P->nd, threads, mb, kern, s);
   }
   if (e != cudaSuccess) return set_error(MMCSF_ERR_CUDA, "two-output walk launch: %s", cudaGetErrorString(e));
   const_cast<mmcsf_format*>(F)->last_launches = 1;
@@ -1278,7 +1450,7 @@ namespace {
 // without a caller override of the traversal or kernel). modes[0..1] get
 // them.
 bool pair_active(const mmcsf_format* F, int R, const mmcsf_kernel_cfg* cfg, int* modes) {
-  if (!F->pair_use || F->impl != MMCSF_IMPL_MMCSF || F->nd != 3 || !native_R(R) || R > 128) return false;
+  if (!F->pair_use || F->impl != MMCSF_IMPL_MMCSF || !native_R(R) || R > 128) return false;
   if (cfg && (cfg->traversal != 0 || cfg->kernel != 0)) return false;
   const CsfPart* P = nullptr;
   for (int p = 0; p < F->nd; ++p)
@@ -1470,7 +1642,7 @@ extern "C" int mmcsf_tune(mmcsf_format* F, int R, int factor_dtype, const void* 
     float bestp = 1e30f;
     int bpc = 0, bpm = 0, bpk = 0;
     for (int kern : {2, 3})
-    for (int mbv = 1; mbv <= 3 && st == MMCSF_OK; ++mbv)
+    for (int mbv = 1; mbv <= 3 && st == MMCSF_OK && (kern == 3 || F->nd == 3); ++mbv)
       for (int c : {256, 512, 1024}) {
         mmcsf_kernel_cfg cfg{};
         cfg.chunk = c;

@@ -404,16 +404,54 @@ def test_two_output_walk(R, dtype, torch_cuda):
                 _check_close(outs[m].cpu().numpy(), ref[m], ("override", dims, f, m))
 
 
+@pytest.mark.parametrize("R", [4, 32, 128])
+@pytest.mark.parametrize("dtype", ["f32", "bf16"])
+def test_two_output_walk_4d(R, dtype, torch_cuda):
+    """The 4-D two-output walk (slice mode and level-1 mode of the partition)
+    against the FP64 oracle: every launch shape and chunk, fiber splits, the
+    fbrS split at 128 (long (o0, o1) runs), and through the all-mode calls."""
+    import mmcsf
+    torch = torch_cuda
+    rng = np.random.default_rng(600 + R)
+    cases = (([40, 30, 50, 20], 20000, True), ([900, 8, 6, 5], 6000, False), ([5, 3, 4, 2000], 20000, False))
+    for dims, n, skew in cases:
+        inds, vals = _rand_coo(rng, dims, n, skew)
+        X = mmcsf.CooTensor.from_arrays(dims, inds, vals)
+        U = [rng.random((d, R)).astype(np.float32) for d in dims]
+        if dtype == "bf16":
+            Ud = [torch.tensor(u, device="cuda").to(torch.bfloat16) for u in U]
+            U = [t.float().cpu().numpy() for t in Ud]
+        else:
+            Ud = [torch.tensor(u, device="cuda") for u in U]
+        ref = [O.mttkrp_coo_f64(dims, inds, vals, m, U) for m in range(4)]
+        for f in (0, 3):
+            F = mmcsf.Format(X, impl=mmcsf.IMPL_MMCSF, mode=0, fiber_threshold=f, views=2)
+            m0, m1 = F.pair_modes()
+            assert (m0, m1) == tuple(F.info(2)["mode_order"][:2])
+            for mb in (1, 2, 3, 4):
+                for chunk in (1, 32, 100, 1024):
+                    outs = F.mttkrp_pair(Ud, cfg={"min_blocks": mb, "chunk": chunk})
+                    for m in (m0, m1):
+                        _check_close(outs[m].cpu().numpy(), ref[m], (dims, f, m, mb, chunk))
+            plan = F.tune(Ud)
+            plan["pair"].update(use=True, chunk=512, min_blocks=2, kernel=3)
+            F.set_plan(plan)
+            outs = F.mttkrp_all(Ud)
+            for m in range(4):
+                _check_close(outs[m].cpu().numpy(), ref[m], ("all+pair", dims, f, m))
+            if dtype == "f32":
+                houts = F.mttkrp_all_host(U)
+                for m in range(4):
+                    _check_close(houts[m], ref[m], ("host+pair", dims, f, m))
+
+
 def test_two_output_walk_errors(torch_cuda):
     import mmcsf
     torch = torch_cuda
     rng = np.random.default_rng(77)
     dims = [20, 30, 10, 8]
     inds, vals = _rand_coo(rng, dims, 2000)
-    X = mmcsf.CooTensor.from_arrays(dims, inds, vals)
     U = [torch.rand(d, 16, device="cuda") for d in dims]
-    with pytest.raises(mmcsf.MmcsfError):
-        mmcsf.Format(X, impl=mmcsf.IMPL_MMCSF).mttkrp_pair(U)  # 4-D
     X3 = mmcsf.CooTensor.from_arrays(dims[:3], inds[:3], vals)
     B = mmcsf.Format(X3, impl=mmcsf.IMPL_BCSF, mode=0)
     with pytest.raises(mmcsf.MmcsfError):

@@ -18,6 +18,7 @@
 //     for the middle modes, per nonzero for the leaf mode (which scatters).
 // Correct for every R (the reference's kernels keep one scalar accumulator per
 // lane across the rank loop and are wrong for R > 32).
+#include <algorithm>
 #include <cuda_bf16.h>
 
 #include <cstring>
@@ -1517,20 +1518,20 @@ extern "C" int mmcsf_mttkrp_all_host(mmcsf_format* F, int R, const float* const*
     MMCSF_CUDA(cudaEventCreateWithFlags(&F->ev_start, cudaEventDisableTiming));
   }
   // order: the largest factor is uploaded last; its own mode (which does not
-  // read it) runs first. With the two-output walk, the mode outside it runs
-  // first and its factor is uploaded last (the walk reads every factor).
-  int pm[2] = {-1, -1};
-  const bool pair = pair_active(F, R, cfg, pm);
+  // read it) runs first, and its output's download overlaps that upload. The
+  // two-output walk is not used here: once the last factor has arrived, one
+  // launch per mode lets the first output's download overlap the next launch
+  // (measured 9.23 against 9.45 ms per call on the 100M-nonzero skewed 3-D
+  // tensor, where the copies take ~6 ms each way).
   int big = 0;
   for (int m = 1; m < nd; ++m)
     if (F->dims[m] > F->dims[big]) big = m;
-  if (pair)
-    for (int m = 0; m < nd; ++m)
-      if (m != pm[0] && m != pm[1]) big = m;
   int order[4], n = 0;
   order[n++] = big;
   for (int m = 0; m < nd; ++m)
     if (m != big) order[n++] = m;
+  // then the larger outputs first, so that their downloads start earlier
+  std::stable_sort(order + 1, order + nd, [&](int x, int y) { return F->dims[x] > F->dims[y]; });
   const void* din[4];
   MMCSF_CUDA(cudaEventRecord(F->ev_start, s));  // staging buffers are free once earlier work on s is done
   MMCSF_CUDA(cudaStreamWaitEvent(F->copy_in, F->ev_start, 0));
@@ -1551,21 +1552,11 @@ extern "C" int mmcsf_mttkrp_all_host(mmcsf_format* F, int R, const float* const*
   };
   for (int q = 0; q < nd; ++q) {
     const int m = order[q];
-    if (pair && m == pm[1]) continue;  // produced with pm[0]
-    const bool both = pair && m == pm[0];
     for (int p = 0; p < nd; ++p)
-      if (p != m || both) MMCSF_CUDA(cudaStreamWaitEvent(s, F->ev_in[p], 0));
-    if (both) {
-      MMCSF_TRY(mmcsf_mttkrp_pair(F, R, MMCSF_DTYPE_F32, din, F->stage_out[pm[0]].as<float>(),
-                                  F->stage_out[pm[1]].as<float>(), nullptr, nullptr, stream));
-      total += F->last_launches;
-      MMCSF_TRY(download(pm[0]));
-      MMCSF_TRY(download(pm[1]));
-    } else {
-      MMCSF_TRY(mmcsf_mttkrp(F, m, R, MMCSF_DTYPE_F32, din, F->stage_out[m].as<float>(), cfg, stream));
-      total += F->last_launches;
-      MMCSF_TRY(download(m));
-    }
+      if (p != m) MMCSF_CUDA(cudaStreamWaitEvent(s, F->ev_in[p], 0));
+    MMCSF_TRY(mmcsf_mttkrp(F, m, R, MMCSF_DTYPE_F32, din, F->stage_out[m].as<float>(), cfg, stream));
+    total += F->last_launches;
+    MMCSF_TRY(download(m));
   }
   MMCSF_CUDA(cudaStreamSynchronize(F->copy_out));
   MMCSF_CUDA(cudaStreamSynchronize(s));

@@ -709,6 +709,15 @@ def main():
             "what": f"{nnz} rows of the {dims[leafm]} x {R} FP32 mode-{leafm} factor gathered by the workload's "
                     f"mode-{leafm} indices and summed (mmcsf_probe_gather), nothing else",
             "dominant_kernel_vs_ceiling": pms.value / unit_ms[di]}
+        # the dominant launch against that rate: factor rows it gathers per
+        # launch (per-nonzero walks and the two-output walks gather every
+        # other level's row at every nonzero) / its time
+        if dker in ("k_mttkrp_pair", "k_mttkrp_pair4", "k_mttkrp_rows"):
+            rows_launch = nnz * (nd - 1)
+            rps = rows_launch / (unit_ms[di] / 1e3)
+            roofline["gather_ceiling"].update({
+                "dominant_rows_per_launch": rows_launch, "dominant_rows_per_s": rps,
+                "dominant_frac_of_gather_rate": rps / (nnz / (pms.value / 1e3))})
     cpu = None
     if not a.no_cpu and world == 1:
         inds_h, vals_h = X.host_arrays()

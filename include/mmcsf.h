@@ -50,7 +50,7 @@ const char* mmcsf_last_error(void);
 int mmcsf_version(void);
 
 /* ---- implementation types: the reference's -t values (src/mttkrp.cu) --- */
-#define MMCSF_IMPL_COO_CPU 1 /* -t 1: reference CPU path (not provided here; see the oracle) */
+#define MMCSF_IMPL_COO_CPU 1 /* -t 1: COO MTTKRP on the host (mmcsf_mttkrp_coo_host) */
 #define MMCSF_IMPL_BCSF 8    /* -t 8: B-CSF, single mode */
 #define MMCSF_IMPL_HBCSF 10  /* -t 10: HB-CSF, single mode */
 #define MMCSF_IMPL_MMCSF 12  /* -t 12: MM-CSF, all modes from one partitioned format */
@@ -201,6 +201,17 @@ typedef struct {
  * B-CSF/HB-CSF formats only the built mode is available. */
 int mmcsf_mttkrp(const mmcsf_format* F, int mode, int R, int factor_dtype, const void* const* d_factors,
                  float* d_out, const mmcsf_kernel_cfg* cfg, void* stream);
+/* -t 1: COO MTTKRP on the HOST, on the tensor's host copy. Replaces
+ * MTTKRP_COO_CPU / MTTKRP_COO_CPU_4D (src/mttkrp_cpu.cpp:60-113): with the
+ * cyclic mode order (mode, mode+1, ...) mod nd, h_out[i0, r] +=
+ * ((v * U1[i1, r]) * U2[i2, r]) [* U3[i3, r]] in FP32. Like the reference it
+ * ADDS to h_out (dims[mode] x R, row-major) without zeroing it. h_factors[m]
+ * (m != mode) are host dims[m] x R float32. threads: 1 runs the reference's
+ * loop in nonzero order (bit-exact to it); T > 1 splits the nonzeros into T
+ * contiguous ranges with private outputs added in range order; 0 = every
+ * hardware thread. Synchronous; touches no device. */
+int mmcsf_mttkrp_coo_host(const mmcsf_coo* X, int mode, int R, const float* const* h_factors, float* h_out,
+                          int threads);
 /* Two modes in one walk (no counterpart in the reference; MM-CSF's reuse of a
  * partition across modes): on a 3-D or 4-D MM-CSF format, the MTTKRP of the
  * partition's slice mode (modes[0], into d_out_slice) and of its middle mode

@@ -7,15 +7,23 @@
 // Differences from the reference, by design:
 //   * errors print a message and return a nonzero exit status (the reference
 //     exit(0)s);
-//   * -t 1 (the serial COO CPU path) is not part of this library;
-//   * -w sets the nonzeros each worker team owns (w * 128) instead of warps
-//     per fiber; without -w the per-mode autotuner chooses;
+//   * -t 1 runs the library's host COO MTTKRP (mmcsf_mttkrp_coo_host) on one
+//     thread, the reference's loop in its order; like the reference it adds
+//     to U[mode] = mode + 0.5 without zeroing it (src/mttkrp.cu:89-92, 105-109);
+//   * -w keeps its meaning, w warps per fiber (src/util.h:194,
+//     src/mttkrp_gpu.cu:3616-3630): the reference launches w warps for each
+//     of the F fibers and every warp takes a share of one fiber's nonzeros.
+//     The kernels here walk nonzero-balanced chunks instead of fibers, so -w
+//     sets the chunk that gives the same number of workers: with G lanes per
+//     factor row (32/G teams per warp), chunk = max(1, N*G / (32*w*F))
+//     nonzeros per team. Without -w the per-mode autotuner chooses;
 //   * -o writes the output of mode -m (every mode is computed for -t 12);
 //   * -i accepts a binary COO file (name ending in .bin, mmcsf_coo_write_bin).
 // Factors are the reference's non-CPD constants U[m] = m + 0.5
 // (src/util.h:3209-3227), so printed values are directly comparable.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -40,12 +48,12 @@ void usage() {
       "options:\n"
       "        -R rank/feature : set the rank (default 32)\n"
       "        -m mode : set the mode of MTTKRP (default 0, MM-CSF evaluates all modes)\n"
-      "        -t implementation type: 8: B-CSF 10: HB-CSF 12: MM-CSF on GPU\n"
+      "        -t implementation type: 1: COO on CPU 8: B-CSF 10: HB-CSF 12: MM-CSF on GPU\n"
       "        -f fiber-splitting threshold: maximum nonzeros per fiber (default none)\n"
       "        -h MM-CSF partition ratio: a mode takes a nonzero when its fiber is h times the others' (default 1)\n"
       "        -P MM-CSF partition rule: 0 all nonzeros to partition 2 as the reference ships (default),\n"
       "           1 the reference's partition heuristic decides\n"
-      "        -w work per team: w*128 nonzeros per worker team (default: autotuned)\n"
+      "        -w warps per fiber: as many workers as w warps for every fiber (default: autotuned)\n"
       "        -b threads per CTA (default 256)\n"
       "        -v verbose: 1 to enable\n"
       "        -c correctness: 1 to check the last mode against a host COO MTTKRP\n"
@@ -83,6 +91,37 @@ int fail(const char* what, int st) {
   return 1;
 }
 
+// -t 1: the COO CPU path (src/mttkrp.cu:105-109) on the reference's
+// constant factors; U[mode] keeps its initial mode + 0.5 (never zeroed).
+int coo_cpu(const Options& o, mmcsf_coo* X, int nd, const uint64_t* dims) {
+  const int R = o.R;
+  std::vector<std::vector<float>> U(nd);
+  std::vector<const float*> fac(nd);
+  for (int m = 0; m < nd; ++m) {
+    U[m].assign(dims[m] * (uint64_t)R, (float)m + 0.5f);
+    fac[m] = U[m].data();
+  }
+  int st = mmcsf_coo_to_host(X);
+  if (st) return fail("host copy", st);
+  auto t0 = std::chrono::steady_clock::now();
+  st = mmcsf_mttkrp_coo_host(X, o.mode, R, fac.data(), U[o.mode].data(), 1);
+  const double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  if (st) return fail("COO CPU MTTKRP", st);
+  std::printf("COO CPU - time: %.3f sec \n", sec);
+  if (!o.outFileName.empty()) {
+    FILE* fo = std::fopen(o.outFileName.c_str(), "w");
+    if (!fo) { std::fprintf(stderr, "cannot write %s\n", o.outFileName.c_str()); return 1; }
+    std::fprintf(fo, "%llu x %d matrix\n", (unsigned long long)dims[o.mode], R);
+    for (uint64_t i = 0; i < dims[o.mode]; ++i) {
+      for (int j = 0; j < R; ++j) std::fprintf(fo, "%.2f\t", U[o.mode][i * R + j]);
+      std::fprintf(fo, "\n");
+    }
+    std::fclose(fo);
+  }
+  mmcsf_coo_destroy(X);
+  return 0;
+}
+
 }  // namespace
 
 int main(int argc, char** argv) {
@@ -91,8 +130,10 @@ int main(int argc, char** argv) {
     usage();
     return 1;
   }
-  if (o.impType != MMCSF_IMPL_MMCSF && o.impType != MMCSF_IMPL_BCSF && o.impType != MMCSF_IMPL_HBCSF) {
-    std::fprintf(stderr, "-t %d is not provided by this library (GPU formats: 8, 10, 12)\n", o.impType);
+  if (o.impType != MMCSF_IMPL_COO_CPU && o.impType != MMCSF_IMPL_MMCSF && o.impType != MMCSF_IMPL_BCSF &&
+      o.impType != MMCSF_IMPL_HBCSF) {
+    std::fprintf(stderr, "-t %d is not provided by this library (1: COO CPU; GPU formats: 8, 10, 12)\n",
+                 o.impType);
     return 1;
   }
   mmcsf_coo* X = nullptr;
@@ -107,6 +148,7 @@ int main(int argc, char** argv) {
     std::fprintf(stderr, "Mode cannot be larger than tensor dimension.\n");
     return 1;
   }
+  if (o.impType == MMCSF_IMPL_COO_CPU) return coo_cpu(o, X, nd, dims);
   mmcsf_build_opts bo{};
   bo.impl = o.impType;
   bo.mode = o.impType == MMCSF_IMPL_MMCSF ? 0 : o.mode;  // check_opt forces mode 0 for -t 12
@@ -132,7 +174,19 @@ int main(int argc, char** argv) {
   }
   const void* fac[4] = {dU[0], dU[1], dU[2], nd == 4 ? dU[3] : nullptr};
   mmcsf_kernel_cfg cfg{};
-  if (o.warpPerSlice > 0) cfg.chunk = o.warpPerSlice * 128;
+  if (o.warpPerSlice > 0) {
+    // workers of the reference's launch: w warps per fiber, summed over the partitions
+    uint64_t fibers = 0;
+    for (int p = 0; p < (o.impType == MMCSF_IMPL_MMCSF ? nd : 1); ++p) {
+      mmcsf_part_info pi{};
+      if (mmcsf_format_info(F, p, &pi) == MMCSF_OK && pi.present) fibers += pi.n_fibers;
+    }
+    const int R4 = (R + 3) / 4;
+    const uint64_t G = R4 >= 32 ? 32 : (R4 >= 16 ? 16 : (R4 >= 8 ? 8 : (R4 >= 4 ? 4 : (R4 >= 2 ? 2 : 1))));
+    const uint64_t workers = 32ull * (uint64_t)o.warpPerSlice * (fibers ? fibers : 1);
+    cfg.chunk = (int)std::max<uint64_t>(1, std::min<uint64_t>(1u << 20, nnz * G / workers));
+    if (o.verbose) std::printf("-w %d: %llu nonzeros per worker team\n", o.warpPerSlice, (unsigned long long)cfg.chunk);
+  }
   if (o.TBsize > 0) cfg.block_threads = o.TBsize;
   const int nmodes = o.impType == MMCSF_IMPL_MMCSF ? nd : 1;
   if (o.warpPerSlice <= 0 && (st = mmcsf_tune(F, R, MMCSF_DTYPE_F32, fac, dOut.data(), s, nullptr)))

@@ -279,7 +279,39 @@ constexpr uint64_t NOALLOC_BYTES = NA_PART_OFF + ((NA_PART * 4 + 255) / 256) * 2
 static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_BYTES];
 
 constexpr int NA_MAX_DEVICES = 64;
+// Per device: the scratch's device address and the id of the context it was
+// taken in. A caller that resets the device (cudaDeviceReset) gets a new
+// primary context whose module, and so whose array, may sit elsewhere; the
+// address is looked up again whenever the current context's id differs.
 unsigned char* g_noalloc_ptr[NA_MAX_DEVICES] = {};
+unsigned long long g_noalloc_ctx[NA_MAX_DEVICES] = {};
+
+// Id of the current context (cuCtxGetCurrent + cuCtxGetId, reached through
+// the runtime's driver entry points so that the library needs no link to the
+// driver library). 0 when the driver does not provide them.
+unsigned long long current_ctx_id() {
+  typedef int (*get_current_t)(void**);
+  typedef int (*get_id_t)(void*, unsigned long long*);
+  static get_current_t get_current = nullptr;
+  static get_id_t get_id = nullptr;
+  static bool looked_up = false;
+  if (!looked_up) {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = reinterpret_cast<get_current_t>(f);
+    f = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<get_id_t>(f);
+    looked_up = true;
+  }
+  void* ctx = nullptr;
+  unsigned long long id = 0;
+  if (!get_current || !get_id || get_current(&ctx) != 0 || !ctx || get_id(ctx, &id) != 0) return 0;
+  return id;
+}
 
 __global__ void k_na_pack(const uint32_t* __restrict__ i0, const uint32_t* __restrict__ i1,
                           const uint32_t* __restrict__ i2, const uint32_t* __restrict__ i3,
@@ -346,17 +378,20 @@ extern "C" int mmcsf_sort_coo_noalloc(int impl, int mode, int nd, const uint64_t
   if (nnz == 0) return MMCSF_OK;
   cudaStream_t s = S(stream);
 
-  // Set-up, once per device, with that device current: the device address
-  // of the scratch array. The first call on a device does this.
+  // Set-up, once per device (and again after the device's context was
+  // replaced), with that device current: the device address of the scratch
+  // array. The first call on a device does this.
   int dev = 0;
   MMCSF_CUDA(cudaGetDevice(&dev));
   if (dev < 0 || dev >= NA_MAX_DEVICES) return set_error(MMCSF_ERR_UNSUPPORTED, "device ordinal %d", dev);
-  if (!g_noalloc_ptr[dev]) {
+  const unsigned long long ctx = current_ctx_id();  // 0: no context current yet, or no driver entry points
+  if (!g_noalloc_ptr[dev] || ctx == 0 || ctx != g_noalloc_ctx[dev]) {
     void* p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);  // makes the primary context current
     if (e != cudaSuccess || !p)
       return set_error(MMCSF_ERR_CUDA, "cudaGetSymbolAddress(scratch) failed: %s", cudaGetErrorString(e));
     g_noalloc_ptr[dev] = static_cast<unsigned char*>(p);
+    g_noalloc_ctx[dev] = current_ctx_id();
   }
   unsigned char* base = g_noalloc_ptr[dev];
   uint64_t* keysA = reinterpret_cast<uint64_t*>(base + NA_KEYS_OFF);

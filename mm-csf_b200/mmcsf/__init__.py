@@ -147,6 +147,23 @@ class CooTensor:
         vals = torch.as_tensor(_CudaArray(vp.value, nnz, "<f4"), device="cuda")
         return inds, vals
 
+    def mttkrp_host(self, mode, factors, out, threads=0):
+        """-t 1: COO MTTKRP on the host (mmcsf_mttkrp_coo_host; replaces
+        MTTKRP_COO_CPU, src/mttkrp_cpu.cpp:60-113). ADDS X_(mode) to `out`
+        (numpy float32 dims[mode] x R, C-contiguous) like the reference;
+        factors: numpy float32 arrays (the mode's own entry is ignored)."""
+        nd, dims, _ = self.info()
+        if not 0 <= mode < nd:
+            raise MmcsfError(1, "Mode cannot be larger than tensor dimension.")
+        check(lib().mmcsf_coo_to_host(self._h))
+        if out.dtype != np.float32 or not out.flags.c_contiguous or out.shape[0] != dims[mode]:
+            raise MmcsfError(1, "out must be a C-contiguous float32 dims[mode] x R array")
+        R = out.shape[1]
+        fs = [np.ascontiguousarray(f, dtype=np.float32) for f in factors]
+        ptrs = (c_voidp * nd)(*[f.ctypes.data if m != mode else None for m, f in enumerate(fs)])
+        check(lib().mmcsf_mttkrp_coo_host(self._h, int(mode), int(R), ptrs, out.ctypes.data, int(threads)))
+        return out
+
     def write_tns(self, path):
         check(lib().mmcsf_coo_write_tns(self._h, path.encode()))
 

@@ -115,6 +115,7 @@ SIGNATURES = {
     "mmcsf_ttm": ([c_voidp, c_int, c_int, c_voidp, c_voidp, c_u64p, c_voidp], c_int),
     "mmcsf_mttkrp_pair": ([c_voidp, c_int, c_int, ctypes.POINTER(c_voidp), c_voidp, c_voidp, ctypes.POINTER(c_int),
                            ctypes.POINTER(KernelCfg), c_voidp], c_int),
+    "mmcsf_mttkrp_coo_host": ([c_voidp, c_int, c_int, ctypes.POINTER(c_voidp), c_voidp, c_int], c_int),
     "mmcsf_sort_coo_noalloc": ([c_int, c_int, c_int, c_u64p, c_u64, ctypes.POINTER(c_voidp), c_voidp,
                                 ctypes.POINTER(c_voidp), c_voidp, c_voidp], c_int),
 }

@@ -39,7 +39,10 @@ OUT_DIR = os.path.join(HERE, "_ref")
 OUT_LIB = os.path.join(OUT_DIR, "libmmcsf_ref.so")
 OUT_LIB_HEUR = os.path.join(OUT_DIR, "libmmcsf_ref_heur.so")
 OVERRIDE_RE = re.compile(r"^(\s*)mode = 2;\s*$")
-DEFAULT_SRC = "/root/reference/src"
+# The reference checkout: $MMCSF_REFERENCE (its root) when set, else a
+# directory named `reference` beside this repository.
+REFERENCE_ROOT = os.environ.get("MMCSF_REFERENCE") or os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference")
+DEFAULT_SRC = os.path.join(REFERENCE_ROOT, "src")
 FILES = ["util.h", "mttkrp_cpu.h", "mttkrp_cpu.cpp", "ttm_cpu.h", "ttm_cpu.cpp"]
 CXXFLAGS = ["-std=c++14", "-fopenmp", "-fPIC", "-Wreturn-type"]
 WARN_RE = re.compile(r"^(?P<file>[^:\s]+):(?P<line>\d+):(?P<col>\d+): warning: "

@@ -8,7 +8,8 @@ the partition override) on the reference's toy.tns and on seeded synthetic
 tensors, and writes inputs and outputs as JSON. The tests compare both the C oracle and
 the CUDA library against these files, so they run without the reference.
 
-Usage: python tests/golden/make_golden.py [--reference /root/reference]
+Usage: python tests/golden/make_golden.py [--reference <reference checkout>]
+(default: $MMCSF_REFERENCE, else a `reference` directory beside this repository)
 """
 import argparse
 import json
@@ -137,7 +138,7 @@ def make_heuristic(tmp, names):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=build_ref.REFERENCE_ROOT)
     ap.add_argument("--ttm-only", action="store_true", help="write ttm.json from the existing cases only")
     ap.add_argument("--heuristic-only", action="store_true",
                     help="write heuristic.json from the existing cases only")

@@ -27,12 +27,39 @@ def test_cli_argument_errors(tmp_path):
     assert os.path.exists(BIN), "build mm-csf_b200 first"
     p = _run([])
     assert p.returncode != 0 and "-t implementation type" in p.stdout
-    p = _run(["-i", "x.tns", "-t", "1"])
-    assert p.returncode != 0 and "-t 1 is not provided" in p.stderr
+    p = _run(["-i", "x.tns", "-t", "7"])
+    assert p.returncode != 0 and "-t 7 is not provided" in p.stderr
     p = _run(["-i", "x.tns", "-z", "3"])
     assert p.returncode != 0 and "unknown option" in p.stderr
     p = _run(["-i", str(tmp_path / "missing.tns"), "-t", "12"])
     assert p.returncode != 0 and "load_tensor failed" in p.stderr
+
+
+@pytest.mark.parametrize("nd", [3, 4])
+def test_cli_coo_cpu(nd, tmp_path):
+    """-t 1 (the reference's COO CPU path, src/mttkrp.cu:105-109) served by the
+    library's host COO MTTKRP: its timing line, and -o equal to the oracle's
+    MTTKRP_COO_CPU on the reference's constant factors, which (as in the
+    reference) adds to U[mode] = mode + 0.5 without zeroing it."""
+    rng = np.random.default_rng(20 + nd)
+    dims = [30, 40, 20] if nd == 3 else [12, 10, 9, 8]
+    n = 2000
+    lin = rng.choice(int(np.prod(dims)), size=n, replace=False)
+    inds = [np.asarray(i, np.uint64) for i in np.unravel_index(lin, dims)]
+    vals = np.round(rng.random(n) + 0.1, 3).astype(np.float32)
+    tns = tmp_path / "x.tns"
+    O.write_tns(str(tns), dims, inds, vals)
+    R = 8
+    U = [np.full((d, R), m + 0.5, np.float32) for m, d in enumerate(dims)]
+    for m in range(nd):
+        out = tmp_path / f"c_{m}.txt"
+        p = _run(["-i", str(tns), "-m", str(m), "-R", str(R), "-t", "1", "-o", str(out)])
+        assert p.returncode == 0, p.stderr
+        assert "COO CPU - time:" in p.stdout
+        head, got = _read_out(out)
+        assert head[0] == str(dims[m]) and got.shape == (dims[m], R)
+        want = O.mttkrp_coo_f32(inds, vals, m, U) + np.float32(m + 0.5)
+        assert np.all(np.abs(got - want) <= 0.006), m  # -o prints %.2f
 
 
 def _read_out(path):
@@ -60,7 +87,7 @@ def test_cli_formats_and_modes(nd, tmp_path):
     U = [np.full((d, R), m + 0.5, np.float32) for m, d in enumerate(dims)]
     for t, modes in ((12, [0]), (8, range(nd)), (10, range(nd))):
         for m in modes:
-            extras = [[], ["-w", "2", "-f", "3"]]
+            extras = [[], ["-w", "2", "-f", "3"], ["-w", "4"]]
             if t == 12:  # the partition heuristic deciding (-P 1), with -h
                 extras += [["-P", "1"], ["-P", "1", "-h", "2", "-f", "3"]]
             for extra in extras:

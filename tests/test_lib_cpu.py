@@ -120,3 +120,41 @@ def test_tns_parallel_parse_and_binary_roundtrip(tmp_path):
         fh.write(b"NOTMAGIC")
     with pytest.raises(mmcsf.MmcsfError):
         mmcsf.CooTensor.load_bin(bpath)
+
+
+@pytest.mark.parametrize("nd", [3, 4])
+def test_host_coo_mttkrp_matches_oracle(nd):
+    """-t 1 served by the library (mmcsf_mttkrp_coo_host): one thread is the
+    reference's loop bit for bit (through the oracle, itself bit-exact to the
+    reference's MTTKRP_COO_CPU); several threads agree within FP32 rounding;
+    like the reference it adds to the output it is given."""
+    import mmcsf
+    rng = np.random.default_rng(7 + nd)
+    dims = [40, 33, 27, 5][:nd]
+    n = 3000
+    inds = [rng.integers(0, d, n).astype(np.uint32) for d in dims]
+    vals = rng.random(n).astype(np.float32)
+    X = mmcsf.CooTensor.from_arrays(dims, inds, vals)
+    R = 12
+    U = [rng.random((d, R)).astype(np.float32) for d in dims]
+    for mode in range(nd):
+        ref = O.mttkrp_coo_f32(inds, vals, mode, U)
+        out = np.zeros((dims[mode], R), np.float32)
+        X.mttkrp_host(mode, U, out, threads=1)
+        assert np.array_equal(out, ref)
+        out4 = np.zeros((dims[mode], R), np.float32)
+        X.mttkrp_host(mode, U, out4, threads=4)
+        assert np.allclose(out4, ref, rtol=1e-5, atol=1e-6)
+        base = np.full((dims[mode], R), mode + 0.5, np.float32)
+        X.mttkrp_host(mode, U, base, threads=1)
+        assert np.allclose(base, ref + (mode + 0.5), rtol=1e-5, atol=1e-5)
+
+
+def test_host_coo_mttkrp_argument_errors():
+    import mmcsf
+    X = mmcsf.CooTensor.from_arrays([4, 4, 4], [np.zeros(2, np.uint32)] * 3, np.ones(2, np.float32))
+    U = [np.ones((4, 4), np.float32)] * 3
+    with pytest.raises(mmcsf.MmcsfError):
+        X.mttkrp_host(3, U, np.zeros((4, 4), np.float32))
+    with pytest.raises(mmcsf.MmcsfError):
+        X.mttkrp_host(0, U, np.zeros((4, 4), np.float64))

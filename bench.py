@@ -22,15 +22,24 @@ roofline   = the dominant launch's kernel: its algorithmic bytes / its average
              its DRAM traffic from the committed ncu summary; the row-gather
              ceiling measured on the same GPU (mmcsf_probe_gather).
 cpu_baseline / --impl reference = the reference's own MTTKRP_COO_CPU
-             (oracle/_ref) on all host threads (nonzero ranges, private
-             outputs summed) on a bounded sample of the same nonzeros,
-             extrapolated to the full workload.
+             (oracle/_ref) over every nonzero on all host threads (contiguous
+             nonzero ranges, private outputs added in the step), each step
+             timed whole, no sample; the reference arm builds its tensor with
+             the host restatement of the generator (oracle/generate.c) and
+             loads nothing of the CUDA library.
+error_vs_fp64 = every output of the timed step against an FP64 MTTKRP of
+             the same factors (largest |d| / (|ref| + 1e-6 max|ref|), and the
+             relative Frobenius norm).
 also       = format_build_ms (device construction), bf16_factors (the step
-             with BF16 factors and its error), ttm (the reference's ttm on
-             the same tensor), cp (CP-ALS and Poisson gradient CP: BF16 vs
-             FP32 seconds per iteration and fits), formats (4-D: B-CSF and
-             HB-CSF beside MM-CSF), partition_heuristic (the same step on the
-             partitions the reference's heuristic picks, partition_rule 1).
+             with BF16 factors, tuned, and its errors), r64 (the same
+             workload at R = 64, FP32 and BF16), config1 (1000^3 uniform,
+             -f 128 -w 1: device, the library's host -t 1 path and the
+             reference's CPU path), skewed4d (the 4-D workload: MM-CSF all
+             modes against B-CSF and HB-CSF per mode), ttm (the reference's
+             ttm on the same tensor), cp (CP-ALS and Poisson gradient CP:
+             BF16 vs FP32 seconds per iteration and fits),
+             partition_heuristic (the same step on the partitions the
+             reference's heuristic picks, partition_rule 1).
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 """
@@ -88,6 +97,9 @@ def parse():
     ap.add_argument("--no-heuristic", action="store_true",
                     help="skip the section on the partition heuristic's MM-CSF (partition_rule 1)")
     ap.add_argument("--cp-scale", type=float, default=1.0, help="scale the CP workloads' nonzero counts")
+    ap.add_argument("--no-r64", action="store_true", help="skip the R=64 section of the skewed 3-D workload")
+    ap.add_argument("--no-config1", action="store_true", help="skip the 1000^3 uniform (config 1) section")
+    ap.add_argument("--no-4d", action="store_true", help="skip the 4-D (B-CSF / HB-CSF / MM-CSF) section")
     return ap.parse_args()
 
 
@@ -191,35 +203,49 @@ def device_coo(X):
     return [i.clone() for i in inds], vals.clone()
 
 
+def host_threads():
+    """Host threads this process may run on."""
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
 class RefCpuMttkrp:
     """All-mode MTTKRP with the reference's own MTTKRP_COO_CPU
     (src/mttkrp_cpu.cpp:60-113, built as oracle/_ref; the C restatement of the
-    oracle when the reference was not built here) on `threads` host threads:
-    thread t runs it on a contiguous range of the first S nonzeros into a
-    private output, and one step also sums the private outputs. The function
-    is serial as shipped (its OpenMP pragma is commented out,
-    src/mttkrp_cpu.cpp:79), so the threads split the nonzeros among calls."""
+    oracle when the reference was not built here) over ALL nonzeros on
+    `threads` host threads: thread t runs it on the t-th contiguous range of
+    the nonzeros into a private zeroed output, and the step also adds the
+    private outputs (rows split across the threads). The function is serial
+    as shipped (its OpenMP pragma is commented out, src/mttkrp_cpu.cpp:79), so
+    the threads split the nonzeros among calls."""
 
-    def __init__(self, inds_host, vals_host, dims, R, S, threads):
+    def __init__(self, inds_host, vals_host, dims, R, threads):
         import ctypes
         import numpy as np
 
         from oracle import oracle as O
         self.kind = "reference" if O.ref_available() else "port"
         self.lib = O.ref_lib() if self.kind == "reference" else O.lib()
-        self.dims, self.R, self.nd, self.S = list(dims), R, len(dims), S
-        self.T = max(1, min(threads, S))
+        self.dims, self.R, self.nd = list(dims), R, len(dims)
+        n = len(vals_host)
+        self.n = n
+        # bound the private outputs at about 24 GB
+        per = max(dims) * R * 4
+        self.T = max(1, min(threads, n, (24 << 30) // max(1, per)))
         rng = np.random.default_rng(0)
         self.U = [rng.random((d, R)).astype(np.float32) for d in dims]
-        cuts = [S * t // self.T for t in range(self.T + 1)]
+        cuts = [n * t // self.T for t in range(self.T + 1)]
         self.parts = []
         fp = ctypes.POINTER(ctypes.c_float)
         for t in range(self.T):
             a, b = cuts[t], cuts[t + 1]
-            ind = [np.ascontiguousarray(i[a:b].astype(np.uint64)) for i in inds_host]
+            ind = [np.ascontiguousarray(i[a:b], dtype=np.uint64) for i in inds_host]
             v = np.ascontiguousarray(vals_host[a:b])
             outs = [np.zeros((d, R), np.float32) for d in dims]
             self.parts.append((ind, v, outs, O._ptr_array(ind), v.ctypes.data_as(fp)))
+        self.out = [np.zeros((d, R), np.float32) for d in dims]
         self.dptr = (ctypes.c_uint64 * self.nd)(*[int(d) for d in dims])
         self.fp = fp
 
@@ -235,34 +261,26 @@ class RefCpuMttkrp:
         else:
             self.lib.orc_mttkrp_coo_f32(self.nd, ctypes.c_uint64(len(v)), ip, vp, m, self.R, fac)
 
+    def _sum(self, t, m):
+        rows = self.dims[m]
+        a, b = rows * t // self.T, rows * (t + 1) // self.T
+        acc = self.out[m][a:b]
+        acc[:] = self.parts[0][2][m][a:b]
+        for u in range(1, self.T):
+            acc += self.parts[u][2][m][a:b]
+
     def step(self):
-        """One all-mode MTTKRP over the sample (threads, then the sums)."""
+        """One all-mode MTTKRP over every nonzero (threads, then the sums)."""
         from concurrent.futures import ThreadPoolExecutor
         with ThreadPoolExecutor(self.T) as ex:
             for m in range(self.nd):
                 list(ex.map(lambda t: self._run(t, m), range(self.T)))
-                acc = self.parts[0][2][m].copy()
-                for t in range(1, self.T):
-                    acc += self.parts[t][2][m]
+                list(ex.map(lambda t: self._sum(t, m), range(self.T)))
 
     def seconds(self):
         t = time.perf_counter()
         self.step()
         return time.perf_counter() - t
-
-
-def reference_cpu(inds_host, vals_host, dims, R, target_s=12.0):
-    """A RefCpuMttkrp on all host threads (at most 16, to bound the private
-    outputs), with S sized so one step takes about target_s seconds."""
-    n_all = len(vals_host)
-    threads = max(1, min(16, os.cpu_count() or 1))
-    S = min(2_000_000, n_all)
-    r = RefCpuMttkrp(inds_host, vals_host, dims, R, S, threads)
-    t = r.seconds()
-    S2 = int(min(n_all, max(S, S * target_s / max(t, 1e-3))))
-    if S2 > S * 1.5:
-        r = RefCpuMttkrp(inds_host, vals_host, dims, R, S2, threads)
-    return r
 
 
 CPALS = dict(dims=[200000, 200000, 200000], nnz=50_000_000, planted=16, noise=0.01, R=16, max_iters=50, tol=1e-5,
@@ -274,21 +292,25 @@ GCP = dict(dims=[100000, 50000, 10000], nnz=20_000_000, zipf=1.05, planted=32, R
                 "loss over every entry")
 
 
-def format_section(X, dims, R, tdt):
+def format_section(X, dims, R, U, rows, hbm_peak, refs=None):
     """Single-mode B-CSF (-t 8) and HB-CSF (-t 10) MTTKRP for every mode, each
-    format built for that mode and tuned, timed like the MM-CSF steps."""
+    format built for that mode and tuned, timed like the MM-CSF steps: per
+    mode its time, algorithmic bytes (the traversal's structure, the touched
+    rows of the other factors, the output once), the fraction of the HBM
+    roofline, and (with `refs`, FP64 outputs per mode) the error against the
+    FP64 oracle."""
     import torch
     import mmcsf
     out = {}
-    g = torch.Generator(device="cuda").manual_seed(99)
-    U = [torch.rand(d, R, device="cuda", generator=g).to(tdt) for d in dims]
+    nd = len(dims)
+    esz = U[0].element_size()
     for name, impl in (("bcsf", mmcsf.IMPL_BCSF), ("hbcsf", mmcsf.IMPL_HBCSF)):
-        ms = []
-        for m in range(len(dims)):
+        ms, gbs, errs = [], [], []
+        for m in range(nd):
             F = mmcsf.Format(X, impl=impl, mode=m)
             o = torch.empty(dims[m], R, device="cuda")
-            outs = [o if q == m else torch.empty(1, R, device="cuda") for q in range(len(dims))]
-            F.tune(U, outs)
+            outs = [o if q == m else torch.empty(1, R, device="cuda") for q in range(nd)]
+            plan = F.tune(U, outs)
             for _ in range(3):
                 F.mttkrp(m, U, o)
             e0 = torch.cuda.Event(enable_timing=True)
@@ -298,10 +320,22 @@ def format_section(X, dims, R, tdt):
                 F.mttkrp(m, U, o)
             e1.record()
             torch.cuda.synchronize()
-            ms.append(e0.elapsed_time(e1) / 10)
+            t = e0.elapsed_time(e1) / 10
+            ms.append(t)
+            pi = F.info(0)
+            kern = plan[m].get("kernel") if plan else None
+            if kern == 3 and pi["mode_order"].index(m) in (0, nd - 1):
+                sb = X.nnz * (12 if nd == 3 else 16) + pi["n_slices"] * 8
+            else:
+                sb = struct_bytes(nd, X.nnz, pi["n_fibers"], pi["n_fbrs"])
+            b = mode_bytes(nd, dims, m, R, esz, sb, rows)
+            gbs.append(b / (t / 1e3) / 1e9)
+            if refs:
+                errs.append(err_vs(o, refs[m]))
             del F
             torch.cuda.empty_cache()
-        out[name] = {"mode_ms": ms, "all_mode_ms": sum(ms)}
+        out[name] = {"mode_ms": ms, "all_mode_ms": sum(ms), "mode_gbs": gbs,
+                     "mode_roofline_frac": [g / hbm_peak for g in gbs], "error_vs_fp64": errs or None}
     return out
 
 
@@ -380,9 +414,41 @@ def time_units(units, steps, stream=None):
     return unit_ms, t0.elapsed_time(t1)
 
 
-def bf16_section(F, U32, outs32, steps, warmup):
-    """The same step with BF16 factors (FP32 accumulation), tuned for them,
-    and the error this costs against the FP32-factor outputs."""
+def fp64_mttkrp(inds_dev, vals_dev, U, mode, chunk=1 << 23):
+    """FP64 MTTKRP of one mode from the COO nonzeros (torch on the device,
+    outside every timed region): the precision oracle the benchmarked outputs
+    are compared with. U: the factors as the kernels read them (FP32 or BF16)."""
+    import torch
+    nd = len(U)
+    R = U[0].shape[1]
+    out = torch.zeros(U[mode].shape[0], R, dtype=torch.float64, device="cuda")
+    U64 = [u.double() if q != mode else None for q, u in enumerate(U)]
+    n = vals_dev.numel()
+    for a in range(0, n, chunk):
+        b = min(n, a + chunk)
+        p = vals_dev[a:b].double().unsqueeze(1).repeat(1, R)
+        for q in range(nd):
+            if q != mode:
+                p *= U64[q].index_select(0, inds_dev[q][a:b].long())
+        out.index_add_(0, inds_dev[mode][a:b].long(), p)
+    del U64
+    return out
+
+
+def err_vs(out, ref):
+    """Error of an output against its FP64 oracle: the largest elementwise
+    |out - ref| / (|ref| + 1e-6 max|ref|) and the relative Frobenius norm."""
+    d = out.double() - ref
+    scale = float(ref.abs().max())
+    return {"max_rel": float((d.abs() / (ref.abs() + 1e-6 * scale)).max()),
+            "frobenius_rel": float(d.norm() / ref.norm())}
+
+
+def bf16_section(F, U32, outs32, steps, warmup, inds_dev, vals_dev, refs32):
+    """The same step with BF16 factors (FP32 accumulation), tuned for them:
+    its time, its error against the FP64 MTTKRP of the same BF16 factors (the
+    kernels' arithmetic), against the FP64 MTTKRP of the FP32 factors (that
+    plus the factors' rounding), and against the FP32-factor outputs."""
     import torch
     U = [u.to(torch.bfloat16) for u in U32]
     outs = [torch.empty_like(o) for o in outs32]
@@ -391,14 +457,20 @@ def bf16_section(F, U32, outs32, steps, warmup):
         F.mttkrp_all(U, outs)
     units = step_units(F, U, outs, plan)
     unit_ms, span = time_units(units, steps)
-    err = []
-    for o, r in zip(outs, outs32):
-        d = (o.double() - r.double())
-        err.append({"frobenius_rel": float(d.norm() / r.double().norm()),
-                    "max_abs_over_max_ref": float(d.abs().max() / r.double().abs().max())})
+    F.mttkrp_all(U, outs)
+    torch.cuda.synchronize()
+    e_same, e_f32, e_out = [], [], []
+    for m, (o, r) in enumerate(zip(outs, outs32)):
+        ref_b = fp64_mttkrp(inds_dev, vals_dev, U, m)
+        e_same.append(err_vs(o, ref_b))
+        del ref_b
+        e_f32.append(err_vs(o, refs32[m]))
+        e_out.append(err_vs(o, r.double()))
     return {"ms_per_step": span / steps, "units": [{"modes": list(u[0]), "ms": t} for u, t in zip(units, unit_ms)],
-            "plan": plan, "error_vs_fp32_factors": err,
-            "note": "BF16-rounded factor rows, FP32 products and accumulation; the error is the factors' rounding"}
+            "plan": plan, "error_vs_fp64_same_factors": e_same, "error_vs_fp64_fp32_factors": e_f32,
+            "error_vs_fp32_factor_outputs": e_out,
+            "note": "BF16-rounded factor rows, FP32 products and accumulation; against the FP32 factors the "
+                    "error is the factors' rounding"}
 
 
 def ttm_section(X, dims, R, mode, rows_touched):
@@ -496,15 +568,289 @@ def cp_section(seed, scale):
     return out
 
 
-def main():
-    a = parse()
+def host_workload_stats(inds, dims, order):
+    """Rows touched per mode, leaf fibers (distinct prefixes of all levels but
+    the leaf, no split) and, in 4-D, distinct level-0/1 prefixes, from host
+    index arrays (numpy)."""
+    import numpy as np
+    rows = [int(np.count_nonzero(np.bincount(i, minlength=d))) for i, d in zip(inds, dims)]
+    key = inds[order[0]].astype(np.int64)
+    nfbrs = 0
+    for li, q in enumerate(order[1:len(order) - 1]):
+        key = key * dims[q] + inds[q].astype(np.int64)
+        if len(order) == 4 and li == 0:
+            nfbrs = int(np.unique(key).size)
+    return rows, int(np.unique(key).size), nfbrs
+
+
+def reference_arm(a, W, config):
+    """--impl reference: the reference's own MTTKRP_COO_CPU (oracle/_ref) over
+    every nonzero of the workload on all host threads, each step timed whole.
+    The tensor comes from the host restatement of the seeded generator
+    (oracle/generate.c, bit-identical to the library's), so nothing of this
+    repository's CUDA library is loaded."""
+    from oracle import oracle as O
+    dims, nd = W["dims"], len(W["dims"])
+    nnz = a.nnz or W["nnz"]
+    R = a.rank or W["R"]
+    esz = 4
+    T = host_threads()
+    t0 = time.perf_counter()
+    inds, vals = O.generate(dims, nnz, W["dist"], W["zipf"], W["val"], a.seed, threads=T)
+    gen_s = time.perf_counter() - t0
+    order = O.order_modes(dims, 2 if nd == 3 else 0)
+    rows, nfib, nfbrs = host_workload_stats(inds, dims, order)
+    sb = struct_bytes(nd, nnz, nfib, nfbrs)
+    step_bytes = sum(mode_bytes(nd, dims, m, R, esz, sb, rows) for m in range(nd))
+    ref = RefCpuMttkrp(inds, vals, dims, R, T)
+    del inds, vals
+    times = []
+    for i in range(a.warmup + a.steps):
+        t = ref.seconds()
+        if i >= a.warmup:
+            times.append(t)
+    ts = statistics.mean(times)
+    val = step_bytes / ts / 1e9
+    line = {"metric": METRIC, "value": val, "unit": "GB/s", "n_gpus": a.gpus, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": ts * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator, host restatement)",
+            "impl": "reference", "config": config,
+            "cpu_baseline": {"value": val, "unit": "GB/s", "cores": ref.T, "nproc": T, "kind": ref.kind,
+                             "ms_per_step": ts * 1e3,
+                             "sample": f"all {nnz} nonzeros, all {nd} modes, every step: MTTKRP_COO_CPU (serial as "
+                                       f"shipped, src/mttkrp_cpu.cpp:79) on {ref.T} of {T} host threads over "
+                                       f"contiguous nonzero ranges, private outputs added in the step; no "
+                                       f"extrapolation"},
+            "e2e": {"value": val, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "generate_s": gen_s}
+    print(json.dumps(line), flush=True)
+
+
+def unit_bytes_for(F, nd, dims, nnz, R, esz, rows, plan, info, modes, per_mode):
+    """Algorithmic bytes of one launch: a single mode's traversal bytes, or
+    for the two-output walk the vals, leaf and middle indices per nonzero,
+    slice offsets and indices, every touched row of all factors once, and
+    both outputs written once."""
+    if len(modes) == 1:
+        return per_mode[modes[0]]
+    return (nnz * (12 if nd == 3 else 16) + info["n_slices"] * 8 + sum(rows[q] * R * esz for q in range(nd))
+            + sum(dims[q] * R * 4 for q in modes))
+
+
+def per_mode_bytes(F, nd, dims, nnz, R, esz, rows, plan, info):
+    """Algorithmic bytes of each mode's MTTKRP under the traversal and kernel
+    the plan runs for it."""
+    out = []
+    for m in range(nd):
+        trav = plan[m]["traversal"] if plan else (2 if F.info(4 + m)["present"] else 1)
+        pi = F.info(4 + m) if trav == 2 else info
+        lvl = pi["mode_order"].index(m)
+        if plan and plan[m].get("kernel") == 3 and (nd == 3 or lvl in (0, nd - 1)):
+            sb = nnz * (12 if nd == 3 else 16) + pi["n_slices"] * 8  # per-nonzero walk
+        else:
+            sb = struct_bytes(nd, nnz, pi["n_fibers"], pi["n_fbrs"])
+        out.append(mode_bytes(nd, dims, m, R, esz, sb, rows))
+    return out
+
+
+def kernel_label(F, nd, plan, info, modes):
+    """(kernel name, description) of one launch of the step."""
+    if len(modes) == 2:
+        k = "k_mttkrp_pair" if nd == 3 else "k_mttkrp_pair4"
+        return k, (f"{k} modes {modes[0]} and {modes[1]} (levels 0 and 1 of order {info['mode_order']}, "
+                   f"MM-CSF partition, one walk)")
+    dom = modes[0]
+    trav = plan[dom]["traversal"] if plan else 1
+    order = F.info(4 + dom)["mode_order"] if trav == 2 else info["mode_order"]
+    lvl = order.index(dom)
+    k = plan[dom].get("kernel", 0) if plan else 0
+    if k == 3 and nd == 4 and lvl not in (0, 3):
+        k = 1  # the 4-D middle levels run the per-team fiber walk
+    name = {1: "k_mttkrp", 2: "k_mttkrp_flat", 3: "k_mttkrp_rows"}.get(k or (2 if nd == 3 else 1))
+    return name, f"{name} mode {dom} (level {lvl} of order {order}, {'view' if trav == 2 else 'MM-CSF partition'})"
+
+
+def run_step(F, nd, dims, nnz, R, U, outs, plan, steps, warmup, info, rows, hbm_peak, peak_kind, workload, dtype,
+             stream=None):
+    """Time the all-mode step launch by launch; returns the per-launch report
+    and the dominant launch's roofline entry."""
+    import torch
+    esz = U[0].element_size()
+    stream = stream or torch.cuda.current_stream()
+    per_mode = per_mode_bytes(F, nd, dims, nnz, R, esz, rows, plan, info)
+    units = step_units(F, U, outs, plan)
+    for _ in range(warmup):
+        F.mttkrp_all(U, outs)
+    launches = F.last_launches
+    unit_ms, total_ms = time_units(units, steps, stream)
+    ub = [unit_bytes_for(F, nd, dims, nnz, R, esz, rows, plan, info, u[0], per_mode) for u in units]
+    di = max(range(len(units)), key=lambda i: unit_ms[i])
+    dk, dlabel = kernel_label(F, nd, plan, info, units[di][0])
+    achieved = ub[di] / (unit_ms[di] / 1e3) / 1e9
+    traffic = traffic_from_profiles(workload, R, dtype, "".join(str(m) for m in units[di][0]), dk)
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
+                "traffic": traffic, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)", "kernel": dlabel,
+                "algorithmic_bytes": ub[di], "avg_ms": unit_ms[di]}
+    report = [{"modes": list(u[0]), "kernel": kernel_label(F, nd, plan, info, u[0])[0], "ms": t,
+               "algorithmic_bytes": b, "roofline_frac": b / (t / 1e3) / 1e9 / hbm_peak}
+              for u, t, b in zip(units, unit_ms, ub)]
+    return {"total_ms": total_ms, "ms_per_step": total_ms / steps, "units": report, "roofline": roofline,
+            "launches_per_step": launches, "dominant": (di, units[di][0], dk)}
+
+
+def fp64_refs(inds_dev, vals_dev, U):
+    return [fp64_mttkrp(inds_dev, vals_dev, U, m) for m in range(len(U))]
+
+
+def r64_section(F, X, dims, rows, nfib, info, steps, warmup, hbm_peak, peak_kind, workload):
+    """The metric's workload at R = 64 (its second rank): the same format,
+    FP32 and BF16 factors, each tuned; step time, the dominant launch's
+    roofline fraction and the FP64 errors. The reference's kernels are only
+    correct up to R = 32 (src/mttkrp_gpu.cu:746-753), so only the oracle
+    checks this rank."""
+    import torch
+    nd, nnz, R = len(dims), X.nnz, 64
+    g = torch.Generator(device="cuda").manual_seed(4321)
+    U = [torch.rand(d, R, device="cuda", generator=g) for d in dims]
+    outs = [torch.empty(d, R, device="cuda") for d in dims]
+    inds_dev, vals_dev = X.device_tensors()
+    sb = struct_bytes(nd, nnz, nfib, info["n_fbrs"] if nd == 4 else 0)
+    res = {}
+    for name, UU in (("f32", U), ("bf16", [u.to(torch.bfloat16) for u in U])):
+        plan = F.tune(UU, outs)
+        r = run_step(F, nd, dims, nnz, R, UU, outs, plan, steps, warmup, info, rows, hbm_peak, peak_kind,
+                     workload, name)
+        F.mttkrp_all(UU, outs)
+        torch.cuda.synchronize()
+        esz = UU[0].element_size()
+        step_bytes = sum(mode_bytes(nd, dims, m, R, esz, sb, rows) for m in range(nd))
+        errs = []
+        for m in range(nd):
+            ref = fp64_mttkrp(inds_dev, vals_dev, UU, m)
+            errs.append(err_vs(outs[m], ref))
+            del ref
+        res[name] = {"ms_per_step": r["ms_per_step"], "value_gbs": step_bytes / (r["ms_per_step"] / 1e3) / 1e9,
+                     "units": r["units"], "roofline_frac": r["roofline"]["frac"], "dominant": r["roofline"]["kernel"],
+                     "plan": plan, "error_vs_fp64": errs}
+    return res
+
+
+def config1_section(steps, warmup, hbm_peak):
+    """1000 x 1000 x 1000, 100,000 uniform nonzeros, R = 32, -f 128, -w 1:
+    MM-CSF mode 0 and all modes on the device (the reference's -w 1 mapped
+    to the worker chunk, and tuned), the library's host COO MTTKRP (-t 1) on
+    one thread and all threads, the reference's MTTKRP_COO_CPU on one
+    thread, and errors against the FP64 oracle."""
     import numpy as np
     import torch
-    import torch.distributed as dist
+    import mmcsf
+    from oracle import oracle as O
+    W = WORKLOADS["uniform3d"]
+    dims, nnz, R = W["dims"], W["nnz"], 32
+    X = mmcsf.CooTensor.generate(dims, nnz, dist=W["dist"], val_dist=W["val"], seed=0)
+    F = mmcsf.Format(X, impl=mmcsf.IMPL_MMCSF, mode=0, fiber_threshold=128, views=1)
+    g = torch.Generator(device="cuda").manual_seed(77)
+    U = [torch.rand(d, R, device="cuda", generator=g) for d in dims]
+    outs = [torch.empty(d, R, device="cuda") for d in dims]
+    inds_dev, vals_dev = X.device_tensors()
+    refs = fp64_refs(inds_dev, vals_dev, U)
+    chunk = F.chunk_for_warps(1, R)
+    cfg = mmcsf.KernelCfg()
+    cfg.chunk = chunk
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    def timed(fn, n):
+        for _ in range(warmup):
+            fn()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(n):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / n
+
+    out = {"workload": W["desc"] + ", -f 128, -w 1", "chunk_for_w1": chunk}
+    out["mode0_w1_ms"] = timed(lambda: F.mttkrp(0, U, outs[0], cfg=cfg), steps)
+    e_w1 = err_vs(outs[0], refs[0])
+    plan = F.tune(U, outs)
+    out["mode0_tuned_ms"] = timed(lambda: F.mttkrp(0, U, outs[0]), steps)
+    out["all_modes_tuned_ms"] = timed(lambda: F.mttkrp_all(U, outs), steps)
+    F.mttkrp_all(U, outs)
+    torch.cuda.synchronize()
+    out["error_vs_fp64"] = {"mode0_w1": e_w1, "all_modes_tuned": [err_vs(o, r) for o, r in zip(outs, refs)]}
+    out["plan"] = plan
+    # host paths: the library's -t 1 and the reference's MTTKRP_COO_CPU
+    inds_h, vals_h = X.host_arrays()
+    Uh = [u.cpu().numpy() for u in U]
+    for name, th in (("host_coo_1thread_ms", 1), ("host_coo_all_threads_ms", 0)):
+        o = np.zeros((dims[0], R), np.float32)
+        t0 = time.perf_counter()
+        for _ in range(5):
+            o[:] = 0
+            X.mttkrp_host(0, Uh, o, threads=th)
+        out[name] = (time.perf_counter() - t0) / 5 * 1e3
+    out["error_vs_fp64"]["host_coo_mode0"] = err_vs(torch.from_numpy(o).cuda(), refs[0])
+    ref = RefCpuMttkrp(inds_h, vals_h, dims, R, 1)
+    t0 = time.perf_counter()
+    for _ in range(5):
+        ref._run(0, 0)
+    out["reference_coo_cpu_mode0_ms"] = (time.perf_counter() - t0) / 5 * 1e3
+    out["reference_kind"] = ref.kind
+    del F, X
+    torch.cuda.empty_cache()
+    return out
+
+
+def skewed4d_section(steps, warmup, seed, hbm_peak, peak_kind):
+    """The 4-D workload (1,000,000 x 20,000 x 5,000 x 200, 140M nonzeros, R =
+    32): MM-CSF over all modes (views for every mode, tuned, the 4-D
+    two-output walk when it wins) against B-CSF (-t 8) and HB-CSF (-t 10) for
+    every mode, FP32 factors, with roofline fractions and FP64 errors; and
+    the MM-CSF step with BF16 factors."""
+    import torch
+    import mmcsf
+    W = WORKLOADS["skewed4d"]
+    dims, nnz, R, nd = W["dims"], W["nnz"], W["R"], 4
+    X = mmcsf.CooTensor.generate(dims, nnz, dist=W["dist"], zipf_s=W["zipf"], val_dist=W["val"], seed=seed)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    F = mmcsf.Format(X, impl=mmcsf.IMPL_MMCSF, mode=0, views=2)
+    torch.cuda.synchronize()
+    build_ms = (time.perf_counter() - t0) * 1e3
+    info = F.info(2)
+    inds_dev, vals_dev = device_coo(X)
+    rows, nfib = workload_stats(inds_dev, dims, info["mode_order"])
+    g = torch.Generator(device="cuda").manual_seed(99)
+    U = [torch.rand(d, R, device="cuda", generator=g) for d in dims]
+    outs = [torch.empty(d, R, device="cuda") for d in dims]
+    plan = F.tune(U, outs)
+    r = run_step(F, nd, dims, nnz, R, U, outs, plan, steps, warmup, info, rows, hbm_peak, peak_kind, "skewed4d", "f32")
+    F.mttkrp_all(U, outs)
+    torch.cuda.synchronize()
+    refs = fp64_refs(inds_dev, vals_dev, U)
+    sb = struct_bytes(nd, nnz, nfib, info["n_fbrs"])
+    step_bytes = sum(mode_bytes(nd, dims, m, R, 4, sb, rows) for m in range(nd))
+    out = {"workload": W["desc"], "format_build_ms": build_ms,
+           "mmcsf": {"ms_per_step": r["ms_per_step"], "value_gbs": step_bytes / (r["ms_per_step"] / 1e3) / 1e9,
+                     "units": r["units"], "roofline": r["roofline"], "plan": plan,
+                     "error_vs_fp64": [err_vs(o, ref) for o, ref in zip(outs, refs)]}}
+    Ub = [u.to(torch.bfloat16) for u in U]
+    planb = F.tune(Ub, outs)
+    rb = run_step(F, nd, dims, nnz, R, Ub, outs, planb, steps, warmup, info, rows, hbm_peak, peak_kind, "skewed4d",
+                  "bf16")
+    out["mmcsf_bf16"] = {"ms_per_step": rb["ms_per_step"], "units": rb["units"],
+                         "roofline_frac": rb["roofline"]["frac"]}
+    del F
+    torch.cuda.empty_cache()
+    out.update(format_section(X, dims, R, U, rows, hbm_peak, refs))
+    del X, inds_dev, vals_dev, refs
+    torch.cuda.empty_cache()
+    return out
+
+
+def main():
+    a = parse()
     W = WORKLOADS[a.workload]
     if a.views is None:
         a.views = W.get("views", 1)
@@ -512,54 +858,23 @@ def main():
     nd = len(dims)
     nnz = a.nnz or W["nnz"]
     R = a.rank or W["R"]
-    esz = 4 if a.dtype == "f32" else 2
-    hbm_peak, peak_kind = peaks()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
     config = {"workload": a.workload, "desc": W["desc"], "nnz": nnz, "R": R,
               "format": f"MM-CSF (-t 12, -m 0), views={a.views}",
               "fiber_threshold": a.fiber_threshold or "none", "factor_dtype": a.dtype,
               "l2": "inputs larger than L2 (structure > 800 MB per step)", "seed": a.seed,
               "parallelism": f"replicas x{world} (each rank its own tensor)"}
-
     if a.impl == "reference":
-        if rank != 0:
-            return
-        torch.cuda.set_device(local)
-        import mmcsf
-        X = mmcsf.CooTensor.generate(dims, nnz, dist=W["dist"], zipf_s=W["zipf"], val_dist=W["val"],
-                                     seed=a.seed)
-        inds_dev, _ = device_coo(X)
-        from oracle import oracle as O
-        order = O.order_modes(dims, 2)
-        rows, nfib = workload_stats(inds_dev, dims, order)
-        per_mode = [mode_bytes(nd, dims, m, R, esz, struct_bytes(nd, nnz, nfib, 0), rows) for m in range(nd)]
-        step_bytes = sum(per_mode)
-        inds_h, vals_h = X.host_arrays()
-        del inds_dev
-        # one step = the reference's MTTKRP_COO_CPU over all modes on a sample
-        # of the nonzeros, sized so warmup + steps finish in a few minutes
-        budget = 150.0 / max(1, a.steps + a.warmup)
-        ref = reference_cpu(inds_h, vals_h, dims, R, target_s=min(20.0, budget))
-        S, kind = ref.S, ref.kind
-        times = []
-        for i in range(a.warmup + a.steps):
-            t = ref.seconds()
-            if i >= a.warmup:
-                times.append(t)
-        ts = statistics.mean(times) * nnz / S
-        val = step_bytes / ts / 1e9
-        line = {"metric": METRIC, "value": val, "unit": "GB/s", "n_gpus": a.gpus, "steps": a.steps,
-                "warmup": a.warmup, "ms_per_step": ts * 1e3, "higher_is_better": True, "scaling": "weak",
-                "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator)", "impl": "reference",
-                "config": config,
-                "cpu_baseline": {"value": val, "unit": "GB/s", "cores": ref.T, "kind": kind,
-                                 "sample": f"first {S} of {nnz} nonzeros, all {nd} modes, MTTKRP_COO_CPU (serial as "
-                                           f"shipped, src/mttkrp_cpu.cpp:79) on {ref.T} threads over nonzero ranges "
-                                           f"with private outputs summed, extrapolated x{nnz / S:.1f}"},
-                "e2e": {"value": val, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-        print(json.dumps(line), flush=True)
+        if rank == 0:
+            reference_arm(a, W, config)
         return
 
-    # ---- our arm ---------------------------------------------------------------
+    import torch
+    import torch.distributed as dist
+    esz = 4 if a.dtype == "f32" else 2
+    hbm_peak, peak_kind = peaks()
     if world > 1:
         torch.cuda.set_device(local)
         import datetime
@@ -575,9 +890,8 @@ def main():
     torch.cuda.synchronize()
     build_ms = (time.perf_counter() - tb0) * 1e3  # device construction: sorts, CSF levels, views, tables
     info = F.info(2)
-    inds_dev, _ = device_coo(X)
+    inds_dev, vals_dev = device_coo(X)
     rows, nfib_nosplit = workload_stats(inds_dev, dims, info["mode_order"])
-    del inds_dev
     g = torch.Generator(device="cuda").manual_seed(1234 + rank)
     tdt = torch.float32 if a.dtype == "f32" else torch.bfloat16
     U = [torch.rand(d, R, device="cuda", generator=g).to(tdt) for d in dims]
@@ -590,31 +904,12 @@ def main():
         plan = None if a.no_tune else F.tune(U, outs)
     # value: the workload's bytes under the MM-CSF partition traversal (the
     # same definition the reference arm uses, so the two values compare as
-    # times); roofline: the bytes of the traversal each mode actually ran
+    # times); roofline: the bytes of the traversal each launch actually ran
     sb_part = struct_bytes(nd, nnz, nfib_nosplit, info["n_fbrs"] if nd == 4 else 0)
     step_bytes = sum(mode_bytes(nd, dims, m, R, esz, sb_part, rows) for m in range(nd))
-    per_mode = []
-    for m in range(nd):
-        trav = plan[m]["traversal"] if plan else (2 if F.info(4 + m)["present"] else 1)
-        pi = F.info(4 + m) if trav == 2 else info
-        lvl = pi["mode_order"].index(m)
-        if plan and plan[m].get("kernel") == 3 and (nd == 3 or lvl in (0, nd - 1)):
-            sb = nnz * 12 + pi["n_slices"] * 8  # per-nonzero walk: vals, leaf, mid; slice offsets and indices
-        else:
-            sb = struct_bytes(nd, nnz, pi["n_fibers"], pi["n_fbrs"])
-        per_mode.append(mode_bytes(nd, dims, m, R, esz, sb, rows))
     stream = torch.cuda.current_stream()
+    per_mode = per_mode_bytes(F, nd, dims, nnz, R, esz, rows, plan, info)
     units = step_units(F, U, outs, plan)
-
-    def unit_bytes(modes):
-        if len(modes) == 1:
-            return per_mode[modes[0]]
-        # the two-output walk: vals, leaf and middle indices per nonzero, slice
-        # offsets and indices, every touched row of the three factors once,
-        # both outputs written once
-        return (nnz * (12 if nd == 3 else 16) + info["n_slices"] * 8 + sum(rows[q] * R * esz for q in range(nd))
-                + sum(dims[q] * R * 4 for q in modes))
-
     for _ in range(a.warmup):
         F.mttkrp_all(U, outs)
     launches_per_step = F.last_launches
@@ -667,92 +962,85 @@ def main():
         if world > 1:
             dist.destroy_process_group()
         return
-    ub = [unit_bytes(u[0]) for u in units]
+    ub = [unit_bytes_for(F, nd, dims, nnz, R, esz, rows, plan, info, u[0], per_mode) for u in units]
     di = max(range(len(units)), key=lambda i: unit_ms[i])
-    dmodes = units[di][0]
+    dk, dlabel = kernel_label(F, nd, plan, info, units[di][0])
     achieved = ub[di] / (unit_ms[di] / 1e3) / 1e9
-    if len(dmodes) == 2:
-        dker = "k_mttkrp_pair" if nd == 3 else "k_mttkrp_pair4"
-        dlabel = (f"{dker} modes {dmodes[0]} and {dmodes[1]} (levels 0 and 1 of order "
-                  f"{info['mode_order']}, MM-CSF partition, one walk)")
-        traffic = traffic_from_profiles(a.workload, R, a.dtype, "".join(str(m) for m in dmodes), dker)
-    else:
-        dom = dmodes[0]
-        dtrav = plan[dom]["traversal"] if plan else 1
-        dorder = F.info(4 + dom)["mode_order"] if dtrav == 2 else info["mode_order"]
-        dlvl = dorder.index(dom)
-        dk = plan[dom].get("kernel", 0) if plan else 0
-        if dk == 3 and nd == 4 and dlvl not in (0, 3):
-            dk = 1  # the 4-D middle levels run the per-team fiber walk
-        dker = {1: "k_mttkrp", 2: "k_mttkrp_flat", 3: "k_mttkrp_rows"}.get(dk or (2 if nd == 3 else 1))
-        dlabel = (f"{dker} mode {dom} (level {dlvl} of order {dorder}, "
-                  f"{'view' if dtrav == 2 else 'MM-CSF partition'})")
-        traffic = traffic_from_profiles(a.workload, R, a.dtype, dom, dker)
+    traffic = traffic_from_profiles(a.workload, R, a.dtype, "".join(str(m) for m in units[di][0]), dk)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
                 "traffic": traffic, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
                 "kernel": dlabel, "algorithmic_bytes": ub[di], "avg_ms": unit_ms[di]}
-    unit_report = [{"modes": list(u[0]), "ms": t, "algorithmic_bytes": b} for u, t, b in zip(units, unit_ms, ub)]
-    mode_ms = [next((t for u, t in zip(units, unit_ms) if u[0] == (m,)), None) for m in range(nd)]
+    unit_report = [{"modes": list(u[0]), "kernel": kernel_label(F, nd, plan, info, u[0])[0], "ms": t,
+                    "algorithmic_bytes": b, "roofline_frac": b / (t / 1e3) / 1e9 / hbm_peak}
+                   for u, t, b in zip(units, unit_ms, ub)]
+    # the outputs of the timed step against the FP64 oracle
+    F.mttkrp_all(U, outs)
+    torch.cuda.synchronize()
+    refs = fp64_refs(inds_dev, vals_dev, U)
+    errors = [err_vs(o, r) for o, r in zip(outs, refs)]
     # gather ceiling: the same GPU gathering the leaf factor's rows for the
     # workload's own leaf-mode index stream with nothing else to do
     if a.dtype == "f32" and R in (16, 32, 64, 128):
         import ctypes
         from mmcsf._lib import lib as _mlib, check as _mcheck
         leafm = info["mode_order"][-1]
-        dinds, _ = X.device_tensors()
         pms = ctypes.c_float()
-        _mcheck(_mlib().mmcsf_probe_gather(ctypes.c_void_p(dinds[leafm].data_ptr()), ctypes.c_uint64(nnz),
+        _mcheck(_mlib().mmcsf_probe_gather(ctypes.c_void_p(inds_dev[leafm].data_ptr()), ctypes.c_uint64(nnz),
                                            ctypes.c_void_p(U[leafm].data_ptr()), ctypes.c_uint64(dims[leafm]), R, 5,
                                            ctypes.byref(pms), ctypes.c_void_p(stream.cuda_stream)))
         roofline["gather_ceiling"] = {
             "ms": pms.value, "rows_per_s": nnz / (pms.value / 1e3),
             "what": f"{nnz} rows of the {dims[leafm]} x {R} FP32 mode-{leafm} factor gathered by the workload's "
-                    f"mode-{leafm} indices and summed (mmcsf_probe_gather), nothing else",
-            "dominant_kernel_vs_ceiling": pms.value / unit_ms[di]}
-        # the dominant launch against that rate: factor rows it gathers per
-        # launch (per-nonzero walks and the two-output walks gather every
-        # other level's row at every nonzero) / its time
-        if dker in ("k_mttkrp_pair", "k_mttkrp_pair4", "k_mttkrp_rows"):
-            rows_launch = nnz * (nd - 1)
-            rps = rows_launch / (unit_ms[di] / 1e3)
-            roofline["gather_ceiling"].update({
-                "dominant_rows_per_launch": rows_launch, "dominant_rows_per_s": rps,
-                "dominant_frac_of_gather_rate": rps / (nnz / (pms.value / 1e3))})
+                    f"mode-{leafm} indices and summed (mmcsf_probe_gather), nothing else"}
     cpu = None
     if not a.no_cpu and world == 1:
         inds_h, vals_h = X.host_arrays()
-        ref = reference_cpu(inds_h, vals_h, dims, R, target_s=12.0)
-        S = ref.S
-        ts = ref.seconds() * nnz / S
-        cpu = {"value": step_bytes / ts / 1e9, "unit": "GB/s", "cores": ref.T, "kind": ref.kind,
-               "ms_per_step": ts * 1e3,
-               "sample": f"first {S} of {nnz} nonzeros, all {nd} modes, MTTKRP_COO_CPU on {ref.T} threads over "
-                         f"nonzero ranges (private outputs summed), extrapolated x{nnz / S:.1f}"}
+        ref = RefCpuMttkrp(inds_h, vals_h, dims, R, host_threads())
+        del inds_h, vals_h
+        ref.seconds()  # warm-up (page faults of the private outputs)
+        ts = min(ref.seconds() for _ in range(2))
+        cpu = {"value": step_bytes / ts / 1e9, "unit": "GB/s", "cores": ref.T, "nproc": host_threads(),
+               "kind": ref.kind, "ms_per_step": ts * 1e3,
+               "sample": f"all {nnz} nonzeros, all {nd} modes: MTTKRP_COO_CPU on {ref.T} host threads over "
+                         f"contiguous nonzero ranges (private outputs added in the step), best of 2 steps after "
+                         f"one warm-up; no extrapolation"}
     bf16 = None
     if a.dtype == "f32" and not a.no_bf16:
         F.mttkrp_all(U, outs)
-        bf16 = bf16_section(F, U, outs, min(a.steps, 20), a.warmup)
+        bf16 = bf16_section(F, U, outs, min(a.steps, 20), a.warmup, inds_dev, vals_dev, refs)
+    r64 = None
+    if a.workload == "skewed3d" and R == 32 and a.dtype == "f32" and not a.no_r64 and not a.nnz:
+        r64 = r64_section(F, X, dims, rows, nfib_nosplit, info, min(a.steps, 20), a.warmup, hbm_peak, peak_kind,
+                          a.workload)
     ttm = ttm_section(X, dims, R, info["mode_order"][0], rows) if nd == 3 and R in (4, 8, 16, 32, 64, 128) else None
     heur = None
     if not a.no_heuristic:
         heur = heuristic_section(X, dims, R, tdt, a.views)
     formats = None
     if nd == 4 and not a.no_formats:
-        fm = format_section(X, dims, R, tdt)
-        fm["mmcsf"] = {"mode_ms": mode_ms, "all_mode_ms": ms_per_step}
+        fm = format_section(X, dims, R, U, rows, hbm_peak, refs)
+        fm["mmcsf"] = {"all_mode_ms": ms_per_step}
         formats = fm
+    del refs
+    del F, X, U, outs, inds_dev, vals_dev
+    torch.cuda.empty_cache()
+    cfg1 = None
+    if not a.no_config1 and a.workload == "skewed3d" and not a.nnz:
+        cfg1 = config1_section(min(a.steps, 20), a.warmup, hbm_peak)
+    w4d = None
+    if not a.no_4d and a.workload == "skewed3d" and not a.nnz:
+        w4d = skewed4d_section(min(a.steps, 10), a.warmup, a.seed, hbm_peak, peak_kind)
     cp = None
     if not a.no_cp:
-        del F, X, U, outs
-        torch.cuda.empty_cache()
         cp = cp_section(a.seed, a.cp_scale)
     line = {"metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": a.dtype, "data": "synthetic (seeded device generator)",
             "config": config, "format_build_ms": build_ms, "units": unit_report, "plan": plan, "format": info,
-            "roofline": roofline,
+            "roofline": roofline, "error_vs_fp64": errors,
             "cpu_baseline": cpu,
             "e2e": e2e, "gpu_launches": launches_per_step * a.steps, "clocks": clocks, "bf16_factors": bf16,
+            "r64": r64, "config1": cfg1, "skewed4d": w4d,
             "ttm": ttm, "cp": cp, "formats": formats, "partition_heuristic": heur}
     print(json.dumps(line), flush=True)
     if world > 1:

@@ -235,6 +235,18 @@ class Format:
                 "nnz": int(pi.nnz), "n_slices": int(pi.n_slices), "n_fbrs": int(pi.n_fbrs),
                 "n_fibers": int(pi.n_fibers), "device_bytes": int(pi.device_bytes)}
 
+    def chunk_for_warps(self, warps, R):
+        """The worker-team chunk equivalent to the reference's -w `warps`
+        warps per fiber (src/util.h:194, src/mttkrp_gpu.cu:3616-3630): the
+        reference launches warps*F warps (F fibers over the partitions); the
+        kernels here have 32/G teams per warp (G lanes per factor row), so
+        the same worker count means max(1, N*G / (32*warps*F)) nonzeros per
+        team. The `mttkrp` command maps -w the same way."""
+        fibers = sum(self.info(p)["n_fibers"] for p in self.partitions())
+        r4 = (int(R) + 3) // 4
+        G = 32 if r4 >= 32 else 16 if r4 >= 16 else 8 if r4 >= 8 else 4 if r4 >= 4 else 2 if r4 >= 2 else 1
+        return int(max(1, min(1 << 20, self.nnz * G // (32 * int(warps) * max(1, fibers)))))
+
     def meta(self):
         r = ctypes.c_int()
         xo = (ctypes.c_int * 4)()

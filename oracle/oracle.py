@@ -29,10 +29,11 @@ _lib = None
 def build(force=False):
     """Compile the C restatement into oracle/_build/libmmcsf_oracle.so."""
     os.makedirs(_BUILD, exist_ok=True)
-    src = os.path.join(HERE, "mmcsf_oracle.c")
-    if force or not os.path.exists(_LIB_PATH) or os.path.getmtime(_LIB_PATH) < os.path.getmtime(src):
-        subprocess.run(["gcc", "-O2", "-ffp-contract=off", "-fPIC", "-shared", "-o", _LIB_PATH, src],
-                       check=True)
+    srcs = [os.path.join(HERE, "mmcsf_oracle.c"), os.path.join(HERE, "generate.c")]
+    if force or not os.path.exists(_LIB_PATH) or any(os.path.getmtime(_LIB_PATH) < os.path.getmtime(s)
+                                                     for s in srcs):
+        subprocess.run(["gcc", "-O2", "-ffp-contract=off", "-fPIC", "-shared", "-pthread", "-o", _LIB_PATH]
+                       + srcs + ["-lm"], check=True)
     return _LIB_PATH
 
 
@@ -470,3 +471,29 @@ def ref_mttkrp_coo(dims, inds, vals, mode, factors):
                                   mode, R, (fp * nd)(*[u.ctypes.data_as(fp) for u in U]))
     assert rc == 0
     return U[mode]
+
+
+# --------------------------------------------------------------------------
+# Seeded synthetic tensors on the host: oracle/generate.c restates the
+# library's generator (mmcsf_generate) for the benchmark's CPU legs.
+# --------------------------------------------------------------------------
+def generate(dims, nnz, dist, zipf_s=1.0, val_dist=0, seed=0, threads=0):
+    """(inds[nd] uint32, vals float32) of the seeded tensor mmcsf_generate
+    makes for the same arguments (uniform / Zipf modes; values uniform (0,1],
+    lognormal or integers 1..50), computed on `threads` host threads."""
+    nd = len(dims)
+    d = (ctypes.c_uint64 * 4)(*[int(x) for x in dims] + [0] * (4 - nd))
+    ds = (ctypes.c_int * 4)(*[int(x) for x in (dist if isinstance(dist, (list, tuple)) else [dist] * nd)]
+                            + [0] * (4 - nd))
+    zs = (ctypes.c_double * 4)(*[float(x) for x in (zipf_s if isinstance(zipf_s, (list, tuple)) else [zipf_s] * nd)]
+                               + [0.0] * (4 - nd))
+    inds = [np.empty(int(nnz), np.uint32) for _ in range(nd)]
+    vals = np.empty(int(nnz), np.float32)
+    T = threads or len(os.sched_getaffinity(0))
+    u32p = ctypes.POINTER(ctypes.c_uint32)
+    rc = lib().orc_generate(nd, d, ctypes.c_uint64(int(nnz)), ds, zs, int(val_dist), ctypes.c_uint64(int(seed)),
+                            int(T), (u32p * nd)(*[i.ctypes.data_as(u32p) for i in inds]),
+                            vals.ctypes.data_as(ctypes.POINTER(ctypes.c_float)))
+    if rc != 0:
+        raise RuntimeError(f"orc_generate failed ({rc})")
+    return inds, vals

@@ -192,7 +192,8 @@ typedef struct {
                         levels, fewer rows in flight per warp */
   int kernel;        /* 0 auto (tuned plan, else 2 for 3-D and 1 for 4-D); 1 per-team fiber walk;
                         2 branch-free fiber walk (3-D; 4-D runs 1); 3 per-nonzero walk (every 3-D
-                        level; 4-D slice and leaf levels; the 4-D middle levels run 1) */
+                        level; 4-D slice and leaf levels; the 4-D middle levels run 1); 4 per-nonzero
+                        walk gathering the middle row once per fiber (3-D slice level; elsewhere 3) */
   int reserved[3];
 } mmcsf_kernel_cfg;
 
@@ -217,7 +218,8 @@ int mmcsf_mttkrp_coo_host(const mmcsf_coo* X, int mode, int R, const float* cons
  * partition's slice mode (modes[0], into d_out_slice) and of its middle mode
  * (modes[1], into d_out_mid) from one traversal that gathers each nonzero's
  * factor rows once. cfg->kernel 2 runs the branch-free fiber walk (the middle
- * row gathered once per fiber), 3 the per-nonzero form (0: the tuned choice);
+ * row gathered once per fiber), 3 the per-nonzero form, 4 the per-nonzero form
+ * with the middle row gathered once per fiber (3-D; 0: the tuned choice);
  * chunk and min_blocks as for mmcsf_mttkrp. With null outputs only `modes` is
  * filled. R in 4..128 (powers of two). */
 int mmcsf_mttkrp_pair(const mmcsf_format* F, int R, int factor_dtype, const void* const* d_factors,

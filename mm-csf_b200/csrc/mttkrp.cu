@@ -24,1145 +24,13 @@
 #include <cstring>
 #include <type_traits>
 
-#include "format.h"
+#include "mttkrp_args.h"
 #include "prims.cuh"
 
 using mmcsf::set_error;
 
 namespace mmcsf {
 namespace {
-
-constexpr unsigned FULL = 0xffffffffu;
-
-template <class T> struct Row;
-template <> struct Row<float> {
-  static __device__ __forceinline__ float4 load(const float* base, uint64_t off) {
-    return __ldg(reinterpret_cast<const float4*>(base + off));
-  }
-};
-template <> struct Row<__nv_bfloat16> {
-  static __device__ __forceinline__ float4 load(const __nv_bfloat16* base, uint64_t off) {
-    uint2 u = __ldg(reinterpret_cast<const uint2*>(base + off));
-    float4 r;
-    r.x = __uint_as_float(u.x << 16);
-    r.y = __uint_as_float(u.x & 0xffff0000u);
-    r.z = __uint_as_float(u.y << 16);
-    r.w = __uint_as_float(u.y & 0xffff0000u);
-    return r;
-  }
-};
-
-__device__ __forceinline__ float4 f4(float a) { return make_float4(a, a, a, a); }
-__device__ __forceinline__ float4 operator*(float4 a, float4 b) {
-  return make_float4(a.x * b.x, a.y * b.y, a.z * b.z, a.w * b.w);
-}
-__device__ __forceinline__ float4 fma4(float s, float4 a, float4 c) {
-  return make_float4(fmaf(s, a.x, c.x), fmaf(s, a.y, c.y), fmaf(s, a.z, c.z), fmaf(s, a.w, c.w));
-}
-__device__ __forceinline__ float4 fma4v(float4 a, float4 b, float4 c) {
-  return make_float4(fmaf(a.x, b.x, c.x), fmaf(a.y, b.y, c.y), fmaf(a.z, b.z, c.z), fmaf(a.w, b.w, c.w));
-}
-// One vector reduction (PTX ISA 8.1+, sm_90+): four floats added at p (16 B aligned).
-__device__ __forceinline__ void red4(float* p, float4 v) {
-  asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(p), "f"(v.x), "f"(v.y), "f"(v.z), "f"(v.w)
-               : "memory");
-}
-
-template <class T>
-struct Args {
-  const float* vals;
-  const uint32_t* leaf;
-  const uint32_t* fptr;   // leaf fibers -> nonzeros [F+1]
-  const uint32_t* fidx;   // leaf-fiber index (o1 in 3-D, o2 in 4-D)
-  const uint32_t* fpar;   // 4-D: fiber -> fbrS
-  const uint32_t* sidx1;  // 4-D: fbrS index (o1)
-  const uint32_t* like;   // o0 per level-1 entry (3-D: fiber, 4-D: fbrS)
-  const uint32_t* cfib;   // first fiber of every team's chunk, or null (binary search)
-  const uint32_t* mid;    // per-nonzero walk: o_{nd-2} of every nonzero
-  const uint32_t* mid2;   // ... 4-D: o1 of every nonzero
-  const uint32_t* snz;    // ... first nonzero of every slice [nslc + 1]
-  const uint32_t* sidx;   // ... slice index (o0) of every slice
-  const uint32_t* cslc;   // ... slice of every team's chunk start, or null (binary search)
-  uint32_t nslc;
-  uint64_t nnz;
-  uint32_t nfib;
-  uint32_t chunk;
-  uint32_t R;
-  const T* U[4];  // factor of mode order[l], by level l
-  float* out;
-  float* out2;  // two-output walk: the middle mode's output
-};
-
-// largest f with fptr[f] <= x
-__device__ __forceinline__ uint32_t find_fiber(const uint32_t* __restrict__ fptr, uint32_t nfib, uint64_t x) {
-  uint32_t lo = 0, hi = nfib - 1;
-  while (lo < hi) {
-    uint32_t mid = (lo + hi + 1) >> 1;
-    if ((uint64_t)__ldg(fptr + mid) <= x) lo = mid; else hi = mid - 1;
-  }
-  return lo;
-}
-
-// ND: 3 or 4. OUT: output level (0 = slice ... ND-1 = leaf). G lanes per row,
-// V float4 per lane, R = 4*G*V (a compile-time constant: row offsets are
-// shifts, not 64-bit multiplies).
-//
-// Per team the only dependent-load chain left per block of G nonzeros is the
-// factor-row gather: leaf indices and values for the next block are loaded
-// while the current block is processed; fiber starts are flagged in bit 31 of
-// the leaf index (no fiber-pointer reads after the initial search); the
-// fibers' metadata (index, slice map) sits in a G-wide register window
-// refilled with one coalesced load every G fibers; and the factor row a fiber
-// needs when it closes is requested as soon as the fiber opens.
-// MB: minimum resident 256-thread CTAs per SM the register allocation must
-// allow; PFX: row gathers in flight per lane. The occupancy level picks the
-// pair (1: 8 rows / 3 CTAs = 80 registers, 2: 8 rows / 4 CTAs = 64,
-// 3: 4 rows / 5 CTAs = 48, 4: 4 rows / 6 CTAs = 40); the tuner picks per mode.
-template <int ND, int OUT, int G, int V, class T, int MB, int PFX>
-__global__ void __launch_bounds__(256, MB) k_mttkrp(const Args<T> a) {
-  constexpr uint32_t R = 4 * G * V;
-  constexpr int LEAF = ND - 1;
-  constexpr uint32_t FLAG = 0x80000000u;
-  constexpr int PF = G > PFX ? PFX : G;  // row gathers in flight per lane per batch
-  const int lane = threadIdx.x & 31;
-  const int tl = lane & (G - 1);
-  const int tb = lane - tl;
-  // kernel parameters in registers
-  const float* __restrict__ vals = a.vals;
-  const uint32_t* __restrict__ leaf = a.leaf;
-  const uint32_t* __restrict__ fidx = a.fidx;
-  const uint32_t* __restrict__ fpar = a.fpar;
-  const uint32_t* __restrict__ sidx1 = a.sidx1;
-  const uint32_t* __restrict__ like = a.like;
-  const uint32_t nfib = a.nfib, chunk = a.chunk;
-  const T* __restrict__ U0 = a.U[0];
-  const T* __restrict__ U1 = a.U[1];
-  const T* __restrict__ U2 = a.U[2];
-  const T* __restrict__ UL = a.U[LEAF];
-  float* __restrict__ out = a.out;
-  const uint32_t c0 = (uint32_t)tl * 4;  // this lane's first column
-  auto ld = [&](const T* U, uint32_t row, int v) -> float4 {
-    return Row<T>::load(U + (uint64_t)row * R, c0 + (uint32_t)(v * G * 4));
-  };
-  auto rd = [&](uint32_t row, int v, float4 x) { red4(out + (uint64_t)row * R + c0 + v * G * 4, x); };
-
-  const uint64_t team = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) / G;
-  // Teams past the end stay in the loop (empty range) so every full-warp
-  // shuffle sees all lanes; all teams run the same number of iterations.
-  const bool active = team * chunk < a.nnz;
-  const uint64_t x0 = active ? team * chunk : a.nnz - 1;
-  const uint64_t x1 = active ? min(x0 + chunk, a.nnz) : x0;
-
-  uint32_t f = a.cfib ? (active ? __ldg(a.cfib + team) : nfib - 1) : find_fiber(a.fptr, nfib, x0);
-  // metadata of the open fiber (ci: b in 3-D, c in 4-D; cp: a in 3-D, fbrS
-  // in 4-D) and of the next one, loaded a fiber ahead
-  auto meta_i = [&](uint32_t q) { return __ldg(fidx + min(q, nfib - 1)); };
-  auto meta_p = [&](uint32_t q) { return (ND == 3) ? __ldg(like + min(q, nfib - 1)) : __ldg(fpar + min(q, nfib - 1)); };
-  uint32_t ci = meta_i(f), cp = meta_p(f);
-  uint32_t nci = meta_i(f + 1), ncp = meta_p(f + 1);
-  uint32_t sb = 0, sa = 0;                   // 4-D: current fbrS's b and a
-  if (ND == 4) { sb = __ldg(sidx1 + cp); sa = __ldg(like + cp); }
-
-  float4 acc[V], acc1[V], acc2[V], crow[V], srow[V];
-#pragma unroll
-  for (int v = 0; v < V; ++v) acc[v] = acc1[v] = acc2[v] = crow[v] = srow[v] = f4(0.f);
-  uint32_t cur_a = (ND == 3) ? cp : sa;  // slice whose accumulation is open (OUT == 0)
-
-  // rows needed per fbrS (4-D) and per fiber, requested when they open
-  auto open_fbrs = [&]() {
-    if constexpr (ND == 4) {
-#pragma unroll
-      for (int v = 0; v < V; ++v) {
-        if constexpr (OUT == 0) srow[v] = ld(U1, sb, v);
-        else if constexpr (OUT == 1) srow[v] = ld(U0, sa, v);
-        else srow[v] = ld(U0, sa, v) * ld(U1, sb, v);
-      }
-    }
-  };
-  auto open_fiber = [&]() {
-#pragma unroll
-    for (int v = 0; v < V; ++v) {
-      if constexpr (ND == 3) {
-        if constexpr (OUT == 0) crow[v] = ld(U1, ci, v);
-        else if constexpr (OUT == 1) crow[v] = ld(U0, cp, v);
-        else crow[v] = ld(U0, cp, v) * ld(U1, ci, v);
-      } else {
-        if constexpr (OUT == 3) crow[v] = srow[v] * ld(U2, ci, v);
-        else if constexpr (OUT != 2) crow[v] = ld(U2, ci, v);
-      }
-    }
-  };
-  open_fbrs();
-  open_fiber();
-
-  // Fold the open fiber's partial (acc) into the level above / the output.
-  auto close_fiber = [&]() {
-    if constexpr (OUT != LEAF) {
-#pragma unroll
-      for (int v = 0; v < V; ++v) {
-        if constexpr (ND == 3 && OUT == 1) rd(ci, v, crow[v] * acc[v]);
-        else if constexpr (ND == 4 && OUT == 2) rd(ci, v, srow[v] * acc[v]);
-        else acc1[v] = fma4v(crow[v], acc[v], acc1[v]);
-      }
-    }
-  };
-  // 4-D: fold the open fbrS (acc1) upward (OUT 0) or out (OUT 1).
-  auto close_fbrs = [&]() {
-#pragma unroll
-    for (int v = 0; v < V; ++v) {
-      if constexpr (ND == 4 && OUT == 1) { rd(sb, v, srow[v] * acc1[v]); acc1[v] = f4(0.f); }
-      else if constexpr (ND == 4 && OUT == 0) { acc2[v] = fma4v(srow[v], acc1[v], acc2[v]); acc1[v] = f4(0.f); }
-    }
-  };
-  auto flush_slice = [&]() {
-#pragma unroll
-    for (int v = 0; v < V; ++v) {
-      if constexpr (OUT == 0 && ND == 3) { rd(cur_a, v, acc1[v]); acc1[v] = f4(0.f); }
-      else if constexpr (OUT == 0) { rd(cur_a, v, acc2[v]); acc2[v] = f4(0.f); }
-    }
-  };
-  // nonzero x opens fiber f+1 (team-uniform branch; no shuffles inside)
-  auto advance = [&]() {
-    close_fiber();
-    ++f;
-    ci = nci;
-    const uint32_t np = ncp;
-    nci = meta_i(f + 1);
-    ncp = meta_p(f + 1);
-    if constexpr (ND == 3) {
-      if (OUT == 0 && np != cur_a) { flush_slice(); cur_a = np; }
-      cp = np;
-    } else {
-      if (np != cp) {  // new fbrS
-        close_fbrs();
-        cp = np;
-        sb = __ldg(sidx1 + cp);
-        sa = __ldg(like + cp);
-        if (OUT == 0 && sa != cur_a) { flush_slice(); cur_a = sa; }
-        open_fbrs();
-      }
-    }
-    open_fiber();
-  };
-
-  uint32_t nk = 0;
-  float nv = 0.f;
-  if (x0 + tl < x1) { nk = __ldg(leaf + x0 + tl); nv = __ldg(vals + x0 + tl); }
-  for (uint32_t it = 0; it < chunk; it += G) {
-    const uint64_t xb = x0 + it;
-    const uint32_t kv = nk;
-    const float vv = nv;
-    {  // next block's indices and values, while this block is processed
-      const uint64_t xn = xb + G + tl;
-      nk = 0;
-      nv = 0.f;
-      if (it + G < chunk && xn < x1) { nk = __ldg(leaf + xn); nv = __ldg(vals + xn); }
-    }
-    // a lane past the range holds val 0 and no flag, and gathers row 0
-    const bool fl = (kv & FLAG) && (xb + tl != x0);
-    const uint32_t fm = (__ballot_sync(FULL, fl) >> tb);
-    const uint32_t k = kv & ~FLAG;
-#pragma unroll
-    for (int jb = 0; jb < G; jb += PF) {
-      float4 rows[PF][V];
-      uint32_t kj[PF];
-#pragma unroll
-      for (int j = 0; j < PF; ++j) {
-        kj[j] = __shfl_sync(FULL, k, tb + jb + j);
-        if constexpr (OUT != LEAF) {
-#pragma unroll
-          for (int v = 0; v < V; ++v) rows[j][v] = ld(UL, kj[j], v);
-        }
-      }
-#pragma unroll
-      for (int j = 0; j < PF; ++j) {
-        const float val = __shfl_sync(FULL, vv, tb + jb + j);
-        if ((fm >> (jb + j)) & 1u) {
-          advance();
-#pragma unroll
-          for (int v = 0; v < V; ++v) acc[v] = f4(0.f);
-        }
-        if constexpr (OUT != LEAF) {
-#pragma unroll
-          for (int v = 0; v < V; ++v) acc[v] = fma4(val, rows[j][v], acc[v]);
-        } else {
-          if (xb + jb + j < x1) {
-#pragma unroll
-            for (int v = 0; v < V; ++v) rd(kj[j], v, f4(val) * crow[v]);
-          }
-        }
-      }
-    }
-  }
-  if (active) {
-    close_fiber();
-    close_fbrs();
-    flush_slice();
-  }
-}
-
-// ---------------------------------------------------------------------------
-// Branch-free 3-D traversal ("flat" kernel). Same teams and nonzero ranges as
-// k_mttkrp, but a fiber start no longer sends its team down a separate code
-// path: every lane locates the fiber of its own nonzero from the block's
-// fiber-start ballot (popcount of the flags at or below it), loads that
-// fiber's metadata only if its nonzero opens the fiber, and the per-nonzero
-// step is the same straight-line code for every team of the warp, with the
-// fiber-open work predicated. Slice changes (rare: one per slice run) take a
-// slower variant of the block, chosen per warp. Arithmetic uses the packed
-// FP32x2 FMA of sm_100 (two fused multiply-adds per instruction).
-__device__ __forceinline__ float4 pfma(float4 a, float4 b, float4 c) {
-  const float2 lo = __ffma2_rn(make_float2(a.x, a.y), make_float2(b.x, b.y), make_float2(c.x, c.y));
-  const float2 hi = __ffma2_rn(make_float2(a.z, a.w), make_float2(b.z, b.w), make_float2(c.z, c.w));
-  return make_float4(lo.x, lo.y, hi.x, hi.y);
-}
-__device__ __forceinline__ float4 pfma_s(float s, float4 b, float4 c) {
-  const float2 ss = make_float2(s, s);
-  const float2 lo = __ffma2_rn(ss, make_float2(b.x, b.y), make_float2(c.x, c.y));
-  const float2 hi = __ffma2_rn(ss, make_float2(b.z, b.w), make_float2(c.z, c.w));
-  return make_float4(lo.x, lo.y, hi.x, hi.y);
-}
-__device__ __forceinline__ float4 pmul(float4 a, float4 b) {
-  const float2 lo = __fmul2_rn(make_float2(a.x, a.y), make_float2(b.x, b.y));
-  const float2 hi = __fmul2_rn(make_float2(a.z, a.w), make_float2(b.z, b.w));
-  return make_float4(lo.x, lo.y, hi.x, hi.y);
-}
-__device__ __forceinline__ float4 pmul_s(float s, float4 b) {
-  const float2 ss = make_float2(s, s);
-  const float2 lo = __fmul2_rn(ss, make_float2(b.x, b.y));
-  const float2 hi = __fmul2_rn(ss, make_float2(b.z, b.w));
-  return make_float4(lo.x, lo.y, hi.x, hi.y);
-}
-
-// OUT 0 (slice rows): acc_s[a] += U1[b] (.) sum_fiber v U2[k]; the fiber's
-//   U1 row is requested when the fiber opens and used when it closes.
-// OUT 1 (fiber rows): out[b] += U0[a] (.) sum_fiber v U2[k], one vector
-//   reduction per fiber.
-// OUT 2 (leaf rows): out[k] += v U0[a] (.) U1[b], one reduction per nonzero;
-//   the fiber's U1 rows for a batch are requested before the batch.
-template <int OUT, int G, int V, class T, int MB, int PFX>
-__global__ void __launch_bounds__(256, MB) k_mttkrp_flat(const Args<T> a) {
-  constexpr uint32_t R = 4 * G * V;
-  constexpr uint32_t FLAG = 0x80000000u;
-  constexpr int PF = G > PFX ? PFX : G;
-  constexpr uint32_t GMASK = G == 32 ? FULL : ((1u << G) - 1u);
-  const int lane = threadIdx.x & 31;
-  const int tl = lane & (G - 1);
-  const int tb = lane - tl;
-  const uint32_t le_mask = tl == 31 ? FULL : ((2u << tl) - 1u);  // lanes 0..tl of the team
-  const float* __restrict__ vals = a.vals;
-  const uint32_t* __restrict__ leaf = a.leaf;
-  const uint32_t* __restrict__ fidx = a.fidx;
-  const uint32_t* __restrict__ like = a.like;
-  const uint32_t chunk = a.chunk;
-  const T* __restrict__ U0 = a.U[0];
-  const T* __restrict__ U1 = a.U[1];
-  const T* __restrict__ U2 = a.U[2];
-  float* __restrict__ out = a.out;
-  float* __restrict__ out2 = a.out2;
-  const uint32_t c0 = (uint32_t)tl * 4;
-  auto ld = [&](const T* U, uint32_t row, int v) -> float4 {
-    return Row<T>::load(U + (uint64_t)row * R, c0 + (uint32_t)(v * G * 4));
-  };
-  auto rd = [&](uint32_t row, int v, float4 x) { red4(out + (uint64_t)row * R + c0 + v * G * 4, x); };
-  auto rd2 = [&](uint32_t row, int v, float4 x) { red4(out2 + (uint64_t)row * R + c0 + v * G * 4, x); };
-
-  const uint64_t team = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) / G;
-  const bool active = team * chunk < a.nnz;
-  const uint64_t x0 = active ? team * chunk : a.nnz - 1;
-  const uint64_t x1 = active ? min(x0 + chunk, a.nnz) : x0;
-
-  uint32_t f = a.cfib ? (active ? __ldg(a.cfib + team) : a.nfib - 1) : find_fiber(a.fptr, a.nfib, x0);
-  uint32_t cb = __ldg(fidx + f);  // open fiber's o1
-  uint32_t ca = __ldg(like + f);  // open slice's o0
-  float4 accf[V], accs[V], rowB[V], rowA[V];
-#pragma unroll
-  for (int v = 0; v < V; ++v) {
-    accf[v] = accs[v] = f4(0.f);
-    if constexpr (OUT == 0) rowB[v] = ld(U1, cb, v);
-    if constexpr (OUT == 1) rowA[v] = ld(U0, ca, v);
-    if constexpr (OUT == 2) { rowA[v] = ld(U0, ca, v); rowB[v] = rowA[v] * ld(U1, cb, v); }
-    if constexpr (OUT == 3) { rowA[v] = ld(U0, ca, v); rowB[v] = ld(U1, cb, v); }
-  }
-
-  // Block pipeline: when block i (G nonzeros) is processed, its indices,
-  // values and fiber metadata are in registers; block i+1's indices are in
-  // flight or ready (their fiber flags decide which metadata to request) and
-  // block i+2's are requested.
-  auto load_kv = [&](uint32_t itb, uint32_t& kk, float& vq) {
-    const uint64_t xx = x0 + itb + tl;
-    kk = 0;
-    vq = 0.f;
-    if (itb < chunk && xx < x1) { kk = __ldg(leaf + xx); vq = __ldg(vals + xx); }
-  };
-  auto load_meta = [&](uint32_t itb, uint32_t kk, uint32_t& fm_, uint32_t& mb_, uint32_t& ma_) {
-    const bool fl_ = (kk & FLAG) && (itb + tl != 0);
-    fm_ = (__ballot_sync(FULL, fl_) >> tb) & GMASK;
-    mb_ = 0;
-    ma_ = 0;
-    if (fl_) {
-      const uint32_t fib = f + __popc(fm_ & le_mask);
-      mb_ = __ldg(fidx + fib);
-      ma_ = __ldg(like + fib);
-    }
-    f += __popc(fm_);
-  };
-  uint32_t kc, kn, fmc, mbc, mac;
-  float vc, vn;
-  load_kv(0, kc, vc);
-  load_kv(G, kn, vn);
-  load_meta(0, kc, fmc, mbc, mac);
-  for (uint32_t it = 0; it < chunk; it += G) {
-    const uint64_t xb = x0 + it;
-    uint32_t kf;
-    float vf;
-    load_kv(it + 2 * G, kf, vf);
-    uint32_t fmn, mbn, man;
-    load_meta(it + G, kn, fmn, mbn, man);
-    const uint32_t kv = kc, fm = fmc, mb = mbc, ma = mac;
-    const float vv = vc;
-    kc = kn; vc = vn; fmc = fmn; mbc = mbn; mac = man;
-    kn = kf; vn = vf;
-    const bool slow = __ballot_sync(FULL, ((fm >> tl) & 1u) && ma != ca) != 0u;  // a slice changes in this block
-    const uint32_t k = kv & ~FLAG;
-
-    auto block = [&](auto slow_tag) {
-      constexpr bool SLOW = decltype(slow_tag)::value;
-#pragma unroll
-      for (int jb = 0; jb < G; jb += PF) {
-        float4 rows[PF][V];
-        uint32_t kj[PF], bj[PF];
-#pragma unroll
-        for (int j = 0; j < PF; ++j) {
-          kj[j] = __shfl_sync(FULL, k, tb + jb + j);
-          if constexpr (OUT == 2) bj[j] = __shfl_sync(FULL, mb, tb + jb + j);
-          if constexpr (OUT != 2) {
-#pragma unroll
-            for (int v = 0; v < V; ++v) rows[j][v] = ld(U2, kj[j], v);
-          } else {
-            if ((fm >> (jb + j)) & 1u) {
-#pragma unroll
-              for (int v = 0; v < V; ++v) rows[j][v] = ld(U1, bj[j], v);
-            }
-          }
-        }
-#pragma unroll
-        for (int j = 0; j < PF; ++j) {
-          const float val = __shfl_sync(FULL, vv, tb + jb + j);
-          if constexpr (OUT != 2) bj[j] = __shfl_sync(FULL, mb, tb + jb + j);
-          uint32_t aj = 0;
-          if constexpr (SLOW) aj = __shfl_sync(FULL, ma, tb + jb + j);
-          if ((fm >> (jb + j)) & 1u) {
-            if constexpr (OUT == 0) {
-#pragma unroll
-              for (int v = 0; v < V; ++v) { accs[v] = pfma(rowB[v], accf[v], accs[v]); accf[v] = f4(0.f); }
-              if constexpr (SLOW) {
-                if (aj != ca) {
-#pragma unroll
-                  for (int v = 0; v < V; ++v) { rd(ca, v, accs[v]); accs[v] = f4(0.f); }
-                  ca = aj;
-                }
-              }
-#pragma unroll
-              for (int v = 0; v < V; ++v) rowB[v] = ld(U1, bj[j], v);
-            } else if constexpr (OUT == 1) {
-#pragma unroll
-              for (int v = 0; v < V; ++v) { rd(cb, v, pmul(rowA[v], accf[v])); accf[v] = f4(0.f); }
-              cb = bj[j];
-              if constexpr (SLOW) {
-                if (aj != ca) {
-                  ca = aj;
-#pragma unroll
-                  for (int v = 0; v < V; ++v) rowA[v] = ld(U0, ca, v);
-                }
-              }
-            } else if constexpr (OUT == 3) {
-              // both outputs: the closing fiber's sum goes to the middle
-              // mode's row and, through its middle row, into the slice sum
-#pragma unroll
-              for (int v = 0; v < V; ++v) {
-                rd2(cb, v, pmul(rowA[v], accf[v]));
-                accs[v] = pfma(rowB[v], accf[v], accs[v]);
-                accf[v] = f4(0.f);
-              }
-              cb = bj[j];
-              if constexpr (SLOW) {
-                if (aj != ca) {
-#pragma unroll
-                  for (int v = 0; v < V; ++v) { rd(ca, v, accs[v]); accs[v] = f4(0.f); }
-                  ca = aj;
-#pragma unroll
-                  for (int v = 0; v < V; ++v) rowA[v] = ld(U0, ca, v);
-                }
-              }
-#pragma unroll
-              for (int v = 0; v < V; ++v) rowB[v] = ld(U1, cb, v);
-            } else {
-              if constexpr (SLOW) {
-                if (aj != ca) {
-                  ca = aj;
-#pragma unroll
-                  for (int v = 0; v < V; ++v) rowA[v] = ld(U0, ca, v);
-                }
-              }
-#pragma unroll
-              for (int v = 0; v < V; ++v) rowB[v] = pmul(rowA[v], rows[j][v]);
-            }
-          }
-          if constexpr (OUT != 2) {
-#pragma unroll
-            for (int v = 0; v < V; ++v) accf[v] = pfma_s(val, rows[j][v], accf[v]);
-          } else {
-            if (xb + jb + j < x1) {
-#pragma unroll
-              for (int v = 0; v < V; ++v) rd(kj[j], v, pmul_s(val, rowB[v]));
-            }
-          }
-        }
-      }
-    };
-    if (slow) block(std::true_type{});
-    else block(std::false_type{});
-  }
-  if (active) {
-#pragma unroll
-    for (int v = 0; v < V; ++v) {
-      if constexpr (OUT == 0) rd(ca, v, pfma(rowB[v], accf[v], accs[v]));
-      if constexpr (OUT == 1) rd(cb, v, pmul(rowA[v], accf[v]));
-      if constexpr (OUT == 3) {
-        rd(ca, v, pfma(rowB[v], accf[v], accs[v]));
-        rd2(cb, v, pmul(rowA[v], accf[v]));
-      }
-    }
-  }
-}
-
-// ---------------------------------------------------------------------------
-// Per-nonzero traversal ("rows" kernel), 3-D and 4-D, for the slice-level
-// (OUT 0) and leaf-level (OUT ND-1) outputs. Every nonzero carries the
-// indices of its middle levels (`mid` = o_{ND-2}, and `mid2` = o1 in 4-D), so
-// a team needs no fiber bookkeeping: per nonzero it combines the middle rows
-// and the leaf row, adding v * U1[b] (.) U2[k] (4-D: v * U1[b] (.) U2[c] (.)
-// U3[k]) to the open slice's accumulator (OUT 0), or scattering
-// v * U0[a] (.) U1[b] [(.) U2[c]] to the leaf row. The middle rows repeat along
-// fibers, so most of their gathers hit L1 (gathering them unconditionally
-// measured faster than predicating the repeats away). Slice changes come from the slices' first nonzero positions
-// (`snz`), not from flags, and a block with a slice change takes a slower
-// variant.
-template <int ND, int OUT, int G, int V, class T, int MB, int PFX>
-__global__ void __launch_bounds__(256, MB) k_mttkrp_rows(const Args<T> a) {
-  static_assert(OUT == 0 || OUT == ND - 1 || (ND == 3 && OUT == 1), "slice, leaf or 3-D middle level");
-  constexpr int LEAF = ND - 1;
-  constexpr bool MIDL = ND == 3 && OUT == 1;  // fiber-row output: sum v U2[k] per fiber, times U0[a], one reduction
-  constexpr uint32_t R = 4 * G * V;
-  constexpr uint32_t FLAG = 0x80000000u;
-  constexpr uint32_t GMASK = G == 32 ? FULL : ((1u << G) - 1u);
-  constexpr int PF = G > PFX ? PFX : G;
-  const int lane = threadIdx.x & 31;
-  const int tl = lane & (G - 1);
-  const int tb = lane - tl;
-  const float* __restrict__ vals = a.vals;
-  const uint32_t* __restrict__ leaf = a.leaf;
-  const uint32_t* __restrict__ mid = a.mid;
-  const uint32_t* __restrict__ mid2 = a.mid2;
-  const uint32_t* __restrict__ snz = a.snz;
-  const uint32_t* __restrict__ sidx = a.sidx;
-  const uint32_t chunk = a.chunk, nslc = a.nslc;
-  const T* __restrict__ U0 = a.U[0];
-  const T* __restrict__ U1 = a.U[1];
-  const T* __restrict__ U2 = a.U[2];
-  const T* __restrict__ UL = a.U[LEAF];
-  float* __restrict__ out = a.out;
-  const uint32_t c0 = (uint32_t)tl * 4;
-  auto ld = [&](const T* U, uint32_t row, int v) -> float4 {
-    return Row<T>::load(U + (uint64_t)row * R, c0 + (uint32_t)(v * G * 4));
-  };
-  auto rd = [&](uint32_t row, int v, float4 x) { red4(out + (uint64_t)row * R + c0 + v * G * 4, x); };
-
-  const uint64_t team = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) / G;
-  const bool active = team * chunk < a.nnz;
-  const uint64_t x0 = active ? team * chunk : a.nnz - 1;
-  const uint64_t x1 = active ? min(x0 + chunk, a.nnz) : x0;
-
-  // open slice: number sl, index ca, first nonzero of the next slice nxt
-  uint32_t sl;
-  if (a.cslc) {
-    sl = active ? __ldg(a.cslc + team) : nslc - 1;
-  } else {
-    uint32_t lo = 0, hi = nslc - 1;
-    while (lo < hi) {
-      const uint32_t m = (lo + hi + 1) >> 1;
-      if ((uint64_t)__ldg(snz + m) <= x0) lo = m; else hi = m - 1;
-    }
-    sl = lo;
-  }
-  uint32_t ca = __ldg(sidx + sl);
-  uint64_t nxt = __ldg(snz + sl + 1);
-  float4 acc[V], rowA[V];
-#pragma unroll
-  for (int v = 0; v < V; ++v) {
-    acc[v] = f4(0.f);
-    if constexpr (OUT == LEAF || MIDL) rowA[v] = ld(U0, ca, v);
-  }
-  [[maybe_unused]] uint32_t bopen = 0;  // middle level: the open fiber's row
-  if constexpr (MIDL) bopen = __ldg(mid + x0);
-
-  auto load_blk = [&](uint32_t itb, uint32_t& kk, uint32_t& bb, uint32_t& qq, float& vq) {
-    const uint64_t xx = x0 + itb + tl;
-    kk = 0;
-    bb = 0;
-    qq = 0;
-    vq = 0.f;
-    if (itb < chunk && xx < x1) {
-      kk = __ldg(leaf + xx);
-      bb = __ldg(mid + xx);
-      if constexpr (ND == 4) qq = __ldg(mid2 + xx);
-      vq = __ldg(vals + xx);
-    }
-  };
-  uint32_t kc, bc, qc, kn, bn, qn;
-  float vc, vn;
-  load_blk(0, kc, bc, qc, vc);
-  load_blk(G, kn, bn, qn, vn);
-  for (uint32_t it = 0; it < chunk; it += G) {
-    const uint64_t xb = x0 + it;
-    const uint32_t k = kc & ~FLAG, b = bc, q = qc;
-    const float vv = vc;
-    [[maybe_unused]] uint32_t fm = 0;  // middle level: nonzero j of the block opens a fiber
-    if constexpr (MIDL) fm = (__ballot_sync(FULL, (kc & FLAG) && (xb + tl != x0)) >> tb) & GMASK;
-    kc = kn; bc = bn; qc = qn; vc = vn;
-    load_blk(it + 2 * G, kn, bn, qn, vn);
-    // a slice starts inside this block for some team of the warp
-    const bool slow = __any_sync(FULL, xb < x1 && xb + G > nxt);
-
-    auto block = [&](auto slow_tag) {
-      constexpr bool SLOW = decltype(slow_tag)::value;
-#pragma unroll
-      for (int jb = 0; jb < G; jb += PF) {
-        [[maybe_unused]] float4 rc[(OUT == 0 || MIDL) ? PF : 1][V];
-        [[maybe_unused]] float4 rb[MIDL ? 1 : PF][V];
-        [[maybe_unused]] float4 rq[ND == 4 ? PF : 1][V];
-        [[maybe_unused]] uint32_t bjs[MIDL ? PF : 1];
-        uint32_t kj[PF];
-#pragma unroll
-        for (int j = 0; j < PF; ++j) {
-          kj[j] = __shfl_sync(FULL, k, tb + jb + j);
-          const uint32_t bj = __shfl_sync(FULL, b, tb + jb + j);
-          [[maybe_unused]] uint32_t qj = 0;
-          if constexpr (ND == 4) qj = __shfl_sync(FULL, q, tb + jb + j);
-          if constexpr (MIDL) bjs[j] = bj;
-#pragma unroll
-          for (int v = 0; v < V; ++v) {
-            if constexpr (MIDL) {
-              rc[j][v] = ld(UL, kj[j], v);
-            } else if constexpr (ND == 3) {
-              rb[j][v] = ld(U1, bj, v);
-            } else {
-              rb[j][v] = ld(U2, bj, v);  // level 2 (fiber index c)
-              rq[j][v] = ld(U1, qj, v);  // level 1 (fbrS index b)
-            }
-            if constexpr (OUT == 0) rc[j][v] = ld(UL, kj[j], v);
-          }
-        }
-#pragma unroll
-        for (int j = 0; j < PF; ++j) {
-          const float val = __shfl_sync(FULL, vv, tb + jb + j);
-          const uint64_t x = xb + jb + j;
-          if constexpr (MIDL) {
-            if ((fm >> (jb + j)) & 1u) {  // the open fiber ends before nonzero j (it is in the old slice)
-#pragma unroll
-              for (int v = 0; v < V; ++v) { rd(bopen, v, pmul(rowA[v], acc[v])); acc[v] = f4(0.f); }
-              bopen = bjs[j];
-            }
-          }
-          if constexpr (SLOW) {
-            if (x < x1 && x == nxt) {  // slice change (slices are never empty)
-              if constexpr (OUT == 0) {
-#pragma unroll
-                for (int v = 0; v < V; ++v) { rd(ca, v, acc[v]); acc[v] = f4(0.f); }
-              }
-              ++sl;
-              ca = __ldg(sidx + sl);
-              nxt = __ldg(snz + sl + 1);
-              if constexpr (OUT == LEAF || MIDL) {
-#pragma unroll
-                for (int v = 0; v < V; ++v) rowA[v] = ld(U0, ca, v);
-              }
-            }
-          }
-          if constexpr (MIDL) {
-#pragma unroll
-            for (int v = 0; v < V; ++v) acc[v] = pfma_s(val, rc[j][v], acc[v]);
-          } else if constexpr (OUT == 0) {
-#pragma unroll
-            for (int v = 0; v < V; ++v) {
-              float4 m = pmul_s(val, rb[j][v]);
-              if constexpr (ND == 4) m = pmul(m, rq[j][v]);
-              acc[v] = pfma(m, rc[j][v], acc[v]);
-            }
-          } else {
-            if (x < x1) {
-#pragma unroll
-              for (int v = 0; v < V; ++v) {
-                float4 m = pmul(rowA[v], rb[j][v]);
-                if constexpr (ND == 4) m = pmul(m, rq[j][v]);
-                rd(kj[j], v, pmul_s(val, m));
-              }
-            }
-          }
-        }
-      }
-    };
-    if (slow) block(std::true_type{});
-    else block(std::false_type{});
-  }
-  if constexpr (OUT == 0) {
-    if (active) {
-#pragma unroll
-      for (int v = 0; v < V; ++v) rd(ca, v, acc[v]);
-    }
-  }
-  if constexpr (MIDL) {
-    if (active) {
-#pragma unroll
-      for (int v = 0; v < V; ++v) rd(bopen, v, pmul(rowA[v], acc[v]));
-    }
-  }
-}
-
-// ---------------------------------------------------------------------------
-// Two outputs from one walk of a 3-D part (MM-CSF's reuse across modes): the
-// slice mode's MTTKRP, out[a] += v U1[b] (.) U2[k], and the middle mode's,
-// out2[b] += U0[a] (.) sum over the fiber (a, b) of v U2[k], share every
-// nonzero's gathers of U1[b] and U2[k]. Slice accumulation as in the
-// per-nonzero walk, fiber sums closed at the leaf-index flags with one vector
-// reduction per fiber; both outputs zeroed by the caller.
-template <int G, int V, class T, int MB, int PFX>
-__global__ void __launch_bounds__(256, MB) k_mttkrp_pair(const Args<T> a) {
-  constexpr uint32_t R = 4 * G * V;
-  constexpr uint32_t FLAG = 0x80000000u;
-  constexpr int PF = G > PFX ? PFX : G;
-  constexpr uint32_t GMASK = G == 32 ? FULL : ((1u << G) - 1u);
-  const int lane = threadIdx.x & 31;
-  const int tl = lane & (G - 1);
-  const int tb = lane - tl;
-  const float* __restrict__ vals = a.vals;
-  const uint32_t* __restrict__ leaf = a.leaf;
-  const uint32_t* __restrict__ mid = a.mid;
-  const uint32_t* __restrict__ snz = a.snz;
-  const uint32_t* __restrict__ sidx = a.sidx;
-  const uint32_t chunk = a.chunk, nslc = a.nslc;
-  const T* __restrict__ U0 = a.U[0];
-  const T* __restrict__ U1 = a.U[1];
-  const T* __restrict__ U2 = a.U[2];
-  float* __restrict__ out = a.out;
-  float* __restrict__ out2 = a.out2;
-  const uint32_t c0 = (uint32_t)tl * 4;
-  auto ld = [&](const T* U, uint32_t row, int v) -> float4 {
-    return Row<T>::load(U + (uint64_t)row * R, c0 + (uint32_t)(v * G * 4));
-  };
-  auto rd = [&](float* o, uint32_t row, int v, float4 x) { red4(o + (uint64_t)row * R + c0 + v * G * 4, x); };
-
-  const uint64_t team = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) / G;
-  const bool active = team * chunk < a.nnz;
-  const uint64_t x0 = active ? team * chunk : a.nnz - 1;
-  const uint64_t x1 = active ? min(x0 + chunk, a.nnz) : x0;
-  uint32_t sl;
-  if (a.cslc) {
-    sl = active ? __ldg(a.cslc + team) : nslc - 1;
-  } else {
-    uint32_t lo = 0, hi = nslc - 1;
-    while (lo < hi) {
-      const uint32_t m = (lo + hi + 1) >> 1;
-      if ((uint64_t)__ldg(snz + m) <= x0) lo = m; else hi = m - 1;
-    }
-    sl = lo;
-  }
-  uint32_t ca = __ldg(sidx + sl);
-  uint64_t nxt = __ldg(snz + sl + 1);
-  uint32_t bopen = __ldg(mid + x0);
-  float4 acc[V], accf[V], rowA[V];
-#pragma unroll
-  for (int v = 0; v < V; ++v) {
-    acc[v] = accf[v] = f4(0.f);
-    rowA[v] = ld(U0, ca, v);
-  }
-  auto load_blk = [&](uint32_t itb, uint32_t& kk, uint32_t& bb, float& vq) {
-    const uint64_t xx = x0 + itb + tl;
-    kk = 0;
-    bb = 0;
-    vq = 0.f;
-    if (itb < chunk && xx < x1) { kk = __ldg(leaf + xx); bb = __ldg(mid + xx); vq = __ldg(vals + xx); }
-  };
-  uint32_t kc, bc, kn, bn;
-  float vc, vn;
-  load_blk(0, kc, bc, vc);
-  load_blk(G, kn, bn, vn);
-  for (uint32_t it = 0; it < chunk; it += G) {
-    const uint64_t xb = x0 + it;
-    const uint32_t k = kc & ~FLAG, b = bc;
-    const float vv = vc;
-    const uint32_t fm = (__ballot_sync(FULL, (kc & FLAG) && (xb + tl != x0)) >> tb) & GMASK;
-    kc = kn; bc = bn; vc = vn;
-    load_blk(it + 2 * G, kn, bn, vn);
-    const bool slow = __any_sync(FULL, xb < x1 && xb + G > nxt);
-    auto block = [&](auto slow_tag) {
-      constexpr bool SLOW = decltype(slow_tag)::value;
-#pragma unroll
-      for (int jb = 0; jb < G; jb += PF) {
-        float4 rb[PF][V], rc[PF][V];
-        uint32_t bjs[PF];
-#pragma unroll
-        for (int j = 0; j < PF; ++j) {
-          const uint32_t kj = __shfl_sync(FULL, k, tb + jb + j);
-          bjs[j] = __shfl_sync(FULL, b, tb + jb + j);
-#pragma unroll
-          for (int v = 0; v < V; ++v) {
-            rb[j][v] = ld(U1, bjs[j], v);
-            rc[j][v] = ld(U2, kj, v);
-          }
-        }
-#pragma unroll
-        for (int j = 0; j < PF; ++j) {
-          const float val = __shfl_sync(FULL, vv, tb + jb + j);
-          const uint64_t x = xb + jb + j;
-          if ((fm >> (jb + j)) & 1u) {  // the open fiber ends before nonzero j (in the open slice)
-#pragma unroll
-            for (int v = 0; v < V; ++v) { rd(out2, bopen, v, pmul(rowA[v], accf[v])); accf[v] = f4(0.f); }
-            bopen = bjs[j];
-          }
-          if constexpr (SLOW) {
-            if (x < x1 && x == nxt) {
-#pragma unroll
-              for (int v = 0; v < V; ++v) { rd(out, ca, v, acc[v]); acc[v] = f4(0.f); }
-              ++sl;
-              ca = __ldg(sidx + sl);
-              nxt = __ldg(snz + sl + 1);
-#pragma unroll
-              for (int v = 0; v < V; ++v) rowA[v] = ld(U0, ca, v);
-            }
-          }
-#pragma unroll
-          for (int v = 0; v < V; ++v) {
-            acc[v] = pfma(pmul_s(val, rb[j][v]), rc[j][v], acc[v]);
-            accf[v] = pfma_s(val, rc[j][v], accf[v]);
-          }
-        }
-      }
-    };
-    if (slow) block(std::true_type{});
-    else block(std::false_type{});
-  }
-  if (active) {
-#pragma unroll
-    for (int v = 0; v < V; ++v) {
-      rd(out, ca, v, acc[v]);
-      rd(out2, bopen, v, pmul(rowA[v], accf[v]));
-    }
-  }
-}
-
-// The 4-D two-output walk: the slice mode's MTTKRP, out[a] += v U1[b] (.)
-// U2[c] (.) U3[k], and the level-1 mode's, out2[b] += U0[a] (.) sum over the
-// (a, b) group of v U2[c] (.) U3[k], from one walk that gathers each
-// nonzero's three rows once (b = mid2, c = mid, k = leaf). A group closes at a
-// leaf-fiber start whose b differs from the open one, or where a slice
-// starts; splits of one (a, b) group (the fbrS split) only add reductions.
-// Both outputs zeroed by the caller.
-template <int G, int V, class T, int MB, int PFX>
-__global__ void __launch_bounds__(256, MB) k_mttkrp_pair4(const Args<T> a) {
-  constexpr uint32_t R = 4 * G * V;
-  constexpr uint32_t FLAG = 0x80000000u;
-  constexpr int PF = G > PFX ? PFX : G;
-  constexpr uint32_t GMASK = G == 32 ? FULL : ((1u << G) - 1u);
-  const int lane = threadIdx.x & 31;
-  const int tl = lane & (G - 1);
-  const int tb = lane - tl;
-  const float* __restrict__ vals = a.vals;
-  const uint32_t* __restrict__ leaf = a.leaf;
-  const uint32_t* __restrict__ mid = a.mid;
-  const uint32_t* __restrict__ mid2 = a.mid2;
-  const uint32_t* __restrict__ snz = a.snz;
-  const uint32_t* __restrict__ sidx = a.sidx;
-  const uint32_t chunk = a.chunk, nslc = a.nslc;
-  const T* __restrict__ U0 = a.U[0];
-  const T* __restrict__ U1 = a.U[1];
-  const T* __restrict__ U2 = a.U[2];
-  const T* __restrict__ U3 = a.U[3];
-  float* __restrict__ out = a.out;
-  float* __restrict__ out2 = a.out2;
-  const uint32_t c0 = (uint32_t)tl * 4;
-  auto ld = [&](const T* U, uint32_t row, int v) -> float4 {
-    return Row<T>::load(U + (uint64_t)row * R, c0 + (uint32_t)(v * G * 4));
-  };
-  auto rd = [&](float* o, uint32_t row, int v, float4 x) { red4(o + (uint64_t)row * R + c0 + v * G * 4, x); };
-
-  const uint64_t team = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) / G;
-  const bool active = team * chunk < a.nnz;
-  const uint64_t x0 = active ? team * chunk : a.nnz - 1;
-  const uint64_t x1 = active ? min(x0 + chunk, a.nnz) : x0;
-  uint32_t sl;
-  if (a.cslc) {
-    sl = active ? __ldg(a.cslc + team) : nslc - 1;
-  } else {
-    uint32_t lo = 0, hi = nslc - 1;
-    while (lo < hi) {
-      const uint32_t m = (lo + hi + 1) >> 1;
-      if ((uint64_t)__ldg(snz + m) <= x0) lo = m; else hi = m - 1;
-    }
-    sl = lo;
-  }
-  uint32_t ca = __ldg(sidx + sl);
-  uint64_t nxt = __ldg(snz + sl + 1);
-  uint32_t bopen = __ldg(mid2 + x0);
-  float4 acc[V], accf[V], rowA[V];
-#pragma unroll
-  for (int v = 0; v < V; ++v) {
-    acc[v] = accf[v] = f4(0.f);
-    rowA[v] = ld(U0, ca, v);
-  }
-  auto load_blk = [&](uint32_t itb, uint32_t& kk, uint32_t& bb, uint32_t& cc, float& vq) {
-    const uint64_t xx = x0 + itb + tl;
-    kk = 0;
-    bb = 0;
-    cc = 0;
-    vq = 0.f;
-    if (itb < chunk && xx < x1) {
-      kk = __ldg(leaf + xx);
-      bb = __ldg(mid2 + xx);
-      cc = __ldg(mid + xx);
-      vq = __ldg(vals + xx);
-    }
-  };
-  uint32_t kc, bc, cc, kn, bn, cn;
-  float vc, vn;
-  load_blk(0, kc, bc, cc, vc);
-  load_blk(G, kn, bn, cn, vn);
-  for (uint32_t it = 0; it < chunk; it += G) {
-    const uint64_t xb = x0 + it;
-    const uint32_t k = kc & ~FLAG, b = bc, c = cc;
-    const float vv = vc;
-    const uint32_t fm = (__ballot_sync(FULL, (kc & FLAG) && (xb + tl != x0)) >> tb) & GMASK;
-    kc = kn; bc = bn; cc = cn; vc = vn;
-    load_blk(it + 2 * G, kn, bn, cn, vn);
-    const bool slow = __any_sync(FULL, xb < x1 && xb + G > nxt);
-    auto block = [&](auto slow_tag) {
-      constexpr bool SLOW = decltype(slow_tag)::value;
-#pragma unroll
-      for (int jb = 0; jb < G; jb += PF) {
-        float4 rb[PF][V], rc[PF][V], rk[PF][V];
-        uint32_t bjs[PF];
-#pragma unroll
-        for (int j = 0; j < PF; ++j) {
-          const uint32_t kj = __shfl_sync(FULL, k, tb + jb + j);
-          const uint32_t cj = __shfl_sync(FULL, c, tb + jb + j);
-          bjs[j] = __shfl_sync(FULL, b, tb + jb + j);
-#pragma unroll
-          for (int v = 0; v < V; ++v) {
-            rb[j][v] = ld(U1, bjs[j], v);
-            rc[j][v] = ld(U2, cj, v);
-            rk[j][v] = ld(U3, kj, v);
-          }
-        }
-#pragma unroll
-        for (int j = 0; j < PF; ++j) {
-          const float val = __shfl_sync(FULL, vv, tb + jb + j);
-          const uint64_t x = xb + jb + j;
-          if ((fm >> (jb + j)) & 1u) {
-            bool close = bjs[j] != bopen;
-            if constexpr (SLOW) close = close || (x < x1 && x == nxt);
-            if (close) {  // the open (a, b) group ends before nonzero j
-#pragma unroll
-              for (int v = 0; v < V; ++v) { rd(out2, bopen, v, pmul(rowA[v], accf[v])); accf[v] = f4(0.f); }
-              bopen = bjs[j];
-            }
-          }
-          if constexpr (SLOW) {
-            if (x < x1 && x == nxt) {
-#pragma unroll
-              for (int v = 0; v < V; ++v) { rd(out, ca, v, acc[v]); acc[v] = f4(0.f); }
-              ++sl;
-              ca = __ldg(sidx + sl);
-              nxt = __ldg(snz + sl + 1);
-#pragma unroll
-              for (int v = 0; v < V; ++v) rowA[v] = ld(U0, ca, v);
-            }
-          }
-#pragma unroll
-          for (int v = 0; v < V; ++v) {
-            const float4 u = pmul(rc[j][v], rk[j][v]);
-            acc[v] = pfma(pmul_s(val, rb[j][v]), u, acc[v]);
-            accf[v] = pfma_s(val, u, accf[v]);
-          }
-        }
-      }
-    };
-    if (slow) block(std::true_type{});
-    else block(std::false_type{});
-  }
-  if (active) {
-#pragma unroll
-    for (int v = 0; v < V; ++v) {
-      rd(out, ca, v, acc[v]);
-      rd(out2, bopen, v, pmul(rowA[v], accf[v]));
-    }
-  }
-}
-
-template <int G, int V, class T>
-cudaError_t launch_pair4(const Args<T>& a, int threads, int mb, cudaStream_t s) {
-  const uint64_t teams = (a.nnz + a.chunk - 1) / a.chunk;
-  const uint64_t blocks = (teams * G + threads - 1) / threads;
-  switch (mb) {
-    case 1: k_mttkrp_pair4<G, V, T, 1, 8><<<(unsigned)blocks, threads, 0, s>>>(a); break;
-    case 3: k_mttkrp_pair4<G, V, T, 2, 2><<<(unsigned)blocks, threads, 0, s>>>(a); break;
-    case 4: k_mttkrp_pair4<G, V, T, 3, 2><<<(unsigned)blocks, threads, 0, s>>>(a); break;
-    default: k_mttkrp_pair4<G, V, T, 2, 4><<<(unsigned)blocks, threads, 0, s>>>(a); break;
-  }
-  return cudaGetLastError();
-}
-
-template <int G, int V, class T>
-cudaError_t launch_pair(const Args<T>& a, int threads, int mb, cudaStream_t s) {
-  const uint64_t teams = (a.nnz + a.chunk - 1) / a.chunk;
-  const uint64_t blocks = (teams * G + threads - 1) / threads;
-  switch (mb) {
-    case 1: k_mttkrp_pair<G, V, T, 2, 8><<<(unsigned)blocks, threads, 0, s>>>(a); break;
-    case 3: k_mttkrp_pair<G, V, T, 4, 4><<<(unsigned)blocks, threads, 0, s>>>(a); break;
-    case 4: k_mttkrp_pair<G, V, T, 5, 4><<<(unsigned)blocks, threads, 0, s>>>(a); break;
-    default: k_mttkrp_pair<G, V, T, 3, 8><<<(unsigned)blocks, threads, 0, s>>>(a); break;
-  }
-  return cudaGetLastError();
-}
-
-template <int OUT, int G, int V, class T>
-cudaError_t launch_flat(const Args<T>& a, int threads, int mb, cudaStream_t s);
-
-// kern 2: the branch-free fiber walk with both outputs; otherwise the
-// per-nonzero form
-template <class T>
-cudaError_t launch_pair_R(const Args<T>& a, int nd, int threads, int mb, int kern, cudaStream_t s) {
-  if (nd == 4) {
-    switch (a.R) {
-      case 4: return launch_pair4<1, 1, T>(a, threads, mb, s);
-      case 8: return launch_pair4<2, 1, T>(a, threads, mb, s);
-      case 16: return launch_pair4<4, 1, T>(a, threads, mb, s);
-      case 32: return launch_pair4<8, 1, T>(a, threads, mb, s);
-      case 64: return launch_pair4<16, 1, T>(a, threads, mb, s);
-      case 128: return launch_pair4<32, 1, T>(a, threads, mb, s);
-      default: return cudaErrorInvalidValue;
-    }
-  }
-  if (kern == 2) {
-    switch (a.R) {
-      case 4: return launch_flat<3, 1, 1, T>(a, threads, mb, s);
-      case 8: return launch_flat<3, 2, 1, T>(a, threads, mb, s);
-      case 16: return launch_flat<3, 4, 1, T>(a, threads, mb, s);
-      case 32: return launch_flat<3, 8, 1, T>(a, threads, mb, s);
-      case 64: return launch_flat<3, 16, 1, T>(a, threads, mb, s);
-      case 128: return launch_flat<3, 32, 1, T>(a, threads, mb, s);
-      default: return cudaErrorInvalidValue;
-    }
-  }
-  switch (a.R) {
-    case 4: return launch_pair<1, 1, T>(a, threads, mb, s);
-    case 8: return launch_pair<2, 1, T>(a, threads, mb, s);
-    case 16: return launch_pair<4, 1, T>(a, threads, mb, s);
-    case 32: return launch_pair<8, 1, T>(a, threads, mb, s);
-    case 64: return launch_pair<16, 1, T>(a, threads, mb, s);
-    case 128: return launch_pair<32, 1, T>(a, threads, mb, s);
-    default: return cudaErrorInvalidValue;
-  }
-}
-
-template <int ND, int OUT, int G, int V, class T>
-cudaError_t launch_one(const Args<T>& a, int threads, int mb, cudaStream_t s) {
-  const uint64_t teams = (a.nnz + a.chunk - 1) / a.chunk;
-  const uint64_t thr = teams * G;
-  const uint64_t blocks = (thr + threads - 1) / threads;
-  switch (mb) {
-    case 1: k_mttkrp<ND, OUT, G, V, T, 3, 8><<<(unsigned)blocks, threads, 0, s>>>(a); break;
-    case 3: k_mttkrp<ND, OUT, G, V, T, 5, 4><<<(unsigned)blocks, threads, 0, s>>>(a); break;
-    case 4: k_mttkrp<ND, OUT, G, V, T, 6, 4><<<(unsigned)blocks, threads, 0, s>>>(a); break;
-    default: k_mttkrp<ND, OUT, G, V, T, 4, 8><<<(unsigned)blocks, threads, 0, s>>>(a); break;
-  }
-  return cudaGetLastError();
-}
-
-template <int OUT, int G, int V, class T>
-cudaError_t launch_flat(const Args<T>& a, int threads, int mb, cudaStream_t s) {
-  const uint64_t teams = (a.nnz + a.chunk - 1) / a.chunk;
-  const uint64_t thr = teams * G;
-  const uint64_t blocks = (thr + threads - 1) / threads;
-  switch (mb) {
-    case 1: k_mttkrp_flat<OUT, G, V, T, 2, 8><<<(unsigned)blocks, threads, 0, s>>>(a); break;
-    case 3: k_mttkrp_flat<OUT, G, V, T, 4, 4><<<(unsigned)blocks, threads, 0, s>>>(a); break;
-    case 4: k_mttkrp_flat<OUT, G, V, T, 5, 4><<<(unsigned)blocks, threads, 0, s>>>(a); break;
-    default: k_mttkrp_flat<OUT, G, V, T, 3, 8><<<(unsigned)blocks, threads, 0, s>>>(a); break;
-  }
-  return cudaGetLastError();
-}
-
-template <int ND, int OUT, int G, int V, class T>
-cudaError_t launch_rows(const Args<T>& a, int threads, int mb, cudaStream_t s) {
-  const uint64_t teams = (a.nnz + a.chunk - 1) / a.chunk;
-  const uint64_t thr = teams * G;
-  const uint64_t blocks = (thr + threads - 1) / threads;
-  switch (mb) {
-    case 1: k_mttkrp_rows<ND, OUT, G, V, T, 2, 8><<<(unsigned)blocks, threads, 0, s>>>(a); break;
-    case 3: k_mttkrp_rows<ND, OUT, G, V, T, 4, 4><<<(unsigned)blocks, threads, 0, s>>>(a); break;
-    case 4: k_mttkrp_rows<ND, OUT, G, V, T, 5, 4><<<(unsigned)blocks, threads, 0, s>>>(a); break;
-    default: k_mttkrp_rows<ND, OUT, G, V, T, 3, 8><<<(unsigned)blocks, threads, 0, s>>>(a); break;
-  }
-  return cudaGetLastError();
-}
-
-// kern: 1 = per-team fiber walk (k_mttkrp), 2 = branch-free walk (3-D only),
-// 3 = per-nonzero walk (slice and leaf levels of parts that carry `mid`)
-template <int ND, int G, int V, class T>
-cudaError_t launch_lvl(const Args<T>& a, int lvl, int kern, int threads, int mb, cudaStream_t s) {
-  if (kern == 3 && lvl == 0) return launch_rows<ND, 0, G, V, T>(a, threads, mb, s);
-  if (kern == 3 && lvl == ND - 1) return launch_rows<ND, ND - 1, G, V, T>(a, threads, mb, s);
-  if constexpr (ND == 3)
-    if (kern == 3 && lvl == 1) return launch_rows<3, 1, G, V, T>(a, threads, mb, s);
-  if constexpr (ND == 3) {
-    if (kern >= 2) {
-      switch (lvl) {
-        case 0: return launch_flat<0, G, V, T>(a, threads, mb, s);
-        case 1: return launch_flat<1, G, V, T>(a, threads, mb, s);
-        case 2: return launch_flat<2, G, V, T>(a, threads, mb, s);
-        default: return cudaErrorInvalidValue;
-      }
-    }
-  }
-  switch (lvl) {
-    case 0: return launch_one<ND, 0, G, V, T>(a, threads, mb, s);
-    case 1: return launch_one<ND, 1, G, V, T>(a, threads, mb, s);
-    case 2: return launch_one<ND, 2, G, V, T>(a, threads, mb, s);
-    default:
-      if constexpr (ND == 4) return launch_one<ND, 3, G, V, T>(a, threads, mb, s);
-      return cudaErrorInvalidValue;
-  }
-}
-
-template <class T>
-cudaError_t launch_R(const Args<T>& a, int nd, int lvl, int kern, int threads, int mb, cudaStream_t s) {
-#define MMCSF_RCASE(RR, GG, VV)                                                        \
-  case RR:                                                                            \
-    return nd == 3 ? launch_lvl<3, GG, VV, T>(a, lvl, kern, threads, mb, s)           \
-                   : launch_lvl<4, GG, VV, T>(a, lvl, kern, threads, mb, s);
-  switch (a.R) {
-    MMCSF_RCASE(4, 1, 1)
-    MMCSF_RCASE(8, 2, 1)
-    MMCSF_RCASE(16, 4, 1)
-    MMCSF_RCASE(32, 8, 1)
-    MMCSF_RCASE(64, 16, 1)
-    MMCSF_RCASE(128, 32, 1)
-    MMCSF_RCASE(256, 32, 2)
-    default: return cudaErrorInvalidValue;
-  }
-#undef MMCSF_RCASE
-}
 
 bool native_R(int R) { return R == 4 || R == 8 || R == 16 || R == 32 || R == 64 || R == 128 || R == 256; }
 int padded_R(int R) {
@@ -1231,7 +99,9 @@ int part_mttkrp(const mmcsf_format* F, const CsfPart& P, int mode, int R, int dt
   int threads = cfg && cfg->block_threads > 0 ? cfg->block_threads : 256;
   const int mb = cfg && cfg->min_blocks > 0 ? cfg->min_blocks : 2;
   int kern = cfg && cfg->kernel > 0 ? cfg->kernel : (P.nd == 3 ? 2 : 1);
-  if (kern < 1 || kern > 3) return set_error(MMCSF_ERR_INVALID, "kernel must be 0, 1, 2 or 3");
+  if (kern < 1 || kern > 4) return set_error(MMCSF_ERR_INVALID, "kernel must be 0, 1, 2, 3 or 4");
+  if (kern == 4 && (P.nd != 3 || lvl != 0)) kern = 3;  // per-fiber middle rows: the 3-D slice level only
+  if (kern == 4 && !P.mid.p) kern = 2;
   if (kern == 3 && (!P.mid.p || (P.nd == 4 && lvl != 0 && lvl != 3))) kern = 2;  // per-nonzero walk not applicable
   if (kern == 2 && P.nd == 4) kern = 1;                                         // no 4-D branch-free fiber walk
   const int slot = CsfPart::cfib_slot((uint64_t)chunk);
@@ -1426,7 +296,7 @@ extern "C" int mmcsf_mttkrp_pair(const mmcsf_format* F, int R, int factor_dtype,
   const int threads = cfg && cfg->block_threads > 0 ? cfg->block_threads : 256;
   const int mb = cfg && cfg->min_blocks > 0 ? cfg->min_blocks : (F->pair_mb ? F->pair_mb : 3);
   const int kern = cfg && cfg->kernel > 0 ? cfg->kernel : F->pair_kernel;
-  if (kern < 0 || kern > 3) return set_error(MMCSF_ERR_INVALID, "kernel must be 0, 1, 2 or 3");
+  if (kern < 0 || kern > 4) return set_error(MMCSF_ERR_INVALID, "kernel must be 0, 1, 2, 3 or 4");
   if (threads % 32 || threads > 256) return set_error(MMCSF_ERR_INVALID, "block_threads must be a multiple of 32, <= 256");
   const int slot = CsfPart::cfib_slot((uint64_t)chunk);
   cudaError_t e;
@@ -1580,11 +450,25 @@ extern "C" int mmcsf_tune(mmcsf_format* F, int R, int factor_dtype, const void* 
     const int m = F->impl == MMCSF_IMPL_MMCSF ? i : F->mode;
     float best = 1e30f;
     int bt = 1, bc = 512, bm = 2, bk = 1;
-    const int nkern = 3;
+    const int nkern = 4;
     for (int trav = 1; trav <= 2 && st == MMCSF_OK; ++trav) {
       if (trav == 2 && !F->views[m].present) continue;
       for (int kern = 1; kern <= nkern && st == MMCSF_OK; ++kern) {
       if (kern == 2 && F->nd == 4) continue;  // 4-D has no branch-free fiber walk
+      if (kern == 4) {  // per-fiber middle rows: only where the mode is the slice level of a 3-D part with `mid`
+        const CsfPart* tp = nullptr;
+        if (trav == 2) tp = &F->views[m];
+        else
+          for (int p = 0; p < F->nd; ++p)
+            if (F->parts[p].present) { tp = &F->parts[p]; break; }
+        if (!tp || tp->nd != 3 || tp->order[0] != m || !tp->mid.p) continue;
+        if (trav == 1 && F->impl == MMCSF_IMPL_MMCSF) {  // every partition must have m at level 0
+          bool all0 = true;
+          for (int p = 0; p < F->nd; ++p)
+            if (F->parts[p].present && F->parts[p].order[0] != m) all0 = false;
+          if (!all0) continue;
+        }
+      }
       for (int mbv = 1; mbv <= 4; ++mbv) {
         for (int c : chunks) {
           mmcsf_kernel_cfg cfg{};
@@ -1632,7 +516,7 @@ extern "C" int mmcsf_tune(mmcsf_format* F, int R, int factor_dtype, const void* 
       native_R(R) && R <= 128) {
     float bestp = 1e30f;
     int bpc = 0, bpm = 0, bpk = 0;
-    for (int kern : {2, 3})
+    for (int kern : {2, 3, 4})
     for (int mbv = 1; mbv <= 3 && st == MMCSF_OK && (kern == 3 || F->nd == 3); ++mbv)
       for (int c : {256, 512, 1024}) {
         mmcsf_kernel_cfg cfg{};
@@ -1686,14 +570,14 @@ extern "C" int mmcsf_set_plan(mmcsf_format* F, const mmcsf_plan* plan) {
     if (plan->traversal[m] == 2 && !F->views[m].present)
       return set_error(MMCSF_ERR_INVALID, "plan uses a view for mode %d that was not built", m);
     if (plan->traversal[m] < 0 || plan->traversal[m] > 2 || plan->chunk[m] < 0 || plan->kernel[m] < 0 ||
-        plan->kernel[m] > 3)
+        plan->kernel[m] > 4)
       return set_error(MMCSF_ERR_INVALID, "bad plan entry for mode %d", m);
     F->plan_traversal[m] = plan->traversal[m];
     F->plan_chunk[m] = plan->chunk[m];
     F->plan_mb[m] = plan->min_blocks[m];
     F->plan_kernel[m] = plan->kernel[m];
   }
-  if (plan->pair_chunk < 0 || plan->pair_min_blocks < 0 || plan->pair_kernel < 0 || plan->pair_kernel > 3)
+  if (plan->pair_chunk < 0 || plan->pair_min_blocks < 0 || plan->pair_kernel < 0 || plan->pair_kernel > 4)
     return set_error(MMCSF_ERR_INVALID, "bad pair entry");
   F->pair_use = plan->pair != 0;
   F->pair_chunk = plan->pair_chunk;

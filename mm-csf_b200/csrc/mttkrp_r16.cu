@@ -1,0 +1,4 @@
+// MTTKRP kernels instantiated for rank R = 16 (FP32 and BF16 factors).
+#include "mttkrp_kernels.cuh"
+
+MMCSF_INSTANTIATE_R(16)

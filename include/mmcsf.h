@@ -264,6 +264,13 @@ int mmcsf_set_plan(mmcsf_format* F, const mmcsf_plan* plan);
  * the same index stream. Every index must be below nrows. */
 int mmcsf_probe_gather(const uint32_t* d_idx, uint64_t n, const float* d_rows, uint64_t nrows, int R, int reps,
                        float* ms_out, void* stream);
+/* The same gather with the rows landed in shared memory by the copy engine
+ * (measurement; no counterpart in the reference): one bulk copy
+ * (cp.async.bulk) per row into a per-warp ring of `stages` x 32 rows, one
+ * mbarrier per stage, one block of `warps` warps per SM. R 16, 32 or 64;
+ * stages 2, 4 or 8. Returns MMCSF_ERR_TIMEOUT if a bounded wait gave up. */
+int mmcsf_probe_gather_tma(const uint32_t* d_idx, uint64_t n, const float* d_rows, uint64_t nrows, int R,
+                           int stages, int warps, int reps, float* ms_out, void* stream);
 
 /* ---- TTM ------------------------------------------------------------------
  * Replaces TTM_GPU / TTM_CPU (src/ttm_gpu.cu:83-143, src/ttm_cpu.cpp:60-86):
@@ -331,11 +338,16 @@ typedef struct {
   int precision;  /* MMCSF_CPD_* */
   int no_graph;   /* 1: run the BF16 form host-driven too */
   uint64_t seed;  /* initial factors uniform in [0,1) when d_init is NULL */
+  int profile;    /* 1: time every phase of every iteration with CUDA events (host-driven loop, also for
+                     BF16) into mmcsf_cpd_result.phase_ms; the events add a few microseconds per phase */
 } mmcsf_cpd_opts;
+#define MMCSF_CPD_PHASES 6 /* MTTKRP, solve (Hadamard + Cholesky/inverse), apply (M V^-1, column norms),
+                              lambda, finish (normalise, store, Gram, fit inner product), fit */
 typedef struct {
   int iters, converged, graph, launches; /* launches: kernels per iteration (graph) or in total */
   double fit;
   double seconds; /* device time of the iteration loop */
+  double phase_ms[MMCSF_CPD_PHASES]; /* with opts.profile: device time of each phase summed over the loop */
   double fit_history[MMCSF_CPD_MAX_HISTORY];
 } mmcsf_cpd_result;
 /* d_init (optional): FP32 initial factors (dims[m] x rank); d_factors_out

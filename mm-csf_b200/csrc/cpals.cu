@@ -456,34 +456,74 @@ struct Als {
     return MMCSF_OK;
   }
 
-  // one ALS iteration, stream-ordered (capturable)
-  int iteration(double xnormsq, cudaGraphConditionalHandle h, int use_handle) {
+  // Per-phase timing (opts.profile): an event at every phase boundary of one
+  // iteration, read back after the iteration.
+  struct Prof {
+    static constexpr int NEV = 4 * 6 + 2;  // up to 4 modes x 6 boundaries + fit
+    cudaEvent_t ev[NEV] = {};
+    int phase[NEV] = {};  // phase that ends at event i
+    int n = 0;
+    double ms[MMCSF_CPD_PHASES] = {};
+    bool ok = false;
+    int init() {
+      for (auto& e : ev) MMCSF_CUDA(cudaEventCreate(&e));
+      ok = true;
+      return MMCSF_OK;
+    }
+    ~Prof() {
+      if (ok)
+        for (auto& e : ev) cudaEventDestroy(e);
+    }
+    void mark(cudaStream_t s, int ph) {  // phase `ph` ends here (-1: start)
+      if (n < NEV) { cudaEventRecord(ev[n], s); phase[n] = ph; ++n; }
+    }
+    int collect() {  // after the stream has synchronised
+      for (int i = 1; i < n; ++i) {
+        float t = 0;
+        MMCSF_CUDA(cudaEventElapsedTime(&t, ev[i - 1], ev[i]));
+        if (phase[i] >= 0) ms[phase[i]] += t;
+      }
+      n = 0;
+      return MMCSF_OK;
+    }
+  };
+
+  // one ALS iteration, stream-ordered (capturable when prof is null)
+  int iteration(double xnormsq, cudaGraphConditionalHandle h, int use_handle, Prof* prof = nullptr) {
     const void* U[4];
     for (int m = 0; m < nd; ++m) U[m] = fac[m].p;
+    auto mark = [&](int ph) { if (prof) prof->mark(s, ph); };
+    mark(-1);
     MMCSF_CUDA(cudaMemsetAsync(inner.p, 0, MAXR * sizeof(double), s));
     for (int m = 0; m < nd; ++m) {
       const uint64_t rows = F->dims[m];
       MMCSF_TRY(mttkrp_mode(F, m, R, dtype, U, M.as<float>(), nullptr, s, &launches));
+      mark(0);
       k_solve<A><<<1, 256, solve_smem(), s>>>(grams.as<A>(), nd, m, R, Vinv.as<A>(), status.as<int>());
       MMCSF_LAUNCH_CHECK();
+      mark(1);
       MMCSF_CUDA(cudaMemsetAsync(colsq.p, 0, MAXR * sizeof(double), s));
       MMCSF_CUDA(cudaMemsetAsync(colmax.p, 0, MAXR * sizeof(unsigned), s));
       k_apply<A><<<grid_for(rows * (uint64_t)R, 256), 256, 0, s>>>(M.as<float>(), rows, R, Vinv.as<A>(),
                                                                    Ut.as<float>(), colsq.as<double>(),
                                                                    colmax.as<unsigned>());
       MMCSF_LAUNCH_CHECK();
+      mark(2);
       k_lambda<<<1, 64, 0, s>>>(colsq.as<double>(), colmax.as<unsigned>(), R, st.as<State>(), lambda.as<double>());
       MMCSF_LAUNCH_CHECK();
+      mark(3);
       MMCSF_CUDA(cudaMemsetAsync(grams.as<A>() + (size_t)m * R * R, 0, (uint64_t)R * R * sizeof(A), s));
       k_finish<T, A><<<std::min<uint64_t>(grid_for(rows, 32), (uint64_t)sm_count() * 4), 256, 0, s>>>(
           Ut.as<float>(), rows, R, lambda.as<double>(), fac[m].as<T>(), grams.as<A>() + (size_t)m * R * R,
           m == nd - 1 ? M.as<float>() : nullptr, inner.as<double>());
       MMCSF_LAUNCH_CHECK();
+      mark(4);
       launches += 4;
     }
     k_fit<A><<<1, 256, 0, s>>>(grams.as<A>(), nd, R, lambda.as<double>(), inner.as<double>(), xnormsq, tol, maxit,
                                st.as<State>(), hist.as<double>(), h, use_handle);
     MMCSF_LAUNCH_CHECK();
+    mark(5);
     ++launches;
     return MMCSF_OK;
   }
@@ -531,7 +571,9 @@ int run_cpd(mmcsf_format* F, const mmcsf_cpd_opts* o, const float* const* d_init
   State hst{};
   int graph_used = 0;
   MMCSF_CUDA(cudaEventRecord(e0, s));
-  if (o->precision == MMCSF_CPD_BF16 && !o->no_graph) {
+  typename Als<T, A>::Prof prof;
+  if (o->profile) MMCSF_TRY(prof.init());
+  if (o->precision == MMCSF_CPD_BF16 && !o->no_graph && !o->profile) {
     // the whole loop as one graph: WHILE node, body = one iteration
     cudaGraph_t g = nullptr;
     cudaGraphExec_t ge = nullptr;
@@ -567,9 +609,10 @@ int run_cpd(mmcsf_format* F, const mmcsf_cpd_opts* o, const float* const* d_init
     graph_used = 1;
   } else {
     for (int it = 0; it < als.maxit; ++it) {
-      MMCSF_TRY(als.iteration(xnormsq, cudaGraphConditionalHandle{}, 0));
+      MMCSF_TRY(als.iteration(xnormsq, cudaGraphConditionalHandle{}, 0, o->profile ? &prof : nullptr));
       MMCSF_CUDA(cudaMemcpyAsync(&hst, als.st.p, sizeof(State), cudaMemcpyDeviceToHost, s));
       MMCSF_CUDA(cudaStreamSynchronize(s));
+      if (o->profile) MMCSF_TRY(prof.collect());
       if (!hst.keep_going) break;
     }
   }
@@ -588,6 +631,7 @@ int run_cpd(mmcsf_format* F, const mmcsf_cpd_opts* o, const float* const* d_init
     res->seconds = ms / 1e3;
     res->graph = graph_used;
     res->launches = als.launches;
+    for (int p = 0; p < MMCSF_CPD_PHASES; ++p) res->phase_ms[p] = o->profile ? prof.ms[p] : 0.0;
     const int nh = std::min(hst.iter, MMCSF_CPD_MAX_HISTORY);
     if (nh > 0) MMCSF_CUDA(cudaMemcpy(res->fit_history, als.hist.p, nh * sizeof(double), cudaMemcpyDeviceToHost));
   }

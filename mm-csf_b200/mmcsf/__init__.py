@@ -8,6 +8,7 @@ import ctypes
 
 import numpy as np
 
+from . import _lib
 from ._lib import (BuildOpts, CpdOpts, CpdResult, GenSpec, KernelCfg, MmcsfError, PartInfo, Plan, c_f32p, c_u32p, c_u64, c_u64p, c_voidp,
                    check, lib)
 
@@ -452,12 +453,14 @@ class Format:
             pl.kernel[m] = e.get("kernel", 0)
         check(lib().mmcsf_set_plan(self._h, ctypes.byref(pl)))
 
-    def cpd(self, rank, max_iters=10, tol=1e-5, precision="fp32", init=None, seed=0, graph=True, stream=None):
+    def cpd(self, rank, max_iters=10, tol=1e-5, precision="fp32", init=None, seed=0, graph=True, stream=None,
+            profile=False):
         """CP-ALS on the device (mmcsf_cpd). precision: "fp32" (FP32 factors and
         small-matrix math, host-driven), "bf16" (BF16 factors, FP64 solve/fit,
         one CUDA graph for the loop unless graph=False) or "fp64solve".
-        init: optional list of FP32 CUDA tensors (dims[m] x rank). Returns a
-        dict with fit, iters, converged, seconds, history, lambda, factors."""
+        init: optional list of FP32 CUDA tensors (dims[m] x rank). profile:
+        time every phase (host-driven loop). Returns a dict with fit, iters,
+        converged, seconds, history, lambda, factors (and phase_ms)."""
         import torch
         prec = {"fp32": 0, "bf16": 1, "fp64solve": 2}[precision]
         o = CpdOpts()
@@ -467,6 +470,7 @@ class Format:
         o.precision = prec
         o.no_graph = 0 if graph else 1
         o.seed = int(seed)
+        o.profile = 1 if profile else 0
         dev = init[0].device if init is not None else torch.device("cuda")
         outs = [torch.empty((d, rank), dtype=torch.float32, device=dev) for d in self.dims]
         ip = None
@@ -484,7 +488,8 @@ class Format:
         return {"fit": res.fit, "iters": res.iters, "converged": bool(res.converged), "seconds": res.seconds,
                 "graph": bool(res.graph), "launches": res.launches,
                 "history": [res.fit_history[i] for i in range(min(res.iters, len(res.fit_history)))],
-                "lambda": np.array([lam[i] for i in range(rank)]), "factors": outs}
+                "lambda": np.array([lam[i] for i in range(rank)]), "factors": outs,
+                "phase_ms": ({n: res.phase_ms[i] for i, n in enumerate(_lib.CPD_PHASE_NAMES)} if profile else None)}
 
     # -- sampled model and adjoint ------------------------------------------
     def partitioning(self):

@@ -52,15 +52,18 @@ class Plan(ctypes.Structure):
 
 class CpdOpts(ctypes.Structure):
     _fields_ = [("rank", c_int), ("max_iters", c_int), ("tol", ctypes.c_double), ("precision", c_int),
-                ("no_graph", c_int), ("seed", c_u64)]
+                ("no_graph", c_int), ("seed", c_u64), ("profile", c_int)]
 
 
 CPD_MAX_HISTORY = 1000
+CPD_PHASES = 6
+CPD_PHASE_NAMES = ("mttkrp", "solve", "apply", "lambda", "finish", "fit")
 
 
 class CpdResult(ctypes.Structure):
     _fields_ = [("iters", c_int), ("converged", c_int), ("graph", c_int), ("launches", c_int),
                 ("fit", ctypes.c_double), ("seconds", ctypes.c_double),
+                ("phase_ms", ctypes.c_double * CPD_PHASES),
                 ("fit_history", ctypes.c_double * CPD_MAX_HISTORY)]
 
 
@@ -108,6 +111,8 @@ SIGNATURES = {
     "mmcsf_format_values": ([c_voidp, ctypes.POINTER(c_voidp), c_u64p], c_int),
     "mmcsf_probe_gather": ([c_voidp, c_u64, c_voidp, c_u64, c_int, c_int, ctypes.POINTER(ctypes.c_float), c_voidp],
                            c_int),
+    "mmcsf_probe_gather_tma": ([c_voidp, c_u64, c_voidp, c_u64, c_int, c_int, c_int, c_int,
+                                ctypes.POINTER(ctypes.c_float), c_voidp], c_int),
     "mmcsf_coo_write_bin": ([c_voidp, ctypes.c_char_p], c_int),
     "mmcsf_coo_load_bin": ([ctypes.c_char_p, ctypes.POINTER(c_voidp)], c_int),
     "mmcsf_poisson_step": ([c_voidp, c_int, c_int, ctypes.POINTER(c_voidp), ctypes.c_float, c_voidp, c_voidp,

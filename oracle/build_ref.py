@@ -38,6 +38,10 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 OUT_DIR = os.path.join(HERE, "_ref")
 OUT_LIB = os.path.join(OUT_DIR, "libmmcsf_ref.so")
 OUT_LIB_HEUR = os.path.join(OUT_DIR, "libmmcsf_ref_heur.so")
+OUT_LIB_GPU = os.path.join(OUT_DIR, "libmmcsf_ref_gpu.so")
+GPU_FILES = ["util.h", "mttkrp_gpu.h", "mttkrp_gpu.cu"]
+NVCC_WARN_RE = re.compile(r"^(?P<file>[^(\s]+)\((?P<line>\d+)\): warning #940-D: missing return statement")
+NVCCFLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-std=c++14", "-Xcompiler", "-fPIC,-fopenmp"]
 OVERRIDE_RE = re.compile(r"^(\s*)mode = 2;\s*$")
 # The reference checkout: $MMCSF_REFERENCE (its root) when set, else a
 # directory named `reference` beside this repository.
@@ -85,6 +89,76 @@ def _patch_missing_returns(build, stderr):
         with open(path, "w") as fh:
             fh.writelines(lines)
     return n
+
+
+def _patch_nvcc_missing_returns(build, stderr):
+    """The same `return 0;` patch for the sites nvcc reports (warning #940,
+    at the function's closing brace)."""
+    sites = {}
+    for line in stderr.splitlines():
+        m = NVCC_WARN_RE.match(line)
+        if m:
+            sites.setdefault(os.path.basename(m.group("file")), set()).add(int(m.group("line")))
+    n = 0
+    for fname, lns in sites.items():
+        path = os.path.join(build, fname)
+        if not os.path.exists(path):
+            continue
+        with open(path) as fh:
+            lines = fh.readlines()
+        for ln in sorted(lns, reverse=True):
+            li = ln - 1
+            while li < len(lines):
+                j = lines[li].find("}")
+                if j >= 0:
+                    lines[li] = lines[li][:j] + "return 0; " + lines[li][j:]
+                    n += 1
+                    break
+                li += 1
+        with open(path, "w") as fh:
+            fh.writelines(lines)
+    return n
+
+
+def build_gpu(src=DEFAULT_SRC, force=False, verbose=True):
+    """The reference's GPU MTTKRP (src/mttkrp_gpu.cu, all of its kernels and
+    drivers) compiled for sm_100a with nvcc, plus oracle/ref_gpu_harness.cu,
+    into oracle/_ref/libmmcsf_ref_gpu.so, from a scratch copy with the same
+    missing-return patch."""
+    if not os.path.isdir(src):
+        raise FileNotFoundError(f"reference sources not found at {src}")
+    if os.path.exists(OUT_LIB_GPU) and not force:
+        return OUT_LIB_GPU
+    os.makedirs(OUT_DIR, exist_ok=True)
+    build_dir = tempfile.mkdtemp(prefix="mmcsf_ref_gpu_build_")
+    try:
+        for f in GPU_FILES:
+            shutil.copy(os.path.join(src, f), os.path.join(build_dir, f))
+            os.chmod(os.path.join(build_dir, f), 0o644)
+        units = [(os.path.join(build_dir, "mttkrp_gpu.cu"), os.path.join(build_dir, "mttkrp_gpu.o")),
+                 (os.path.join(HERE, "ref_gpu_harness.cu"), os.path.join(build_dir, "harness.o"))]
+        total = 0
+        for _ in range(4):
+            patched = 0
+            for srcf, obj in units:
+                cmd = ["nvcc"] + NVCCFLAGS + ["-I", build_dir, "-I", os.path.join(HERE, "shim"), "-c", srcf, "-o", obj]
+                p = subprocess.run(cmd, cwd=build_dir, capture_output=True, text=True)
+                if p.returncode != 0:
+                    raise RuntimeError(f"compiling {srcf} failed:\n{p.stderr[-4000:]}")
+                patched += _patch_nvcc_missing_returns(build_dir, p.stderr)
+            total += patched
+            if patched == 0:
+                break
+        else:
+            raise RuntimeError("missing-return patching did not converge")
+        cmd = ["nvcc", "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-Xcompiler", "-fopenmp", "-o",
+               OUT_LIB_GPU] + [o for _, o in units] + ["-lgomp"]
+        subprocess.run(cmd, check=True, cwd=build_dir)
+        if verbose:
+            print(f"built {OUT_LIB_GPU} ({total} missing-return sites patched in the scratch copy)")
+        return OUT_LIB_GPU
+    finally:
+        shutil.rmtree(build_dir, ignore_errors=True)
 
 
 def _remove_partition_override(build):
@@ -159,12 +233,13 @@ def build(src=DEFAULT_SRC, force=False, verbose=True, variant="shipped"):
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
-    ap.add_argument("--src", default=os.environ.get("MMCSF_REFERENCE_SRC", DEFAULT_SRC))
+    ap.add_argument("--src", default=DEFAULT_SRC)
     ap.add_argument("--force", action="store_true")
     a = ap.parse_args()
     try:
         build(a.src, a.force)
         build(a.src, a.force, variant="heuristic")
+        build_gpu(a.src, a.force)
     except Exception as e:  # noqa: BLE001
         print(f"reference build failed: {e}", file=sys.stderr)
         sys.exit(1)

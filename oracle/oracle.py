@@ -497,3 +497,55 @@ def generate(dims, nnz, dist, zipf_s=1.0, val_dist=0, seed=0, threads=0):
     if rc != 0:
         raise RuntimeError(f"orc_generate failed ({rc})")
     return inds, vals
+
+
+# --------------------------------------------------------------------------
+# The reference's own GPU MTTKRP (src/mttkrp_gpu.cu:3380-3784), built for
+# sm_100a as oracle/_ref/libmmcsf_ref_gpu.so by oracle/build_ref.py.
+# --------------------------------------------------------------------------
+_REF_GPU_LIB = os.path.join(HERE, "_ref", "libmmcsf_ref_gpu.so")
+_ref_gpu = None
+
+
+def ref_gpu_available():
+    return os.path.exists(_REF_GPU_LIB)
+
+
+def ref_gpu_lib():
+    global _ref_gpu
+    if _ref_gpu is None:
+        _ref_gpu = ctypes.CDLL(_REF_GPU_LIB)
+    return _ref_gpu
+
+
+def ref_mihcsr_gpu(dims, R, part, mode_order, fbr_ptr, fbr_idx, fbr_like, leaf, vals, warp_per_slice=4,
+                   tb_size=128, fiber_per_warp=1):
+    """Run MTTKRP_MIHCSR_GPU on one MM-CSF partition given by the reference's
+    arrays (fbr_ptr / fbr_idx per level, fbrLikeSlcInds, the leaf index of
+    every nonzero, values), with the reference's constant factors U[m] = m +
+    0.5 and its -w / -b / -s. Returns (Total GPU time in ms as it prints it, the
+    last mode's output)."""
+    nd = len(dims)
+    u64 = ctypes.c_uint64
+    P = ctypes.POINTER(u64)
+    fp = [np.ascontiguousarray(a, dtype=np.uint64) for a in fbr_ptr]
+    fi = [np.ascontiguousarray(a, dtype=np.uint64) for a in fbr_idx]
+    nfib = len(fp[-1])
+    like = np.ascontiguousarray(fbr_like, dtype=np.uint64)
+    if len(like) < nfib:  # the reference's copy reads nFibers entries; the last one it leaves unset
+        like = np.concatenate([like, np.full(nfib - len(like), like[-1] if len(like) else 0, np.uint64)])
+    lf = np.ascontiguousarray(leaf, dtype=np.uint64)
+    v = np.ascontiguousarray(vals, dtype=np.float32)
+    out = np.zeros((dims[-1], R), np.float32)
+    ms = ctypes.c_double()
+    rc = ref_gpu_lib().ref_mihcsr_gpu(
+        nd, (u64 * nd)(*[int(d) for d in dims]), int(R), int(warp_per_slice), int(tb_size), int(fiber_per_warp),
+        int(part),
+        (ctypes.c_int * nd)(*[int(m) for m in mode_order]), (P * (nd - 1))(*[a.ctypes.data_as(P) for a in fp]),
+        (u64 * (nd - 1))(*[len(a) for a in fp]), (P * (nd - 1))(*[a.ctypes.data_as(P) for a in fi]),
+        (u64 * (nd - 1))(*[len(a) for a in fi]), like.ctypes.data_as(P), u64(nfib),
+        (P * nd)(*[lf.ctypes.data_as(P)] * nd), v.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), u64(len(v)),
+        out.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), ctypes.byref(ms))
+    if rc != 0:
+        raise RuntimeError(f"ref_mihcsr_gpu failed ({rc})")
+    return ms.value, out

@@ -41,6 +41,12 @@ also       = format_build_ms (device construction), bf16_factors (the step
              partition_heuristic (the same step on the partitions the
              reference's heuristic picks, partition_rule 1).
 
+--gpus N > 1 (torchrun) = ONE tensor row-sharded across the ranks: every
+             mode's rows are split by nonzero count, each rank runs the
+             MTTKRP of its rows of every mode on single-mode CSFs of its
+             shards, no collective in the step (mmcsf.dist; strong scaling,
+             max over ranks). --sharded runs that path on one GPU too.
+
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 """
 import argparse
@@ -100,6 +106,8 @@ def parse():
     ap.add_argument("--no-r64", action="store_true", help="skip the R=64 section of the skewed 3-D workload")
     ap.add_argument("--no-config1", action="store_true", help="skip the 1000^3 uniform (config 1) section")
     ap.add_argument("--no-4d", action="store_true", help="skip the 4-D (B-CSF / HB-CSF / MM-CSF) section")
+    ap.add_argument("--sharded", action="store_true",
+                    help="run the row-sharded multi-GPU path (the default for --gpus N > 1) also on one GPU")
     return ap.parse_args()
 
 
@@ -849,6 +857,127 @@ def skewed4d_section(steps, warmup, seed, hbm_peak, peak_kind):
     return out
 
 
+def sharded_arm(a, W, config, world, rank, local):
+    """--gpus N > 1 (or --sharded): ONE tensor (the same seeded tensor on
+    every rank) with every mode's rows split across the ranks (mmcsf.dist
+    ShardedMttkrp: each rank runs, for every mode, the MTTKRP of its owned
+    rows on a single-mode CSF of its shard; no exchange in the step). Total
+    work is fixed as N grows (strong scaling); value = the workload's
+    algorithmic bytes (the single-GPU definition) / the step time, max over
+    ranks."""
+    import torch
+    import torch.distributed as dist
+    import mmcsf
+    from mmcsf import dist as D
+    dims, nd = W["dims"], len(W["dims"])
+    nnz = a.nnz or W["nnz"]
+    R = a.rank or W["R"]
+    hbm_peak, peak_kind = peaks()
+    X = mmcsf.CooTensor.generate(dims, nnz, dist=W["dist"], zipf_s=W["zipf"], val_dist=W["val"], seed=a.seed)
+    inds_dev, vals_dev = device_coo(X)
+    order = [2] + sorted([m for m in range(nd) if m != 2], key=lambda m: (dims[m], m))
+    rows, nfib = workload_stats(inds_dev, dims, order)
+    step_bytes = sum(mode_bytes(nd, dims, m, R, 4, struct_bytes(nd, nnz, nfib, 0), rows) for m in range(nd))
+    del X
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    sm = D.ShardedMttkrp(dims, inds_dev, vals_dev, device="cuda")
+    torch.cuda.synchronize()
+    build_ms = (time.perf_counter() - t0) * 1e3
+    del inds_dev, vals_dev
+    torch.cuda.empty_cache()
+    g = torch.Generator(device="cuda").manual_seed(1234)
+    U = [torch.rand(d, R, device="cuda", generator=g) for d in dims]
+    slabs = [torch.empty(max(1, hi - lo), R, device="cuda") for lo, hi in sm.rows]
+    sm.tune(U)
+    stream = torch.cuda.current_stream()
+    units = [((m,), lambda m=m: sm.local(m, U, out=slabs[m][:sm.rows[m][1] - sm.rows[m][0]])) for m in range(nd)]
+    for _ in range(a.warmup):
+        for _, fn in units:
+            fn()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    sampler = ClockSampler(local) if rank == 0 else None
+    if sampler:
+        sampler.start()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    unit_ms, total_ms = time_units(units, a.steps, stream)
+    if world > 1:
+        dist.barrier()
+    clocks = sampler.stop() if sampler else None
+    tmax = torch.tensor([total_ms], device="cuda")
+    if world > 1:
+        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+    total_ms = float(tmax.item())
+    ms_per_step = total_ms / a.steps
+    value = step_bytes * a.steps / (total_ms / 1e3) / 1e9
+    # e2e: every factor up from pinned host memory (the shards read rows of
+    # all of them), every owned output slab down, per step
+    hU = [u.cpu().pin_memory() for u in U]
+    hO = [torch.empty(s_.shape).pin_memory() for s_ in slabs]
+    dU = [torch.empty_like(u) for u in U]
+
+    def e2e_step():
+        for h, d in zip(hU, dU):
+            d.copy_(h, non_blocking=True)
+        for m in range(nd):
+            lo, hi = sm.rows[m]
+            sm.local(m, dU, out=slabs[m][:hi - lo])
+            hO[m].copy_(slabs[m], non_blocking=True)
+    for _ in range(2):
+        e2e_step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ke = max(1, min(a.steps, 10))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(ke):
+        e2e_step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    em = torch.tensor([e0.elapsed_time(e1) / ke], device="cuda")
+    if world > 1:
+        dist.all_reduce(em, op=dist.ReduceOp.MAX)
+    e_ms = float(em.item())
+    hb = sum(d * R * 4 for d in dims)
+    db = sum(s_.numel() * 4 for s_ in slabs)
+    shard_info = torch.tensor([float(x) for x in sm.shard_nnz], device="cuda")
+    all_info = [torch.zeros_like(shard_info) for _ in range(world)] if world > 1 else [shard_info]
+    if world > 1:
+        dist.all_gather(all_info, shard_info)
+    if rank == 0:
+        di = max(range(nd), key=lambda i: unit_ms[i])
+        # the dominant launch's share of the workload's bytes: its mode's bytes x the shard's share of nonzeros
+        ub = mode_bytes(nd, dims, di, R, 4, struct_bytes(nd, nnz, nfib, 0), rows) * sm.shard_nnz[di] / nnz
+        achieved = ub / (unit_ms[di] / 1e3) / 1e9
+        line = {"metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": a.steps,
+                "warmup": a.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "strong",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded device generator)",
+                "config": dict(config, parallelism=f"row-sharded x{world}: every mode's rows split across the ranks "
+                                                   f"by nonzero count, each rank's MTTKRP writes only its rows (no "
+                                                   f"collective in the step)"),
+                "format_build_ms": build_ms,
+                "units": [{"modes": [m], "ms": t, "rank": 0, "shard_nnz": sm.shard_nnz[m]} for m, t in
+                          zip(range(nd), unit_ms)],
+                "shard_nnz_per_rank": [[int(x) for x in t.tolist()] for t in all_info],
+                "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                             "frac": achieved / hbm_peak, "traffic": None,
+                             "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                             "kernel": f"rank 0, mode {di} on its B-CSF shard (bytes: the mode's share by nonzeros)",
+                             "algorithmic_bytes": ub, "avg_ms": unit_ms[di]},
+                "cpu_baseline": None,
+                "e2e": {"value": step_bytes / (e_ms / 1e3) / 1e9, "unit": "GB/s", "ms_per_step": e_ms,
+                        "h2d_bytes_per_step": hb, "d2h_bytes_per_step": db},
+                "gpu_launches": nd * a.steps, "clocks": clocks}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
 def main():
     a = parse()
     W = WORKLOADS[a.workload]
@@ -865,7 +994,7 @@ def main():
               "format": f"MM-CSF (-t 12, -m 0), views={a.views}",
               "fiber_threshold": a.fiber_threshold or "none", "factor_dtype": a.dtype,
               "l2": "inputs larger than L2 (structure > 800 MB per step)", "seed": a.seed,
-              "parallelism": f"replicas x{world} (each rank its own tensor)"}
+              "parallelism": "single GPU"}
     if a.impl == "reference":
         if rank == 0:
             reference_arm(a, W, config)
@@ -881,9 +1010,12 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     else:
         torch.cuda.set_device(0)
+    if world > 1 or a.sharded:
+        sharded_arm(a, W, config, world, rank, local)
+        return
     import mmcsf
     X = mmcsf.CooTensor.generate(dims, nnz, dist=W["dist"], zipf_s=W["zipf"], val_dist=W["val"],
-                                 seed=a.seed + rank)
+                                 seed=a.seed)
     torch.cuda.synchronize()
     tb0 = time.perf_counter()
     F = mmcsf.Format(X, impl=mmcsf.IMPL_MMCSF, mode=0, fiber_threshold=a.fiber_threshold, views=a.views)

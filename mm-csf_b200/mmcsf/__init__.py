@@ -80,6 +80,20 @@ class CooTensor:
         return cls(h)
 
     @classmethod
+    def from_device(cls, dims, inds, vals, stream=None):
+        """Copy device arrays (torch CUDA tensors: int32/uint32 indices per
+        mode, float32 values) into a new handle (mmcsf_coo_create_device)."""
+        nd = len(dims)
+        d = (c_u64 * nd)(*[int(x) for x in dims])
+        ind = [i.contiguous() for i in inds]
+        v = vals.contiguous()
+        ptrs = (c_voidp * nd)(*[ctypes.c_void_p(i.data_ptr()) for i in ind])
+        h = c_voidp()
+        check(lib().mmcsf_coo_create_device(nd, d, c_u64(int(v.numel())), ptrs, ctypes.c_void_p(v.data_ptr()),
+                                            _stream(stream), ctypes.byref(h)))
+        return cls(h)
+
+    @classmethod
     def generate(cls, dims, nnz, dist=DIST_UNIFORM, zipf_s=1.0, val_dist=VAL_UNIFORM01, seed=0, stream=None,
                  planted_rank=0, noise=0.0, poisson=False):
         """Seeded synthetic tensor generated on the device (see mmcsf_generate).

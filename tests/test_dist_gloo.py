@@ -1,7 +1,10 @@
-"""Sharded one-tensor MTTKRP and CP-ALS across ranks (mmcsf.dist), run as two
-gloo processes on the CPU. The per-rank compute is the FP64 COO MTTKRP of the
-oracle on that rank's shard (the CUDA kernels are covered by the GPU tests);
-what is tested here is the sharding, the exchange and the replicated solve."""
+"""Sharded one-tensor MTTKRP and CP-ALS across ranks (mmcsf.dist): every rank
+owns a row range of every mode. Run as two and three gloo processes on the
+CPU. The per-rank compute is the FP64 COO MTTKRP of the oracle on that rank's
+shard of the mode (the CUDA kernels are covered by the GPU tests); what is
+tested here is the sharding (ranges tile every mode, every nonzero in exactly
+one shard per mode), the exchange (all-gather of owned rows, all-reduced
+Grams and norms) and the replicated solve."""
 import os
 import socket
 import sys
@@ -43,15 +46,16 @@ def _free_port():
     return port
 
 
-def _local_fn(sm):
-    def f(mode, factors):
-        U = [t.detach().cpu().numpy().astype(np.float64) for t in factors]
-        return torch.tensor(CO.mttkrp64(sm.dims, sm.inds, sm.vals, mode, U), dtype=torch.float32)
-    return f
-
-
-class _Box:  # lets the local function see the ShardedMttkrp it serves
-    sm = None
+def _local_fn(sm, mode, factors):
+    """This rank's rows of mode `mode` from the FP64 oracle on the rank's
+    shard of that mode (the shard's mode index is rebased to the row range)."""
+    lo, hi = sm.owned(mode)
+    si, sv = sm.shards[mode]
+    dims = list(sm.dims)
+    dims[mode] = hi - lo
+    U = [t.detach().cpu().numpy().astype(np.float64) for t in factors]
+    U[mode] = np.zeros((hi - lo, U[mode].shape[1]))
+    return torch.tensor(CO.mttkrp64(dims, si, sv, mode, U), dtype=torch.float32)
 
 
 def _worker(rank, world, port, what, seed):
@@ -61,9 +65,7 @@ def _worker(rank, world, port, what, seed):
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
     try:
         dims, inds, vals = _tensor(seed, planted=4 if what == "als" else 0)
-        box = _Box()
-        sm = D.ShardedMttkrp(dims, inds, vals, local_mttkrp=lambda m, f: _local_fn(box.sm)(m, f))
-        box.sm = sm
+        sm = D.ShardedMttkrp(dims, inds, vals, local_mttkrp=_local_fn)
         rng = np.random.default_rng(seed + 1)
         R = 4
         U = [rng.random((d, R)).astype(np.float32) for d in dims]
@@ -74,14 +76,21 @@ def _worker(rank, world, port, what, seed):
                 want = CO.mttkrp64(dims, inds, vals, m, [u.astype(np.float64) for u in U])
                 got = outs[m].numpy().astype(np.float64)
                 assert np.abs(got - want).max() <= 1e-5 * np.abs(want).max(), (rank, m)
-            # root mode left sharded: only owned rows are nonzero on this rank
-            part = sm.mttkrp(sm.root, Ut, full=False).numpy()
-            lo, hi = sm.rows
-            assert not np.any(part[:lo]) and not np.any(part[hi:])
-            # every nonzero lives on exactly one rank
-            n = torch.tensor([sm.nnz])
-            dist.all_reduce(n)
-            assert int(n) == len(vals)
+                # without the gather: exactly this rank's rows, and no exchange needed
+                lo, hi = sm.owned(m)
+                part = sm.mttkrp(m, Ut, gather=False).numpy().astype(np.float64)
+                assert part.shape[0] == hi - lo
+                assert np.abs(part - want[lo:hi]).max() <= 1e-5 * np.abs(want).max(), (rank, m)
+                # the ranks' row ranges tile the mode
+                b = torch.tensor([lo, hi])
+                allb = [torch.zeros_like(b) for _ in range(world)]
+                dist.all_gather(allb, b)
+                assert int(allb[0][0]) == 0 and int(allb[-1][1]) == dims[m]
+                assert all(int(allb[r][1]) == int(allb[r + 1][0]) for r in range(world - 1))
+                # every nonzero lives in exactly one rank's shard of each mode
+                n = torch.tensor([sm.shard_nnz[m]])
+                dist.all_reduce(n)
+                assert int(n) == len(vals)
         else:
             Uo, lam_o, fit_o, hist_o = CO.cp_als(dims, inds, vals, U, max_iters=8, tol=1e-12)
             Ug, lam_g, fit_g, hist_g = D.dist_cp_als(sm, Ut, max_iters=8, tol=1e-12)
@@ -97,9 +106,10 @@ def _worker(rank, world, port, what, seed):
         dist.destroy_process_group()
 
 
+@pytest.mark.parametrize("world", [2, 3])
 @pytest.mark.parametrize("what", ["mttkrp", "als"])
-def test_two_ranks_gloo(what):
-    mp.spawn(_worker, args=(2, _free_port(), what, 3), nprocs=2, join=True)
+def test_ranks_gloo(what, world):
+    mp.spawn(_worker, args=(world, _free_port(), what, 3), nprocs=world, join=True)
 
 
 def test_shard_slices_balance():

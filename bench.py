@@ -30,9 +30,13 @@ cpu_baseline / --impl reference = the reference's own MTTKRP_COO_CPU
 error_vs_fp64 = every output of the timed step against an FP64 MTTKRP of
              the same factors (largest |d| / (|ref| + 1e-6 max|ref|), and the
              relative Frobenius norm).
+reference_gpu = the reference's own GPU MTTKRP (MTTKRP_MIHCSR_GPU, built for
+             sm_100a) on this GPU and the same arrays, at its defaults and
+             its benchmark script's settings, beside this step.
 also       = format_build_ms (device construction), bf16_factors (the step
              with BF16 factors, tuned, and its errors), r64 (the same
-             workload at R = 64, FP32 and BF16), config1 (1000^3 uniform,
+             workload at R = 64, FP32 and BF16), autotune (the tuner choosing
+             -f and each mode's factor precision), config1 (1000^3 uniform,
              -f 128 -w 1: device, the library's host -t 1 path and the
              reference's CPU path), skewed4d (the 4-D workload: MM-CSF all
              modes against B-CSF and HB-CSF per mode), ttm (the reference's
@@ -106,6 +110,8 @@ def parse():
     ap.add_argument("--no-r64", action="store_true", help="skip the R=64 section of the skewed 3-D workload")
     ap.add_argument("--no-config1", action="store_true", help="skip the 1000^3 uniform (config 1) section")
     ap.add_argument("--no-4d", action="store_true", help="skip the 4-D (B-CSF / HB-CSF / MM-CSF) section")
+    ap.add_argument("--no-autotune", action="store_true", help="skip the -f / precision autotuner section")
+    ap.add_argument("--no-refgpu", action="store_true", help="skip the reference's own GPU MTTKRP on this GPU")
     ap.add_argument("--sharded", action="store_true",
                     help="run the row-sharded multi-GPU path (the default for --gpus N > 1) also on one GPU")
     return ap.parse_args()
@@ -521,7 +527,7 @@ def cp_section(seed, scale):
     nnz = int(c["nnz"] * scale)
     X = mmcsf.CooTensor.generate(c["dims"], nnz, dist=[0, 0, 0], val_dist=mmcsf.VAL_UNIFORM01, seed=seed + 11,
                                  planted_rank=c["planted"], noise=c["noise"])
-    F = mmcsf.Format(X, impl=mmcsf.IMPL_MMCSF, views=1)
+    F = mmcsf.Format(X, impl=mmcsf.IMPL_MMCSF, views=2)  # every mode can run as a slice level
     del X
     g = torch.Generator(device="cuda").manual_seed(seed + 5)
     R = c["R"]
@@ -532,10 +538,13 @@ def cp_section(seed, scale):
         F.cpd(R, max_iters=2, tol=c["tol"], precision=prec, init=init)       # warm-up (tables, graph code)
         r = F.cpd(R, max_iters=c["max_iters"], tol=c["tol"], precision=prec, init=init)
         fx = F.cpd(R, max_iters=c["max_iters"], tol=1e-15, precision=prec, init=init)  # every iteration
+        pr = F.cpd(R, max_iters=20, tol=1e-15, precision=prec, init=init, profile=True)  # per-phase times
         runs[prec] = {"seconds_to_converge": r["seconds"], "iters_to_converge": r["iters"], "fit": r["fit"],
                       "converged": r["converged"], "graph": r["graph"], "launches": r["launches"],
                       "fixed_iters": fx["iters"], "fixed_seconds": fx["seconds"],
-                      "s_per_iter": fx["seconds"] / max(1, fx["iters"]), "fixed_fit": fx["fit"]}
+                      "s_per_iter": fx["seconds"] / max(1, fx["iters"]), "fixed_fit": fx["fit"],
+                      "phase_ms_per_iter": {k: v / pr["iters"] for k, v in pr["phase_ms"].items()},
+                      "phase_note": "host-driven profiled run (events at every phase boundary), 20 iterations"}
     f32, b16 = runs["fp32"], runs["bf16"]
     out["cp_als"] = {"workload": c["desc"] + (f" (nnz scaled to {nnz})" if scale != 1.0 else ""),
                      "runs": runs, "fit_gap_bf16_vs_fp32": abs(b16["fit"] - f32["fit"]),
@@ -549,7 +558,7 @@ def cp_section(seed, scale):
     nnz = int(c["nnz"] * scale)
     X = mmcsf.CooTensor.generate(c["dims"], nnz, dist=[1, 1, 1], zipf_s=c["zipf"], seed=seed + 13,
                                  planted_rank=c["planted"], poisson=True)
-    F = mmcsf.Format(X, impl=mmcsf.IMPL_MMCSF, views=1)
+    F = mmcsf.Format(X, impl=mmcsf.IMPL_MMCSF, views=2)
     del X
     R = c["R"]
     g = torch.Generator(device="cuda").manual_seed(seed + 7)
@@ -857,6 +866,87 @@ def skewed4d_section(steps, warmup, seed, hbm_peak, peak_kind):
     return out
 
 
+def reference_gpu_section(X, F, dims, R, ours_ms):
+    """The reference's own GPU MTTKRP (MTTKRP_MIHCSR_GPU,
+    src/mttkrp_gpu.cu:3380-3784, built for sm_100a from its sources as
+    oracle/_ref/libmmcsf_ref_gpu.so) on this B200, on the MM-CSF arrays this
+    library builds (bit-exact to the reference's builders), at its defaults
+    (-w 4 -s 1 -b 128, no split) and at the settings of its own benchmark
+    script (scripts/run_all.sh:22-23: -f 128 -w 1 -s 4 -b 128 and -s 16 -b
+    512). Its "Total GPU time" (the sum of its per-launch event times,
+    src/mttkrp_gpu.cu:3757) beside this library's all-mode step. R <= 32
+    only: its kernels are wrong above 32 (src/mttkrp_gpu.cu:746-753)."""
+    import numpy as np
+    import torch
+    import mmcsf
+    from oracle import oracle as O
+    if not O.ref_gpu_available():
+        return {"unavailable": "oracle/_ref/libmmcsf_ref_gpu.so was not built (needs the reference sources)"}
+    if R > 32:
+        return {"unavailable": "the reference's kernels are correct only for R <= 32"}
+    info = F.info(2)
+    Uc = [torch.full((d, R), m + 0.5, device="cuda") for m, d in enumerate(dims)]
+    mine = F.mttkrp(len(dims) - 1, Uc).cpu().numpy()
+    runs = {}
+    for w, s_, b, f in ((4, 1, 128, 0), (1, 4, 128, 128), (1, 16, 512, 128)):
+        G = F if f == 0 else mmcsf.Format(X, impl=mmcsf.IMPL_MMCSF, mode=0, fiber_threshold=f)
+        arr = dict(fbr_ptr=[G.export(2, "fbrPtr0"), G.export(2, "fbrPtr1")],
+                   fbr_idx=[G.export(2, "fbrIdx0"), G.export(2, "fbrIdx1")],
+                   fbr_like=G.export(2, "fbrLikeSlcInds"), leaf=G.export(2, "indsLeaf"), vals=G.export_f32(2, "vals"))
+        if G is not F:
+            del G
+        torch.cuda.empty_cache()
+        ms, out = O.ref_mihcsr_gpu(dims, R, 2, info["mode_order"], warp_per_slice=w, tb_size=b, fiber_per_warp=s_,
+                                   **arr)
+        runs[f"-w {w} -s {s_} -b {b} -f {f or 'none'}"] = {
+            "total_gpu_ms": ms, "last_mode_max_abs_diff_over_max": float(np.abs(out - mine).max() / np.abs(mine).max())}
+        del arr
+    best = min(runs.values(), key=lambda r: r["total_gpu_ms"])["total_gpu_ms"]
+    return {"what": "MTTKRP_MIHCSR_GPU, all modes, R=32, FP32, the reference's kernels built for sm_100a",
+            "runs": runs, "best_total_gpu_ms": best, "ours_ms_per_step": ours_ms, "speedup_vs_best": best / ours_ms}
+
+
+def autotune_section(X, dims, R, steps, warmup, inds_dev, vals_dev, budget=1e-3):
+    """The autotuner over the fiber-split threshold (-f none / 128 / 32, each
+    format rebuilt) and the factor precision per mode (BF16 copies of the
+    FP32 factors where faster and within `budget` of the FP32-factor
+    output): the chosen -f, the per-mode plan, the mixed all-mode step's
+    time and its errors against the FP64 oracle of the FP32 factors."""
+    import torch
+    import mmcsf
+    g = torch.Generator(device="cuda").manual_seed(1234)
+    U = [torch.rand(d, R, device="cuda", generator=g) for d in dims]
+    outs = [torch.empty(d, R, device="cuda") for d in dims]
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    F, plan = mmcsf.autotune(X, U, views=1, f_candidates=(0, 128, 32), error_budget=budget, outs=outs)
+    torch.cuda.synchronize()
+    tune_s = time.perf_counter() - t0
+    for _ in range(warmup):
+        F.mttkrp_all(U, outs)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(steps):
+        F.mttkrp_all(U, outs)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    F.mttkrp_all(U, outs)
+    torch.cuda.synchronize()
+    errs = []
+    for m in range(len(dims)):
+        ref = fp64_mttkrp(inds_dev, vals_dev, U, m)
+        errs.append(err_vs(outs[m], ref))
+        del ref
+    out = {"error_budget": budget, "f_candidates": [0, 128, 32], "chosen_fiber_threshold": plan["fiber_threshold"],
+           "plan": plan, "ms_per_step": ms, "launches_per_step": F.last_launches, "tune_and_build_s": tune_s,
+           "error_vs_fp64_fp32_factors": errs}
+    del F
+    torch.cuda.empty_cache()
+    return out
+
+
 def sharded_arm(a, W, config, world, rank, local):
     """--gpus N > 1 (or --sharded): ONE tensor (the same seeded tensor on
     every rank) with every mode's rows split across the ranks (mmcsf.dist
@@ -1030,7 +1120,7 @@ def main():
     outs = [torch.empty(d, R, device="cuda") for d in dims]
     if a.plan_file:
         with open(a.plan_file) as fh:
-            plan = {(k if k == "pair" else int(k)): v for k, v in json.load(fh).items()}
+            plan = {(int(k) if k.isdigit() else k): v for k, v in json.load(fh).items()}
         F.set_plan(plan)
     else:
         plan = None if a.no_tune else F.tune(U, outs)
@@ -1144,6 +1234,12 @@ def main():
     if a.workload == "skewed3d" and R == 32 and a.dtype == "f32" and not a.no_r64 and not a.nnz:
         r64 = r64_section(F, X, dims, rows, nfib_nosplit, info, min(a.steps, 20), a.warmup, hbm_peak, peak_kind,
                           a.workload)
+    refgpu = None
+    if nd == 3 and a.dtype == "f32" and not a.no_refgpu and not a.nnz and a.fiber_threshold == 0:
+        refgpu = reference_gpu_section(X, F, dims, R, ms_per_step)
+    auto = None
+    if a.workload == "skewed3d" and R == 32 and a.dtype == "f32" and not a.no_autotune and not a.nnz:
+        auto = autotune_section(X, dims, R, min(a.steps, 20), a.warmup, inds_dev, vals_dev)
     ttm = ttm_section(X, dims, R, info["mode_order"][0], rows) if nd == 3 and R in (4, 8, 16, 32, 64, 128) else None
     heur = None
     if not a.no_heuristic:
@@ -1172,7 +1268,7 @@ def main():
             "roofline": roofline, "error_vs_fp64": errors,
             "cpu_baseline": cpu,
             "e2e": e2e, "gpu_launches": launches_per_step * a.steps, "clocks": clocks, "bf16_factors": bf16,
-            "r64": r64, "config1": cfg1, "skewed4d": w4d,
+            "reference_gpu": refgpu, "r64": r64, "autotune": auto, "config1": cfg1, "skewed4d": w4d,
             "ttm": ttm, "cp": cp, "formats": formats, "partition_heuristic": heur}
     print(json.dumps(line), flush=True)
     if world > 1:

@@ -250,12 +250,43 @@ typedef struct {
   float ms[4];      /* best time per mode */
   int pair;         /* 1: mmcsf_mttkrp_all runs the partition's two upper modes in one walk (mmcsf_mttkrp_pair) */
   int pair_chunk, pair_min_blocks;
-  int pair_kernel;  /* 2: branch-free fiber walk with both outputs; 3 (or 0): per-nonzero form */
+  int pair_kernel;  /* 2: branch-free fiber walk with both outputs; 3 (or 0): per-nonzero form; 4: per-nonzero
+                       form with the middle row once per fiber */
   float pair_ms;    /* best time of that walk (both modes) */
+  int factor_dtype; /* MMCSF_DTYPE_* of the factors the plan is for (mmcsf_set_plan files the entries under it) */
+  /* per-mode precision (mmcsf_tune_precision): with FP32 factors, mmcsf_mttkrp_all runs each launch at the
+   * type chosen here, converting the factors to BF16 once per call when any launch reads BF16 */
+  int mixed;         /* 1: mode_dtype / pair_dtype apply (the per-mode entries above are those of the chosen type) */
+  int mode_dtype[4];
+  int pair_dtype;
+  float bf16_error[4]; /* relative Frobenius difference of the mode's output with BF16-rounded factors against
+                          its output with the FP32 factors */
+  float ms_f32[4], ms_bf16[4]; /* best single-mode time per type */
+  float pair_ms_f32, pair_ms_bf16;
+  float convert_ms;    /* the once-per-call FP32 -> BF16 conversion of all factors */
+  int fiber_threshold; /* -f of the format (mmcsf_autotune: the threshold it chose; 0: no split) */
 } mmcsf_plan;
 int mmcsf_tune(mmcsf_format* F, int R, int factor_dtype, const void* const* d_factors, float* const* d_outs,
                void* stream, mmcsf_plan* plan);
 int mmcsf_set_plan(mmcsf_format* F, const mmcsf_plan* plan);
+/* Per-mode precision (no counterpart in the reference): tunes the format for
+ * FP32 factors and for BF16 copies of them (the plain tuner, twice), measures
+ * for every mode the relative Frobenius difference its BF16-factor output
+ * makes against its FP32-factor output, and picks for every launch of the
+ * all-mode step (each mode, and the two-output walk) the faster type whose
+ * error is within error_budget; BF16 is dropped where it does not pay for
+ * the conversion. mmcsf_mttkrp_all with FP32 factors then follows the plan.
+ * error_budget 0 keeps every launch FP32. */
+int mmcsf_tune_precision(mmcsf_format* F, int R, const float* const* d_factors, float* const* d_outs,
+                         double error_budget, void* stream, mmcsf_plan* plan);
+/* Autotuner over the fiber-split threshold (the reference's -f, set by hand
+ * there): builds the format of `base` for every threshold in f_candidates
+ * (0 = no split), tunes each (mmcsf_tune_precision with error_budget), and
+ * returns the one whose tuned all-mode step is fastest, its plan (with
+ * fiber_threshold) in *plan. The formats not chosen are freed. */
+int mmcsf_autotune(mmcsf_coo* X, const mmcsf_build_opts* base, const uint64_t* f_candidates, int n_candidates,
+                   int R, const float* const* d_factors, float* const* d_outs, double error_budget, void* stream,
+                   mmcsf_format** out, mmcsf_plan* plan);
 
 /* Row-gather probe (measurement; no counterpart in the reference): average
  * milliseconds over `reps` launches of a kernel that only gathers and sums

@@ -1,8 +1,8 @@
 // mttkrp — command-line driver with the reference's flags (src/util.h:3341-3442,
 // src/mttkrp.cu:72-472), on top of the C ABI in include/mmcsf.h.
 //
-//   mttkrp -i X.tns [-m mode] [-R rank] [-t 8|10|12] [-f fiber-threshold]
-//          [-w warps] [-b block] [-v 0|1] [-c 0|1] [-o out.txt]
+//   mttkrp -i X.tns [-m mode] [-R rank] [-t 1|8|10|12] [-f fiber-threshold]
+//          [-w warps] [-b block] [-e budget] [-v 0|1] [-c 0|1] [-o out.txt]
 //
 // Differences from the reference, by design:
 //   * errors print a message and return a nonzero exit status (the reference
@@ -16,7 +16,11 @@
 //     The kernels here walk nonzero-balanced chunks instead of fibers, so -w
 //     sets the chunk that gives the same number of workers: with G lanes per
 //     factor row (32/G teams per warp), chunk = max(1, N*G / (32*w*F))
-//     nonzeros per team. Without -w the per-mode autotuner chooses;
+//     nonzeros per team. Without -w the per-mode autotuner chooses, and
+//     without -f as well it also picks -f among none, 128 and 32 (each
+//     candidate format built and tuned, mmcsf_autotune); -e (no counterpart
+//     in the reference) lets it run modes on BF16 factor copies within that
+//     error budget;
 //   * -o writes the output of mode -m (every mode is computed for -t 12);
 //   * -i accepts a binary COO file (name ending in .bin, mmcsf_coo_write_bin).
 // Factors are the reference's non-CPD constants U[m] = m + 0.5
@@ -39,6 +43,7 @@ namespace {
 struct Options {  // the reference's Options fields this driver uses (src/util.h:189-236)
   int R = 32, mode = 0, impType = 1, warpPerSlice = 0, TBsize = 0, MIfbTh = 1, partitionRule = 0;
   uint64_t fbrThreashold = 0;
+  double errBudget = 0;  // -e: BF16-factor error budget for the per-mode precision tuner (0: FP32 only)
   bool verbose = false, correctness = false;
   std::string inFileName, outFileName;
 };
@@ -54,6 +59,9 @@ void usage() {
       "        -P MM-CSF partition rule: 0 all nonzeros to partition 2 as the reference ships (default),\n"
       "           1 the reference's partition heuristic decides\n"
       "        -w warps per fiber: as many workers as w warps for every fiber (default: autotuned)\n"
+      "        -e error budget: without -w, run modes on BF16 factor copies where faster and within this\n"
+      "           relative change of their output (default 0: FP32 only). Without -w and -f the tuner also\n"
+      "           picks -f among none, 128 and 32 (-v 1 prints the choice)\n"
       "        -b threads per CTA (default 256)\n"
       "        -v verbose: 1 to enable\n"
       "        -c correctness: 1 to check the last mode against a host COO MTTKRP\n"
@@ -79,6 +87,7 @@ bool parse(int argc, char** argv, Options& o) {
       case 'o': o.outFileName = v; break;
       case 'h': o.MIfbTh = std::atoi(v); break;
       case 'P': o.partitionRule = std::atoi(v); break;
+      case 'e': o.errBudget = std::atof(v); break;
       case 's': case 'g': case 'l': case 'p': case 'q': case 'r': break;  // accepted, unused
       default: std::fprintf(stderr, "unknown option: -%c\n", c); return false;
     }
@@ -158,11 +167,6 @@ int main(int argc, char** argv) {
   bo.partition_ratio = o.MIfbTh;
   cudaStream_t s = nullptr;
   mmcsf_format* F = nullptr;
-  auto t0 = std::chrono::steady_clock::now();
-  if ((st = mmcsf_build(X, &bo, s, &F))) return fail("format construction", st);
-  double build_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
-  if (o.verbose) std::printf("format construction (device): %.3f ms\n", build_ms);
-
   const int R = o.R;
   std::vector<float*> dU(nd), dOut(nd);
   std::vector<std::vector<float>> hU(nd);
@@ -173,6 +177,22 @@ int main(int argc, char** argv) {
     cudaMemcpy(dU[m], hU[m].data(), dims[m] * (uint64_t)R * 4, cudaMemcpyHostToDevice);
   }
   const void* fac[4] = {dU[0], dU[1], dU[2], nd == 4 ? dU[3] : nullptr};
+  const float* facf[4] = {dU[0], dU[1], dU[2], nd == 4 ? dU[3] : nullptr};
+  // without -w and -f the tuner also picks -f (each candidate format built and tuned)
+  const bool autotune = o.warpPerSlice <= 0 && o.fbrThreashold == 0;
+  mmcsf_plan plan{};
+  auto t0 = std::chrono::steady_clock::now();
+  if (autotune) {
+    if ((st = mmcsf_autotune(X, &bo, nullptr, 0, R, facf, dOut.data(), o.errBudget, s, &F, &plan)))
+      return fail("autotune", st);
+  } else {
+    if ((st = mmcsf_build(X, &bo, s, &F))) return fail("format construction", st);
+  }
+  double build_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  if (o.verbose) std::printf("format construction (device)%s: %.3f ms\n", autotune ? " and autotuning" : "", build_ms);
+  if (o.verbose && autotune)
+    std::printf("autotuned -f %d%s\n", plan.fiber_threshold, plan.fiber_threshold ? "" : " (no split)");
+
   mmcsf_kernel_cfg cfg{};
   if (o.warpPerSlice > 0) {
     // workers of the reference's launch: w warps per fiber, summed over the partitions
@@ -189,13 +209,29 @@ int main(int argc, char** argv) {
   }
   if (o.TBsize > 0) cfg.block_threads = o.TBsize;
   const int nmodes = o.impType == MMCSF_IMPL_MMCSF ? nd : 1;
-  if (o.warpPerSlice <= 0 && (st = mmcsf_tune(F, R, MMCSF_DTYPE_F32, fac, dOut.data(), s, nullptr)))
-    return fail("autotune", st);
+  if (!autotune && o.warpPerSlice <= 0) {
+    st = (o.impType == MMCSF_IMPL_MMCSF && o.errBudget > 0)
+             ? mmcsf_tune_precision(F, R, facf, dOut.data(), o.errBudget, s, &plan)
+             : mmcsf_tune(F, R, MMCSF_DTYPE_F32, fac, dOut.data(), s, &plan);
+    if (st) return fail("autotune", st);
+  }
+  if (o.verbose && o.warpPerSlice <= 0 && plan.mixed)
+    for (int m = 0; m < nd; ++m)
+      std::printf("mode %d: %s factors (relative change %.2e)\n", m,
+                  plan.mode_dtype[m] == MMCSF_DTYPE_BF16 ? "BF16" : "FP32", plan.bf16_error[m]);
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
   float total = 0;
-  for (int q = 0; q < nmodes; ++q) {
+  const bool all_call = o.impType == MMCSF_IMPL_MMCSF && o.warpPerSlice <= 0;
+  if (all_call) {  // the tuned all-mode call (two-output walk, per-mode precision)
+    cudaEventRecord(e0, s);
+    if ((st = mmcsf_mttkrp_all(F, R, MMCSF_DTYPE_F32, fac, dOut.data(), nullptr, s))) return fail("MTTKRP", st);
+    cudaEventRecord(e1, s);
+    cudaEventSynchronize(e1);
+    cudaEventElapsedTime(&total, e0, e1);
+  }
+  for (int q = 0; q < nmodes && !all_call; ++q) {
     const int m = o.impType == MMCSF_IMPL_MMCSF ? q : o.mode;
     cudaEventRecord(e0, s);
     if ((st = mmcsf_mttkrp(F, m, R, MMCSF_DTYPE_F32, fac, dOut[m], o.warpPerSlice > 0 ? &cfg : nullptr, s)))

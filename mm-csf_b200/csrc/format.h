@@ -89,12 +89,23 @@ struct mmcsf_format {
   uint64_t fbr_th = 0;
   mmcsf::CsfPart parts[4];
   mmcsf::CsfPart views[4];  // views[m]: a CSF with mode m at level 0 (order_modes(m))
-  int plan_traversal[4] = {0, 0, 0, 0};  // tuned: 1 partitions, 2 view (0 = untuned)
-  int plan_chunk[4] = {0, 0, 0, 0};
-  int plan_mb[4] = {0, 0, 0, 0};
-  int plan_kernel[4] = {0, 0, 0, 0};
-  int pair_chunk = 0, pair_mb = 0, pair_kernel = 0;  // the two-output walk's launch shape (0: defaults)
-  bool pair_use = false;            // mmcsf_mttkrp_all runs the partition's two upper modes in one walk
+  // tuned plans, one per factor type (index: MMCSF_DTYPE_F32 / _BF16)
+  int plan_traversal[2][4] = {};  // 1 partitions, 2 view (0 = untuned)
+  int plan_chunk[2][4] = {};
+  int plan_mb[2][4] = {};
+  int plan_kernel[2][4] = {};
+  float plan_ms[2][4] = {};
+  int pair_chunk[2] = {}, pair_mb[2] = {}, pair_kernel[2] = {};  // the two-output walk's launch shape (0: defaults)
+  bool pair_use[2] = {};      // mmcsf_mttkrp_all runs the partition's two upper modes in one walk
+  float pair_ms[2] = {};
+  // per-mode precision (mmcsf_tune_precision): with FP32 factors, mmcsf_mttkrp_all runs mode m's kernel on
+  // BF16 copies of the factors where mode_dtype[m] (or pair_dtype, for the two-output walk) says so
+  bool mixed = false;
+  int mode_dtype[4] = {};
+  bool mixed_pair = false;  // the mixed plan runs the two-output walk
+  int pair_dtype = 0;
+  mmcsf::DevBuf bf16_fac[4];  // BF16 copies of the caller's factors (mixed plans)
+  int fiber_threshold_tuned = -1;  // mmcsf_autotune: the -f the format was chosen with
   mmcsf::HybExtra hyb;
   int last_launches = 0;
   // staging for the host-buffer MTTKRP entry point

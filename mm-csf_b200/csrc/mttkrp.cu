@@ -21,6 +21,7 @@
 #include <algorithm>
 #include <cuda_bf16.h>
 
+#include <cmath>
 #include <cstring>
 #include <type_traits>
 
@@ -139,12 +140,13 @@ int mttkrp_mode_vals(const mmcsf_format* F, int mode, int R, int dtype, const vo
                      float* out, const mmcsf_kernel_cfg* cfg, cudaStream_t s, int* launches) {
   MMCSF_CUDA(cudaMemsetAsync(out, 0, F->dims[mode] * (uint64_t)R * sizeof(float), s));
   int trav = cfg ? cfg->traversal : 0;
-  if (trav == 0) trav = F->plan_traversal[mode] ? F->plan_traversal[mode] : (F->views[mode].present ? 2 : 1);
+  const int d = dtype == MMCSF_DTYPE_BF16 ? 1 : 0;  // the plan tuned for this factor type
+  if (trav == 0) trav = F->plan_traversal[d][mode] ? F->plan_traversal[d][mode] : (F->views[mode].present ? 2 : 1);
   mmcsf_kernel_cfg c{};
   if (cfg) c = *cfg;
-  if (c.chunk == 0) c.chunk = F->plan_chunk[mode];
-  if (c.min_blocks == 0) c.min_blocks = F->plan_mb[mode];
-  if (c.kernel == 0) c.kernel = F->plan_kernel[mode];
+  if (c.chunk == 0) c.chunk = F->plan_chunk[d][mode];
+  if (c.min_blocks == 0) c.min_blocks = F->plan_mb[d][mode];
+  if (c.kernel == 0) c.kernel = F->plan_kernel[d][mode];
   if (trav == 2) {
     const CsfPart& V = F->views[mode];
     if (!V.present) return set_error(MMCSF_ERR_INVALID, "no view for mode %d (build with views)", mode);
@@ -236,6 +238,31 @@ extern "C" int mmcsf_mttkrp(const mmcsf_format* F, int mode, int R, int factor_d
   return st;
 }
 
+__global__ void k_to_bf16(const float* __restrict__ in, __nv_bfloat16* __restrict__ out, uint64_t n) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    out[i] = __float2bfloat16_rn(in[i]);
+}
+
+// sums[0] += sum (a - b)^2, sums[1] += sum b^2 (FP64)
+__global__ void k_diff_norms(const float* __restrict__ a, const float* __restrict__ b, uint64_t n,
+                             double* __restrict__ sums) {
+  __shared__ double p0[256], p1[256];
+  double s0 = 0, s1 = 0;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const double d = (double)a[i] - (double)b[i];
+    s0 += d * d;
+    s1 += (double)b[i] * (double)b[i];
+  }
+  p0[threadIdx.x] = s0;
+  p1[threadIdx.x] = s1;
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) {
+    if (threadIdx.x < w) { p0[threadIdx.x] += p0[threadIdx.x + w]; p1[threadIdx.x] += p1[threadIdx.x + w]; }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) { atomicAdd(sums, p0[0]); atomicAdd(sums + 1, p1[0]); }
+}
+
 __global__ void k_scale_cols(float* __restrict__ M, uint64_t rows, int R, const float* __restrict__ lam) {
   const uint64_t n = rows * (uint64_t)R;
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
@@ -292,10 +319,11 @@ extern "C" int mmcsf_mttkrp_pair(const mmcsf_format* F, int R, int factor_dtype,
   cudaStream_t s = S(stream);
   MMCSF_CUDA(cudaMemsetAsync(d_out_slice, 0, F->dims[P->order[0]] * (uint64_t)R * sizeof(float), s));
   MMCSF_CUDA(cudaMemsetAsync(d_out_mid, 0, F->dims[P->order[1]] * (uint64_t)R * sizeof(float), s));
-  const int chunk = cfg && cfg->chunk > 0 ? cfg->chunk : (F->pair_chunk ? F->pair_chunk : 256);
+  const int d = factor_dtype == MMCSF_DTYPE_BF16 ? 1 : 0;
+  const int chunk = cfg && cfg->chunk > 0 ? cfg->chunk : (F->pair_chunk[d] ? F->pair_chunk[d] : 256);
   const int threads = cfg && cfg->block_threads > 0 ? cfg->block_threads : 256;
-  const int mb = cfg && cfg->min_blocks > 0 ? cfg->min_blocks : (F->pair_mb ? F->pair_mb : 3);
-  const int kern = cfg && cfg->kernel > 0 ? cfg->kernel : F->pair_kernel;
+  const int mb = cfg && cfg->min_blocks > 0 ? cfg->min_blocks : (F->pair_mb[d] ? F->pair_mb[d] : 3);
+  const int kern = cfg && cfg->kernel > 0 ? cfg->kernel : F->pair_kernel[d];
   if (kern < 0 || kern > 4) return set_error(MMCSF_ERR_INVALID, "kernel must be 0, 1, 2, 3 or 4");
   if (threads % 32 || threads > 256) return set_error(MMCSF_ERR_INVALID, "block_threads must be a multiple of 32, <= 256");
   const int slot = CsfPart::cfib_slot((uint64_t)chunk);
@@ -320,8 +348,8 @@ namespace {
 // The tuned plan runs the partition's two upper modes in one walk (only
 // without a caller override of the traversal or kernel). modes[0..1] get
 // them.
-bool pair_active(const mmcsf_format* F, int R, const mmcsf_kernel_cfg* cfg, int* modes) {
-  if (!F->pair_use || F->impl != MMCSF_IMPL_MMCSF || !native_R(R) || R > 128) return false;
+bool pair_active(const mmcsf_format* F, int R, bool want, const mmcsf_kernel_cfg* cfg, int* modes) {
+  if (!want || F->impl != MMCSF_IMPL_MMCSF || !native_R(R) || R > 128) return false;
   if (cfg && (cfg->traversal != 0 || cfg->kernel != 0)) return false;
   const CsfPart* P = nullptr;
   for (int p = 0; p < F->nd; ++p)
@@ -344,14 +372,40 @@ extern "C" int mmcsf_mttkrp_all(const mmcsf_format* F, int R, int factor_dtype, 
     return set_error(MMCSF_ERR_INVALID, "all-mode MTTKRP needs an MM-CSF format (-t 12)");
   int total = 0;
   int pm[2] = {-1, -1};
-  const bool pair = pair_active(F, R, cfg, pm);
+  // a per-mode precision plan (mmcsf_tune_precision) with FP32 factors: the
+  // launches it assigns to BF16 read BF16 copies of the factors, converted here
+  const bool mixed = F->mixed && factor_dtype == MMCSF_DTYPE_F32 && !(cfg && (cfg->traversal || cfg->kernel));
+  const void* bf[4] = {nullptr, nullptr, nullptr, nullptr};
+  auto dt_of = [&](int m) { return mixed ? F->mode_dtype[m] : factor_dtype; };
+  const int pdt = mixed ? F->pair_dtype : factor_dtype;
+  bool need_bf16 = false;
+  if (mixed) {
+    for (int m = 0; m < F->nd; ++m) need_bf16 = need_bf16 || F->mode_dtype[m] == MMCSF_DTYPE_BF16;
+    need_bf16 = need_bf16 || (F->mixed_pair && F->pair_dtype == MMCSF_DTYPE_BF16);
+  }
+  if (need_bf16) {
+    cudaStream_t s = S(stream);
+    for (int m = 0; m < F->nd; ++m) {
+      const uint64_t n = F->dims[m] * (uint64_t)R;
+      if (F->bf16_fac[m].bytes < n * 2)  // kept by the format between calls (allocated on first use)
+        MMCSF_CUDA(const_cast<mmcsf_format*>(F)->bf16_fac[m].alloc(n * 2));
+      k_to_bf16<<<grid_for(n, 256), 256, 0, s>>>(static_cast<const float*>(d_factors[m]),
+                                                 F->bf16_fac[m].as<__nv_bfloat16>(), n);
+      MMCSF_LAUNCH_CHECK();
+      bf[m] = F->bf16_fac[m].p;
+      ++total;
+    }
+  }
+  auto fac = [&](int dt) { return dt == MMCSF_DTYPE_BF16 && need_bf16 ? bf : d_factors; };
+  const bool pair = pair_active(F, R, mixed ? F->mixed_pair : F->pair_use[factor_dtype == MMCSF_DTYPE_BF16 ? 1 : 0],
+                                cfg, pm);
   if (pair) {
-    MMCSF_TRY(mmcsf_mttkrp_pair(F, R, factor_dtype, d_factors, d_outs[pm[0]], d_outs[pm[1]], nullptr, nullptr, stream));
+    MMCSF_TRY(mmcsf_mttkrp_pair(F, R, pdt, fac(pdt), d_outs[pm[0]], d_outs[pm[1]], nullptr, nullptr, stream));
     total += F->last_launches;
   }
   for (int m = 0; m < F->nd; ++m) {
     if (pair && (m == pm[0] || m == pm[1])) continue;
-    MMCSF_TRY(mmcsf_mttkrp(F, m, R, factor_dtype, d_factors, d_outs[m], cfg, stream));
+    MMCSF_TRY(mmcsf_mttkrp(F, m, R, dt_of(m), fac(dt_of(m)), d_outs[m], cfg, stream));
     total += F->last_launches;
   }
   const_cast<mmcsf_format*>(F)->last_launches = total;
@@ -438,6 +492,7 @@ extern "C" int mmcsf_tune(mmcsf_format* F, int R, int factor_dtype, const void* 
                           float* const* d_outs, void* stream, mmcsf_plan* plan) {
   MMCSF_TRY(check_call(F, R, factor_dtype));
   if (!d_factors || !d_outs) return set_error(MMCSF_ERR_INVALID, "null pointer");
+  const int d = factor_dtype == MMCSF_DTYPE_BF16 ? 1 : 0;
   cudaStream_t s = S(stream);
   cudaEvent_t e0, e1;
   MMCSF_CUDA(cudaEventCreate(&e0));
@@ -446,6 +501,7 @@ extern "C" int mmcsf_tune(mmcsf_format* F, int R, int factor_dtype, const void* 
   const int nmodes = F->impl == MMCSF_IMPL_MMCSF ? F->nd : 1;
   float best_ms[4] = {0, 0, 0, 0};
   int st = MMCSF_OK;
+  F->mixed = false;  // a plain tune runs every launch at the caller's factor type
   for (int i = 0; i < nmodes && st == MMCSF_OK; ++i) {
     const int m = F->impl == MMCSF_IMPL_MMCSF ? i : F->mode;
     float best = 1e30f;
@@ -494,10 +550,11 @@ extern "C" int mmcsf_tune(mmcsf_format* F, int R, int factor_dtype, const void* 
       }
       }
     }
-    F->plan_traversal[m] = bt;
-    F->plan_chunk[m] = bc;
-    F->plan_mb[m] = bm;
-    F->plan_kernel[m] = bk;
+    F->plan_traversal[d][m] = bt;
+    F->plan_chunk[d][m] = bc;
+    F->plan_mb[d][m] = bm;
+    F->plan_kernel[d][m] = bk;
+    F->plan_ms[d][m] = best;
     best_ms[m] = best;
     if (plan) {
       plan->traversal[m] = bt;
@@ -509,7 +566,8 @@ extern "C" int mmcsf_tune(mmcsf_format* F, int R, int factor_dtype, const void* 
   }
   // the two upper modes of the partition in one walk, kept when it beats the
   // two modes' best single-mode plans
-  F->pair_use = false;
+  F->pair_use[d] = false;
+  F->pair_ms[d] = 0.f;
   int pm[2] = {-1, -1};
   if (st == MMCSF_OK && F->impl == MMCSF_IMPL_MMCSF &&
       mmcsf_mttkrp_pair(F, R, factor_dtype, nullptr, nullptr, nullptr, pm, nullptr, stream) == MMCSF_OK &&
@@ -541,14 +599,15 @@ extern "C" int mmcsf_tune(mmcsf_format* F, int R, int factor_dtype, const void* 
         if (st != MMCSF_OK) break;
         if (ms < bestp) { bestp = ms; bpc = c; bpm = mbv; bpk = kern; }
       }
-    if (st == MMCSF_OK && bestp < best_ms[pm[0]] + best_ms[pm[1]]) {
-      F->pair_use = true;
-      F->pair_chunk = bpc;
-      F->pair_mb = bpm;
-      F->pair_kernel = bpk;
+    if (st == MMCSF_OK) {
+      F->pair_use[d] = bestp < best_ms[pm[0]] + best_ms[pm[1]];
+      F->pair_chunk[d] = bpc;
+      F->pair_mb[d] = bpm;
+      F->pair_kernel[d] = bpk;
+      F->pair_ms[d] = bestp;
     }
     if (plan && st == MMCSF_OK) {
-      plan->pair = F->pair_use ? 1 : 0;
+      plan->pair = F->pair_use[d] ? 1 : 0;
       plan->pair_chunk = bpc;
       plan->pair_min_blocks = bpm;
       plan->pair_kernel = bpk;
@@ -559,29 +618,257 @@ extern "C" int mmcsf_tune(mmcsf_format* F, int R, int factor_dtype, const void* 
     plan->pair_chunk = plan->pair_min_blocks = plan->pair_kernel = 0;
     plan->pair_ms = 0.f;
   }
+  if (plan) {
+    plan->factor_dtype = factor_dtype;
+    plan->mixed = 0;
+    for (int m = 0; m < 4; ++m) {
+      plan->mode_dtype[m] = factor_dtype;
+      plan->bf16_error[m] = 0.f;
+    }
+    plan->pair_dtype = factor_dtype;
+    // -f of the format: 0 for no split (the reference's default 99999999, src/util.h:212)
+    plan->fiber_threshold = F->fiber_threshold_tuned >= 0 ? F->fiber_threshold_tuned
+                            : (F->fbr_th >= 99999999ull ? 0 : (int)std::min<uint64_t>(F->fbr_th, 0x7fffffff));
+  }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   return st;
 }
 
+namespace {
+// Relative Frobenius norm ||a - b|| / ||b|| of two device arrays.
+int rel_frob(const float* a, const float* b, uint64_t n, cudaStream_t s, double* out) {
+  DevBuf sums;
+  MMCSF_CUDA(sums.alloc(16));
+  MMCSF_CUDA(cudaMemsetAsync(sums.p, 0, 16, s));
+  k_diff_norms<<<std::min<uint64_t>(grid_for(n, 256), (uint64_t)sm_count() * 8), 256, 0, s>>>(a, b, n,
+                                                                                                sums.as<double>());
+  MMCSF_LAUNCH_CHECK();
+  double h[2] = {0, 0};
+  MMCSF_CUDA(cudaMemcpyAsync(h, sums.p, 16, cudaMemcpyDeviceToHost, s));
+  MMCSF_CUDA(cudaStreamSynchronize(s));
+  *out = h[1] > 0 ? std::sqrt(h[0] / h[1]) : (h[0] > 0 ? 1.0 : 0.0);
+  return MMCSF_OK;
+}
+}  // namespace
+
+extern "C" int mmcsf_tune_precision(mmcsf_format* F, int R, const float* const* d_factors, float* const* d_outs,
+                                    double error_budget, void* stream, mmcsf_plan* plan) {
+  MMCSF_TRY(check_call(F, R, MMCSF_DTYPE_F32));
+  if (!d_factors || !d_outs) return set_error(MMCSF_ERR_INVALID, "null pointer");
+  if (F->impl != MMCSF_IMPL_MMCSF)
+    return set_error(MMCSF_ERR_INVALID, "per-mode precision plans are for MM-CSF formats (-t 12)");
+  if (!(error_budget >= 0)) return set_error(MMCSF_ERR_INVALID, "error budget must be >= 0");
+  cudaStream_t s = S(stream);
+  const int nd = F->nd;
+  const void* f32[4] = {d_factors[0], d_factors[1], d_factors[2], nd == 4 ? d_factors[3] : nullptr};
+  const void* b16[4] = {nullptr, nullptr, nullptr, nullptr};
+  uint64_t maxrows = 0;
+  for (int m = 0; m < nd; ++m) {
+    const uint64_t n = F->dims[m] * (uint64_t)R;
+    if (F->bf16_fac[m].bytes < n * 2) MMCSF_CUDA(F->bf16_fac[m].alloc(n * 2));
+    b16[m] = F->bf16_fac[m].p;
+    maxrows = std::max(maxrows, F->dims[m]);
+  }
+  // the conversion every mixed all-mode call makes, timed
+  cudaEvent_t e0, e1;
+  MMCSF_CUDA(cudaEventCreate(&e0));
+  MMCSF_CUDA(cudaEventCreate(&e1));
+  float conv_ms = 0;
+  for (int rep = 0; rep < 2; ++rep) {
+    MMCSF_CUDA(cudaEventRecord(e0, s));
+    for (int m = 0; m < nd; ++m) {
+      const uint64_t n = F->dims[m] * (uint64_t)R;
+      k_to_bf16<<<grid_for(n, 256), 256, 0, s>>>(d_factors[m], F->bf16_fac[m].as<__nv_bfloat16>(), n);
+      MMCSF_LAUNCH_CHECK();
+    }
+    MMCSF_CUDA(cudaEventRecord(e1, s));
+    MMCSF_CUDA(cudaEventSynchronize(e1));
+    cudaEventElapsedTime(&conv_ms, e0, e1);
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  mmcsf_plan p32{}, p16{};
+  MMCSF_TRY(mmcsf_tune(F, R, MMCSF_DTYPE_F32, f32, d_outs, stream, &p32));
+  MMCSF_TRY(mmcsf_tune(F, R, MMCSF_DTYPE_BF16, b16, d_outs, stream, &p16));
+  // the error BF16 factors cost, per mode: the BF16-factor output against the FP32-factor output
+  DevBuf tmp;
+  MMCSF_CUDA(tmp.alloc(maxrows * R * 4));
+  double err[4] = {0, 0, 0, 0};
+  for (int m = 0; m < nd; ++m) {
+    MMCSF_TRY(mmcsf_mttkrp(F, m, R, MMCSF_DTYPE_F32, f32, d_outs[m], nullptr, stream));
+    MMCSF_TRY(mmcsf_mttkrp(F, m, R, MMCSF_DTYPE_BF16, b16, tmp.as<float>(), nullptr, stream));
+    MMCSF_TRY(rel_frob(tmp.as<float>(), d_outs[m], F->dims[m] * (uint64_t)R, s, &err[m]));
+  }
+  // choose: per mode the faster type within the budget; the two-output walk
+  // at the faster admissible type when it beats its two modes
+  int dt[4] = {0, 0, 0, 0};
+  float unit_ms[4] = {0, 0, 0, 0};
+  for (int m = 0; m < nd; ++m) {
+    const bool ok16 = err[m] <= error_budget;
+    dt[m] = (ok16 && p16.ms[m] < p32.ms[m]) ? MMCSF_DTYPE_BF16 : MMCSF_DTYPE_F32;
+    unit_ms[m] = dt[m] == MMCSF_DTYPE_BF16 ? p16.ms[m] : p32.ms[m];
+  }
+  bool use_pair = false;
+  int pdt = MMCSF_DTYPE_F32;
+  int pm[2] = {-1, -1};
+  if (mmcsf_mttkrp_pair(F, R, MMCSF_DTYPE_F32, nullptr, nullptr, nullptr, pm, nullptr, stream) == MMCSF_OK &&
+      p32.pair_ms > 0) {
+    const bool ok16 = err[pm[0]] <= error_budget && err[pm[1]] <= error_budget && p16.pair_ms > 0;
+    pdt = (ok16 && p16.pair_ms < p32.pair_ms) ? MMCSF_DTYPE_BF16 : MMCSF_DTYPE_F32;
+    const float pms = pdt == MMCSF_DTYPE_BF16 ? p16.pair_ms : p32.pair_ms;
+    use_pair = pms < unit_ms[pm[0]] + unit_ms[pm[1]];
+  }
+  bool any16 = use_pair && pdt == MMCSF_DTYPE_BF16;
+  for (int m = 0; m < nd; ++m)
+    if (!(use_pair && (m == pm[0] || m == pm[1])) && dt[m] == MMCSF_DTYPE_BF16) any16 = true;
+  // the conversion is paid once per call: drop BF16 where it does not pay for it
+  if (any16) {
+    float saved = 0;
+    if (use_pair && pdt == MMCSF_DTYPE_BF16) saved += p32.pair_ms - p16.pair_ms;
+    for (int m = 0; m < nd; ++m)
+      if (!(use_pair && (m == pm[0] || m == pm[1])) && dt[m] == MMCSF_DTYPE_BF16) saved += p32.ms[m] - p16.ms[m];
+    if (saved <= conv_ms) {
+      any16 = false;
+      for (int m = 0; m < nd; ++m) dt[m] = MMCSF_DTYPE_F32;
+      pdt = MMCSF_DTYPE_F32;
+      use_pair = F->pair_use[0];
+    }
+  }
+  F->mixed = any16;
+  for (int m = 0; m < nd; ++m) F->mode_dtype[m] = dt[m];
+  F->pair_dtype = pdt;
+  F->mixed_pair = use_pair;
+  if (plan) {
+    *plan = mmcsf_plan{};
+    for (int m = 0; m < nd; ++m) {
+      const mmcsf_plan& q = dt[m] == MMCSF_DTYPE_BF16 ? p16 : p32;
+      plan->traversal[m] = q.traversal[m];
+      plan->chunk[m] = q.chunk[m];
+      plan->min_blocks[m] = q.min_blocks[m];
+      plan->kernel[m] = q.kernel[m];
+      plan->ms[m] = q.ms[m];
+      plan->mode_dtype[m] = dt[m];
+      plan->bf16_error[m] = (float)err[m];
+      plan->ms_f32[m] = p32.ms[m];
+      plan->ms_bf16[m] = p16.ms[m];
+    }
+    const mmcsf_plan& q = pdt == MMCSF_DTYPE_BF16 ? p16 : p32;
+    plan->pair = use_pair ? 1 : 0;
+    plan->pair_chunk = q.pair_chunk;
+    plan->pair_min_blocks = q.pair_min_blocks;
+    plan->pair_kernel = q.pair_kernel;
+    plan->pair_ms = q.pair_ms;
+    plan->pair_dtype = pdt;
+    plan->pair_ms_f32 = p32.pair_ms;
+    plan->pair_ms_bf16 = p16.pair_ms;
+    plan->factor_dtype = MMCSF_DTYPE_F32;
+    plan->mixed = any16 ? 1 : 0;
+    plan->convert_ms = conv_ms;
+    plan->fiber_threshold = p32.fiber_threshold;
+  }
+  return MMCSF_OK;
+}
+
+namespace {
+// Device time of one call under a tuned plan: the launches it runs (the
+// two-output walk or its two modes, the other modes) plus the conversion of a
+// mixed plan. B-CSF / HB-CSF formats: their one mode.
+float plan_step_ms(const mmcsf_format* F, const mmcsf_plan& p) {
+  if (F->impl != MMCSF_IMPL_MMCSF) return p.ms[F->mode];
+  int pm[2] = {-1, -1};
+  const bool pair = p.pair && mmcsf_mttkrp_pair(F, 32, MMCSF_DTYPE_F32, nullptr, nullptr, nullptr, pm, nullptr,
+                                                nullptr) == MMCSF_OK;
+  float t = pair ? p.pair_ms : 0.f;
+  for (int m = 0; m < F->nd; ++m)
+    if (!(pair && (m == pm[0] || m == pm[1]))) t += p.ms[m];
+  return t + (p.mixed ? p.convert_ms : 0.f);
+}
+}  // namespace
+
+extern "C" int mmcsf_autotune(mmcsf_coo* X, const mmcsf_build_opts* base, const uint64_t* f_candidates,
+                              int n_candidates, int R, const float* const* d_factors, float* const* d_outs,
+                              double error_budget, void* stream, mmcsf_format** out, mmcsf_plan* plan) {
+  if (!X || !base || !d_factors || !d_outs || !out) return set_error(MMCSF_ERR_INVALID, "null argument");
+  static const uint64_t defaults[] = {0, 128, 32};
+  if (!f_candidates || n_candidates <= 0) {
+    f_candidates = defaults;
+    n_candidates = 3;
+  }
+  mmcsf_format* best = nullptr;
+  mmcsf_plan best_plan{};
+  float best_ms = 0.f;
+  for (int i = 0; i < n_candidates; ++i) {
+    mmcsf_build_opts o = *base;
+    o.fiber_threshold = f_candidates[i];
+    mmcsf_format* F = nullptr;
+    int st = mmcsf_build(X, &o, stream, &F);
+    mmcsf_plan p{};
+    if (st == MMCSF_OK)
+      st = F->impl == MMCSF_IMPL_MMCSF
+               ? mmcsf_tune_precision(F, R, d_factors, d_outs, error_budget, stream, &p)
+               : mmcsf_tune(F, R, MMCSF_DTYPE_F32, reinterpret_cast<const void* const*>(d_factors), d_outs, stream,
+                            &p);
+    if (st != MMCSF_OK) {
+      if (F) mmcsf_format_destroy(F);
+      if (best) mmcsf_format_destroy(best);
+      return st;
+    }
+    F->fiber_threshold_tuned = (int)std::min<uint64_t>(f_candidates[i], 0x7fffffff);
+    p.fiber_threshold = F->fiber_threshold_tuned;
+    const float t = plan_step_ms(F, p);
+    if (!best || t < best_ms) {
+      if (best) mmcsf_format_destroy(best);
+      best = F;
+      best_ms = t;
+      best_plan = p;
+    } else {
+      mmcsf_format_destroy(F);
+    }
+  }
+  *out = best;
+  if (plan) *plan = best_plan;
+  return MMCSF_OK;
+}
+
 extern "C" int mmcsf_set_plan(mmcsf_format* F, const mmcsf_plan* plan) {
   if (!F || !plan) return set_error(MMCSF_ERR_INVALID, "null argument");
+  if (plan->factor_dtype != MMCSF_DTYPE_F32 && plan->factor_dtype != MMCSF_DTYPE_BF16)
+    return set_error(MMCSF_ERR_INVALID, "plan factor_dtype must be MMCSF_DTYPE_F32 or MMCSF_DTYPE_BF16");
   for (int m = 0; m < F->nd; ++m) {
     if (plan->traversal[m] == 2 && !F->views[m].present)
       return set_error(MMCSF_ERR_INVALID, "plan uses a view for mode %d that was not built", m);
     if (plan->traversal[m] < 0 || plan->traversal[m] > 2 || plan->chunk[m] < 0 || plan->kernel[m] < 0 ||
         plan->kernel[m] > 4)
       return set_error(MMCSF_ERR_INVALID, "bad plan entry for mode %d", m);
-    F->plan_traversal[m] = plan->traversal[m];
-    F->plan_chunk[m] = plan->chunk[m];
-    F->plan_mb[m] = plan->min_blocks[m];
-    F->plan_kernel[m] = plan->kernel[m];
+    if (plan->mixed && plan->mode_dtype[m] != MMCSF_DTYPE_F32 && plan->mode_dtype[m] != MMCSF_DTYPE_BF16)
+      return set_error(MMCSF_ERR_INVALID, "bad mode_dtype for mode %d", m);
   }
   if (plan->pair_chunk < 0 || plan->pair_min_blocks < 0 || plan->pair_kernel < 0 || plan->pair_kernel > 4)
     return set_error(MMCSF_ERR_INVALID, "bad pair entry");
-  F->pair_use = plan->pair != 0;
-  F->pair_chunk = plan->pair_chunk;
-  F->pair_mb = plan->pair_min_blocks;
-  F->pair_kernel = plan->pair_kernel;
+  if (plan->mixed && plan->pair_dtype != MMCSF_DTYPE_F32 && plan->pair_dtype != MMCSF_DTYPE_BF16)
+    return set_error(MMCSF_ERR_INVALID, "bad pair_dtype");
+  for (int m = 0; m < F->nd; ++m) {
+    // a mixed plan's per-mode entries belong to the type chosen for the mode
+    const int d = plan->mixed ? (plan->mode_dtype[m] == MMCSF_DTYPE_BF16) : (plan->factor_dtype == MMCSF_DTYPE_BF16);
+    F->plan_traversal[d][m] = plan->traversal[m];
+    F->plan_chunk[d][m] = plan->chunk[m];
+    F->plan_mb[d][m] = plan->min_blocks[m];
+    F->plan_kernel[d][m] = plan->kernel[m];
+  }
+  const int pd = plan->mixed ? (plan->pair_dtype == MMCSF_DTYPE_BF16) : (plan->factor_dtype == MMCSF_DTYPE_BF16);
+  F->pair_chunk[pd] = plan->pair_chunk;
+  F->pair_mb[pd] = plan->pair_min_blocks;
+  F->pair_kernel[pd] = plan->pair_kernel;
+  if (plan->mixed) {
+    F->mixed = true;
+    F->mixed_pair = plan->pair != 0;
+    F->pair_dtype = plan->pair_dtype;
+    for (int m = 0; m < F->nd; ++m) F->mode_dtype[m] = plan->mode_dtype[m];
+    if (F->impl != MMCSF_IMPL_MMCSF) return set_error(MMCSF_ERR_INVALID, "mixed plans are for MM-CSF formats");
+  } else {
+    F->mixed = false;
+    F->pair_use[pd] = plan->pair != 0;
+  }
   return MMCSF_OK;
 }

@@ -23,7 +23,7 @@ VAL_UNIFORM01 = 0
 VAL_LOGNORMAL = 1
 VAL_INT1_50 = 2
 
-__all__ = ["CooTensor", "Format", "MmcsfError", "KernelCfg", "IMPL_BCSF", "IMPL_HBCSF", "IMPL_MMCSF",
+__all__ = ["CooTensor", "Format", "autotune", "MmcsfError", "KernelCfg", "IMPL_BCSF", "IMPL_HBCSF", "IMPL_MMCSF",
            "DTYPE_F32", "DTYPE_BF16", "current_stream"]
 
 
@@ -428,10 +428,34 @@ class Format:
         check(lib().mmcsf_mttkrp_all_host(self._h, R, fp, op, self._cfg(cfg), _stream(stream)))
         return outs
 
+    def _plan_dict(self, pl):
+        n = self.nd if self.impl == IMPL_MMCSF else 1
+        modes = list(range(self.nd)) if self.impl == IMPL_MMCSF else [self.mode]
+        dn = {DTYPE_F32: "f32", DTYPE_BF16: "bf16"}
+        plan = {m: {"traversal": pl.traversal[m], "chunk": pl.chunk[m], "min_blocks": pl.min_blocks[m],
+                    "kernel": pl.kernel[m], "ms": pl.ms[m]} for m in modes[:n]}
+        if pl.mixed:
+            for m in modes[:n]:
+                plan[m].update(dtype=dn[pl.mode_dtype[m]], bf16_error=pl.bf16_error[m], ms_f32=pl.ms_f32[m],
+                               ms_bf16=pl.ms_bf16[m])
+        if self.impl == IMPL_MMCSF:
+            plan["pair"] = {"use": bool(pl.pair), "chunk": pl.pair_chunk, "min_blocks": pl.pair_min_blocks,
+                            "kernel": pl.pair_kernel, "ms": pl.pair_ms}
+            if pl.mixed:
+                plan["pair"].update(dtype=dn[pl.pair_dtype], ms_f32=pl.pair_ms_f32, ms_bf16=pl.pair_ms_bf16)
+        plan["dtype"] = dn[pl.factor_dtype]
+        plan["mixed"] = bool(pl.mixed)
+        plan["fiber_threshold"] = pl.fiber_threshold
+        if pl.mixed:
+            plan["convert_ms"] = pl.convert_ms
+        return plan
+
     def tune(self, factors, outs=None, stream=None):
-        """Autotune traversal, kernel, chunk and occupancy per mode (mmcsf_tune);
-        returns the plan: {mode: {...}} plus, for MM-CSF, "pair": the
-        two-output walk's best setting and whether mttkrp_all uses it."""
+        """Autotune traversal, kernel, chunk and occupancy per mode for the
+        factors' type (mmcsf_tune; one plan is kept per factor type); returns
+        the plan: {mode: {...}} plus, for MM-CSF, "pair": the two-output
+        walk's best setting and whether mttkrp_all uses it, and "dtype",
+        "fiber_threshold"."""
         import torch
         R = factors[0].shape[1]
         if outs is None:
@@ -440,31 +464,48 @@ class Format:
         op = (c_voidp * self.nd)(*[_ptr(o) for o in outs])
         pl = Plan()
         check(lib().mmcsf_tune(self._h, R, self._dtype(factors), fp, op, _stream(stream), ctypes.byref(pl)))
-        n = self.nd if self.impl == IMPL_MMCSF else 1
-        modes = range(self.nd) if self.impl == IMPL_MMCSF else [self.mode]
-        plan = {m: {"traversal": pl.traversal[m], "chunk": pl.chunk[m], "min_blocks": pl.min_blocks[m],
-                    "kernel": pl.kernel[m], "ms": pl.ms[m]} for m in list(modes)[:n]}
-        if self.impl == IMPL_MMCSF:
-            plan["pair"] = {"use": bool(pl.pair), "chunk": pl.pair_chunk, "min_blocks": pl.pair_min_blocks,
-                            "kernel": pl.pair_kernel, "ms": pl.pair_ms}
-        return plan
+        return self._plan_dict(pl)
+
+    def tune_precision(self, factors, outs=None, error_budget=0.0, stream=None):
+        """Per-mode precision plan for FP32 factors (mmcsf_tune_precision):
+        every launch of mttkrp_all runs BF16 factor copies where that is faster
+        and the mode's output moves by at most error_budget (relative
+        Frobenius) against the FP32-factor output. Returns the plan with, per
+        mode, "dtype", "bf16_error", "ms_f32", "ms_bf16"."""
+        import torch
+        R = factors[0].shape[1]
+        if outs is None:
+            outs = [torch.empty((d, R), dtype=torch.float32, device=factors[0].device) for d in self.dims]
+        fp = (c_voidp * self.nd)(*[_ptr(f) for f in factors])
+        op = (c_voidp * self.nd)(*[_ptr(o) for o in outs])
+        pl = Plan()
+        check(lib().mmcsf_tune_precision(self._h, R, fp, op, ctypes.c_double(error_budget), _stream(stream),
+                                         ctypes.byref(pl)))
+        return self._plan_dict(pl)
 
     def set_plan(self, plan):
-        """Install a plan as returned by tune() (JSON round trips allowed:
-        string mode keys are accepted)."""
+        """Install a plan as returned by tune() / tune_precision() (JSON round
+        trips allowed: string mode keys are accepted)."""
         pl = Plan()
+        dt = {"f32": DTYPE_F32, "bf16": DTYPE_BF16}
+        pl.factor_dtype = dt[plan.get("dtype", "f32")]
+        pl.mixed = 1 if plan.get("mixed") else 0
         for m, e in plan.items():
+            if m in ("dtype", "mixed", "fiber_threshold", "convert_ms"):
+                continue
             if m == "pair":
                 pl.pair = 1 if e.get("use") else 0
                 pl.pair_chunk = e.get("chunk", 0)
                 pl.pair_min_blocks = e.get("min_blocks", 0)
                 pl.pair_kernel = e.get("kernel", 0)
+                pl.pair_dtype = dt[e.get("dtype", "f32")]
                 continue
             m = int(m)
             pl.traversal[m] = e["traversal"]
             pl.chunk[m] = e["chunk"]
             pl.min_blocks[m] = e.get("min_blocks", 0)
             pl.kernel[m] = e.get("kernel", 0)
+            pl.mode_dtype[m] = dt[e.get("dtype", "f32")]
         check(lib().mmcsf_set_plan(self._h, ctypes.byref(pl)))
 
     def cpd(self, rank, max_iters=10, tol=1e-5, precision="fp32", init=None, seed=0, graph=True, stream=None,
@@ -605,6 +646,34 @@ class Format:
         n = ctypes.c_int()
         check(lib().mmcsf_format_last_launches(self._h, ctypes.byref(n)))
         return n.value
+
+
+def autotune(coo, factors, impl=IMPL_MMCSF, mode=0, views=0, partition_rule=0, f_candidates=(0, 128, 32),
+             error_budget=0.0, outs=None, stream=None):
+    """Build the format for every fiber-split threshold in f_candidates (0 =
+    no split), tune each (per-mode precision within error_budget for MM-CSF),
+    and return (the fastest format, its plan) (mmcsf_autotune). factors: FP32
+    CUDA tensors."""
+    import torch
+    nd, dims, _ = coo.info()
+    R = factors[0].shape[1]
+    if outs is None:
+        outs = [torch.empty((d, R), dtype=torch.float32, device=factors[0].device) for d in dims]
+    o = BuildOpts()
+    o.impl, o.mode, o.views, o.partition_rule = impl, mode, int(views), int(partition_rule)
+    fc = (c_u64 * len(f_candidates))(*[int(f) for f in f_candidates])
+    fp = (c_voidp * nd)(*[_ptr(f) for f in factors])
+    op = (c_voidp * nd)(*[_ptr(x) for x in outs])
+    h = c_voidp()
+    pl = Plan()
+    check(lib().mmcsf_autotune(coo._h, ctypes.byref(o), fc, len(f_candidates), R, fp, op, ctypes.c_double(error_budget),
+                               _stream(stream), ctypes.byref(h), ctypes.byref(pl)))
+    F = Format.__new__(Format)
+    F._h = h
+    F.impl = impl
+    F.mode = mode
+    F.nd, F.dims, F.nnz = coo.info()
+    return F, F._plan_dict(pl)
 
 
 class _CudaArray:

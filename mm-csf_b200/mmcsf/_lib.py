@@ -47,7 +47,10 @@ class Plan(ctypes.Structure):
     _fields_ = [("traversal", c_int * 4), ("chunk", c_int * 4), ("min_blocks", c_int * 4),
                 ("kernel", c_int * 4), ("ms", ctypes.c_float * 4), ("pair", c_int), ("pair_chunk", c_int),
                 ("pair_min_blocks", c_int), ("pair_kernel", c_int),
-                ("pair_ms", ctypes.c_float)]
+                ("pair_ms", ctypes.c_float), ("factor_dtype", c_int), ("mixed", c_int), ("mode_dtype", c_int * 4),
+                ("pair_dtype", c_int), ("bf16_error", ctypes.c_float * 4), ("ms_f32", ctypes.c_float * 4),
+                ("ms_bf16", ctypes.c_float * 4), ("pair_ms_f32", ctypes.c_float), ("pair_ms_bf16", ctypes.c_float),
+                ("convert_ms", ctypes.c_float), ("fiber_threshold", c_int)]
 
 
 class CpdOpts(ctypes.Structure):
@@ -103,6 +106,11 @@ SIGNATURES = {
     "mmcsf_tune": ([c_voidp, c_int, c_int, ctypes.POINTER(c_voidp), ctypes.POINTER(c_voidp), c_voidp,
                     ctypes.POINTER(Plan)], c_int),
     "mmcsf_set_plan": ([c_voidp, ctypes.POINTER(Plan)], c_int),
+    "mmcsf_tune_precision": ([c_voidp, c_int, ctypes.POINTER(c_voidp), ctypes.POINTER(c_voidp), ctypes.c_double,
+                              c_voidp, ctypes.POINTER(Plan)], c_int),
+    "mmcsf_autotune": ([c_voidp, ctypes.POINTER(BuildOpts), c_u64p, c_int, c_int, ctypes.POINTER(c_voidp),
+                        ctypes.POINTER(c_voidp), ctypes.c_double, c_voidp, ctypes.POINTER(c_voidp),
+                        ctypes.POINTER(Plan)], c_int),
     "mmcsf_cpd": ([c_voidp, ctypes.POINTER(CpdOpts), ctypes.POINTER(c_voidp), ctypes.POINTER(c_voidp),
                    ctypes.POINTER(ctypes.c_double), ctypes.POINTER(CpdResult), c_voidp], c_int),
     "mmcsf_sampled_model": ([c_voidp, c_int, c_int, ctypes.POINTER(c_voidp), c_voidp, c_voidp, c_voidp], c_int),

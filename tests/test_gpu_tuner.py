@@ -1,0 +1,129 @@
+"""The autotuner's choices beyond launch shapes: the factor precision per mode
+(mmcsf_tune_precision) and the fiber-split threshold (mmcsf_autotune, the
+reference's -f, which it leaves to the user).
+
+* error budget 0 keeps every launch FP32; the outputs match the FP64 oracle
+  within 1e-5;
+* a budget BF16 fits within gives a plan whose BF16 modes read BF16-rounded
+  factors: every mode matches the FP64 oracle of the factors that mode read
+  (BF16-rounded or FP32) within 1e-5, and the plan's measured error of each
+  BF16 mode is its actual change against the FP32-factor output;
+* set_plan of that plan reproduces it exactly (a fresh format);
+* mmcsf_autotune picks one of the candidate thresholds, builds that format
+  (its arrays are the ones the threshold gives), and its outputs match;
+* the mttkrp command without -w / -f reports the threshold it chose."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+RTOL = 1e-5
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+@pytest.fixture(scope="module")
+def torch_cuda():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return torch
+
+
+def _close(got, ref, ctx):
+    got = np.asarray(got, np.float64)
+    fro = np.linalg.norm(got - ref) / np.linalg.norm(ref)
+    assert fro <= RTOL, (ctx, fro)
+
+
+def _tensor(torch, seed=3):
+    import mmcsf
+    dims = [3000, 9000, 200]
+    X = mmcsf.CooTensor.generate(dims, 300000, dist=[1, 1, 1], zipf_s=1.1, val_dist=1, seed=seed)
+    inds, vals = X.host_arrays()
+    return X, dims, [i.astype(np.uint64) for i in inds], vals
+
+
+@pytest.mark.parametrize("R", [16, 32])
+def test_precision_plan(R, torch_cuda):
+    torch = torch_cuda
+    import mmcsf
+    X, dims, inds, vals = _tensor(torch)
+    rng = np.random.default_rng(R)
+    U = [rng.random((d, R)).astype(np.float32) for d in dims]
+    Ud = [torch.tensor(u, device="cuda") for u in U]
+    Ub = [t.to(torch.bfloat16).float().cpu().numpy() for t in Ud]
+    ref32 = [O.mttkrp_coo_f64(dims, inds, vals, m, U) for m in range(3)]
+    ref16 = [O.mttkrp_coo_f64(dims, inds, vals, m, Ub) for m in range(3)]
+    F = mmcsf.Format(X, impl=mmcsf.IMPL_MMCSF, views=1)
+    # budget 0: FP32 everywhere
+    p0 = F.tune_precision(Ud, error_budget=0.0)
+    assert not p0["mixed"] and all(p0[m].get("dtype", "f32") == "f32" for m in range(3))
+    outs = F.mttkrp_all(Ud)
+    for m in range(3):
+        _close(outs[m].cpu().numpy(), ref32[m], ("budget 0", m))
+    # a budget BF16 fits within
+    p1 = F.tune_precision(Ud, error_budget=1.0)
+    assert p1["dtype"] == "f32"
+    for m in range(3):
+        if p1["mixed"]:
+            e = p1[m]["bf16_error"]
+            actual = np.linalg.norm(ref16[m] - ref32[m]) / np.linalg.norm(ref32[m])
+            assert 0 < e < 1e-2 and abs(e - actual) <= 0.1 * actual + 1e-6, (m, e, actual)
+    for rep in range(2):
+        outs = F.mttkrp_all(Ud)
+        for m in range(3):
+            read_bf16 = p1["mixed"] and (
+                (p1["pair"]["use"] and m in F.pair_modes() and p1["pair"]["dtype"] == "bf16")
+                or (not (p1["pair"]["use"] and m in F.pair_modes()) and p1[m]["dtype"] == "bf16"))
+            _close(outs[m].cpu().numpy(), ref16[m] if read_bf16 else ref32[m], ("mixed", m, read_bf16))
+    # the plan installs on a fresh format and gives the same outputs
+    G = mmcsf.Format(X, impl=mmcsf.IMPL_MMCSF, views=1)
+    G.set_plan(p1)
+    outs2 = G.mttkrp_all(Ud)
+    for m in range(3):
+        assert torch.allclose(outs2[m], outs[m], rtol=1e-6, atol=0), m
+
+
+def test_autotune_fiber_threshold(torch_cuda):
+    torch = torch_cuda
+    import mmcsf
+    X, dims, inds, vals = _tensor(torch, seed=5)
+    rng = np.random.default_rng(9)
+    R = 32
+    U = [rng.random((d, R)).astype(np.float32) for d in dims]
+    Ud = [torch.tensor(u, device="cuda") for u in U]
+    F, plan = mmcsf.autotune(X, Ud, views=1, f_candidates=(0, 64, 8))
+    assert plan["fiber_threshold"] in (0, 64, 8)
+    want = mmcsf.Format(X, impl=mmcsf.IMPL_MMCSF, fiber_threshold=plan["fiber_threshold"])
+    for name in ("fbrPtr0", "fbrIdx0", "fbrPtr1", "fbrIdx1"):
+        assert np.array_equal(F.export(2, name), want.export(2, name)), name
+    outs = F.mttkrp_all(Ud)
+    for m in range(3):
+        _close(outs[m].cpu().numpy(), O.mttkrp_coo_f64(dims, inds, vals, m, U), ("autotune", m))
+    # a plain re-tune of the chosen format reports the same threshold
+    assert F.tune(Ud)["fiber_threshold"] == plan["fiber_threshold"]
+    # B-CSF: the threshold tuned with the single-mode tuner
+    B, pb = mmcsf.autotune(X, Ud, impl=mmcsf.IMPL_BCSF, mode=1, f_candidates=(0, 16))
+    assert pb["fiber_threshold"] in (0, 16)
+    _close(B.mttkrp(1, Ud).cpu().numpy(), O.mttkrp_coo_f64(dims, inds, vals, 1, U), "bcsf autotune")
+
+
+def test_cli_autotune(torch_cuda, tmp_path):
+    rng = np.random.default_rng(4)
+    dims = [50, 70, 40]
+    n = 4000
+    lin = rng.choice(int(np.prod(dims)), size=n, replace=False)
+    inds = [np.asarray(i, np.uint64) for i in np.unravel_index(lin, dims)]
+    vals = np.round(rng.random(n) + 0.1, 3).astype(np.float32)
+    tns = tmp_path / "x.tns"
+    O.write_tns(str(tns), dims, inds, vals)
+    binp = os.path.join(ROOT, "mm-csf_b200", "bin", "mttkrp")
+    for extra in ([], ["-e", "0.01"]):
+        p = subprocess.run([binp, "-i", str(tns), "-R", "16", "-t", "12", "-c", "1", "-v", "1"] + extra,
+                           capture_output=True, text=True, timeout=300)
+        assert p.returncode == 0, p.stderr
+        assert "autotuned -f" in p.stdout and "Correctness pass!" in p.stdout, p.stdout

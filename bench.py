@@ -568,8 +568,10 @@ def cp_section(seed, scale):
         F.tune([t.to(torch.bfloat16) for t in init] if prec == "bf16" else init)  # plan for this factor type
         gcp.gcp_poisson(F, R, iters=3, lr=c["lr"], precision=prec, init=init)  # warm-up
         r = gcp.gcp_poisson(F, R, iters=c["iters"], lr=c["lr"], precision=prec, init=init)
+        pr = gcp.gcp_poisson(F, R, iters=20, lr=c["lr"], precision=prec, init=init, profile=True)
         runs[prec] = {"ms_per_iter": r["ms"][-1] / r["iters"], "iters": r["iters"], "loss_first": r["loss"][0],
-                      "loss_final": r["loss"][-1], "ms": r["ms"], "loss": r["loss"]}
+                      "loss_final": r["loss"][-1], "ms": r["ms"], "loss": r["loss"],
+                      "phase_ms_per_iter": {k: v / pr["iters"] for k, v in pr["phase_ms"].items()}}
     f32, b16 = runs["fp32"], runs["bf16"]
     target = f32["loss_final"] * (1 + 1e-4)
     t_b16 = next((t for t, l in zip(b16["ms"], b16["loss"]) if l <= target), None)

@@ -112,6 +112,7 @@ struct mmcsf_format {
   mmcsf::DevBuf stage_in[4], stage_out[4];
   int stage_R = 0;
   mmcsf::DevBuf vals_scratch;  // caller values reordered for a view traversal
+  mmcsf::DevBuf leaf64;        // FP64 accumulation of leaf-level (per-nonzero scatter) MTTKRP outputs
   mmcsf::DevBuf ttm_side;      // TTM: per-chunk partial rows of fibers that cross chunk starts
   cudaStream_t copy_in = nullptr, copy_out = nullptr;
   cudaEvent_t ev_in[4] = {}, ev_done[4] = {}, ev_start = nullptr;

@@ -87,6 +87,11 @@ void fill_args(Args<T>& a, const CsfPart& P, const float* vals_override, int slo
   a.out = out;
 }
 
+__global__ void k_add_f64(const double* __restrict__ in, uint64_t n, float* __restrict__ out) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    out[i] = (float)((double)out[i] + in[i]);
+}
+
 // MTTKRP on one part for tensor mode `mode`; out must be zeroed by the caller.
 int part_mttkrp(const mmcsf_format* F, const CsfPart& P, int mode, int R, int dtype, const void* const* U,
                 float* out, const mmcsf_kernel_cfg* cfg, cudaStream_t s, int* launches,
@@ -100,25 +105,44 @@ int part_mttkrp(const mmcsf_format* F, const CsfPart& P, int mode, int R, int dt
   int threads = cfg && cfg->block_threads > 0 ? cfg->block_threads : 256;
   const int mb = cfg && cfg->min_blocks > 0 ? cfg->min_blocks : 2;
   int kern = cfg && cfg->kernel > 0 ? cfg->kernel : (P.nd == 3 ? 2 : 1);
-  if (kern < 1 || kern > 4) return set_error(MMCSF_ERR_INVALID, "kernel must be 0, 1, 2, 3 or 4");
+  if (kern < 1 || kern > 5) return set_error(MMCSF_ERR_INVALID, "kernel must be 0, 1, 2, 3, 4 or 5");
   if (kern == 4 && (P.nd != 3 || lvl != 0)) kern = 3;  // per-fiber middle rows: the 3-D slice level only
-  if (kern == 4 && !P.mid.p) kern = 2;
+  if (kern == 5 && P.nd != 3) kern = 3;                 // vector index loads: 3-D
+  if ((kern == 4 || kern == 5) && !P.mid.p) kern = 2;
   if (kern == 3 && (!P.mid.p || (P.nd == 4 && lvl != 0 && lvl != 3))) kern = 2;  // per-nonzero walk not applicable
   if (kern == 2 && P.nd == 4) kern = 1;                                         // no 4-D branch-free fiber walk
   const int slot = CsfPart::cfib_slot((uint64_t)chunk);
   if (threads % 32 || threads > 256) return set_error(MMCSF_ERR_INVALID, "block_threads must be a multiple of 32, <= 256");
+  // the leaf level scatters one reduction per nonzero: accumulate in FP64
+  // (kept by the format), then add into the output once
+  const bool leaf = lvl == P.nd - 1;
+  const uint64_t nout = F->dims[mode] * (uint64_t)R;
+  double* o64 = nullptr;
+  if (leaf) {
+    mmcsf_format* Fm = const_cast<mmcsf_format*>(F);
+    if (Fm->leaf64.bytes < nout * 8) MMCSF_CUDA(Fm->leaf64.alloc(nout * 8));
+    o64 = Fm->leaf64.as<double>();
+    MMCSF_CUDA(cudaMemsetAsync(o64, 0, nout * 8, s));
+  }
   cudaError_t e;
   if (dtype == MMCSF_DTYPE_F32) {
     Args<float> a{};
     fill_args(a, P, vals_override, slot, chunk, R, U, out);
+    a.out64 = o64;
     e = launch_R<float>(a, P.nd, lvl, kern, threads, mb, s);
   } else {
     Args<__nv_bfloat16> a{};
     fill_args(a, P, vals_override, slot, chunk, R, U, out);
+    a.out64 = o64;
     e = launch_R<__nv_bfloat16>(a, P.nd, lvl, kern, threads, mb, s);
   }
   if (e != cudaSuccess) return set_error(MMCSF_ERR_CUDA, "MTTKRP launch failed: %s", cudaGetErrorString(e));
   if (launches) ++*launches;
+  if (leaf) {
+    k_add_f64<<<grid_for(nout, 256), 256, 0, s>>>(o64, nout, out);
+    MMCSF_LAUNCH_CHECK();
+    if (launches) ++*launches;
+  }
   return MMCSF_OK;
 }
 
@@ -324,7 +348,7 @@ extern "C" int mmcsf_mttkrp_pair(const mmcsf_format* F, int R, int factor_dtype,
   const int threads = cfg && cfg->block_threads > 0 ? cfg->block_threads : 256;
   const int mb = cfg && cfg->min_blocks > 0 ? cfg->min_blocks : (F->pair_mb[d] ? F->pair_mb[d] : 3);
   const int kern = cfg && cfg->kernel > 0 ? cfg->kernel : F->pair_kernel[d];
-  if (kern < 0 || kern > 4) return set_error(MMCSF_ERR_INVALID, "kernel must be 0, 1, 2, 3 or 4");
+  if (kern < 0 || kern > 5) return set_error(MMCSF_ERR_INVALID, "kernel must be 0, 1, 2, 3, 4 or 5");
   if (threads % 32 || threads > 256) return set_error(MMCSF_ERR_INVALID, "block_threads must be a multiple of 32, <= 256");
   const int slot = CsfPart::cfib_slot((uint64_t)chunk);
   cudaError_t e;
@@ -506,11 +530,12 @@ extern "C" int mmcsf_tune(mmcsf_format* F, int R, int factor_dtype, const void* 
     const int m = F->impl == MMCSF_IMPL_MMCSF ? i : F->mode;
     float best = 1e30f;
     int bt = 1, bc = 512, bm = 2, bk = 1;
-    const int nkern = 4;
+    const int nkern = 5;
     for (int trav = 1; trav <= 2 && st == MMCSF_OK; ++trav) {
       if (trav == 2 && !F->views[m].present) continue;
       for (int kern = 1; kern <= nkern && st == MMCSF_OK; ++kern) {
       if (kern == 2 && F->nd == 4) continue;  // 4-D has no branch-free fiber walk
+      if (kern == 5 && (F->nd != 3 || R < 16)) continue;  // vector index loads: 3-D, teams of >= 4 lanes
       if (kern == 4) {  // per-fiber middle rows: only where the mode is the slice level of a 3-D part with `mid`
         const CsfPart* tp = nullptr;
         if (trav == 2) tp = &F->views[m];
@@ -574,8 +599,8 @@ extern "C" int mmcsf_tune(mmcsf_format* F, int R, int factor_dtype, const void* 
       native_R(R) && R <= 128) {
     float bestp = 1e30f;
     int bpc = 0, bpm = 0, bpk = 0;
-    for (int kern : {2, 3, 4})
-    for (int mbv = 1; mbv <= 3 && st == MMCSF_OK && (kern == 3 || F->nd == 3); ++mbv)
+    for (int kern : {2, 3, 4, 5})
+    for (int mbv = 1; mbv <= 3 && st == MMCSF_OK && (kern == 3 || F->nd == 3) && (kern != 5 || R >= 16); ++mbv)
       for (int c : {256, 512, 1024}) {
         mmcsf_kernel_cfg cfg{};
         cfg.chunk = c;
@@ -839,12 +864,12 @@ extern "C" int mmcsf_set_plan(mmcsf_format* F, const mmcsf_plan* plan) {
     if (plan->traversal[m] == 2 && !F->views[m].present)
       return set_error(MMCSF_ERR_INVALID, "plan uses a view for mode %d that was not built", m);
     if (plan->traversal[m] < 0 || plan->traversal[m] > 2 || plan->chunk[m] < 0 || plan->kernel[m] < 0 ||
-        plan->kernel[m] > 4)
+        plan->kernel[m] > 5)
       return set_error(MMCSF_ERR_INVALID, "bad plan entry for mode %d", m);
     if (plan->mixed && plan->mode_dtype[m] != MMCSF_DTYPE_F32 && plan->mode_dtype[m] != MMCSF_DTYPE_BF16)
       return set_error(MMCSF_ERR_INVALID, "bad mode_dtype for mode %d", m);
   }
-  if (plan->pair_chunk < 0 || plan->pair_min_blocks < 0 || plan->pair_kernel < 0 || plan->pair_kernel > 4)
+  if (plan->pair_chunk < 0 || plan->pair_min_blocks < 0 || plan->pair_kernel < 0 || plan->pair_kernel > 5)
     return set_error(MMCSF_ERR_INVALID, "bad pair entry");
   if (plan->mixed && plan->pair_dtype != MMCSF_DTYPE_F32 && plan->pair_dtype != MMCSF_DTYPE_BF16)
     return set_error(MMCSF_ERR_INVALID, "bad pair_dtype");

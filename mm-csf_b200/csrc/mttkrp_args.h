@@ -31,7 +31,8 @@ struct Args {
   uint32_t R;
   const T* U[4];  // factor of mode order[l], by level l
   float* out;
-  float* out2;  // two-output walk: the middle mode's output
+  float* out2;    // two-output walk: the middle mode's output
+  double* out64;  // leaf-level outputs: per-nonzero scatters accumulate here in FP64 (converted by the host code)
 };
 
 template <class T, int R>

@@ -66,6 +66,16 @@ __device__ __forceinline__ void red4(float* p, float4 v) {
   asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(p), "f"(v.x), "f"(v.y), "f"(v.z), "f"(v.w)
                : "memory");
 }
+// The leaf-level scatter's reduction: four FP64 additions. A leaf row of a
+// skewed tensor receives up to ~10^6 per-nonzero terms, whose sequential FP32
+// rounding reaches ~1e-4 relative; in FP64 it stays far below 1e-5.
+__device__ __forceinline__ void red4_f64(double* p, float4 v) {
+  asm volatile(
+      "red.global.add.f64 [%0], %1;\n\tred.global.add.f64 [%0+8], %2;\n\t"
+      "red.global.add.f64 [%0+16], %3;\n\tred.global.add.f64 [%0+24], %4;" ::"l"(p),
+      "d"((double)v.x), "d"((double)v.y), "d"((double)v.z), "d"((double)v.w)
+      : "memory");
+}
 
 
 // largest f with fptr[f] <= x
@@ -120,6 +130,7 @@ __global__ void __launch_bounds__(256, MB) k_mttkrp(const Args<T> a) {
     return Row<T>::load(U + (uint64_t)row * R, c0 + (uint32_t)(v * G * 4));
   };
   auto rd = [&](uint32_t row, int v, float4 x) { red4(out + (uint64_t)row * R + c0 + v * G * 4, x); };
+  [[maybe_unused]] auto rd64 = [&](uint32_t row, int v, float4 x) { red4_f64(a.out64 + (uint64_t)row * R + c0 + v * G * 4, x); };
 
   const uint64_t team = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) / G;
   // Teams past the end stay in the loop (empty range) so every full-warp
@@ -263,7 +274,7 @@ __global__ void __launch_bounds__(256, MB) k_mttkrp(const Args<T> a) {
         } else {
           if (xb + jb + j < x1) {
 #pragma unroll
-            for (int v = 0; v < V; ++v) rd(kj[j], v, f4(val) * crow[v]);
+            for (int v = 0; v < V; ++v) rd64(kj[j], v, f4(val) * crow[v]);
           }
         }
       }
@@ -340,6 +351,7 @@ __global__ void __launch_bounds__(256, MB) k_mttkrp_flat(const Args<T> a) {
     return Row<T>::load(U + (uint64_t)row * R, c0 + (uint32_t)(v * G * 4));
   };
   auto rd = [&](uint32_t row, int v, float4 x) { red4(out + (uint64_t)row * R + c0 + v * G * 4, x); };
+  [[maybe_unused]] auto rd64 = [&](uint32_t row, int v, float4 x) { red4_f64(a.out64 + (uint64_t)row * R + c0 + v * G * 4, x); };
   auto rd2 = [&](uint32_t row, int v, float4 x) { red4(out2 + (uint64_t)row * R + c0 + v * G * 4, x); };
 
   const uint64_t team = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) / G;
@@ -490,7 +502,7 @@ __global__ void __launch_bounds__(256, MB) k_mttkrp_flat(const Args<T> a) {
           } else {
             if (xb + jb + j < x1) {
 #pragma unroll
-              for (int v = 0; v < V; ++v) rd(kj[j], v, pmul_s(val, rowB[v]));
+              for (int v = 0; v < V; ++v) rd64(kj[j], v, pmul_s(val, rowB[v]));
             }
           }
         }
@@ -553,6 +565,7 @@ __global__ void __launch_bounds__(256, MB) k_mttkrp_rows(const Args<T> a) {
     return Row<T>::load(U + (uint64_t)row * R, c0 + (uint32_t)(v * G * 4));
   };
   auto rd = [&](uint32_t row, int v, float4 x) { red4(out + (uint64_t)row * R + c0 + v * G * 4, x); };
+  [[maybe_unused]] auto rd64 = [&](uint32_t row, int v, float4 x) { red4_f64(a.out64 + (uint64_t)row * R + c0 + v * G * 4, x); };
 
   const uint64_t team = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) / G;
   const bool active = team * chunk < a.nnz;
@@ -681,7 +694,7 @@ __global__ void __launch_bounds__(256, MB) k_mttkrp_rows(const Args<T> a) {
               for (int v = 0; v < V; ++v) {
                 float4 m = pmul(rowA[v], rb[j][v]);
                 if constexpr (ND == 4) m = pmul(m, rq[j][v]);
-                rd(kj[j], v, pmul_s(val, m));
+                rd64(kj[j], v, pmul_s(val, m));
               }
             }
           }
@@ -986,6 +999,334 @@ __global__ void __launch_bounds__(256, MB) k_mttkrp_fib(const Args<T> a) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// Per-nonzero walks with vector index loads ("rowsv" / "pairv", kernel 5),
+// 3-D, G >= 4. The same walks as k_mttkrp_rows (slice, middle and leaf
+// levels) and k_mttkrp_pair, but a team reads its nonzeros' leaf indices,
+// middle indices and values four at a time: lane tl of a team holds nonzeros
+// 4 tl .. 4 tl + 3 of a super-block of 4G, loaded as one 16-byte vector per
+// array, and nonzero j of the super-block's sub-block sb (G nonzeros) comes
+// to the team by one shuffle from lane tb + sb G/4 + j/4, component j % 4.
+// Each of those loads touches one 64-byte (G = 4) to 512-byte (G = 32) span
+// per team instead of a G x 4-byte span per G nonzeros: about a quarter of
+// the L1 wavefronts the index loads cost. Needs chunk % 4 == 0 and 16-byte
+// aligned index/value arrays (the host checks both).
+template <class U4> __device__ __forceinline__ uint32_t comp4(const U4& u, int c) {
+  return c == 0 ? u.x : (c == 1 ? u.y : (c == 2 ? u.z : u.w));
+}
+__device__ __forceinline__ float comp4f(const float4& u, int c) {
+  return c == 0 ? u.x : (c == 1 ? u.y : (c == 2 ? u.z : u.w));
+}
+
+template <int OUT, int G, int V, class T, int MB, int PFX>
+__global__ void __launch_bounds__(256, MB) k_mttkrp_rowsv(const Args<T> a) {
+  static_assert(G >= 4 && G % 4 == 0, "vector index loads need teams of 4, 8, 16 or 32 lanes");
+  constexpr int LEAF = 2;
+  constexpr bool MIDL = OUT == 1;
+  constexpr uint32_t R = 4 * G * V;
+  constexpr uint32_t FLAG = 0x80000000u;
+  constexpr int PF = G > PFX ? PFX : G;
+  constexpr uint32_t SB = 4 * G;
+  const int lane = threadIdx.x & 31;
+  const int tl = lane & (G - 1);
+  const int tb = lane - tl;
+  const float* __restrict__ vals = a.vals;
+  const uint32_t* __restrict__ leaf = a.leaf;
+  const uint32_t* __restrict__ mid = a.mid;
+  const uint32_t* __restrict__ snz = a.snz;
+  const uint32_t* __restrict__ sidx = a.sidx;
+  const uint32_t chunk = a.chunk, nslc = a.nslc;
+  const T* __restrict__ U0 = a.U[0];
+  const T* __restrict__ U1 = a.U[1];
+  const T* __restrict__ UL = a.U[LEAF];
+  float* __restrict__ out = a.out;
+  const uint32_t c0 = (uint32_t)tl * 4;
+  auto ld = [&](const T* U, uint32_t row, int v) -> float4 {
+    return Row<T>::load(U + (uint64_t)row * R, c0 + (uint32_t)(v * G * 4));
+  };
+  auto rd = [&](uint32_t row, int v, float4 x) { red4(out + (uint64_t)row * R + c0 + v * G * 4, x); };
+  [[maybe_unused]] auto rd64 = [&](uint32_t row, int v, float4 x) {
+    red4_f64(a.out64 + (uint64_t)row * R + c0 + v * G * 4, x);
+  };
+
+  const uint64_t team = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) / G;
+  const bool active = team * chunk < a.nnz;
+  const uint64_t x0 = active ? team * chunk : a.nnz - 1;
+  const uint64_t x1 = active ? min(x0 + chunk, a.nnz) : x0;
+  uint32_t sl;
+  if (a.cslc) {
+    sl = active ? __ldg(a.cslc + team) : nslc - 1;
+  } else {
+    uint32_t lo = 0, hi = nslc - 1;
+    while (lo < hi) {
+      const uint32_t m = (lo + hi + 1) >> 1;
+      if ((uint64_t)__ldg(snz + m) <= x0) lo = m; else hi = m - 1;
+    }
+    sl = lo;
+  }
+  uint32_t ca = __ldg(sidx + sl);
+  uint64_t nxt = __ldg(snz + sl + 1);
+  float4 acc[V], rowA[V];
+#pragma unroll
+  for (int v = 0; v < V; ++v) {
+    acc[v] = f4(0.f);
+    if constexpr (OUT == LEAF || MIDL) rowA[v] = ld(U0, ca, v);
+  }
+  [[maybe_unused]] uint32_t bopen = 0;
+  if constexpr (MIDL) bopen = __ldg(mid + x0);
+
+  // this lane's four nonzeros of the super-block at offset its
+  auto load_sb = [&](uint32_t its, uint4& K, uint4& B, float4& W) {
+    const uint64_t xx = x0 + its + 4 * (uint32_t)tl;
+    if (xx + 3 < x1) {
+      K = __ldg(reinterpret_cast<const uint4*>(leaf + xx));
+      B = __ldg(reinterpret_cast<const uint4*>(mid + xx));
+      W = __ldg(reinterpret_cast<const float4*>(vals + xx));
+    } else {
+      K = make_uint4(0u, 0u, 0u, 0u);
+      B = K;
+      W = f4(0.f);
+      if (xx < x1) { K.x = __ldg(leaf + xx); B.x = __ldg(mid + xx); W.x = __ldg(vals + xx); }
+      if (xx + 1 < x1) { K.y = __ldg(leaf + xx + 1); B.y = __ldg(mid + xx + 1); W.y = __ldg(vals + xx + 1); }
+      if (xx + 2 < x1) { K.z = __ldg(leaf + xx + 2); B.z = __ldg(mid + xx + 2); W.z = __ldg(vals + xx + 2); }
+    }
+  };
+  uint4 Kc, Bc, Kn, Bn;
+  float4 Wc, Wn;
+  load_sb(0, Kc, Bc, Wc);
+  for (uint32_t its = 0; its < chunk; its += SB) {
+    load_sb(its + SB, Kn, Bn, Wn);  // the next super-block, while this one is processed
+    [[maybe_unused]] uint32_t bal[4] = {0u, 0u, 0u, 0u};  // middle level: fiber starts, by component
+    if constexpr (MIDL) {
+#pragma unroll
+      for (int c = 0; c < 4; ++c)
+        bal[c] = __ballot_sync(FULL, (comp4(Kc, c) & FLAG) && (x0 + its + 4 * (uint32_t)tl + c != x0));
+    }
+    for (int sb = 0; sb < 4; ++sb) {
+      const uint64_t xb = x0 + its + (uint32_t)sb * G;
+      const int src0 = tb + sb * (G / 4);
+      const bool slow = __any_sync(FULL, xb < x1 && xb + G > nxt);
+      auto block = [&](auto slow_tag) {
+        constexpr bool SLOW = decltype(slow_tag)::value;
+#pragma unroll
+        for (int jb = 0; jb < G; jb += PF) {
+          [[maybe_unused]] float4 rc[(OUT == 0 || MIDL) ? PF : 1][V];
+          [[maybe_unused]] float4 rb[MIDL ? 1 : PF][V];
+          [[maybe_unused]] uint32_t bjs[MIDL ? PF : 1];
+          uint32_t kj[PF];
+#pragma unroll
+          for (int j = 0; j < PF; ++j) {
+            const int jj = jb + j, src = src0 + (jj >> 2);
+            kj[j] = __shfl_sync(FULL, comp4(Kc, jj & 3), src) & ~FLAG;
+            const uint32_t bj = __shfl_sync(FULL, comp4(Bc, jj & 3), src);
+            if constexpr (MIDL) bjs[j] = bj;
+#pragma unroll
+            for (int v = 0; v < V; ++v) {
+              if constexpr (MIDL) rc[j][v] = ld(UL, kj[j], v);
+              else rb[j][v] = ld(U1, bj, v);
+              if constexpr (OUT == 0) rc[j][v] = ld(UL, kj[j], v);
+            }
+          }
+#pragma unroll
+          for (int j = 0; j < PF; ++j) {
+            const int jj = jb + j, src = src0 + (jj >> 2);
+            const float val = __shfl_sync(FULL, comp4f(Wc, jj & 3), src);
+            const uint64_t x = xb + jj;
+            if constexpr (MIDL) {
+              if ((bal[jj & 3] >> src) & 1u) {  // the open fiber ends before nonzero jj
+#pragma unroll
+                for (int v = 0; v < V; ++v) { rd(bopen, v, pmul(rowA[v], acc[v])); acc[v] = f4(0.f); }
+                bopen = bjs[j];
+              }
+            }
+            if constexpr (SLOW) {
+              if (x < x1 && x == nxt) {
+                if constexpr (OUT == 0) {
+#pragma unroll
+                  for (int v = 0; v < V; ++v) { rd(ca, v, acc[v]); acc[v] = f4(0.f); }
+                }
+                ++sl;
+                ca = __ldg(sidx + sl);
+                nxt = __ldg(snz + sl + 1);
+                if constexpr (OUT == LEAF || MIDL) {
+#pragma unroll
+                  for (int v = 0; v < V; ++v) rowA[v] = ld(U0, ca, v);
+                }
+              }
+            }
+            if constexpr (MIDL) {
+#pragma unroll
+              for (int v = 0; v < V; ++v) acc[v] = pfma_s(val, rc[j][v], acc[v]);
+            } else if constexpr (OUT == 0) {
+#pragma unroll
+              for (int v = 0; v < V; ++v) acc[v] = pfma(pmul_s(val, rb[j][v]), rc[j][v], acc[v]);
+            } else {
+              if (x < x1) {
+#pragma unroll
+                for (int v = 0; v < V; ++v) rd64(kj[j], v, pmul_s(val, pmul(rowA[v], rb[j][v])));
+              }
+            }
+          }
+        }
+      };
+      if (slow) block(std::true_type{});
+      else block(std::false_type{});
+    }
+    Kc = Kn; Bc = Bn; Wc = Wn;
+  }
+  if constexpr (OUT == 0) {
+    if (active) {
+#pragma unroll
+      for (int v = 0; v < V; ++v) rd(ca, v, acc[v]);
+    }
+  }
+  if constexpr (MIDL) {
+    if (active) {
+#pragma unroll
+      for (int v = 0; v < V; ++v) rd(bopen, v, pmul(rowA[v], acc[v]));
+    }
+  }
+}
+
+template <int G, int V, class T, int MB, int PFX>
+__global__ void __launch_bounds__(256, MB) k_mttkrp_pairv(const Args<T> a) {
+  static_assert(G >= 4 && G % 4 == 0, "vector index loads need teams of 4, 8, 16 or 32 lanes");
+  constexpr uint32_t R = 4 * G * V;
+  constexpr uint32_t FLAG = 0x80000000u;
+  constexpr int PF = G > PFX ? PFX : G;
+  constexpr uint32_t SB = 4 * G;
+  const int lane = threadIdx.x & 31;
+  const int tl = lane & (G - 1);
+  const int tb = lane - tl;
+  const float* __restrict__ vals = a.vals;
+  const uint32_t* __restrict__ leaf = a.leaf;
+  const uint32_t* __restrict__ mid = a.mid;
+  const uint32_t* __restrict__ snz = a.snz;
+  const uint32_t* __restrict__ sidx = a.sidx;
+  const uint32_t chunk = a.chunk, nslc = a.nslc;
+  const T* __restrict__ U0 = a.U[0];
+  const T* __restrict__ U1 = a.U[1];
+  const T* __restrict__ U2 = a.U[2];
+  float* __restrict__ out = a.out;
+  float* __restrict__ out2 = a.out2;
+  const uint32_t c0 = (uint32_t)tl * 4;
+  auto ld = [&](const T* U, uint32_t row, int v) -> float4 {
+    return Row<T>::load(U + (uint64_t)row * R, c0 + (uint32_t)(v * G * 4));
+  };
+  auto rd = [&](float* o, uint32_t row, int v, float4 x) { red4(o + (uint64_t)row * R + c0 + v * G * 4, x); };
+
+  const uint64_t team = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) / G;
+  const bool active = team * chunk < a.nnz;
+  const uint64_t x0 = active ? team * chunk : a.nnz - 1;
+  const uint64_t x1 = active ? min(x0 + chunk, a.nnz) : x0;
+  uint32_t sl;
+  if (a.cslc) {
+    sl = active ? __ldg(a.cslc + team) : nslc - 1;
+  } else {
+    uint32_t lo = 0, hi = nslc - 1;
+    while (lo < hi) {
+      const uint32_t m = (lo + hi + 1) >> 1;
+      if ((uint64_t)__ldg(snz + m) <= x0) lo = m; else hi = m - 1;
+    }
+    sl = lo;
+  }
+  uint32_t ca = __ldg(sidx + sl);
+  uint64_t nxt = __ldg(snz + sl + 1);
+  uint32_t bopen = __ldg(mid + x0);
+  float4 acc[V], accf[V], rowA[V];
+#pragma unroll
+  for (int v = 0; v < V; ++v) {
+    acc[v] = accf[v] = f4(0.f);
+    rowA[v] = ld(U0, ca, v);
+  }
+  auto load_sb = [&](uint32_t its, uint4& K, uint4& B, float4& W) {
+    const uint64_t xx = x0 + its + 4 * (uint32_t)tl;
+    if (xx + 3 < x1) {
+      K = __ldg(reinterpret_cast<const uint4*>(leaf + xx));
+      B = __ldg(reinterpret_cast<const uint4*>(mid + xx));
+      W = __ldg(reinterpret_cast<const float4*>(vals + xx));
+    } else {
+      K = make_uint4(0u, 0u, 0u, 0u);
+      B = K;
+      W = f4(0.f);
+      if (xx < x1) { K.x = __ldg(leaf + xx); B.x = __ldg(mid + xx); W.x = __ldg(vals + xx); }
+      if (xx + 1 < x1) { K.y = __ldg(leaf + xx + 1); B.y = __ldg(mid + xx + 1); W.y = __ldg(vals + xx + 1); }
+      if (xx + 2 < x1) { K.z = __ldg(leaf + xx + 2); B.z = __ldg(mid + xx + 2); W.z = __ldg(vals + xx + 2); }
+    }
+  };
+  uint4 Kc, Bc, Kn, Bn;
+  float4 Wc, Wn;
+  load_sb(0, Kc, Bc, Wc);
+  for (uint32_t its = 0; its < chunk; its += SB) {
+    load_sb(its + SB, Kn, Bn, Wn);
+    uint32_t bal[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c)
+      bal[c] = __ballot_sync(FULL, (comp4(Kc, c) & FLAG) && (x0 + its + 4 * (uint32_t)tl + c != x0));
+    for (int sb = 0; sb < 4; ++sb) {
+      const uint64_t xb = x0 + its + (uint32_t)sb * G;
+      const int src0 = tb + sb * (G / 4);
+      const bool slow = __any_sync(FULL, xb < x1 && xb + G > nxt);
+      auto block = [&](auto slow_tag) {
+        constexpr bool SLOW = decltype(slow_tag)::value;
+#pragma unroll
+        for (int jb = 0; jb < G; jb += PF) {
+          float4 rb[PF][V], rc[PF][V];
+          uint32_t bjs[PF];
+#pragma unroll
+          for (int j = 0; j < PF; ++j) {
+            const int jj = jb + j, src = src0 + (jj >> 2);
+            const uint32_t kj = __shfl_sync(FULL, comp4(Kc, jj & 3), src) & ~FLAG;
+            bjs[j] = __shfl_sync(FULL, comp4(Bc, jj & 3), src);
+#pragma unroll
+            for (int v = 0; v < V; ++v) {
+              rb[j][v] = ld(U1, bjs[j], v);
+              rc[j][v] = ld(U2, kj, v);
+            }
+          }
+#pragma unroll
+          for (int j = 0; j < PF; ++j) {
+            const int jj = jb + j, src = src0 + (jj >> 2);
+            const float val = __shfl_sync(FULL, comp4f(Wc, jj & 3), src);
+            const uint64_t x = xb + jj;
+            if ((bal[jj & 3] >> src) & 1u) {  // the open fiber ends before nonzero jj (in the open slice)
+#pragma unroll
+              for (int v = 0; v < V; ++v) { rd(out2, bopen, v, pmul(rowA[v], accf[v])); accf[v] = f4(0.f); }
+              bopen = bjs[j];
+            }
+            if constexpr (SLOW) {
+              if (x < x1 && x == nxt) {
+#pragma unroll
+                for (int v = 0; v < V; ++v) { rd(out, ca, v, acc[v]); acc[v] = f4(0.f); }
+                ++sl;
+                ca = __ldg(sidx + sl);
+                nxt = __ldg(snz + sl + 1);
+#pragma unroll
+                for (int v = 0; v < V; ++v) rowA[v] = ld(U0, ca, v);
+              }
+            }
+#pragma unroll
+            for (int v = 0; v < V; ++v) {
+              acc[v] = pfma(pmul_s(val, rb[j][v]), rc[j][v], acc[v]);
+              accf[v] = pfma_s(val, rc[j][v], accf[v]);
+            }
+          }
+        }
+      };
+      if (slow) block(std::true_type{});
+      else block(std::false_type{});
+    }
+    Kc = Kn; Bc = Bn; Wc = Wn;
+  }
+  if (active) {
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      rd(out, ca, v, acc[v]);
+      rd(out2, bopen, v, pmul(rowA[v], accf[v]));
+    }
+  }
+}
+
 // The 4-D two-output walk: the slice mode's MTTKRP, out[a] += v U1[b] (.)
 // U2[c] (.) U3[k], and the level-1 mode's, out2[b] += U0[a] (.) sum over the
 // (a, b) group of v U2[c] (.) U3[k], from one walk that gathers each
@@ -1175,6 +1516,39 @@ cudaError_t launch_fib(const Args<T>& a, int threads, int mb, cudaStream_t s) {
 template <int OUT, int G, int V, class T>
 cudaError_t launch_flat(const Args<T>& a, int threads, int mb, cudaStream_t s);
 
+template <int OUT, int G, int V, class T>
+cudaError_t launch_rowsv(const Args<T>& a, int threads, int mb, cudaStream_t s) {
+  const uint64_t teams = (a.nnz + a.chunk - 1) / a.chunk;
+  const uint64_t blocks = (teams * G + threads - 1) / threads;
+  switch (mb) {
+    case 1: k_mttkrp_rowsv<OUT, G, V, T, 2, 8><<<(unsigned)blocks, threads, 0, s>>>(a); break;
+    case 3: k_mttkrp_rowsv<OUT, G, V, T, 4, 4><<<(unsigned)blocks, threads, 0, s>>>(a); break;
+    case 4: k_mttkrp_rowsv<OUT, G, V, T, 5, 4><<<(unsigned)blocks, threads, 0, s>>>(a); break;
+    default: k_mttkrp_rowsv<OUT, G, V, T, 3, 8><<<(unsigned)blocks, threads, 0, s>>>(a); break;
+  }
+  return cudaGetLastError();
+}
+
+template <int G, int V, class T>
+cudaError_t launch_pairv(const Args<T>& a, int threads, int mb, cudaStream_t s) {
+  const uint64_t teams = (a.nnz + a.chunk - 1) / a.chunk;
+  const uint64_t blocks = (teams * G + threads - 1) / threads;
+  switch (mb) {
+    case 1: k_mttkrp_pairv<G, V, T, 2, 8><<<(unsigned)blocks, threads, 0, s>>>(a); break;
+    case 3: k_mttkrp_pairv<G, V, T, 4, 4><<<(unsigned)blocks, threads, 0, s>>>(a); break;
+    case 4: k_mttkrp_pairv<G, V, T, 5, 4><<<(unsigned)blocks, threads, 0, s>>>(a); break;
+    default: k_mttkrp_pairv<G, V, T, 3, 8><<<(unsigned)blocks, threads, 0, s>>>(a); break;
+  }
+  return cudaGetLastError();
+}
+
+// The vector index loads need chunk % 4 == 0 and 16-byte aligned arrays.
+template <class T>
+bool vec_ok(const Args<T>& a) {
+  auto al = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; };
+  return a.chunk % 4 == 0 && al(a.vals) && al(a.leaf) && al(a.mid);
+}
+
 // kern 2: the branch-free fiber walk with both outputs; otherwise the
 // per-nonzero form
 
@@ -1226,6 +1600,16 @@ cudaError_t launch_rows(const Args<T>& a, int threads, int mb, cudaStream_t s) {
 // elsewhere as 3)
 template <int ND, int G, int V, class T>
 cudaError_t launch_lvl(const Args<T>& a, int lvl, int kern, int threads, int mb, cudaStream_t s) {
+  if constexpr (ND == 3 && G >= 4) {
+    if (kern == 5 && vec_ok(a)) {
+      switch (lvl) {
+        case 0: return launch_rowsv<0, G, V, T>(a, threads, mb, s);
+        case 1: return launch_rowsv<1, G, V, T>(a, threads, mb, s);
+        default: return launch_rowsv<2, G, V, T>(a, threads, mb, s);
+      }
+    }
+  }
+  if (kern == 5) kern = 3;  // 4-D, R < 16 or unaligned: the per-nonzero walk with scalar index loads
   if constexpr (ND == 3)
     if (kern == 4 && lvl == 0) return launch_fib<false, G, V, T>(a, threads, mb, s);
   if (kern == 4) kern = 3;  // the per-fiber middle row applies to the 3-D slice level; elsewhere the per-nonzero walk
@@ -1268,7 +1652,8 @@ cudaError_t launch_fixed(const Args<T>& a, int nd, int lvl, int kern, int thread
 
 // The two-output walks (R <= 128). kern 2: the branch-free fiber walk with
 // both outputs; 4: the per-nonzero walk with the middle row once per fiber;
-// otherwise the per-nonzero form. 4-D runs its own walk.
+// 5: the per-nonzero form with vector index loads; otherwise the per-nonzero
+// form. 4-D runs its own walk.
 template <class T, int R>
 cudaError_t launch_pair_fixed(const Args<T>& a, int nd, int threads, int mb, int kern, cudaStream_t s) {
   if constexpr (R > 128) {
@@ -1276,6 +1661,8 @@ cudaError_t launch_pair_fixed(const Args<T>& a, int nd, int threads, int mb, int
   } else {
     constexpr int G = R / 4;
     if (nd == 4) return launch_pair4<G, 1, T>(a, threads, mb, s);
+    if constexpr (G >= 4)
+      if (kern == 5 && vec_ok(a)) return launch_pairv<G, 1, T>(a, threads, mb, s);
     if (kern == 4) return launch_fib<true, G, 1, T>(a, threads, mb, s);
     if (kern == 2) return launch_flat<3, G, 1, T>(a, threads, mb, s);
     return launch_pair<G, 1, T>(a, threads, mb, s);

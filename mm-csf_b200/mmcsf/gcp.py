@@ -126,7 +126,7 @@ def poisson_loss(fmt, factors, y, lam=None, precision="fp32", eps=1e-10, fused=T
 
 
 def gcp_poisson(fmt, rank, iters=100, lr=0.05, precision="fp32", init=None, seed=0, eps=1e-10,
-                stop_loss=None, rescale=True):
+                stop_loss=None, rescale=True, profile=False):
     """Projected-Adam Poisson CP (nonnegative factors, no lambda).
 
     init: optional list of dims[m] x rank nonnegative FP32 CUDA tensors
@@ -136,8 +136,12 @@ def gcp_poisson(fmt, rank, iters=100, lr=0.05, precision="fp32", init=None, seed
     factor entry, so one setting serves tensors of any size.
     stop_loss: stop once the loss is at or below this value (one host sync
     per iteration; None runs every iteration without host syncs).
+    profile: also time the phases of every iteration with CUDA events
+    (forward: the fused sampled-model / loss / slice-mode gradient pass and
+    the colsum terms; backward: the other modes' adjoints; optimizer: Adam
+    and the projection), returned as phase_ms summed over the iterations.
     Returns dict(loss=[...], ms=[...] cumulative device time after each
-    iteration, factors, iters, seconds)."""
+    iteration, factors, iters, seconds[, phase_ms])."""
     dev = torch.device("cuda")
     g = torch.Generator(device="cpu").manual_seed(seed)
     if init is None:
@@ -163,14 +167,23 @@ def gcp_poisson(fmt, rank, iters=100, lr=0.05, precision="fp32", init=None, seed
     t0 = time.perf_counter()
     ev[0].record()
     n_done = 0
+    pev = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(iters)] if profile else None
     for it in range(iters):
+        if profile:
+            pev[it][0].record()
         opt.zero_grad(set_to_none=True)
         loss = poisson_loss(fmt, masters, y, None, precision, eps)
+        if profile:
+            pev[it][1].record()
         loss.backward()
+        if profile:
+            pev[it][2].record()
         opt.step()
         with torch.no_grad():
             for p in masters:
                 p.clamp_(min=0.0)
+        if profile:
+            pev[it][3].record()
         losses.append(loss.detach())
         ev[it + 1].record()
         n_done = it + 1
@@ -179,5 +192,10 @@ def gcp_poisson(fmt, rank, iters=100, lr=0.05, precision="fp32", init=None, seed
     torch.cuda.synchronize()
     secs = time.perf_counter() - t0
     ms = [ev[0].elapsed_time(ev[i + 1]) for i in range(n_done)]
-    return {"loss": [float(v) for v in torch.stack(losses).cpu()], "ms": ms, "iters": n_done, "seconds": secs,
-            "factors": [p.detach() for p in masters], "step": step}
+    out = {"loss": [float(v) for v in torch.stack(losses).cpu()], "ms": ms, "iters": n_done, "seconds": secs,
+           "factors": [p.detach() for p in masters], "step": step}
+    if profile:
+        names = ("forward", "backward", "optimizer")
+        out["phase_ms"] = {n: sum(pev[i][k].elapsed_time(pev[i][k + 1]) for i in range(n_done))
+                           for k, n in enumerate(names)}
+    return out

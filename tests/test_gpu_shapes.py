@@ -82,7 +82,7 @@ def test_skewed_shape_every_traversal(R, skewed, torch_cuda):
     want = [O.mttkrp_coo_f64(dims, inds, vals, m, U) for m in range(3)]
     F = mmcsf.Format(X, impl=mmcsf.IMPL_MMCSF, mode=0, views=2)
     for m in range(3):
-        for trav in (1, 2):
+        for trav in ((1, 2) if F.info(4 + m)["present"] else (1,)):  # the partition's slice mode has no view
             for kern in (1, 2, 3, 4, 5):
                 for mb in (1, 2, 3, 4):
                     cfg = {"traversal": trav, "kernel": kern, "min_blocks": mb, "chunk": 512}

@@ -139,6 +139,9 @@ typedef struct {
                                0 none, 1 = modes at the leaf level of the MM-CSF partition, 2 = every mode */
   int partition_ratio;      /* -h (Opt.MIfbTh): a mode wins a nonzero when its fiber is at least this many
                                times the others' (0 = the reference default 1); partition_rule 1 only */
+  int view_order;           /* mode order of the views (no counterpart in the reference): 0 the reference's
+                               order for a mode-m CSF (the rest by ascending length), 1 the rest by descending
+                               length, so the shortest mode (the smallest factor) sits at the leaf level */
 } mmcsf_build_opts;
 
 typedef struct mmcsf_format mmcsf_format;

@@ -689,7 +689,8 @@ extern "C" int mmcsf_build(mmcsf_coo* X, const mmcsf_build_opts* opts, void* str
   if (opts->impl == MMCSF_IMPL_BCSF) MMCSF_TRY(compute_bins(P, true, s, L));
   if (opts->impl == MMCSF_IMPL_MMCSF && opts->views) {
     // Slice-major views: a CSF whose level 0 is mode m, in the reference's
-    // order for a mode-m CSF (order_tensormode), fully sorted, no splits.
+    // order for a mode-m CSF (order_tensormode) or, with view_order 1, the
+    // remaining modes longest first, fully sorted, no splits.
     for (int m = 0; m < nd; ++m) {
       bool at_leaf = false, root_everywhere = true;
       for (int p = 0; p < nd; ++p) {
@@ -701,6 +702,7 @@ extern "C" int mmcsf_build(mmcsf_coo* X, const mmcsf_build_opts* opts, void* str
       if (root_everywhere) continue;  // the partitions already serve m at level 0
       int vo[4];
       order_modes(nd, X->dims, m, vo);
+      if (opts->view_order == 1) std::reverse(vo + 1, vo + nd);  // the shortest mode at the leaf level
       std::vector<int> vkeys(vo, vo + nd);
       DevBuf vs[4], vv, vperm;
       MMCSF_TRY(sort_coo(X, vkeys, vs, vv, s, L, &vperm));

@@ -212,11 +212,15 @@ class Format:
     reference default). partition_rule 0 is the reference as shipped (every
     nonzero in partition 2); 1 lets its partition heuristic decide
     (mm_partition_reuseBased without the override at src/util.h:2517), with
-    partition_ratio as -h. Replaces the builder chain the reference's main
-    runs (src/mttkrp.cu:72-389)."""
+    partition_ratio as -h. views: 0 none, 1 for the modes at the partition's
+    leaf level, 2 for every mode (CSFs with the mode at level 0, for MTTKRP);
+    view_order 0 orders a view's other modes as the reference orders a
+    mode-m CSF (ascending length), 1 longest first (the smallest factor at
+    the leaf). Replaces the builder chain the reference's main runs
+    (src/mttkrp.cu:72-389)."""
 
     def __init__(self, coo, impl=IMPL_MMCSF, mode=0, fiber_threshold=0, keep_coo=False, views=0,
-                 partition_rule=0, partition_ratio=0, stream=None):
+                 partition_rule=0, partition_ratio=0, stream=None, view_order=0):
         o = BuildOpts()
         o.impl = impl
         o.mode = mode
@@ -225,6 +229,7 @@ class Format:
         o.keep_coo = 1 if keep_coo else 0
         o.views = int(views)
         o.partition_ratio = int(partition_ratio)
+        o.view_order = int(view_order)
         h = c_voidp()
         check(lib().mmcsf_build(coo._h, ctypes.byref(o), _stream(stream), ctypes.byref(h)))
         self._h = h
@@ -649,7 +654,7 @@ class Format:
 
 
 def autotune(coo, factors, impl=IMPL_MMCSF, mode=0, views=0, partition_rule=0, f_candidates=(0, 128, 32),
-             error_budget=0.0, outs=None, stream=None):
+             error_budget=0.0, outs=None, stream=None, view_order=0):
     """Build the format for every fiber-split threshold in f_candidates (0 =
     no split), tune each (per-mode precision within error_budget for MM-CSF),
     and return (the fastest format, its plan) (mmcsf_autotune). factors: FP32
@@ -661,6 +666,7 @@ def autotune(coo, factors, impl=IMPL_MMCSF, mode=0, views=0, partition_rule=0, f
         outs = [torch.empty((d, R), dtype=torch.float32, device=factors[0].device) for d in dims]
     o = BuildOpts()
     o.impl, o.mode, o.views, o.partition_rule = impl, mode, int(views), int(partition_rule)
+    o.view_order = int(view_order)
     fc = (c_u64 * len(f_candidates))(*[int(f) for f in f_candidates])
     fp = (c_voidp * nd)(*[_ptr(f) for f in factors])
     op = (c_voidp * nd)(*[_ptr(x) for x in outs])

@@ -30,7 +30,7 @@ class GenSpec(ctypes.Structure):
 
 class BuildOpts(ctypes.Structure):
     _fields_ = [("impl", c_int), ("mode", c_int), ("fiber_threshold", c_u64), ("partition_rule", c_int),
-                ("keep_coo", c_int), ("views", c_int), ("partition_ratio", c_int)]
+                ("keep_coo", c_int), ("views", c_int), ("partition_ratio", c_int), ("view_order", c_int)]
 
 
 class PartInfo(ctypes.Structure):

@@ -51,6 +51,36 @@ template <> struct Row<__nv_bfloat16> {
   }
 };
 
+// Columns a lane owns. FP32 (and BF16 with one float4 per lane): lane tl of a
+// team of G holds columns 4 tl + 4 G v, v < V, so one load instruction of the
+// team covers a contiguous 16 G-byte piece of the row. BF16 with V even
+// (R >= 32): the lane holds the 4 V contiguous columns 4 V tl .. 4 V tl +
+// 4 V - 1, loaded as V / 2 16-byte vectors; a 64-byte row (R = 32) is then
+// one load of a 4-lane team, so a warp serves 8 nonzeros per instruction.
+template <class T, int G, int V>
+struct Cols {
+  static constexpr bool PACK = std::is_same<T, __nv_bfloat16>::value && V % 2 == 0;
+  static __device__ __forceinline__ uint32_t of(int tl, int v) {
+    return PACK ? (uint32_t)(4 * V * tl + 4 * v) : (uint32_t)(4 * tl + 4 * G * v);
+  }
+};
+// 4 BF16 values (the half h of a 16-byte vector of 8) widened to FP32
+__device__ __forceinline__ float4 bf16x4_to_f32(uint32_t lo, uint32_t hi) {
+  return make_float4(__uint_as_float(lo << 16), __uint_as_float(lo & 0xffff0000u), __uint_as_float(hi << 16),
+                     __uint_as_float(hi & 0xffff0000u));
+}
+// Row piece v of a lane (columns Cols::of(tl, v)) from row base `rb`.
+template <class T, int G, int V>
+__device__ __forceinline__ float4 load_piece(const T* rb, int tl, int v) {
+  if constexpr (Cols<T, G, V>::PACK) {
+    // both halves of the same 16-byte vector: the two calls read one address
+    const uint4 u = __ldg(reinterpret_cast<const uint4*>(rb + 4 * V * tl + 8 * (v / 2)));
+    return (v & 1) ? bf16x4_to_f32(u.z, u.w) : bf16x4_to_f32(u.x, u.y);
+  } else {
+    return Row<T>::load(rb, Cols<T, G, V>::of(tl, v));
+  }
+}
+
 __device__ __forceinline__ float4 f4(float a) { return make_float4(a, a, a, a); }
 __device__ __forceinline__ float4 operator*(float4 a, float4 b) {
   return make_float4(a.x * b.x, a.y * b.y, a.z * b.z, a.w * b.w);
@@ -125,12 +155,11 @@ __global__ void __launch_bounds__(256, MB) k_mttkrp(const Args<T> a) {
   const T* __restrict__ U2 = a.U[2];
   const T* __restrict__ UL = a.U[LEAF];
   float* __restrict__ out = a.out;
-  const uint32_t c0 = (uint32_t)tl * 4;  // this lane's first column
   auto ld = [&](const T* U, uint32_t row, int v) -> float4 {
-    return Row<T>::load(U + (uint64_t)row * R, c0 + (uint32_t)(v * G * 4));
+    return load_piece<T, G, V>(U + (uint64_t)row * R, tl, v);
   };
-  auto rd = [&](uint32_t row, int v, float4 x) { red4(out + (uint64_t)row * R + c0 + v * G * 4, x); };
-  [[maybe_unused]] auto rd64 = [&](uint32_t row, int v, float4 x) { red4_f64(a.out64 + (uint64_t)row * R + c0 + v * G * 4, x); };
+  auto rd = [&](uint32_t row, int v, float4 x) { red4(out + (uint64_t)row * R + Cols<T, G, V>::of(tl, v), x); };
+  [[maybe_unused]] auto rd64 = [&](uint32_t row, int v, float4 x) { red4_f64(a.out64 + (uint64_t)row * R + Cols<T, G, V>::of(tl, v), x); };
 
   const uint64_t team = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) / G;
   // Teams past the end stay in the loop (empty range) so every full-warp
@@ -346,13 +375,12 @@ __global__ void __launch_bounds__(256, MB) k_mttkrp_flat(const Args<T> a) {
   const T* __restrict__ U2 = a.U[2];
   float* __restrict__ out = a.out;
   float* __restrict__ out2 = a.out2;
-  const uint32_t c0 = (uint32_t)tl * 4;
   auto ld = [&](const T* U, uint32_t row, int v) -> float4 {
-    return Row<T>::load(U + (uint64_t)row * R, c0 + (uint32_t)(v * G * 4));
+    return load_piece<T, G, V>(U + (uint64_t)row * R, tl, v);
   };
-  auto rd = [&](uint32_t row, int v, float4 x) { red4(out + (uint64_t)row * R + c0 + v * G * 4, x); };
-  [[maybe_unused]] auto rd64 = [&](uint32_t row, int v, float4 x) { red4_f64(a.out64 + (uint64_t)row * R + c0 + v * G * 4, x); };
-  auto rd2 = [&](uint32_t row, int v, float4 x) { red4(out2 + (uint64_t)row * R + c0 + v * G * 4, x); };
+  auto rd = [&](uint32_t row, int v, float4 x) { red4(out + (uint64_t)row * R + Cols<T, G, V>::of(tl, v), x); };
+  [[maybe_unused]] auto rd64 = [&](uint32_t row, int v, float4 x) { red4_f64(a.out64 + (uint64_t)row * R + Cols<T, G, V>::of(tl, v), x); };
+  auto rd2 = [&](uint32_t row, int v, float4 x) { red4(out2 + (uint64_t)row * R + Cols<T, G, V>::of(tl, v), x); };
 
   const uint64_t team = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) / G;
   const bool active = team * chunk < a.nnz;
@@ -560,12 +588,11 @@ __global__ void __launch_bounds__(256, MB) k_mttkrp_rows(const Args<T> a) {
   const T* __restrict__ U2 = a.U[2];
   const T* __restrict__ UL = a.U[LEAF];
   float* __restrict__ out = a.out;
-  const uint32_t c0 = (uint32_t)tl * 4;
   auto ld = [&](const T* U, uint32_t row, int v) -> float4 {
-    return Row<T>::load(U + (uint64_t)row * R, c0 + (uint32_t)(v * G * 4));
+    return load_piece<T, G, V>(U + (uint64_t)row * R, tl, v);
   };
-  auto rd = [&](uint32_t row, int v, float4 x) { red4(out + (uint64_t)row * R + c0 + v * G * 4, x); };
-  [[maybe_unused]] auto rd64 = [&](uint32_t row, int v, float4 x) { red4_f64(a.out64 + (uint64_t)row * R + c0 + v * G * 4, x); };
+  auto rd = [&](uint32_t row, int v, float4 x) { red4(out + (uint64_t)row * R + Cols<T, G, V>::of(tl, v), x); };
+  [[maybe_unused]] auto rd64 = [&](uint32_t row, int v, float4 x) { red4_f64(a.out64 + (uint64_t)row * R + Cols<T, G, V>::of(tl, v), x); };
 
   const uint64_t team = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) / G;
   const bool active = team * chunk < a.nnz;
@@ -745,11 +772,10 @@ __global__ void __launch_bounds__(256, MB) k_mttkrp_pair(const Args<T> a) {
   const T* __restrict__ U2 = a.U[2];
   float* __restrict__ out = a.out;
   float* __restrict__ out2 = a.out2;
-  const uint32_t c0 = (uint32_t)tl * 4;
   auto ld = [&](const T* U, uint32_t row, int v) -> float4 {
-    return Row<T>::load(U + (uint64_t)row * R, c0 + (uint32_t)(v * G * 4));
+    return load_piece<T, G, V>(U + (uint64_t)row * R, tl, v);
   };
-  auto rd = [&](float* o, uint32_t row, int v, float4 x) { red4(o + (uint64_t)row * R + c0 + v * G * 4, x); };
+  auto rd = [&](float* o, uint32_t row, int v, float4 x) { red4(o + (uint64_t)row * R + Cols<T, G, V>::of(tl, v), x); };
 
   const uint64_t team = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) / G;
   const bool active = team * chunk < a.nnz;
@@ -885,11 +911,10 @@ __global__ void __launch_bounds__(256, MB) k_mttkrp_fib(const Args<T> a) {
   const T* __restrict__ U2 = a.U[2];
   float* __restrict__ out = a.out;
   float* __restrict__ out2 = a.out2;
-  const uint32_t c0 = (uint32_t)tl * 4;
   auto ld = [&](const T* U, uint32_t row, int v) -> float4 {
-    return Row<T>::load(U + (uint64_t)row * R, c0 + (uint32_t)(v * G * 4));
+    return load_piece<T, G, V>(U + (uint64_t)row * R, tl, v);
   };
-  auto rd = [&](float* o, uint32_t row, int v, float4 x) { red4(o + (uint64_t)row * R + c0 + v * G * 4, x); };
+  auto rd = [&](float* o, uint32_t row, int v, float4 x) { red4(o + (uint64_t)row * R + Cols<T, G, V>::of(tl, v), x); };
 
   const uint64_t team = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) / G;
   const bool active = team * chunk < a.nnz;
@@ -1040,13 +1065,12 @@ __global__ void __launch_bounds__(256, MB) k_mttkrp_rowsv(const Args<T> a) {
   const T* __restrict__ U1 = a.U[1];
   const T* __restrict__ UL = a.U[LEAF];
   float* __restrict__ out = a.out;
-  const uint32_t c0 = (uint32_t)tl * 4;
   auto ld = [&](const T* U, uint32_t row, int v) -> float4 {
-    return Row<T>::load(U + (uint64_t)row * R, c0 + (uint32_t)(v * G * 4));
+    return load_piece<T, G, V>(U + (uint64_t)row * R, tl, v);
   };
-  auto rd = [&](uint32_t row, int v, float4 x) { red4(out + (uint64_t)row * R + c0 + v * G * 4, x); };
+  auto rd = [&](uint32_t row, int v, float4 x) { red4(out + (uint64_t)row * R + Cols<T, G, V>::of(tl, v), x); };
   [[maybe_unused]] auto rd64 = [&](uint32_t row, int v, float4 x) {
-    red4_f64(a.out64 + (uint64_t)row * R + c0 + v * G * 4, x);
+    red4_f64(a.out64 + (uint64_t)row * R + Cols<T, G, V>::of(tl, v), x);
   };
 
   const uint64_t team = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) / G;
@@ -1209,11 +1233,10 @@ __global__ void __launch_bounds__(256, MB) k_mttkrp_pairv(const Args<T> a) {
   const T* __restrict__ U2 = a.U[2];
   float* __restrict__ out = a.out;
   float* __restrict__ out2 = a.out2;
-  const uint32_t c0 = (uint32_t)tl * 4;
   auto ld = [&](const T* U, uint32_t row, int v) -> float4 {
-    return Row<T>::load(U + (uint64_t)row * R, c0 + (uint32_t)(v * G * 4));
+    return load_piece<T, G, V>(U + (uint64_t)row * R, tl, v);
   };
-  auto rd = [&](float* o, uint32_t row, int v, float4 x) { red4(o + (uint64_t)row * R + c0 + v * G * 4, x); };
+  auto rd = [&](float* o, uint32_t row, int v, float4 x) { red4(o + (uint64_t)row * R + Cols<T, G, V>::of(tl, v), x); };
 
   const uint64_t team = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) / G;
   const bool active = team * chunk < a.nnz;
@@ -1356,11 +1379,10 @@ __global__ void __launch_bounds__(256, MB) k_mttkrp_pair4(const Args<T> a) {
   const T* __restrict__ U3 = a.U[3];
   float* __restrict__ out = a.out;
   float* __restrict__ out2 = a.out2;
-  const uint32_t c0 = (uint32_t)tl * 4;
   auto ld = [&](const T* U, uint32_t row, int v) -> float4 {
-    return Row<T>::load(U + (uint64_t)row * R, c0 + (uint32_t)(v * G * 4));
+    return load_piece<T, G, V>(U + (uint64_t)row * R, tl, v);
   };
-  auto rd = [&](float* o, uint32_t row, int v, float4 x) { red4(o + (uint64_t)row * R + c0 + v * G * 4, x); };
+  auto rd = [&](float* o, uint32_t row, int v, float4 x) { red4(o + (uint64_t)row * R + Cols<T, G, V>::of(tl, v), x); };
 
   const uint64_t team = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) / G;
   const bool active = team * chunk < a.nnz;
@@ -1642,10 +1664,21 @@ cudaError_t launch_lvl(const Args<T>& a, int lvl, int kern, int threads, int mb,
 // Launch for one rank R (a compile-time constant: G lanes per row, V float4
 // per lane, R = 4 G V). Each R is instantiated in its own translation unit
 // (mttkrp_r<R>.cu) so the kernel variants compile in parallel.
+// Lanes per factor row (G) and float4 per lane (V) for rank R: FP32 rows are
+// covered by one 16-byte vector per lane (G = R / 4, at most 32); BF16 rows
+// of R >= 32 by V = 2 (two float4 from one 16-byte vector of 8 BF16), so
+// G = R / 8 lanes read a row with one load each.
+template <class T, int R>
+struct TeamShape {
+  static constexpr bool BF = std::is_same<T, __nv_bfloat16>::value && R >= 32;
+  static constexpr int G = BF ? (R / 8 > 32 ? 32 : R / 8) : (R >= 128 ? 32 : R / 4);
+  static constexpr int V = R / (4 * G);
+};
+
 template <class T, int R>
 cudaError_t launch_fixed(const Args<T>& a, int nd, int lvl, int kern, int threads, int mb, cudaStream_t s) {
-  constexpr int G = R >= 128 ? 32 : R / 4;
-  constexpr int V = R / (4 * G);
+  constexpr int G = TeamShape<T, R>::G;
+  constexpr int V = TeamShape<T, R>::V;
   return nd == 3 ? launch_lvl<3, G, V, T>(a, lvl, kern, threads, mb, s)
                  : launch_lvl<4, G, V, T>(a, lvl, kern, threads, mb, s);
 }
@@ -1659,13 +1692,14 @@ cudaError_t launch_pair_fixed(const Args<T>& a, int nd, int threads, int mb, int
   if constexpr (R > 128) {
     return cudaErrorInvalidValue;
   } else {
-    constexpr int G = R / 4;
-    if (nd == 4) return launch_pair4<G, 1, T>(a, threads, mb, s);
+    constexpr int G = TeamShape<T, R>::G;
+    constexpr int V = TeamShape<T, R>::V;
+    if (nd == 4) return launch_pair4<G, V, T>(a, threads, mb, s);
     if constexpr (G >= 4)
-      if (kern == 5 && vec_ok(a)) return launch_pairv<G, 1, T>(a, threads, mb, s);
-    if (kern == 4) return launch_fib<true, G, 1, T>(a, threads, mb, s);
-    if (kern == 2) return launch_flat<3, G, 1, T>(a, threads, mb, s);
-    return launch_pair<G, 1, T>(a, threads, mb, s);
+      if (kern == 5 && vec_ok(a)) return launch_pairv<G, V, T>(a, threads, mb, s);
+    if (kern == 4) return launch_fib<true, G, V, T>(a, threads, mb, s);
+    if (kern == 2) return launch_flat<3, G, V, T>(a, threads, mb, s);
+    return launch_pair<G, V, T>(a, threads, mb, s);
   }
 }
 

@@ -1216,6 +1216,16 @@ def main():
             "ms": pms.value, "rows_per_s": nnz / (pms.value / 1e3),
             "what": f"{nnz} rows of the {dims[leafm]} x {R} FP32 mode-{leafm} factor gathered by the workload's "
                     f"mode-{leafm} indices and summed (mmcsf_probe_gather), nothing else"}
+        if R in (16, 32, 64):
+            # the same rows landed in shared memory by the copy engine (one bulk copy per row, mbarriers)
+            tma = {}
+            for st_, w_ in ((4, 8), (8, 6)):
+                tms = ctypes.c_float()
+                rc = _mlib().mmcsf_probe_gather_tma(ctypes.c_void_p(inds_dev[leafm].data_ptr()), ctypes.c_uint64(nnz),
+                                                    ctypes.c_void_p(U[leafm].data_ptr()), ctypes.c_uint64(dims[leafm]),
+                                                    R, st_, w_, 3, ctypes.byref(tms), ctypes.c_void_p(stream.cuda_stream))
+                tma[f"stages{st_}_warps{w_}"] = tms.value if rc == 0 else None
+            roofline["gather_ceiling"]["tma_bulk_copy_ms"] = tma
     cpu = None
     if not a.no_cpu and world == 1:
         inds_h, vals_h = X.host_arrays()

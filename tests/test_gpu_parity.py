@@ -503,7 +503,8 @@ def test_views_and_tuner(nd, torch_cuda):
             out = F.mttkrp(m, Ud, cfg={"traversal": trav})
             _check_close(out.cpu().numpy(), ref[m], ("view", nd, m, trav))
     plan = F.tune(Ud)
-    assert set(plan) == set(range(nd)) | {"pair"}
+    assert set(plan) == set(range(nd)) | {"pair", "dtype", "mixed", "fiber_threshold"}
+    assert plan["dtype"] == "f32" and plan["mixed"] is False
     assert plan["pair"]["use"] in (True, False) and (nd == 3 or not plan["pair"]["use"])
     outs = F.mttkrp_all(Ud)
     torch.cuda.synchronize()

@@ -570,6 +570,7 @@ int chunk_fibers(CsfPart& P, cudaStream_t s, Launches& L) {
 using namespace mmcsf;
 
 extern "C" int mmcsf_build(mmcsf_coo* X, const mmcsf_build_opts* opts, void* stream, mmcsf_format** out) {
+  MMCSF_RANGE("mmcsf_build");
   if (!X || !opts || !out) return set_error(MMCSF_ERR_INVALID, "null argument");
   const int nd = X->nd;
   if (opts->impl != MMCSF_IMPL_MMCSF && opts->impl != MMCSF_IMPL_BCSF && opts->impl != MMCSF_IMPL_HBCSF)

@@ -7,9 +7,21 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/mmcsf.h"
 
 namespace mmcsf {
+
+// An NVTX range over a scope, so that a profiler's timeline shows the
+// library's entry points and CP-ALS phases by name (header-only NVTX 3: with
+// no tool attached a push/pop is a call through a no-op pointer).
+struct Range {
+  explicit Range(const char* name) { nvtxRangePushA(name); }
+  ~Range() { nvtxRangePop(); }
+  Range(const Range&) = delete;
+  Range& operator=(const Range&) = delete;
+};
 
 // Record a message for mmcsf_last_error() and return the status.
 int set_error(int status, const char* fmt, ...);
@@ -49,6 +61,8 @@ struct DevBuf {
 inline cudaStream_t S(void* s) { return static_cast<cudaStream_t>(s); }
 
 }  // namespace mmcsf
+
+#define MMCSF_RANGE(name) ::mmcsf::Range mmcsf_range_(name)
 
 // Evaluate a CUDA call; on failure record and return MMCSF_ERR_CUDA (or NOMEM).
 #define MMCSF_CUDA(call)                                                                        \

@@ -70,6 +70,7 @@ inline const char* parse_f32(const char* p, const char* e, float* out) {
 
 extern "C" int mmcsf_coo_create(int nd, const uint64_t* dims, uint64_t nnz, const uint32_t* const* inds,
                                 const float* vals, mmcsf_coo** out) {
+  MMCSF_RANGE("mmcsf_coo_create");
   if (!out || !dims || (nnz && (!inds || !vals))) return set_error(MMCSF_ERR_INVALID, "null argument");
   MMCSF_TRY(check_shape(nd, dims, nnz));
   mmcsf_coo* X = new (std::nothrow) mmcsf_coo;
@@ -94,6 +95,7 @@ extern "C" int mmcsf_coo_create(int nd, const uint64_t* dims, uint64_t nnz, cons
 
 extern "C" int mmcsf_coo_create_device(int nd, const uint64_t* dims, uint64_t nnz, const uint32_t* const* d_inds,
                                        const float* d_vals, void* stream, mmcsf_coo** out) {
+  MMCSF_RANGE("mmcsf_coo_create_device");
   if (!out || !dims || (nnz && (!d_inds || !d_vals))) return set_error(MMCSF_ERR_INVALID, "null argument");
   MMCSF_TRY(check_shape(nd, dims, nnz));
   mmcsf_coo* X = new (std::nothrow) mmcsf_coo;
@@ -119,6 +121,7 @@ extern "C" int mmcsf_coo_create_device(int nd, const uint64_t* dims, uint64_t nn
 }
 
 extern "C" int mmcsf_coo_load_tns(const char* path, mmcsf_coo** out) {
+  MMCSF_RANGE("mmcsf_coo_load_tns");
   if (!path || !out) return set_error(MMCSF_ERR_INVALID, "null argument");
   FILE* f = fopen(path, "rb");
   if (!f) return set_error(MMCSF_ERR_IO, "%s does not exist!", path);
@@ -326,6 +329,7 @@ extern "C" int mmcsf_coo_write_bin(mmcsf_coo* X, const char* path) {
 }
 
 extern "C" int mmcsf_coo_load_bin(const char* path, mmcsf_coo** out) {
+  MMCSF_RANGE("mmcsf_coo_load_bin");
   if (!path || !out) return set_error(MMCSF_ERR_INVALID, "null argument");
   FILE* f = fopen(path, "rb");
   if (!f) return set_error(MMCSF_ERR_IO, "%s does not exist!", path);

@@ -60,6 +60,7 @@ void coo_range(const uint32_t* const* ind, const float* vals, uint64_t x0, uint6
 
 extern "C" int mmcsf_mttkrp_coo_host(const mmcsf_coo* X, int mode, int R, const float* const* h_factors,
                                      float* h_out, int threads) {
+  MMCSF_RANGE("mmcsf_mttkrp_coo_host");
   if (!X || !h_factors || !h_out) return set_error(MMCSF_ERR_INVALID, "null argument");
   const int nd = X->nd;
   if (mode < 0 || mode >= nd) return set_error(MMCSF_ERR_INVALID, "Mode cannot be larger than tensor dimension.");

@@ -490,6 +490,7 @@ struct Als {
 
   // one ALS iteration, stream-ordered (capturable when prof is null)
   int iteration(double xnormsq, cudaGraphConditionalHandle h, int use_handle, Prof* prof = nullptr) {
+    MMCSF_RANGE("mmcsf_cpd.iteration");
     const void* U[4];
     for (int m = 0; m < nd; ++m) U[m] = fac[m].p;
     auto mark = [&](int ph) { if (prof) prof->mark(s, ph); };
@@ -645,6 +646,7 @@ int run_cpd(mmcsf_format* F, const mmcsf_cpd_opts* o, const float* const* d_init
 
 extern "C" int mmcsf_cpd(mmcsf_format* F, const mmcsf_cpd_opts* opts, const float* const* d_init,
                          float* const* d_factors_out, double* lambda_out, mmcsf_cpd_result* result, void* stream) {
+  MMCSF_RANGE("mmcsf_cpd");
   using namespace mmcsf;
   if (!F || !opts) return set_error(MMCSF_ERR_INVALID, "null argument");
   if (F->impl != MMCSF_IMPL_MMCSF) return set_error(MMCSF_ERR_INVALID, "CP-ALS needs an MM-CSF format (-t 12)");

@@ -57,6 +57,7 @@ bool starts(const char* s, const char* p, int* num) {
 
 extern "C" int mmcsf_format_export(const mmcsf_format* F, int part, const char* name, uint64_t* dst, uint64_t cap,
                                    uint64_t* count) {
+  MMCSF_RANGE("mmcsf_format_export");
   if (!F || !name) return set_error(MMCSF_ERR_INVALID, "null argument");
   if (part < 0 || part > 3) return set_error(MMCSF_ERR_INVALID, "bad part %d", part);
   const int nd = F->nd;

@@ -177,6 +177,7 @@ int bits_for(uint64_t v) {  // bits to hold values 0..v-1
 }  // namespace
 
 extern "C" int mmcsf_generate(const mmcsf_gen_spec* spec, void* stream, mmcsf_coo** out) {
+  MMCSF_RANGE("mmcsf_generate");
   using namespace mmcsf;
   if (!spec || !out) return set_error(MMCSF_ERR_INVALID, "null argument");
   const int nd = spec->nd;

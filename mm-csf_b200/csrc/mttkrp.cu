@@ -105,10 +105,11 @@ int part_mttkrp(const mmcsf_format* F, const CsfPart& P, int mode, int R, int dt
   int threads = cfg && cfg->block_threads > 0 ? cfg->block_threads : 256;
   const int mb = cfg && cfg->min_blocks > 0 ? cfg->min_blocks : 2;
   int kern = cfg && cfg->kernel > 0 ? cfg->kernel : (P.nd == 3 ? 2 : 1);
-  if (kern < 1 || kern > 5) return set_error(MMCSF_ERR_INVALID, "kernel must be 0, 1, 2, 3, 4 or 5");
+  if (kern < 1 || kern > 6) return set_error(MMCSF_ERR_INVALID, "kernel must be 0 .. 6");
   if (kern == 4 && (P.nd != 3 || lvl != 0)) kern = 3;  // per-fiber middle rows: the 3-D slice level only
+  if (kern == 6 && (P.nd != 3 || lvl != 0)) kern = 5;  // warp-interleaved walk: the 3-D slice level only
   if (kern == 5 && P.nd != 3) kern = 3;                 // vector index loads: 3-D
-  if ((kern == 4 || kern == 5) && !P.mid.p) kern = 2;
+  if ((kern == 4 || kern == 5 || kern == 6) && !P.mid.p) kern = 2;
   if (kern == 3 && (!P.mid.p || (P.nd == 4 && lvl != 0 && lvl != 3))) kern = 2;  // per-nonzero walk not applicable
   if (kern == 2 && P.nd == 4) kern = 1;                                         // no 4-D branch-free fiber walk
   const int slot = CsfPart::cfib_slot((uint64_t)chunk);
@@ -239,6 +240,7 @@ int with_padding(const mmcsf_format* F, int R, int dtype, const void* const* U, 
 
 extern "C" int mmcsf_mttkrp(const mmcsf_format* F, int mode, int R, int factor_dtype, const void* const* d_factors,
                             float* d_out, const mmcsf_kernel_cfg* cfg, void* stream) {
+  MMCSF_RANGE("mmcsf_mttkrp");
   MMCSF_TRY(check_call(F, R, factor_dtype));
   if (mode < 0 || mode >= F->nd) return set_error(MMCSF_ERR_INVALID, "Mode cannot be larger than tensor dimension.");
   if (!d_factors || !d_out) return set_error(MMCSF_ERR_INVALID, "null pointer");
@@ -296,6 +298,7 @@ __global__ void k_scale_cols(float* __restrict__ M, uint64_t rows, int R, const 
 extern "C" int mmcsf_cp_adjoint(const mmcsf_format* F, int mode, int R, int factor_dtype,
                                 const void* const* d_factors, const float* d_lambda, const float* d_grad,
                                 float* d_out, const mmcsf_kernel_cfg* cfg, void* stream) {
+  MMCSF_RANGE("mmcsf_cp_adjoint");
   MMCSF_TRY(check_call(F, R, factor_dtype));
   if (mode < 0 || mode >= F->nd) return set_error(MMCSF_ERR_INVALID, "Mode cannot be larger than tensor dimension.");
   if (!d_factors || !d_out || !d_grad) return set_error(MMCSF_ERR_INVALID, "null pointer");
@@ -328,6 +331,7 @@ extern "C" int mmcsf_cp_adjoint(const mmcsf_format* F, int mode, int R, int fact
 extern "C" int mmcsf_mttkrp_pair(const mmcsf_format* F, int R, int factor_dtype, const void* const* d_factors,
                                  float* d_out_slice, float* d_out_mid, int* modes, const mmcsf_kernel_cfg* cfg,
                                  void* stream) {
+  MMCSF_RANGE("mmcsf_mttkrp_pair");
   MMCSF_TRY(check_call(F, R, factor_dtype));
   if (F->impl != MMCSF_IMPL_MMCSF) return set_error(MMCSF_ERR_INVALID, "the two-output walk needs an MM-CSF format");
   const CsfPart* P = nullptr;
@@ -348,7 +352,7 @@ extern "C" int mmcsf_mttkrp_pair(const mmcsf_format* F, int R, int factor_dtype,
   const int threads = cfg && cfg->block_threads > 0 ? cfg->block_threads : 256;
   const int mb = cfg && cfg->min_blocks > 0 ? cfg->min_blocks : (F->pair_mb[d] ? F->pair_mb[d] : 3);
   const int kern = cfg && cfg->kernel > 0 ? cfg->kernel : F->pair_kernel[d];
-  if (kern < 0 || kern > 5) return set_error(MMCSF_ERR_INVALID, "kernel must be 0, 1, 2, 3, 4 or 5");
+  if (kern < 0 || kern > 6) return set_error(MMCSF_ERR_INVALID, "kernel must be 0 .. 6");
   if (threads % 32 || threads > 256) return set_error(MMCSF_ERR_INVALID, "block_threads must be a multiple of 32, <= 256");
   const int slot = CsfPart::cfib_slot((uint64_t)chunk);
   cudaError_t e;
@@ -390,6 +394,7 @@ bool pair_active(const mmcsf_format* F, int R, bool want, const mmcsf_kernel_cfg
 
 extern "C" int mmcsf_mttkrp_all(const mmcsf_format* F, int R, int factor_dtype, const void* const* d_factors,
                                 float* const* d_outs, const mmcsf_kernel_cfg* cfg, void* stream) {
+  MMCSF_RANGE("mmcsf_mttkrp_all");
   MMCSF_TRY(check_call(F, R, factor_dtype));
   if (!d_factors || !d_outs) return set_error(MMCSF_ERR_INVALID, "null pointer");
   if (F->impl != MMCSF_IMPL_MMCSF)
@@ -443,6 +448,7 @@ extern "C" int mmcsf_mttkrp_all(const mmcsf_format* F, int R, int factor_dtype, 
 // mode finishes. With pinned host buffers the copies and kernels overlap.
 extern "C" int mmcsf_mttkrp_all_host(mmcsf_format* F, int R, const float* const* h_factors, float* const* h_outs,
                                      const mmcsf_kernel_cfg* cfg, void* stream) {
+  MMCSF_RANGE("mmcsf_mttkrp_all_host");
   MMCSF_TRY(check_call(F, R, MMCSF_DTYPE_F32));
   if (!h_factors || !h_outs) return set_error(MMCSF_ERR_INVALID, "null pointer");
   if (F->impl != MMCSF_IMPL_MMCSF)
@@ -514,6 +520,7 @@ extern "C" int mmcsf_mttkrp_all_host(mmcsf_format* F, int R, const float* const*
 
 extern "C" int mmcsf_tune(mmcsf_format* F, int R, int factor_dtype, const void* const* d_factors,
                           float* const* d_outs, void* stream, mmcsf_plan* plan) {
+  MMCSF_RANGE("mmcsf_tune");
   MMCSF_TRY(check_call(F, R, factor_dtype));
   if (!d_factors || !d_outs) return set_error(MMCSF_ERR_INVALID, "null pointer");
   const int d = factor_dtype == MMCSF_DTYPE_BF16 ? 1 : 0;
@@ -530,12 +537,13 @@ extern "C" int mmcsf_tune(mmcsf_format* F, int R, int factor_dtype, const void* 
     const int m = F->impl == MMCSF_IMPL_MMCSF ? i : F->mode;
     float best = 1e30f;
     int bt = 1, bc = 512, bm = 2, bk = 1;
-    const int nkern = 5;
+    const int nkern = 6;
     for (int trav = 1; trav <= 2 && st == MMCSF_OK; ++trav) {
       if (trav == 2 && !F->views[m].present) continue;
       for (int kern = 1; kern <= nkern && st == MMCSF_OK; ++kern) {
       if (kern == 2 && F->nd == 4) continue;  // 4-D has no branch-free fiber walk
       if (kern == 5 && (F->nd != 3 || R < 16)) continue;  // vector index loads: 3-D, teams of >= 4 lanes
+      if (kern == 6 && (F->nd != 3 || R < 8)) continue;   // warp-interleaved walk: 3-D
       if (kern == 4) {  // per-fiber middle rows: only where the mode is the slice level of a 3-D part with `mid`
         const CsfPart* tp = nullptr;
         if (trav == 2) tp = &F->views[m];
@@ -599,8 +607,10 @@ extern "C" int mmcsf_tune(mmcsf_format* F, int R, int factor_dtype, const void* 
       native_R(R) && R <= 128) {
     float bestp = 1e30f;
     int bpc = 0, bpm = 0, bpk = 0;
-    for (int kern : {2, 3, 4, 5})
-    for (int mbv = 1; mbv <= 3 && st == MMCSF_OK && (kern == 3 || F->nd == 3) && (kern != 5 || R >= 16); ++mbv)
+    for (int kern : {2, 3, 4, 5, 6})
+    for (int mbv = 1; mbv <= 3 && st == MMCSF_OK && (kern == 3 || F->nd == 3) && (kern != 5 || R >= 16) &&
+                      (kern != 6 || R >= 8);
+         ++mbv)
       for (int c : {256, 512, 1024}) {
         mmcsf_kernel_cfg cfg{};
         cfg.chunk = c;
@@ -679,6 +689,7 @@ int rel_frob(const float* a, const float* b, uint64_t n, cudaStream_t s, double*
 
 extern "C" int mmcsf_tune_precision(mmcsf_format* F, int R, const float* const* d_factors, float* const* d_outs,
                                     double error_budget, void* stream, mmcsf_plan* plan) {
+  MMCSF_RANGE("mmcsf_tune_precision");
   MMCSF_TRY(check_call(F, R, MMCSF_DTYPE_F32));
   if (!d_factors || !d_outs) return set_error(MMCSF_ERR_INVALID, "null pointer");
   if (F->impl != MMCSF_IMPL_MMCSF)
@@ -814,6 +825,7 @@ float plan_step_ms(const mmcsf_format* F, const mmcsf_plan& p) {
 extern "C" int mmcsf_autotune(mmcsf_coo* X, const mmcsf_build_opts* base, const uint64_t* f_candidates,
                               int n_candidates, int R, const float* const* d_factors, float* const* d_outs,
                               double error_budget, void* stream, mmcsf_format** out, mmcsf_plan* plan) {
+  MMCSF_RANGE("mmcsf_autotune");
   if (!X || !base || !d_factors || !d_outs || !out) return set_error(MMCSF_ERR_INVALID, "null argument");
   static const uint64_t defaults[] = {0, 128, 32};
   if (!f_candidates || n_candidates <= 0) {
@@ -864,12 +876,12 @@ extern "C" int mmcsf_set_plan(mmcsf_format* F, const mmcsf_plan* plan) {
     if (plan->traversal[m] == 2 && !F->views[m].present)
       return set_error(MMCSF_ERR_INVALID, "plan uses a view for mode %d that was not built", m);
     if (plan->traversal[m] < 0 || plan->traversal[m] > 2 || plan->chunk[m] < 0 || plan->kernel[m] < 0 ||
-        plan->kernel[m] > 5)
+        plan->kernel[m] > 6)
       return set_error(MMCSF_ERR_INVALID, "bad plan entry for mode %d", m);
     if (plan->mixed && plan->mode_dtype[m] != MMCSF_DTYPE_F32 && plan->mode_dtype[m] != MMCSF_DTYPE_BF16)
       return set_error(MMCSF_ERR_INVALID, "bad mode_dtype for mode %d", m);
   }
-  if (plan->pair_chunk < 0 || plan->pair_min_blocks < 0 || plan->pair_kernel < 0 || plan->pair_kernel > 5)
+  if (plan->pair_chunk < 0 || plan->pair_min_blocks < 0 || plan->pair_kernel < 0 || plan->pair_kernel > 6)
     return set_error(MMCSF_ERR_INVALID, "bad pair entry");
   if (plan->mixed && plan->pair_dtype != MMCSF_DTYPE_F32 && plan->pair_dtype != MMCSF_DTYPE_BF16)
     return set_error(MMCSF_ERR_INVALID, "bad pair_dtype");

@@ -1496,6 +1496,224 @@ __global__ void __launch_bounds__(256, MB) k_mttkrp_pair4(const Args<T> a) {
   }
 }
 
+// A lane's piece of one factor row as loaded (FP32: V float4; BF16 with V
+// even: V / 2 16-byte vectors of 8 values; other BF16: V 8-byte vectors),
+// widened to FP32 only where it is used, so rows in flight hold half the
+// registers at BF16.
+template <class T, int G, int V>
+struct RawPiece {
+  static constexpr bool BF = std::is_same<T, __nv_bfloat16>::value;
+  static constexpr bool PACK = Cols<T, G, V>::PACK;
+  using W = std::conditional_t<!BF, float4, std::conditional_t<PACK, uint4, uint2>>;
+  static constexpr int N = PACK ? V / 2 : V;
+  W w[N];
+  __device__ __forceinline__ void load(const T* rb, int tl) {
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+      if constexpr (!BF) w[i] = __ldg(reinterpret_cast<const float4*>(rb + Cols<T, G, V>::of(tl, i)));
+      else if constexpr (PACK) w[i] = __ldg(reinterpret_cast<const uint4*>(rb + 4 * V * tl + 8 * i));
+      else w[i] = __ldg(reinterpret_cast<const uint2*>(rb + Cols<T, G, V>::of(tl, i)));
+    }
+  }
+  __device__ __forceinline__ float4 get(int v) const {
+    if constexpr (!BF) {
+      return w[v];
+    } else if constexpr (PACK) {
+      const uint4& u = w[v / 2];
+      return (v & 1) ? bf16x4_to_f32(u.z, u.w) : bf16x4_to_f32(u.x, u.y);
+    } else {
+      return bf16x4_to_f32(w[v].x, w[v].y);
+    }
+  }
+};
+
+// ---------------------------------------------------------------------------
+// Per-nonzero walks of a 3-D part with `mid` whose teams are interleaved over
+// one range of nonzeros per warp (kernel 6): the slice-level MTTKRP, out[a] +=
+// v U1[b] (.) U2[k], and with PAIR also the middle mode's, out2[b] += U0[a]
+// (.) sum over the fiber (a, b) of v U2[k] (the two-output walk).
+//
+// The warp owns the NT = 32 / G teams' chunks as one range [x0, x1). Team t
+// takes the groups of 4Q consecutive nonzeros g = NT j + t (j = 0, 1, ...),
+// and every lane of the team loads the group's leaf indices, middle indices
+// and values itself, Q 16-byte vectors per array. One load instruction of
+// the warp then reads the NT teams' adjacent vectors, one 128-byte line at
+// most (G >= 4), so the index loads cost 3Q L1 wavefronts per 4Q NT nonzeros
+// (0.19 per nonzero at G = 8, Q = 1) and nothing is broadcast; the shuffle
+// broadcast of the contiguous-chunk walks costs ~1.1 wavefronts per nonzero
+// at G = 8 (three shuffles per team per nonzero, four teams per shuffle, and
+// the index loads). Each team keeps its own slice state; with PAIR also its
+// own open fiber, which closes when the middle index or the slice changes, so
+// a fiber spread over several teams' groups is reduced once per team. Needs
+// chunk % 4 == 0 and 16-byte aligned index/value arrays; outputs zeroed by
+// the caller.
+template <bool PAIR, int Q, int G, int V, class T, int MB>
+__global__ void __launch_bounds__(256, MB) k_mttkrp_il(const Args<T> a) {
+  constexpr uint32_t NT = 32 / G;
+  constexpr uint32_t R = 4 * G * V;
+  constexpr uint32_t FLAG = 0x80000000u;
+  constexpr uint32_t NONE = 0xffffffffu;
+  constexpr uint32_t GS = 4 * Q;     // nonzeros per group
+  constexpr uint32_t STEP = GS * NT;  // nonzeros per warp iteration
+  using Piece = RawPiece<T, G, V>;
+  const int lane = threadIdx.x & 31;
+  const int tl = lane & (G - 1);
+  const uint32_t t = (uint32_t)lane / G;
+  const float* __restrict__ vals = a.vals;
+  const uint32_t* __restrict__ leaf = a.leaf;
+  const uint32_t* __restrict__ mid = a.mid;
+  const uint32_t* __restrict__ snz = a.snz;
+  const uint32_t* __restrict__ sidx = a.sidx;
+  const T* __restrict__ U0 = a.U[0];
+  const T* __restrict__ U1 = a.U[1];
+  const T* __restrict__ U2 = a.U[2];
+  float* __restrict__ out = a.out;
+  [[maybe_unused]] float* __restrict__ out2 = a.out2;
+  auto rd = [&](float* o, uint32_t row, int v, float4 x) { red4(o + (uint64_t)row * R + Cols<T, G, V>::of(tl, v), x); };
+
+  // the warp's range (warp-uniform; the kernel has no warp-collective steps)
+  const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t span = (uint64_t)a.chunk * NT;
+  const uint64_t x0 = warp * span;
+  if (x0 >= a.nnz) return;
+  const uint64_t x1 = min(x0 + span, a.nnz);
+  uint32_t sl;
+  if (a.cslc) {
+    sl = __ldg(a.cslc + warp * NT);  // the slice of nonzero (warp NT) chunk = x0
+  } else {
+    uint32_t lo = 0, hi = a.nslc - 1;
+    while (lo < hi) {
+      const uint32_t m = (lo + hi + 1) >> 1;
+      if ((uint64_t)__ldg(snz + m) <= x0) lo = m; else hi = m - 1;
+    }
+    sl = lo;
+  }
+  uint32_t ca = __ldg(sidx + sl);
+  uint64_t nxt = __ldg(snz + sl + 1);
+  float4 acc[V];
+  [[maybe_unused]] float4 accf[V], rowA[V];
+#pragma unroll
+  for (int v = 0; v < V; ++v) {
+    acc[v] = f4(0.f);
+    if constexpr (PAIR) {
+      accf[v] = f4(0.f);
+      rowA[v] = load_piece<T, G, V>(U0 + (uint64_t)ca * R, tl, v);
+    }
+  }
+  [[maybe_unused]] uint32_t bopen = NONE;
+
+  // this team's group of the warp iteration starting at xs; positions at or
+  // past x1 read as index 0, value 0 and are skipped
+  auto load_grp = [&](uint64_t xs, uint4 (&K)[Q], uint4 (&B)[Q], float4 (&W)[Q]) {
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      const uint64_t xx = xs + GS * t + 4 * q;
+      if (xx + 3 < x1) {
+        K[q] = __ldg(reinterpret_cast<const uint4*>(leaf + xx));
+        B[q] = __ldg(reinterpret_cast<const uint4*>(mid + xx));
+        W[q] = __ldg(reinterpret_cast<const float4*>(vals + xx));
+      } else {
+        K[q] = make_uint4(0u, 0u, 0u, 0u);
+        B[q] = K[q];
+        W[q] = f4(0.f);
+        if (xx < x1) { K[q].x = __ldg(leaf + xx); B[q].x = __ldg(mid + xx); W[q].x = __ldg(vals + xx); }
+        if (xx + 1 < x1) { K[q].y = __ldg(leaf + xx + 1); B[q].y = __ldg(mid + xx + 1); W[q].y = __ldg(vals + xx + 1); }
+        if (xx + 2 < x1) { K[q].z = __ldg(leaf + xx + 2); B[q].z = __ldg(mid + xx + 2); W[q].z = __ldg(vals + xx + 2); }
+      }
+    }
+  };
+  uint4 Kc[Q], Bc[Q], Kn[Q], Bn[Q];
+  float4 Wc[Q], Wn[Q];
+  load_grp(x0, Kc, Bc, Wc);
+  for (uint64_t xs = x0; xs < x1; xs += STEP) {
+    load_grp(xs + STEP, Kn, Bn, Wn);  // the next group, while this one is processed
+    const uint64_t xg = xs + GS * t;
+    Piece rb[GS], rc[GS];
+#pragma unroll
+    for (int j = 0; j < (int)GS; ++j) {
+      const uint32_t k = comp4(Kc[j >> 2], j & 3) & ~FLAG;
+      const uint32_t b = comp4(Bc[j >> 2], j & 3);
+      rb[j].load(U1 + (uint64_t)b * R, tl);
+      rc[j].load(U2 + (uint64_t)k * R, tl);
+    }
+#pragma unroll
+    for (int j = 0; j < (int)GS; ++j) {
+      const uint64_t x = xg + j;
+      if (x < x1) {
+        const float val = comp4f(Wc[j >> 2], j & 3);
+        if (x >= nxt) {  // the team's slice ends before nonzero x
+#pragma unroll
+          for (int v = 0; v < V; ++v) { rd(out, ca, v, acc[v]); acc[v] = f4(0.f); }
+          if constexpr (PAIR) {
+            if (bopen != NONE) {
+#pragma unroll
+              for (int v = 0; v < V; ++v) rd(out2, bopen, v, pmul(rowA[v], accf[v]));
+            }
+#pragma unroll
+            for (int v = 0; v < V; ++v) accf[v] = f4(0.f);
+            bopen = NONE;
+          }
+          do {
+            ++sl;
+            nxt = __ldg(snz + sl + 1);
+          } while (x >= nxt);
+          ca = __ldg(sidx + sl);
+          if constexpr (PAIR) {
+#pragma unroll
+            for (int v = 0; v < V; ++v) rowA[v] = load_piece<T, G, V>(U0 + (uint64_t)ca * R, tl, v);
+          }
+        }
+        if constexpr (PAIR) {
+          const uint32_t b = comp4(Bc[j >> 2], j & 3);
+          if (b != bopen) {  // the team's open fiber ends before nonzero x
+            if (bopen != NONE) {
+#pragma unroll
+              for (int v = 0; v < V; ++v) rd(out2, bopen, v, pmul(rowA[v], accf[v]));
+            }
+#pragma unroll
+            for (int v = 0; v < V; ++v) accf[v] = f4(0.f);
+            bopen = b;
+          }
+        }
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+          const float4 c = rc[j].get(v);
+          acc[v] = pfma(pmul_s(val, rb[j].get(v)), c, acc[v]);
+          if constexpr (PAIR) accf[v] = pfma_s(val, c, accf[v]);
+        }
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < Q; ++q) { Kc[q] = Kn[q]; Bc[q] = Bn[q]; Wc[q] = Wn[q]; }
+  }
+#pragma unroll
+  for (int v = 0; v < V; ++v) rd(out, ca, v, acc[v]);
+  if constexpr (PAIR) {
+    if (bopen != NONE) {
+#pragma unroll
+      for (int v = 0; v < V; ++v) rd(out2, bopen, v, pmul(rowA[v], accf[v]));
+    }
+  }
+}
+
+// occupancy levels of kernel 6: (CTAs per SM the registers must allow, groups
+// of 4 nonzeros per team and iteration) = 1: (2, 2), 2: (2, 1), 3: (3, 1),
+// 4: (4, 1)
+template <bool PAIR, int G, int V, class T>
+cudaError_t launch_il(const Args<T>& a, int threads, int mb, cudaStream_t s) {
+  constexpr uint64_t NT = 32 / G;
+  const uint64_t teams = (a.nnz + a.chunk - 1) / a.chunk;
+  const uint64_t warps = (teams + NT - 1) / NT;
+  const uint64_t blocks = (warps * 32 + threads - 1) / threads;
+  switch (mb) {
+    case 1: k_mttkrp_il<PAIR, 2, G, V, T, 2><<<(unsigned)blocks, threads, 0, s>>>(a); break;
+    case 3: k_mttkrp_il<PAIR, 1, G, V, T, 3><<<(unsigned)blocks, threads, 0, s>>>(a); break;
+    case 4: k_mttkrp_il<PAIR, 1, G, V, T, 4><<<(unsigned)blocks, threads, 0, s>>>(a); break;
+    default: k_mttkrp_il<PAIR, 1, G, V, T, 2><<<(unsigned)blocks, threads, 0, s>>>(a); break;
+  }
+  return cudaGetLastError();
+}
+
 template <int G, int V, class T>
 cudaError_t launch_pair4(const Args<T>& a, int threads, int mb, cudaStream_t s) {
   const uint64_t teams = (a.nnz + a.chunk - 1) / a.chunk;
@@ -1619,9 +1837,16 @@ cudaError_t launch_rows(const Args<T>& a, int threads, int mb, cudaStream_t s) {
 // kern: 1 = per-team fiber walk (k_mttkrp), 2 = branch-free walk (3-D only),
 // 3 = per-nonzero walk (slice and leaf levels of parts that carry `mid`),
 // 4 = per-nonzero walk with the middle row once per fiber (3-D slice level;
-// elsewhere as 3)
+// elsewhere as 3), 5 = per-nonzero walk with vector index loads (3-D), 6 = the
+// warp-interleaved per-nonzero walk (3-D slice level; elsewhere as 5)
 template <int ND, int G, int V, class T>
 cudaError_t launch_lvl(const Args<T>& a, int lvl, int kern, int threads, int mb, cudaStream_t s) {
+  if constexpr (ND == 3) {
+    if (kern == 6) {
+      if (lvl == 0 && vec_ok(a)) return launch_il<false, G, V, T>(a, threads, mb, s);
+      kern = 5;  // the interleaved walk covers the slice level; elsewhere the vector-load walk
+    }
+  }
   if constexpr (ND == 3 && G >= 4) {
     if (kern == 5 && vec_ok(a)) {
       switch (lvl) {
@@ -1685,8 +1910,8 @@ cudaError_t launch_fixed(const Args<T>& a, int nd, int lvl, int kern, int thread
 
 // The two-output walks (R <= 128). kern 2: the branch-free fiber walk with
 // both outputs; 4: the per-nonzero walk with the middle row once per fiber;
-// 5: the per-nonzero form with vector index loads; otherwise the per-nonzero
-// form. 4-D runs its own walk.
+// 5: the per-nonzero form with vector index loads; 6: the warp-interleaved
+// per-nonzero form; otherwise the per-nonzero form. 4-D runs its own walk.
 template <class T, int R>
 cudaError_t launch_pair_fixed(const Args<T>& a, int nd, int threads, int mb, int kern, cudaStream_t s) {
   if constexpr (R > 128) {
@@ -1695,6 +1920,8 @@ cudaError_t launch_pair_fixed(const Args<T>& a, int nd, int threads, int mb, int
     constexpr int G = TeamShape<T, R>::G;
     constexpr int V = TeamShape<T, R>::V;
     if (nd == 4) return launch_pair4<G, V, T>(a, threads, mb, s);
+    if (kern == 6 && vec_ok(a)) return launch_il<true, G, V, T>(a, threads, mb, s);
+    if (kern == 6) kern = 5;
     if constexpr (G >= 4)
       if (kern == 5 && vec_ok(a)) return launch_pairv<G, V, T>(a, threads, mb, s);
     if (kern == 4) return launch_fib<true, G, V, T>(a, threads, mb, s);

@@ -416,6 +416,7 @@ using namespace mmcsf;
 
 extern "C" int mmcsf_sampled_model(const mmcsf_format* F, int R, int factor_dtype, const void* const* d_factors,
                                    const float* d_lambda, float* d_out, void* stream) {
+  MMCSF_RANGE("mmcsf_sampled_model");
   if (!F || !d_factors || !d_out) return set_error(MMCSF_ERR_INVALID, "null argument");
   if (F->impl == MMCSF_IMPL_HBCSF) return set_error(MMCSF_ERR_UNSUPPORTED, "not available for HB-CSF formats");
   if (R != 4 && R != 8 && R != 16 && R != 32 && R != 64 && R != 128 && R != 256)
@@ -472,6 +473,7 @@ extern "C" int mmcsf_sampled_model(const mmcsf_format* F, int R, int factor_dtyp
 extern "C" int mmcsf_poisson_step(const mmcsf_format* F, int R, int factor_dtype, const void* const* d_factors,
                                   float eps, float* d_w, float* d_grad_root, double* d_loss, int* root_mode,
                                   void* stream) {
+  MMCSF_RANGE("mmcsf_poisson_step");
   if (!F || !d_factors || !d_w || !d_grad_root || !d_loss) return set_error(MMCSF_ERR_INVALID, "null argument");
   if (F->impl == MMCSF_IMPL_HBCSF) return set_error(MMCSF_ERR_UNSUPPORTED, "not available for HB-CSF formats");
   if (R != 4 && R != 8 && R != 16 && R != 32 && R != 64)

@@ -164,6 +164,7 @@ using namespace mmcsf;
 
 extern "C" int mmcsf_ttm(const mmcsf_format* F, int R, int factor_dtype, const void* d_factor, float* d_Y,
                          uint64_t* n_fibers, void* stream) {
+  MMCSF_RANGE("mmcsf_ttm");
   if (!F) return set_error(MMCSF_ERR_INVALID, "null format");
   if (F->impl != MMCSF_IMPL_BCSF) return set_error(MMCSF_ERR_INVALID, "TTM runs on a B-CSF format (-t 8) of the mode");
   const CsfPart& P = F->parts[0];

@@ -317,7 +317,7 @@ def test_kernel_variants_3d(R, dtype, torch_cuda):
             for m in range(3):
                 travs = (1, 2) if F.info(4 + m)["present"] else (1,)
                 for trav in travs:
-                    for kern in (1, 2, 3, 4, 5):
+                    for kern in (1, 2, 3, 4, 5, 6):
                         for mb in (1, 2, 3, 4):
                             for chunk in (64, 1000):
                                 cfg = {"traversal": trav, "kernel": kern, "min_blocks": mb, "chunk": chunk}
@@ -325,7 +325,7 @@ def test_kernel_variants_3d(R, dtype, torch_cuda):
                                 _check_close(out.cpu().numpy(), ref[m], (dims, f, m, cfg))
             if f == 0:
                 B = mmcsf.Format(X, impl=mmcsf.IMPL_BCSF, mode=1, fiber_threshold=4)
-                for kern in (1, 2, 3, 4, 5):
+                for kern in (1, 2, 3, 4, 5, 6):
                     out = B.mttkrp(1, Ud, cfg={"kernel": kern})
                     _check_close(out.cpu().numpy(), ref[1], ("bcsf", dims, kern))
 
@@ -387,7 +387,7 @@ def test_two_output_walk(R, dtype, torch_cuda):
             m0, m1 = F.pair_modes()
             order = F.info(2)["mode_order"]
             assert (m0, m1) == (order[0], order[1])
-            for kern in (2, 3, 4, 5):
+            for kern in (2, 3, 4, 5, 6):
                 for mb in (1, 2, 3, 4):
                     for chunk in (1, 32, 100, 1024):
                         outs = F.mttkrp_pair(Ud, cfg={"min_blocks": mb, "chunk": chunk, "kernel": kern})
@@ -399,7 +399,7 @@ def test_two_output_walk(R, dtype, torch_cuda):
             F.set_plan(plan)
             F.mttkrp_all(Ud)
             separate = F.last_launches
-            for kern in (2, 3, 4, 5):
+            for kern in (2, 3, 4, 5, 6):
                 plan["pair"].update(use=True, chunk=256, min_blocks=2, kernel=kern)
                 F.set_plan(plan)
                 for _ in range(2):

@@ -180,6 +180,20 @@ int mmcsf_format_export(const mmcsf_format* F, int part, const char* name, uint6
 int mmcsf_format_export_f32(const mmcsf_format* F, int part, const char* name, float* dst, uint64_t cap,
                             uint64_t* count);
 
+/* Format check (no counterpart in the reference, which trusts its builders):
+ * validates on the device every index the MTTKRP kernels dereference, for
+ * every part (partitions, views, HB-CSF COO/CSL/CSF parts): index arrays
+ * below rows[m] (the row count of mode m's factor; NULL = the tensor's dims),
+ * pointer arrays starting at 0, strictly increasing and ending at the next
+ * level's count, the leaf fiber flags at exactly the fiber starts, the
+ * per-nonzero middle indices, the slice starts and the chunk-start tables.
+ * Reads are bounded by the allocations, so a corrupt array is reported, not
+ * followed. MMCSF_ERR_INVALID names the array and the first bad position.
+ * Synchronises `stream`. A library built with -DMMCSF_BOUNDS (make
+ * lib/libmmcsf_bounds.so) runs it once per format before the first launch of
+ * every compute entry point. */
+int mmcsf_format_check(const mmcsf_format* F, const uint64_t* rows, void* stream);
+
 /* ---- MTTKRP -------------------------------------------------------------
  * Replaces MTTKRP_MIHCSR_GPU (src/mttkrp_gpu.cu:3380-3784), MTTKRP_B_HCSR_GPU
  * (:1850-2129) and MTTKRP_HYB_GPU (:2530-2851). Factor matrices are

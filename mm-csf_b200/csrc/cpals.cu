@@ -649,6 +649,7 @@ extern "C" int mmcsf_cpd(mmcsf_format* F, const mmcsf_cpd_opts* opts, const floa
   MMCSF_RANGE("mmcsf_cpd");
   using namespace mmcsf;
   if (!F || !opts) return set_error(MMCSF_ERR_INVALID, "null argument");
+  MMCSF_TRY(bounds_gate(F, stream));
   if (F->impl != MMCSF_IMPL_MMCSF) return set_error(MMCSF_ERR_INVALID, "CP-ALS needs an MM-CSF format (-t 12)");
   const int R = opts->rank;
   if (R < 1 || R > MAXR) return set_error(MMCSF_ERR_INVALID, "CP-ALS rank must be in [1, %d]", MAXR);

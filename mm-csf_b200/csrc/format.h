@@ -108,6 +108,7 @@ struct mmcsf_format {
   int fiber_threshold_tuned = -1;  // mmcsf_autotune: the -f the format was chosen with
   mmcsf::HybExtra hyb;
   int last_launches = 0;
+  bool checked = false;  // bounds-checked build: mmcsf_format_check passed once
   // staging for the host-buffer MTTKRP entry point
   mmcsf::DevBuf stage_in[4], stage_out[4];
   int stage_R = 0;
@@ -126,3 +127,22 @@ struct mmcsf_format {
     if (ev_start) cudaEventDestroy(ev_start);
   }
 };
+
+namespace mmcsf {
+// Bounds-checked build (-DMMCSF_BOUNDS): every compute entry point validates
+// the format once (mmcsf_format_check) before its first launch on it, so no
+// kernel follows an index the check has not seen. Otherwise a no-op.
+inline int bounds_gate(const mmcsf_format* F, void* stream) {
+#ifdef MMCSF_BOUNDS
+  if (F && !F->checked) {
+    const int st = mmcsf_format_check(F, nullptr, stream);
+    if (st != MMCSF_OK) return st;
+    const_cast<mmcsf_format*>(F)->checked = true;
+  }
+#else
+  (void)F;
+  (void)stream;
+#endif
+  return MMCSF_OK;
+}
+}  // namespace mmcsf

@@ -243,6 +243,7 @@ extern "C" int mmcsf_mttkrp(const mmcsf_format* F, int mode, int R, int factor_d
   MMCSF_RANGE("mmcsf_mttkrp");
   MMCSF_TRY(check_call(F, R, factor_dtype));
   if (mode < 0 || mode >= F->nd) return set_error(MMCSF_ERR_INVALID, "Mode cannot be larger than tensor dimension.");
+  MMCSF_TRY(bounds_gate(F, stream));
   if (!d_factors || !d_out) return set_error(MMCSF_ERR_INVALID, "null pointer");
   if (F->impl != MMCSF_IMPL_MMCSF && mode != F->mode)
     return set_error(MMCSF_ERR_INVALID, "this format was built for mode %d only", F->mode);
@@ -301,6 +302,7 @@ extern "C" int mmcsf_cp_adjoint(const mmcsf_format* F, int mode, int R, int fact
   MMCSF_RANGE("mmcsf_cp_adjoint");
   MMCSF_TRY(check_call(F, R, factor_dtype));
   if (mode < 0 || mode >= F->nd) return set_error(MMCSF_ERR_INVALID, "Mode cannot be larger than tensor dimension.");
+  MMCSF_TRY(bounds_gate(F, stream));
   if (!d_factors || !d_out || !d_grad) return set_error(MMCSF_ERR_INVALID, "null pointer");
   if (F->impl == MMCSF_IMPL_HBCSF) return set_error(MMCSF_ERR_UNSUPPORTED, "not available for HB-CSF formats");
   if (F->impl != MMCSF_IMPL_MMCSF && mode != F->mode)
@@ -343,6 +345,7 @@ extern "C" int mmcsf_mttkrp_pair(const mmcsf_format* F, int R, int factor_dtype,
     return set_error(MMCSF_ERR_UNSUPPORTED, "the two-output walk needs the per-nonzero middle indices");
   if (modes) { modes[0] = P->order[0]; modes[1] = P->order[1]; }
   if (!d_factors || !d_out_slice || !d_out_mid) return modes ? MMCSF_OK : set_error(MMCSF_ERR_INVALID, "null pointer");
+  MMCSF_TRY(bounds_gate(F, stream));
   if (!native_R(R) || R > 128) return set_error(MMCSF_ERR_UNSUPPORTED, "the two-output walk runs R in 4..128");
   cudaStream_t s = S(stream);
   MMCSF_CUDA(cudaMemsetAsync(d_out_slice, 0, F->dims[P->order[0]] * (uint64_t)R * sizeof(float), s));
@@ -397,6 +400,7 @@ extern "C" int mmcsf_mttkrp_all(const mmcsf_format* F, int R, int factor_dtype, 
   MMCSF_RANGE("mmcsf_mttkrp_all");
   MMCSF_TRY(check_call(F, R, factor_dtype));
   if (!d_factors || !d_outs) return set_error(MMCSF_ERR_INVALID, "null pointer");
+  MMCSF_TRY(bounds_gate(F, stream));
   if (F->impl != MMCSF_IMPL_MMCSF)
     return set_error(MMCSF_ERR_INVALID, "all-mode MTTKRP needs an MM-CSF format (-t 12)");
   int total = 0;
@@ -451,6 +455,7 @@ extern "C" int mmcsf_mttkrp_all_host(mmcsf_format* F, int R, const float* const*
   MMCSF_RANGE("mmcsf_mttkrp_all_host");
   MMCSF_TRY(check_call(F, R, MMCSF_DTYPE_F32));
   if (!h_factors || !h_outs) return set_error(MMCSF_ERR_INVALID, "null pointer");
+  MMCSF_TRY(bounds_gate(F, stream));
   if (F->impl != MMCSF_IMPL_MMCSF)
     return set_error(MMCSF_ERR_INVALID, "all-mode MTTKRP needs an MM-CSF format (-t 12)");
   cudaStream_t s = S(stream);

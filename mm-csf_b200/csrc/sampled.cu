@@ -418,6 +418,7 @@ extern "C" int mmcsf_sampled_model(const mmcsf_format* F, int R, int factor_dtyp
                                    const float* d_lambda, float* d_out, void* stream) {
   MMCSF_RANGE("mmcsf_sampled_model");
   if (!F || !d_factors || !d_out) return set_error(MMCSF_ERR_INVALID, "null argument");
+  MMCSF_TRY(bounds_gate(F, stream));
   if (F->impl == MMCSF_IMPL_HBCSF) return set_error(MMCSF_ERR_UNSUPPORTED, "not available for HB-CSF formats");
   if (R != 4 && R != 8 && R != 16 && R != 32 && R != 64 && R != 128 && R != 256)
     return set_error(MMCSF_ERR_UNSUPPORTED, "sampled model runs ranks 4, 8, ..., 256");
@@ -475,6 +476,7 @@ extern "C" int mmcsf_poisson_step(const mmcsf_format* F, int R, int factor_dtype
                                   void* stream) {
   MMCSF_RANGE("mmcsf_poisson_step");
   if (!F || !d_factors || !d_w || !d_grad_root || !d_loss) return set_error(MMCSF_ERR_INVALID, "null argument");
+  MMCSF_TRY(bounds_gate(F, stream));
   if (F->impl == MMCSF_IMPL_HBCSF) return set_error(MMCSF_ERR_UNSUPPORTED, "not available for HB-CSF formats");
   if (R != 4 && R != 8 && R != 16 && R != 32 && R != 64)
     return set_error(MMCSF_ERR_UNSUPPORTED, "the fused Poisson step runs ranks 4, 8, 16, 32, 64");

@@ -166,6 +166,7 @@ extern "C" int mmcsf_ttm(const mmcsf_format* F, int R, int factor_dtype, const v
                          uint64_t* n_fibers, void* stream) {
   MMCSF_RANGE("mmcsf_ttm");
   if (!F) return set_error(MMCSF_ERR_INVALID, "null format");
+  MMCSF_TRY(bounds_gate(F, stream));
   if (F->impl != MMCSF_IMPL_BCSF) return set_error(MMCSF_ERR_INVALID, "TTM runs on a B-CSF format (-t 8) of the mode");
   const CsfPart& P = F->parts[0];
   if (P.nd != 3) return set_error(MMCSF_ERR_UNSUPPORTED, "TTM is 3-D (as the reference's)");

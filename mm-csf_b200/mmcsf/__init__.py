@@ -255,6 +255,16 @@ class Format:
                 "nnz": int(pi.nnz), "n_slices": int(pi.n_slices), "n_fbrs": int(pi.n_fbrs),
                 "n_fibers": int(pi.n_fibers), "device_bytes": int(pi.device_bytes)}
 
+    def check(self, rows=None, stream=None):
+        """Validate every index the kernels dereference (mmcsf_format_check):
+        index arrays below `rows` (the factors' row counts; default the
+        tensor's dims), pointers, fiber flags, per-nonzero indices and chunk
+        tables. Raises MmcsfError naming the array and first bad position."""
+        r = None
+        if rows is not None:
+            r = (c_u64 * 4)(*[int(x) for x in rows] + [0] * (4 - len(rows)))
+        check(lib().mmcsf_format_check(self._h, r, _stream(stream)))
+
     def chunk_for_warps(self, warps, R):
         """The worker-team chunk equivalent to the reference's -w `warps`
         warps per fiber (src/util.h:194, src/mttkrp_gpu.cu:3616-3630): the

@@ -6,7 +6,9 @@ import ctypes
 import os
 
 _PKG_ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-LIB_PATH = os.path.join(_PKG_ROOT, "lib", "libmmcsf.so")
+# MMCSF_LIBRARY selects another in-tree build, e.g. lib/libmmcsf_bounds.so
+# (every compute entry point validates a format once before launching on it)
+LIB_PATH = os.environ.get("MMCSF_LIBRARY") or os.path.join(_PKG_ROOT, "lib", "libmmcsf.so")
 
 c_u64 = ctypes.c_uint64
 c_u64p = ctypes.POINTER(ctypes.c_uint64)
@@ -103,6 +105,7 @@ SIGNATURES = {
     "mmcsf_mttkrp_all_host": ([c_voidp, c_int, ctypes.POINTER(c_voidp), ctypes.POINTER(c_voidp),
                                ctypes.POINTER(KernelCfg), c_voidp], c_int),
     "mmcsf_format_last_launches": ([c_voidp, ctypes.POINTER(c_int)], c_int),
+    "mmcsf_format_check": ([c_voidp, c_u64p, c_voidp], c_int),
     "mmcsf_tune": ([c_voidp, c_int, c_int, ctypes.POINTER(c_voidp), ctypes.POINTER(c_voidp), c_voidp,
                     ctypes.POINTER(Plan)], c_int),
     "mmcsf_set_plan": ([c_voidp, ctypes.POINTER(Plan)], c_int),

@@ -31,6 +31,10 @@ def test_library_exports_every_declared_symbol():
     for n in sorted(names):
         assert hasattr(L, n), n
         assert n in _lib.SIGNATURES, f"binding missing for {n}"
+    # the bounds-checked build exports the same interface
+    B = ctypes.CDLL(os.path.join(ROOT, "mm-csf_b200", "lib", "libmmcsf_bounds.so"))
+    for n in sorted(names):
+        assert hasattr(B, n), ("bounds build", n)
 
 
 def test_status_strings_and_version():

@@ -76,6 +76,9 @@ WORKLOADS = {
                      desc="500000x2000000x20000, 100M nnz, Zipf(1.1) per mode, lognormal values, R=32"),
     "uniform3d": dict(dims=[1000, 1000, 1000], nnz=100_000, dist=[0, 0, 0], zipf=1.0, val=0, R=32,
                       desc="1000^3, 100k uniform nnz, R=32"),
+    "cpals3d": dict(dims=[200000, 200000, 200000], nnz=50_000_000, dist=[0, 0, 0], zipf=1.0, val=0, R=16, views=2,
+                    desc="200000^3, 50M uniform nnz, R=16: the CP-ALS tensor's index structure (values uniform), "
+                         "every mode through its view"),
     "skewed4d": dict(dims=[1000000, 20000, 5000, 200], nnz=140_000_000, dist=[1, 1, 1, 0], zipf=1.0, val=2, R=32,
                      views=2,
                      desc="1000000x20000x5000x200, 140M nnz, Zipf(1.0) modes 0-2, uniform mode 3, integer values "
@@ -100,7 +103,8 @@ def parse():
     ap.add_argument("--views", type=int, default=None,
                     help="0 none, 1 leaf-level modes, 2 every mode (default: the workload's)")
     ap.add_argument("--no-tune", action="store_true")
-    ap.add_argument("--plan-file", default="", help="JSON plan (as printed by a tuned run) to use instead of tuning")
+    ap.add_argument("--plan-file", default="",
+                    help="JSON plan (as printed by a tuned run) to use instead of tuning: a file, or the JSON itself")
     ap.add_argument("--no-cp", action="store_true", help="skip the CP-ALS and Poisson gradient-CP sections")
     ap.add_argument("--no-formats", action="store_true", help="4-D workloads: skip the B-CSF / HB-CSF section")
     ap.add_argument("--no-bf16", action="store_true", help="skip the BF16-factor section")
@@ -1121,8 +1125,12 @@ def main():
     U = [torch.rand(d, R, device="cuda", generator=g).to(tdt) for d in dims]
     outs = [torch.empty(d, R, device="cuda") for d in dims]
     if a.plan_file:
-        with open(a.plan_file) as fh:
-            plan = {(int(k) if k.isdigit() else k): v for k, v in json.load(fh).items()}
+        if a.plan_file.lstrip().startswith("{"):
+            pj = json.loads(a.plan_file)
+        else:
+            with open(a.plan_file) as fh:
+                pj = json.load(fh)
+        plan = {(int(k) if k.isdigit() else k): v for k, v in pj.items()}
         F.set_plan(plan)
     else:
         plan = None if a.no_tune else F.tune(U, outs)

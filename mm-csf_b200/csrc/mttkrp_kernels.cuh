@@ -51,20 +51,14 @@ template <> struct Row<__nv_bfloat16> {
   }
 };
 
-// Columns a lane owns. FP32 (and BF16 with one float4 per lane): lane tl of a
-// team of G holds columns 4 tl + 4 G v, v < V, so one load instruction of the
-// team covers a contiguous 16 G-byte piece of the row. BF16 with V even
-// (R >= 32): the lane holds the 4 V contiguous columns 4 V tl .. 4 V tl +
-// 4 V - 1, loaded as V / 2 16-byte vectors; a 64-byte row (R = 32) is then
-// one load of a 4-lane team, so a warp serves 8 nonzeros per instruction.
+// Columns a lane owns: lane tl of a team of G holds columns 4 tl + 4 G v,
+// v < V, so one load instruction of the team covers a contiguous 16 G-byte
+// (FP32) or 8 G-byte (BF16) piece of the row.
 template <class T, int G, int V>
 struct Cols {
-  static constexpr bool PACK = std::is_same<T, __nv_bfloat16>::value && V % 2 == 0;
-  static __device__ __forceinline__ uint32_t of(int tl, int v) {
-    return PACK ? (uint32_t)(4 * V * tl + 4 * v) : (uint32_t)(4 * tl + 4 * G * v);
-  }
+  static __device__ __forceinline__ uint32_t of(int tl, int v) { return (uint32_t)(4 * tl + 4 * G * v); }
 };
-// 4 BF16 values (the half h of a 16-byte vector of 8) widened to FP32
+// 4 BF16 values (two 32-bit words) widened to FP32
 __device__ __forceinline__ float4 bf16x4_to_f32(uint32_t lo, uint32_t hi) {
   return make_float4(__uint_as_float(lo << 16), __uint_as_float(lo & 0xffff0000u), __uint_as_float(hi << 16),
                      __uint_as_float(hi & 0xffff0000u));
@@ -72,13 +66,7 @@ __device__ __forceinline__ float4 bf16x4_to_f32(uint32_t lo, uint32_t hi) {
 // Row piece v of a lane (columns Cols::of(tl, v)) from row base `rb`.
 template <class T, int G, int V>
 __device__ __forceinline__ float4 load_piece(const T* rb, int tl, int v) {
-  if constexpr (Cols<T, G, V>::PACK) {
-    // both halves of the same 16-byte vector: the two calls read one address
-    const uint4 u = __ldg(reinterpret_cast<const uint4*>(rb + 4 * V * tl + 8 * (v / 2)));
-    return (v & 1) ? bf16x4_to_f32(u.z, u.w) : bf16x4_to_f32(u.x, u.y);
-  } else {
-    return Row<T>::load(rb, Cols<T, G, V>::of(tl, v));
-  }
+  return Row<T>::load(rb, Cols<T, G, V>::of(tl, v));
 }
 
 __device__ __forceinline__ float4 f4(float a) { return make_float4(a, a, a, a); }
@@ -1496,34 +1484,21 @@ __global__ void __launch_bounds__(256, MB) k_mttkrp_pair4(const Args<T> a) {
   }
 }
 
-// A lane's piece of one factor row as loaded (FP32: V float4; BF16 with V
-// even: V / 2 16-byte vectors of 8 values; other BF16: V 8-byte vectors),
-// widened to FP32 only where it is used, so rows in flight hold half the
-// registers at BF16.
+// A lane's piece of one factor row as loaded (FP32: V float4; BF16: V 8-byte
+// vectors), widened to FP32 only where it is used, so rows in flight hold
+// half the registers at BF16.
 template <class T, int G, int V>
 struct RawPiece {
   static constexpr bool BF = std::is_same<T, __nv_bfloat16>::value;
-  static constexpr bool PACK = Cols<T, G, V>::PACK;
-  using W = std::conditional_t<!BF, float4, std::conditional_t<PACK, uint4, uint2>>;
-  static constexpr int N = PACK ? V / 2 : V;
-  W w[N];
+  using W = std::conditional_t<BF, uint2, float4>;
+  W w[V];
   __device__ __forceinline__ void load(const T* rb, int tl) {
 #pragma unroll
-    for (int i = 0; i < N; ++i) {
-      if constexpr (!BF) w[i] = __ldg(reinterpret_cast<const float4*>(rb + Cols<T, G, V>::of(tl, i)));
-      else if constexpr (PACK) w[i] = __ldg(reinterpret_cast<const uint4*>(rb + 4 * V * tl + 8 * i));
-      else w[i] = __ldg(reinterpret_cast<const uint2*>(rb + Cols<T, G, V>::of(tl, i)));
-    }
+    for (int i = 0; i < V; ++i) w[i] = __ldg(reinterpret_cast<const W*>(rb + Cols<T, G, V>::of(tl, i)));
   }
   __device__ __forceinline__ float4 get(int v) const {
-    if constexpr (!BF) {
-      return w[v];
-    } else if constexpr (PACK) {
-      const uint4& u = w[v / 2];
-      return (v & 1) ? bf16x4_to_f32(u.z, u.w) : bf16x4_to_f32(u.x, u.y);
-    } else {
-      return bf16x4_to_f32(w[v].x, w[v].y);
-    }
+    if constexpr (BF) return bf16x4_to_f32(w[v].x, w[v].y);
+    else return w[v];
   }
 };
 
@@ -1636,53 +1611,62 @@ __global__ void __launch_bounds__(256, MB) k_mttkrp_il(const Args<T> a) {
       rb[j].load(U1 + (uint64_t)b * R, tl);
       rc[j].load(U2 + (uint64_t)k * R, tl);
     }
+    // FAST: the whole group lies before x1 and in the team's open slice (the
+    // common case), so no nonzero needs the end or slice tests
+    auto body = [&](auto fast_tag) {
+      constexpr bool FAST = decltype(fast_tag)::value;
 #pragma unroll
-    for (int j = 0; j < (int)GS; ++j) {
-      const uint64_t x = xg + j;
-      if (x < x1) {
-        const float val = comp4f(Wc[j >> 2], j & 3);
-        if (x >= nxt) {  // the team's slice ends before nonzero x
+      for (int j = 0; j < (int)GS; ++j) {
+        const uint64_t x = xg + j;
+        if (FAST || x < x1) {
+          const float val = comp4f(Wc[j >> 2], j & 3);
+          if constexpr (!FAST) {
+            if (x >= nxt) {  // the team's slice ends before nonzero x
 #pragma unroll
-          for (int v = 0; v < V; ++v) { rd(out, ca, v, acc[v]); acc[v] = f4(0.f); }
-          if constexpr (PAIR) {
-            if (bopen != NONE) {
+              for (int v = 0; v < V; ++v) { rd(out, ca, v, acc[v]); acc[v] = f4(0.f); }
+              if constexpr (PAIR) {
+                if (bopen != NONE) {
 #pragma unroll
-              for (int v = 0; v < V; ++v) rd(out2, bopen, v, pmul(rowA[v], accf[v]));
+                  for (int v = 0; v < V; ++v) rd(out2, bopen, v, pmul(rowA[v], accf[v]));
+                }
+#pragma unroll
+                for (int v = 0; v < V; ++v) accf[v] = f4(0.f);
+                bopen = NONE;
+              }
+              do {
+                ++sl;
+                nxt = __ldg(snz + sl + 1);
+              } while (x >= nxt);
+              ca = __ldg(sidx + sl);
+              if constexpr (PAIR) {
+#pragma unroll
+                for (int v = 0; v < V; ++v) rowA[v] = load_piece<T, G, V>(U0 + (uint64_t)ca * R, tl, v);
+              }
             }
-#pragma unroll
-            for (int v = 0; v < V; ++v) accf[v] = f4(0.f);
-            bopen = NONE;
           }
-          do {
-            ++sl;
-            nxt = __ldg(snz + sl + 1);
-          } while (x >= nxt);
-          ca = __ldg(sidx + sl);
           if constexpr (PAIR) {
+            const uint32_t b = comp4(Bc[j >> 2], j & 3);
+            if (b != bopen) {  // the team's open fiber ends before nonzero x
+              if (bopen != NONE) {
 #pragma unroll
-            for (int v = 0; v < V; ++v) rowA[v] = load_piece<T, G, V>(U0 + (uint64_t)ca * R, tl, v);
-          }
-        }
-        if constexpr (PAIR) {
-          const uint32_t b = comp4(Bc[j >> 2], j & 3);
-          if (b != bopen) {  // the team's open fiber ends before nonzero x
-            if (bopen != NONE) {
+                for (int v = 0; v < V; ++v) rd(out2, bopen, v, pmul(rowA[v], accf[v]));
+              }
 #pragma unroll
-              for (int v = 0; v < V; ++v) rd(out2, bopen, v, pmul(rowA[v], accf[v]));
+              for (int v = 0; v < V; ++v) accf[v] = f4(0.f);
+              bopen = b;
             }
-#pragma unroll
-            for (int v = 0; v < V; ++v) accf[v] = f4(0.f);
-            bopen = b;
           }
-        }
 #pragma unroll
-        for (int v = 0; v < V; ++v) {
-          const float4 c = rc[j].get(v);
-          acc[v] = pfma(pmul_s(val, rb[j].get(v)), c, acc[v]);
-          if constexpr (PAIR) accf[v] = pfma_s(val, c, accf[v]);
+          for (int v = 0; v < V; ++v) {
+            const float4 c = rc[j].get(v);
+            acc[v] = pfma(pmul_s(val, rb[j].get(v)), c, acc[v]);
+            if constexpr (PAIR) accf[v] = pfma_s(val, c, accf[v]);
+          }
         }
       }
-    }
+    };
+    if (xg + GS <= x1 && xg + GS <= nxt) body(std::true_type{});
+    else body(std::false_type{});
 #pragma unroll
     for (int q = 0; q < Q; ++q) { Kc[q] = Kn[q]; Bc[q] = Bn[q]; Wc[q] = Wn[q]; }
   }
@@ -1889,14 +1873,13 @@ cudaError_t launch_lvl(const Args<T>& a, int lvl, int kern, int threads, int mb,
 // Launch for one rank R (a compile-time constant: G lanes per row, V float4
 // per lane, R = 4 G V). Each R is instantiated in its own translation unit
 // (mttkrp_r<R>.cu) so the kernel variants compile in parallel.
-// Lanes per factor row (G) and float4 per lane (V) for rank R: FP32 rows are
-// covered by one 16-byte vector per lane (G = R / 4, at most 32); BF16 rows
-// of R >= 32 by V = 2 (two float4 from one 16-byte vector of 8 BF16), so
-// G = R / 8 lanes read a row with one load each.
+// Lanes per factor row (G) and float4 per lane (V) for rank R: a 16-byte
+// (FP32) or 8-byte (BF16) piece per lane, at most 32 lanes. (BF16 teams of
+// R / 8 lanes, each reading 8 contiguous values with one 16-byte load, were
+// slower at R = 32 and 64: 3.34 against 3.07 ms per all-mode step.)
 template <class T, int R>
 struct TeamShape {
-  static constexpr bool BF = std::is_same<T, __nv_bfloat16>::value && R >= 32;
-  static constexpr int G = BF ? (R / 8 > 32 ? 32 : R / 8) : (R >= 128 ? 32 : R / 4);
+  static constexpr int G = R >= 128 ? 32 : R / 4;
   static constexpr int V = R / (4 * G);
 };
 

@@ -668,18 +668,28 @@ def per_mode_bytes(F, nd, dims, nnz, R, esz, rows, plan, info):
         trav = plan[m]["traversal"] if plan else (2 if F.info(4 + m)["present"] else 1)
         pi = F.info(4 + m) if trav == 2 else info
         lvl = pi["mode_order"].index(m)
-        if plan and plan[m].get("kernel") == 3 and (nd == 3 or lvl in (0, nd - 1)):
-            sb = nnz * (12 if nd == 3 else 16) + pi["n_slices"] * 8  # per-nonzero walk
+        k = plan[m].get("kernel") if plan else 0
+        if (k == 3 and (nd == 3 or lvl in (0, nd - 1))) or (nd == 3 and k in (4, 5, 6, 7) and lvl == 0) \
+                or (nd == 3 and k == 5):
+            sb = nnz * (12 if nd == 3 else 16) + pi["n_slices"] * 8  # per-nonzero walks (vals, leaf, mid)
         else:
             sb = struct_bytes(nd, nnz, pi["n_fibers"], pi["n_fbrs"])
         out.append(mode_bytes(nd, dims, m, R, esz, sb, rows))
     return out
 
 
+# kernel names by mmcsf_kernel_cfg.kernel: one mode, and the two-output walk
+SINGLE_KERNELS = {1: "k_mttkrp", 2: "k_mttkrp_flat", 3: "k_mttkrp_rows", 4: "k_mttkrp_fib", 5: "k_mttkrp_rowsv",
+                  6: "k_mttkrp_il", 7: "k_mttkrp_stg"}
+PAIR_KERNELS = {0: "k_mttkrp_pair", 2: "k_mttkrp_flat", 3: "k_mttkrp_pair", 4: "k_mttkrp_fib", 5: "k_mttkrp_pairv",
+                6: "k_mttkrp_il", 7: "k_mttkrp_stg"}
+
+
 def kernel_label(F, nd, plan, info, modes):
     """(kernel name, description) of one launch of the step."""
     if len(modes) == 2:
-        k = "k_mttkrp_pair" if nd == 3 else "k_mttkrp_pair4"
+        pk = plan.get("pair", {}).get("kernel", 0) if plan else 0
+        k = PAIR_KERNELS.get(pk, "k_mttkrp_pair") if nd == 3 else "k_mttkrp_pair4"
         return k, (f"{k} modes {modes[0]} and {modes[1]} (levels 0 and 1 of order {info['mode_order']}, "
                    f"MM-CSF partition, one walk)")
     dom = modes[0]
@@ -687,9 +697,16 @@ def kernel_label(F, nd, plan, info, modes):
     order = F.info(4 + dom)["mode_order"] if trav == 2 else info["mode_order"]
     lvl = order.index(dom)
     k = plan[dom].get("kernel", 0) if plan else 0
+    k = k or (2 if nd == 3 else 1)
+    if nd == 3 and k == 7 and lvl != 0:
+        k = 6  # the staged walk covers the 3-D slice level (R 16..128, every rank this benchmark runs)
+    if nd == 3 and k in (4, 6) and lvl != 0:
+        k = 5 if k == 6 else 3
+    if nd == 4 and k in (4, 5, 6, 7):
+        k = 3
     if k == 3 and nd == 4 and lvl not in (0, 3):
         k = 1  # the 4-D middle levels run the per-team fiber walk
-    name = {1: "k_mttkrp", 2: "k_mttkrp_flat", 3: "k_mttkrp_rows"}.get(k or (2 if nd == 3 else 1))
+    name = SINGLE_KERNELS[k]
     return name, f"{name} mode {dom} (level {lvl} of order {order}, {'view' if trav == 2 else 'MM-CSF partition'})"
 
 

@@ -214,7 +214,11 @@ typedef struct {
                         5 per-nonzero walk with 16-byte index/value loads (3-D, R >= 16, chunk % 4 == 0;
                         elsewhere 3); 6 per-nonzero walk with the teams of a warp interleaved over one
                         range, each team loading its own 16-byte index/value vectors (3-D slice level,
-                        chunk % 4 == 0; elsewhere 5) */
+                        chunk % 4 == 0; elsewhere 5); 7 per-nonzero walk with the factor rows staged in
+                        shared memory several steps ahead of their use and the middle row once per fiber
+                        (3-D slice level, R 16..128; elsewhere 6; its grid is one block per SM and its teams
+                        split the nonzeros evenly, so chunk is not used; min_blocks 1..4 picks steps of 4, 4, 8,
+                        8 nonzeros per team with 2, 3, 2, 3 stages in flight) */
   int reserved[3];
 } mmcsf_kernel_cfg;
 
@@ -242,7 +246,8 @@ int mmcsf_mttkrp_coo_host(const mmcsf_coo* X, int mode, int R, const float* cons
  * row gathered once per fiber), 3 the per-nonzero form, 4 the per-nonzero form
  * with the middle row gathered once per fiber (3-D), 5 the per-nonzero form
  * with 16-byte index loads (3-D, R >= 16), 6 the warp-interleaved per-nonzero
- * form (3-D; 0: the tuned choice);
+ * form (3-D), 7 the form with the rows staged in shared memory (3-D, R 16..128;
+ * 0: the tuned choice);
  * chunk and min_blocks as for mmcsf_mttkrp. With null outputs only `modes` is
  * filled. R in 4..128 (powers of two). */
 int mmcsf_mttkrp_pair(const mmcsf_format* F, int R, int factor_dtype, const void* const* d_factors,
@@ -275,7 +280,8 @@ typedef struct {
   int pair_chunk, pair_min_blocks;
   int pair_kernel;  /* 2: branch-free fiber walk with both outputs; 3 (or 0): per-nonzero form; 4: per-nonzero
                        form with the middle row once per fiber; 5: per-nonzero form with 16-byte index loads;
-                       6: warp-interleaved per-nonzero form */
+                       6: warp-interleaved per-nonzero form; 7: per-nonzero form with the rows staged in
+                       shared memory */
   float pair_ms;    /* best time of that walk (both modes) */
   int factor_dtype; /* MMCSF_DTYPE_* of the factors the plan is for (mmcsf_set_plan files the entries under it) */
   /* per-mode precision (mmcsf_tune_precision): with FP32 factors, mmcsf_mttkrp_all runs each launch at the

@@ -105,11 +105,12 @@ int part_mttkrp(const mmcsf_format* F, const CsfPart& P, int mode, int R, int dt
   int threads = cfg && cfg->block_threads > 0 ? cfg->block_threads : 256;
   const int mb = cfg && cfg->min_blocks > 0 ? cfg->min_blocks : 2;
   int kern = cfg && cfg->kernel > 0 ? cfg->kernel : (P.nd == 3 ? 2 : 1);
-  if (kern < 1 || kern > 6) return set_error(MMCSF_ERR_INVALID, "kernel must be 0 .. 6");
+  if (kern < 1 || kern > 7) return set_error(MMCSF_ERR_INVALID, "kernel must be 0 .. 7");
+  if (kern == 7 && (P.nd != 3 || lvl != 0 || R < 16 || R > 128)) kern = 6;  // staged rows: 3-D slice level, R 16..128
   if (kern == 4 && (P.nd != 3 || lvl != 0)) kern = 3;  // per-fiber middle rows: the 3-D slice level only
   if (kern == 6 && (P.nd != 3 || lvl != 0)) kern = 5;  // warp-interleaved walk: the 3-D slice level only
   if (kern == 5 && P.nd != 3) kern = 3;                 // vector index loads: 3-D
-  if ((kern == 4 || kern == 5 || kern == 6) && !P.mid.p) kern = 2;
+  if ((kern == 4 || kern == 5 || kern == 6 || kern == 7) && !P.mid.p) kern = 2;
   if (kern == 3 && (!P.mid.p || (P.nd == 4 && lvl != 0 && lvl != 3))) kern = 2;  // per-nonzero walk not applicable
   if (kern == 2 && P.nd == 4) kern = 1;                                         // no 4-D branch-free fiber walk
   const int slot = CsfPart::cfib_slot((uint64_t)chunk);
@@ -355,7 +356,7 @@ extern "C" int mmcsf_mttkrp_pair(const mmcsf_format* F, int R, int factor_dtype,
   const int threads = cfg && cfg->block_threads > 0 ? cfg->block_threads : 256;
   const int mb = cfg && cfg->min_blocks > 0 ? cfg->min_blocks : (F->pair_mb[d] ? F->pair_mb[d] : 3);
   const int kern = cfg && cfg->kernel > 0 ? cfg->kernel : F->pair_kernel[d];
-  if (kern < 0 || kern > 6) return set_error(MMCSF_ERR_INVALID, "kernel must be 0 .. 6");
+  if (kern < 0 || kern > 7) return set_error(MMCSF_ERR_INVALID, "kernel must be 0 .. 7");
   if (threads % 32 || threads > 256) return set_error(MMCSF_ERR_INVALID, "block_threads must be a multiple of 32, <= 256");
   const int slot = CsfPart::cfib_slot((uint64_t)chunk);
   cudaError_t e;
@@ -542,14 +543,15 @@ extern "C" int mmcsf_tune(mmcsf_format* F, int R, int factor_dtype, const void* 
     const int m = F->impl == MMCSF_IMPL_MMCSF ? i : F->mode;
     float best = 1e30f;
     int bt = 1, bc = 512, bm = 2, bk = 1;
-    const int nkern = 6;
+    const int nkern = 7;
     for (int trav = 1; trav <= 2 && st == MMCSF_OK; ++trav) {
       if (trav == 2 && !F->views[m].present) continue;
       for (int kern = 1; kern <= nkern && st == MMCSF_OK; ++kern) {
       if (kern == 2 && F->nd == 4) continue;  // 4-D has no branch-free fiber walk
       if (kern == 5 && (F->nd != 3 || R < 16)) continue;  // vector index loads: 3-D, teams of >= 4 lanes
       if (kern == 6 && (F->nd != 3 || R < 8)) continue;   // warp-interleaved walk: 3-D
-      if (kern == 4) {  // per-fiber middle rows: only where the mode is the slice level of a 3-D part with `mid`
+      if (kern == 7 && (F->nd != 3 || R < 16 || R > 128)) continue;  // staged rows: 3-D, R 16..128
+      if (kern == 4 || kern == 7) {  // per-fiber middle rows: only where the mode is the slice level of a 3-D part with `mid`
         const CsfPart* tp = nullptr;
         if (trav == 2) tp = &F->views[m];
         else
@@ -565,6 +567,7 @@ extern "C" int mmcsf_tune(mmcsf_format* F, int R, int factor_dtype, const void* 
       }
       for (int mbv = 1; mbv <= 4; ++mbv) {
         for (int c : chunks) {
+          if (kern == 7 && c != chunks[0]) break;  // kernel 7 sizes its own ranges: one timing per level
           mmcsf_kernel_cfg cfg{};
           cfg.chunk = c;
           cfg.traversal = trav;
@@ -612,11 +615,12 @@ extern "C" int mmcsf_tune(mmcsf_format* F, int R, int factor_dtype, const void* 
       native_R(R) && R <= 128) {
     float bestp = 1e30f;
     int bpc = 0, bpm = 0, bpk = 0;
-    for (int kern : {2, 3, 4, 5, 6})
-    for (int mbv = 1; mbv <= 3 && st == MMCSF_OK && (kern == 3 || F->nd == 3) && (kern != 5 || R >= 16) &&
-                      (kern != 6 || R >= 8);
+    for (int kern : {2, 3, 4, 5, 6, 7})
+    for (int mbv = 1; mbv <= (kern == 7 ? 4 : 3) && st == MMCSF_OK && (kern == 3 || F->nd == 3) &&
+                      (kern != 5 || R >= 16) && (kern != 6 || R >= 8) && (kern != 7 || R >= 16);
          ++mbv)
       for (int c : {256, 512, 1024}) {
+        if (kern == 7 && c != 256) break;  // kernel 7 sizes its own ranges
         mmcsf_kernel_cfg cfg{};
         cfg.chunk = c;
         cfg.min_blocks = mbv;
@@ -881,12 +885,12 @@ extern "C" int mmcsf_set_plan(mmcsf_format* F, const mmcsf_plan* plan) {
     if (plan->traversal[m] == 2 && !F->views[m].present)
       return set_error(MMCSF_ERR_INVALID, "plan uses a view for mode %d that was not built", m);
     if (plan->traversal[m] < 0 || plan->traversal[m] > 2 || plan->chunk[m] < 0 || plan->kernel[m] < 0 ||
-        plan->kernel[m] > 6)
+        plan->kernel[m] > 7)
       return set_error(MMCSF_ERR_INVALID, "bad plan entry for mode %d", m);
     if (plan->mixed && plan->mode_dtype[m] != MMCSF_DTYPE_F32 && plan->mode_dtype[m] != MMCSF_DTYPE_BF16)
       return set_error(MMCSF_ERR_INVALID, "bad mode_dtype for mode %d", m);
   }
-  if (plan->pair_chunk < 0 || plan->pair_min_blocks < 0 || plan->pair_kernel < 0 || plan->pair_kernel > 6)
+  if (plan->pair_chunk < 0 || plan->pair_min_blocks < 0 || plan->pair_kernel < 0 || plan->pair_kernel > 7)
     return set_error(MMCSF_ERR_INVALID, "bad pair entry");
   if (plan->mixed && plan->pair_dtype != MMCSF_DTYPE_F32 && plan->pair_dtype != MMCSF_DTYPE_BF16)
     return set_error(MMCSF_ERR_INVALID, "bad pair_dtype");

@@ -1698,6 +1698,340 @@ cudaError_t launch_il(const Args<T>& a, int threads, int mb, cudaStream_t s) {
   return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------------------
+// Per-nonzero walk with the factor rows staged in shared memory (kernel 7),
+// 3-D parts with `mid`: the slice-level MTTKRP, out[a] += sum over fibers
+// (a, b) of U1[b] (.) t_f, t_f = sum over the fiber of v U2[k], and with PAIR
+// also the middle mode's, out2[b] += U0[a] (.) t_f (the two-output walk).
+//
+// The walks above issue one batch of row gathers into registers and then
+// wait a full memory latency before they can use any of it, so each warp
+// keeps rows in flight only part of the time, and registers bound how many.
+// Here the rows go to shared memory with cp.async (16-byte pieces, L2 only;
+// 8-byte pieces for BF16 factors), D steps of GS nonzeros per team ahead of
+// their use, and the indices and values another D steps ahead of that, so
+// every warp keeps D steps of rows in flight continuously whatever the
+// latency. A lane copies exactly the pieces of each row it later reads (its
+// columns of the team's rows), so the row ring needs no synchronisation
+// beyond the lane's own cp.async.wait_group; the index ring, copied by the
+// warp together and read by every lane of a team, is guarded by __syncwarp.
+//
+// The middle row is fetched once per fiber (when the middle index changes
+// along the team's nonzeros) and used when the fiber closes: acc += U1[b] (.)
+// t_f. A team walks a contiguous range of nonzeros; the grid is one block per
+// SM with as many warps as the rings allow in shared memory (at most 24), and
+// the ranges split the nonzeros evenly over all teams. Positions are 32-bit
+// (a format holds fewer than 2^32 nonzeros). Needs 16-byte aligned index and
+// value arrays; outputs zeroed by the caller.
+__device__ __forceinline__ uint32_t sm_addr(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+// 16 bytes global -> shared, bypassing L1; the first n bytes are copied and
+// the rest of the 16 zero-filled (n = 0 reads nothing)
+__device__ __forceinline__ void cpa16(uint32_t dst, const void* src, uint32_t n) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(n) : "memory");
+}
+__device__ __forceinline__ void cpa_row16(uint32_t dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cpa_row8(uint32_t dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cpa_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cpa_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// Shared-memory layout of kernel 7, per warp: DI = 2 D index stages (three
+// arrays x NT teams x GS / 4 16-byte vectors), then D row stages (leaf and
+// middle slots x GS nonzeros x V pieces x 32 lanes).
+template <int G, int V, class T, int GS, int D>
+struct StgShape {
+  static constexpr uint32_t NT = 32 / G;
+  static constexpr uint32_t DI = 2 * D;
+  static constexpr uint32_t PB = std::is_same<T, __nv_bfloat16>::value ? 8 : 16;
+  static constexpr uint32_t NV = GS / 4;
+  static constexpr uint32_t NIV = 3 * NT * NV;
+  static constexpr uint32_t NR = (NIV + 31) / 32;  // copy rounds per index stage
+  static constexpr uint32_t IDX_STAGE = NIV * 16;
+  static constexpr uint32_t ROW_STAGE = 2 * GS * V * 32 * PB;
+  static constexpr uint32_t WARP_BYTES = DI * IDX_STAGE + D * ROW_STAGE;
+  static constexpr uint32_t MAX_SMEM = 227 * 1024;
+  static constexpr uint32_t WPB = MAX_SMEM / WARP_BYTES > 24 ? 24 : MAX_SMEM / WARP_BYTES;
+};
+
+template <bool PAIR, int G, int V, class T, int GS, int D>
+__global__ void __launch_bounds__(32 * StgShape<G, V, T, GS, D>::WPB, 1) k_mttkrp_stg(const Args<T> a) {
+  using SS = StgShape<G, V, T, GS, D>;
+  static_assert(GS == 4 || GS == 8, "steps of 4 or 8 nonzeros per team");
+  constexpr uint32_t NT = SS::NT, DI = SS::DI, NV = SS::NV, NR = SS::NR;
+  constexpr uint32_t R = 4 * G * V;
+  constexpr uint32_t FLAG = 0x80000000u;
+  constexpr uint32_t NONE = 0xffffffffu;
+  constexpr bool BF = std::is_same<T, __nv_bfloat16>::value;
+  using Piece = std::conditional_t<BF, uint2, float4>;
+  extern __shared__ __align__(128) unsigned char stg_smem[];
+  const int lane = threadIdx.x & 31;
+  const int tl = lane & (G - 1);
+  const uint32_t t = (uint32_t)lane / G;
+  unsigned char* const wsm = stg_smem + (threadIdx.x >> 5) * SS::WARP_BYTES;
+  unsigned char* const isc = wsm;                                   // index stages
+  unsigned char* const rsc = wsm + DI * SS::IDX_STAGE + lane * SS::PB;  // this lane's row pieces
+  const uint32_t* __restrict__ snz = a.snz;
+  const uint32_t* __restrict__ sidx = a.sidx;
+  const T* __restrict__ U0 = a.U[0];
+  const T* __restrict__ U1 = a.U[1];
+  const T* __restrict__ U2 = a.U[2];
+  float* __restrict__ out = a.out;
+  [[maybe_unused]] float* __restrict__ out2 = a.out2;
+  const uint32_t chunk = a.chunk, nnz = (uint32_t)a.nnz;
+  const uint32_t nsteps = chunk / GS;
+  auto rd = [&](float* o, uint32_t row, int v, float4 x) { red4(o + (uint64_t)row * R + Cols<T, G, V>::of(tl, v), x); };
+
+  // the warp's first team, and this team's range [x0, x1) (empty past nnz)
+  const uint32_t team0 = (uint32_t)((blockIdx.x * (uint64_t)blockDim.x + (threadIdx.x & ~31u)) / G);
+  const uint32_t x0 = (uint32_t)min((uint64_t)(team0 + t) * chunk, (uint64_t)nnz);
+  const uint32_t x1 = (uint32_t)min((uint64_t)x0 + chunk, (uint64_t)nnz);
+
+  // index copies: lane q of round r copies vector q = (array, team, vec) of
+  // every index stage; its source advances GS nonzeros per stage
+  const void* ibase_src[NR];
+  uint32_t ip[NR], ie[NR];
+  bool iq[NR];
+#pragma unroll
+  for (uint32_t r = 0; r < NR; ++r) {
+    const uint32_t q = r * 32 + (uint32_t)lane;
+    iq[r] = q < SS::NIV;
+    const uint32_t arr = q / (NT * NV), tt = (q / NV) % NT, vec = q % NV;
+    const uint32_t s0 = (uint32_t)min((uint64_t)(team0 + tt) * chunk, (uint64_t)nnz);
+    ip[r] = s0 + 4 * vec;
+    ie[r] = (uint32_t)min((uint64_t)s0 + chunk, (uint64_t)nnz);
+    ibase_src[r] = arr == 0 ? (const void*)a.leaf : arr == 1 ? (const void*)a.mid : (const void*)a.vals;
+  }
+  auto issue_idx = [&](uint32_t slot) {
+    const uint32_t dst = sm_addr(isc + slot * SS::IDX_STAGE) + (uint32_t)lane * 16;
+#pragma unroll
+    for (uint32_t r = 0; r < NR; ++r) {
+      if (iq[r]) {
+        const uint32_t n = ip[r] < ie[r] ? min(16u, (ie[r] - ip[r]) * 4) : 0u;
+        cpa16(dst + r * 512, n ? (const void*)((const uint32_t*)ibase_src[r] + ip[r]) : ibase_src[r], n);
+        ip[r] += GS;
+      }
+    }
+  };
+  // this team's vector vec of array arr in index stage `slot`
+  auto ivec = [&](uint32_t slot, uint32_t arr, uint32_t vec) -> uint4 {
+    return *reinterpret_cast<const uint4*>(isc + slot * SS::IDX_STAGE + ((arr * NT + t) * NV + vec) * 16);
+  };
+  auto piece_at = [&](uint32_t rslot, uint32_t kind, uint32_t j, int v) -> unsigned char* {
+    return rsc + rslot * SS::ROW_STAGE + ((kind * GS + j) * V + v) * 32 * SS::PB;
+  };
+  auto copy_row = [&](unsigned char* dst, const T* U, uint32_t row, int v) {
+    const T* src = U + (uint64_t)row * R + Cols<T, G, V>::of(tl, v);
+    if constexpr (BF) cpa_row8(sm_addr(dst), src);
+    else cpa_row16(sm_addr(dst), src);
+  };
+  auto widen = [&](const Piece& p) -> float4 {
+    if constexpr (BF) return bf16x4_to_f32(p.x, p.y);
+    else return p;
+  };
+  // row stage: this team's leaf rows, and the middle row wherever the middle
+  // index changes along the team's nonzeros (bq: the last one seen)
+  uint32_t bq = NONE, xr = x0;
+  auto issue_rows = [&](uint32_t islot, uint32_t rslot) {
+    uint32_t K[GS], B[GS];
+#pragma unroll
+    for (uint32_t c = 0; c < NV; ++c) {
+      const uint4 k4 = ivec(islot, 0, c), b4 = ivec(islot, 1, c);
+      K[4 * c] = k4.x; K[4 * c + 1] = k4.y; K[4 * c + 2] = k4.z; K[4 * c + 3] = k4.w;
+      B[4 * c] = b4.x; B[4 * c + 1] = b4.y; B[4 * c + 2] = b4.z; B[4 * c + 3] = b4.w;
+    }
+    const bool full = xr + GS <= x1;
+#pragma unroll
+    for (uint32_t j = 0; j < GS; ++j) {
+      if (full || xr + j < x1) {
+#pragma unroll
+        for (int v = 0; v < V; ++v) copy_row(piece_at(rslot, 0, j, v), U2, K[j] & ~FLAG, v);
+        if (B[j] != bq) {
+#pragma unroll
+          for (int v = 0; v < V; ++v) copy_row(piece_at(rslot, 1, j, v), U1, B[j], v);
+          bq = B[j];
+        }
+      }
+    }
+    xr += GS;
+  };
+
+  // open slice of this team
+  uint32_t sl = 0;
+  if (x0 < x1) {
+    uint32_t lo = 0, hi = a.nslc - 1;
+    while (lo < hi) {
+      const uint32_t mm = (lo + hi + 1) >> 1;
+      if (__ldg(snz + mm) <= x0) lo = mm; else hi = mm - 1;
+    }
+    sl = lo;
+  }
+  uint32_t ca = __ldg(sidx + sl);
+  uint32_t nxt = __ldg(snz + sl + 1);
+  float4 acc[V], accf[V], rowB[V];
+  [[maybe_unused]] float4 rowA[V];
+#pragma unroll
+  for (int v = 0; v < V; ++v) {
+    acc[v] = accf[v] = rowB[v] = f4(0.f);
+    if constexpr (PAIR) rowA[v] = load_piece<T, G, V>(U0 + (uint64_t)ca * R, tl, v);
+  }
+  uint32_t bopen = NONE, blast = NONE;
+  auto close_fiber = [&]() {
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      acc[v] = pfma(rowB[v], accf[v], acc[v]);
+      if constexpr (PAIR) rd(out2, bopen, v, pmul(rowA[v], accf[v]));
+      accf[v] = f4(0.f);
+    }
+  };
+
+  // prologue: the first D index stages, then (once they have landed) the
+  // first D row stages with index stages D .. 2D-1, one commit group each
+#pragma unroll 1
+  for (uint32_t m = 0; m < (uint32_t)D; ++m) issue_idx(m);
+  cpa_commit();
+  cpa_wait<0>();
+  __syncwarp();
+#pragma unroll 1
+  for (uint32_t m = 0; m < (uint32_t)D; ++m) {
+    if (m < nsteps) issue_rows(m, m);
+    issue_idx(m + D);
+    cpa_commit();
+  }
+
+  uint32_t is = 0, rs = 0;  // index and row slots of step n
+  uint32_t xg = x0;
+#pragma unroll 1
+  for (uint32_t n = 0; n < nsteps; ++n) {
+    // the commit group of step n - D (rows of step n, indices of step n + D)
+    cpa_wait<D - 1>();
+    __syncwarp();
+    uint32_t B[GS];
+    float Wv[GS];
+    Piece lv[GS][V];
+#pragma unroll
+    for (uint32_t c = 0; c < NV; ++c) {
+      const uint4 b4 = ivec(is, 1, c), w4 = ivec(is, 2, c);
+      B[4 * c] = b4.x; B[4 * c + 1] = b4.y; B[4 * c + 2] = b4.z; B[4 * c + 3] = b4.w;
+      Wv[4 * c] = __uint_as_float(w4.x); Wv[4 * c + 1] = __uint_as_float(w4.y);
+      Wv[4 * c + 2] = __uint_as_float(w4.z); Wv[4 * c + 3] = __uint_as_float(w4.w);
+    }
+#pragma unroll
+    for (uint32_t j = 0; j < GS; ++j)
+#pragma unroll
+      for (int v = 0; v < V; ++v) lv[j][v] = *reinterpret_cast<const Piece*>(piece_at(rs, 0, j, v));
+    auto mid_row = [&](uint32_t j) {
+#pragma unroll
+      for (int v = 0; v < V; ++v) rowB[v] = widen(*reinterpret_cast<const Piece*>(piece_at(rs, 1, j, v)));
+    };
+    if (xg + GS <= x1 && xg + GS <= nxt && bopen != NONE) {
+      // the common case: a fiber is open (so bopen == blast) and the whole
+      // step lies in the open slice and the range
+#pragma unroll
+      for (uint32_t j = 0; j < GS; ++j) {
+        if (B[j] != blast) {
+          close_fiber();
+          mid_row(j);
+          blast = bopen = B[j];
+        }
+#pragma unroll
+        for (int v = 0; v < V; ++v) accf[v] = pfma_s(Wv[j], widen(lv[j][v]), accf[v]);
+      }
+    } else {
+#pragma unroll
+      for (uint32_t j = 0; j < GS; ++j) {
+        const uint32_t x = xg + j;
+        if (x < x1) {
+          if (x >= nxt) {  // the slice ends before nonzero x
+            if (bopen != NONE) close_fiber();
+#pragma unroll
+            for (int v = 0; v < V; ++v) { rd(out, ca, v, acc[v]); acc[v] = f4(0.f); }
+            do {
+              ++sl;
+              nxt = __ldg(snz + sl + 1);
+            } while (x >= nxt);
+            ca = __ldg(sidx + sl);
+            if constexpr (PAIR) {
+#pragma unroll
+              for (int v = 0; v < V; ++v) rowA[v] = load_piece<T, G, V>(U0 + (uint64_t)ca * R, tl, v);
+            }
+            bopen = NONE;
+          }
+          const uint32_t b = B[j];
+          if (b != bopen) {  // the open fiber ends before nonzero x
+            if (bopen != NONE) close_fiber();
+            bopen = b;
+          }
+          if (b != blast) {  // its middle row was staged with this nonzero
+            mid_row(j);
+            blast = b;
+          }
+#pragma unroll
+          for (int v = 0; v < V; ++v) accf[v] = pfma_s(Wv[j], widen(lv[j][v]), accf[v]);
+        }
+      }
+    }
+    __syncwarp();  // every lane is done with index stage `is` before it is refilled
+    const uint32_t is2 = is + D < DI ? is + D : is + D - DI;
+    if (n + D < nsteps) issue_rows(is2, rs);
+    issue_idx(is);
+    cpa_commit();
+    is = is + 1 == DI ? 0 : is + 1;
+    rs = rs + 1 == (uint32_t)D ? 0 : rs + 1;
+    xg += GS;
+  }
+  cpa_wait<0>();  // nothing of this warp's ring is left in flight at exit
+  if (x0 < x1) {
+    if (bopen != NONE) close_fiber();
+#pragma unroll
+    for (int v = 0; v < V; ++v) rd(out, ca, v, acc[v]);
+  }
+}
+
+// Kernel 7's launch. Occupancy level -> (nonzeros per team and step, stages):
+// 1: (4, 2), 2: (4, 3), 3: (8, 2), 4: (8, 3); warps per block as many as the
+// rings fit in 227 KB of shared memory (at most 24); one block per SM; every
+// team an equal range of nonzeros (a multiple of the step).
+template <bool PAIR, int G, int V, class T, int GS, int D>
+cudaError_t launch_stg_d(Args<T> a, cudaStream_t s) {
+  using SS = StgShape<G, V, T, GS, D>;
+  constexpr int wpb = (int)SS::WPB;
+  static_assert(wpb >= 1, "rings exceed shared memory");
+  const uint64_t per_block = (uint64_t)wpb * SS::NT * GS;  // nonzeros per block at the smallest range
+  uint64_t blocks = (a.nnz + per_block - 1) / per_block;
+  const uint64_t nsm = (uint64_t)sm_count();
+  if (blocks > nsm) blocks = nsm;
+  const uint64_t teams = blocks * wpb * SS::NT;
+  uint64_t chunk = (a.nnz + teams - 1) / teams;
+  chunk = (chunk + GS - 1) / GS * GS;
+  if (a.nnz + chunk + 2 * GS >= 0xffffffffull) return cudaErrorInvalidValue;  // 32-bit positions
+  a.chunk = (uint32_t)chunk;
+  a.cslc = nullptr;
+  const size_t smem = (size_t)wpb * SS::WARP_BYTES;
+  auto k = k_mttkrp_stg<PAIR, G, V, T, GS, D>;
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  k<<<(unsigned)blocks, wpb * 32, smem, s>>>(a);
+  return cudaGetLastError();
+}
+
+template <bool PAIR, int G, int V, class T>
+cudaError_t launch_stg(const Args<T>& a, int mb, cudaStream_t s) {
+  switch (mb) {
+    case 1: return launch_stg_d<PAIR, G, V, T, 4, 2>(a, s);
+    case 3: return launch_stg_d<PAIR, G, V, T, 8, 2>(a, s);
+    case 4: return launch_stg_d<PAIR, G, V, T, 8, 3>(a, s);
+    default: return launch_stg_d<PAIR, G, V, T, 4, 3>(a, s);
+  }
+}
+
 template <int G, int V, class T>
 cudaError_t launch_pair4(const Args<T>& a, int threads, int mb, cudaStream_t s) {
   const uint64_t teams = (a.nnz + a.chunk - 1) / a.chunk;
@@ -1822,9 +2156,15 @@ cudaError_t launch_rows(const Args<T>& a, int threads, int mb, cudaStream_t s) {
 // 3 = per-nonzero walk (slice and leaf levels of parts that carry `mid`),
 // 4 = per-nonzero walk with the middle row once per fiber (3-D slice level;
 // elsewhere as 3), 5 = per-nonzero walk with vector index loads (3-D), 6 = the
-// warp-interleaved per-nonzero walk (3-D slice level; elsewhere as 5)
+// warp-interleaved per-nonzero walk (3-D slice level; elsewhere as 5), 7 = the
+// walk with rows staged in shared memory (3-D slice level, R 16..128;
+// elsewhere as 6)
 template <int ND, int G, int V, class T>
 cudaError_t launch_lvl(const Args<T>& a, int lvl, int kern, int threads, int mb, cudaStream_t s) {
+  if constexpr (ND == 3 && G >= 4 && V == 1) {
+    if (kern == 7 && lvl == 0 && vec_ok(a)) return launch_stg<false, G, V, T>(a, mb, s);
+  }
+  if (kern == 7) kern = 6;  // the staged walk covers the 3-D slice level at R 16..128; elsewhere kernel 6's rule
   if constexpr (ND == 3) {
     if (kern == 6) {
       if (lvl == 0 && vec_ok(a)) return launch_il<false, G, V, T>(a, threads, mb, s);
@@ -1894,7 +2234,8 @@ cudaError_t launch_fixed(const Args<T>& a, int nd, int lvl, int kern, int thread
 // The two-output walks (R <= 128). kern 2: the branch-free fiber walk with
 // both outputs; 4: the per-nonzero walk with the middle row once per fiber;
 // 5: the per-nonzero form with vector index loads; 6: the warp-interleaved
-// per-nonzero form; otherwise the per-nonzero form. 4-D runs its own walk.
+// per-nonzero form; 7: the form with rows staged in shared memory (R >= 16);
+// otherwise the per-nonzero form. 4-D runs its own walk.
 template <class T, int R>
 cudaError_t launch_pair_fixed(const Args<T>& a, int nd, int threads, int mb, int kern, cudaStream_t s) {
   if constexpr (R > 128) {
@@ -1903,6 +2244,9 @@ cudaError_t launch_pair_fixed(const Args<T>& a, int nd, int threads, int mb, int
     constexpr int G = TeamShape<T, R>::G;
     constexpr int V = TeamShape<T, R>::V;
     if (nd == 4) return launch_pair4<G, V, T>(a, threads, mb, s);
+    if constexpr (G >= 4 && V == 1)
+      if (kern == 7 && vec_ok(a)) return launch_stg<true, G, V, T>(a, mb, s);
+    if (kern == 7) kern = 6;
     if (kern == 6 && vec_ok(a)) return launch_il<true, G, V, T>(a, threads, mb, s);
     if (kern == 6) kern = 5;
     if constexpr (G >= 4)

@@ -294,10 +294,11 @@ def test_full_size_skewed_elementwise(views, torch_cuda):
 @pytest.mark.parametrize("R", [4, 32, 128, 256])
 @pytest.mark.parametrize("dtype", ["f32", "bf16"])
 def test_kernel_variants_3d(R, dtype, torch_cuda):
-    """The four 3-D traversals (per-team fiber walk, branch-free fiber walk,
-    per-nonzero walk, per-nonzero walk with the middle row once per fiber) at every
-    occupancy level, on the partition and on the views, with fiber splits and
-    with many short slices (slice changes inside most blocks)."""
+    """The 3-D kernels (per-team fiber walk, branch-free fiber walk,
+    per-nonzero walk, per-nonzero walk with the middle row once per fiber,
+    vector index loads, warp-interleaved walk, rows staged in shared memory) at
+    every occupancy level, on the partition and on the views, with fiber
+    splits and with many short slices (slice changes inside most blocks)."""
     import mmcsf
     torch = torch_cuda
     rng = np.random.default_rng(300 + R)
@@ -317,7 +318,7 @@ def test_kernel_variants_3d(R, dtype, torch_cuda):
             for m in range(3):
                 travs = (1, 2) if F.info(4 + m)["present"] else (1,)
                 for trav in travs:
-                    for kern in (1, 2, 3, 4, 5, 6):
+                    for kern in (1, 2, 3, 4, 5, 6, 7):
                         for mb in (1, 2, 3, 4):
                             for chunk in (64, 1000):
                                 cfg = {"traversal": trav, "kernel": kern, "min_blocks": mb, "chunk": chunk}
@@ -325,7 +326,7 @@ def test_kernel_variants_3d(R, dtype, torch_cuda):
                                 _check_close(out.cpu().numpy(), ref[m], (dims, f, m, cfg))
             if f == 0:
                 B = mmcsf.Format(X, impl=mmcsf.IMPL_BCSF, mode=1, fiber_threshold=4)
-                for kern in (1, 2, 3, 4, 5, 6):
+                for kern in (1, 2, 3, 4, 5, 6, 7):
                     out = B.mttkrp(1, Ud, cfg={"kernel": kern})
                     _check_close(out.cpu().numpy(), ref[1], ("bcsf", dims, kern))
 
@@ -361,6 +362,44 @@ def test_kernel_variants_4d(R, dtype, torch_cuda):
                                 _check_close(out.cpu().numpy(), ref[m], (dims, f, m, cfg))
 
 
+@pytest.mark.parametrize("R", [16, 32, 64, 128])
+@pytest.mark.parametrize("dtype", ["f32", "bf16"])
+def test_staged_walk_edges(R, dtype, torch_cuda):
+    """Kernel 7 (rows staged in shared memory, even nonzero ranges per team):
+    nonzero counts below, at and just past a team's 8-nonzero step and a
+    block's share (most teams empty, ranges ending mid-step), one slice, one
+    fiber, fibers of one nonzero, a middle index repeated across slices, at
+    every stage count, single mode and two-output walk, against the FP64
+    oracle."""
+    import mmcsf
+    torch = torch_cuda
+    rng = np.random.default_rng(700 + R)
+    cases = [([4, 5, 6], 1), ([4, 5, 6], 7), ([4, 5, 6], 9), ([9, 9, 9], 300), ([1, 30, 4000], 3000),
+             ([1, 1, 5000], 4000), ([5000, 3, 1], 2500), ([60, 2, 300], 20000), ([3000, 40, 3000], 50000)]
+    for dims, n in cases:
+        inds, vals = _rand_coo(rng, dims, n)
+        X = mmcsf.CooTensor.from_arrays(dims, inds, vals)
+        U = [rng.random((d, R)).astype(np.float32) for d in dims]
+        if dtype == "bf16":
+            Ud = [torch.tensor(u, device="cuda").to(torch.bfloat16) for u in U]
+            U = [t.float().cpu().numpy() for t in Ud]
+        else:
+            Ud = [torch.tensor(u, device="cuda") for u in U]
+        ref = [O.mttkrp_coo_f64(dims, inds, vals, m, U) for m in range(3)]
+        for f in (0, 2):
+            F = mmcsf.Format(X, impl=mmcsf.IMPL_MMCSF, mode=0, fiber_threshold=f, views=2)
+            m0, m1 = F.pair_modes()
+            for mb in (1, 2, 3, 4):
+                for m in range(3):
+                    for trav in ((1, 2) if F.info(4 + m)["present"] else (1,)):
+                        cfg = {"traversal": trav, "kernel": 7, "min_blocks": mb}
+                        _check_close(F.mttkrp(m, Ud, cfg=cfg).cpu().numpy(), ref[m], (dims, n, f, m, cfg))
+                for rep in range(2):  # the outputs are zeroed by every call
+                    outs = F.mttkrp_pair(Ud, cfg={"kernel": 7, "min_blocks": mb})
+                    for m in (m0, m1):
+                        _check_close(outs[m].cpu().numpy(), ref[m], ("pair", dims, n, f, mb, m, rep))
+
+
 @pytest.mark.parametrize("R", [4, 8, 32, 64, 128])
 @pytest.mark.parametrize("dtype", ["f32", "bf16"])
 def test_two_output_walk(R, dtype, torch_cuda):
@@ -387,7 +426,7 @@ def test_two_output_walk(R, dtype, torch_cuda):
             m0, m1 = F.pair_modes()
             order = F.info(2)["mode_order"]
             assert (m0, m1) == (order[0], order[1])
-            for kern in (2, 3, 4, 5, 6):
+            for kern in (2, 3, 4, 5, 6, 7):
                 for mb in (1, 2, 3, 4):
                     for chunk in (1, 32, 100, 1024):
                         outs = F.mttkrp_pair(Ud, cfg={"min_blocks": mb, "chunk": chunk, "kernel": kern})
@@ -399,7 +438,7 @@ def test_two_output_walk(R, dtype, torch_cuda):
             F.set_plan(plan)
             F.mttkrp_all(Ud)
             separate = F.last_launches
-            for kern in (2, 3, 4, 5, 6):
+            for kern in (2, 3, 4, 5, 6, 7):
                 plan["pair"].update(use=True, chunk=256, min_blocks=2, kernel=kern)
                 F.set_plan(plan)
                 for _ in range(2):
@@ -476,7 +515,7 @@ def test_two_output_walk_errors(torch_cuda):
     with pytest.raises(mmcsf.MmcsfError):
         F.set_plan({"pair": {"use": True, "chunk": -1, "min_blocks": 1}})
     with pytest.raises(mmcsf.MmcsfError):
-        F.set_plan({"pair": {"use": True, "chunk": 256, "min_blocks": 1, "kernel": 7}})
+        F.set_plan({"pair": {"use": True, "chunk": 256, "min_blocks": 1, "kernel": 8}})
 
 
 @pytest.mark.parametrize("nd", [3, 4])

@@ -83,13 +83,13 @@ def test_skewed_shape_every_traversal(R, skewed, torch_cuda):
     F = mmcsf.Format(X, impl=mmcsf.IMPL_MMCSF, mode=0, views=2)
     for m in range(3):
         for trav in ((1, 2) if F.info(4 + m)["present"] else (1,)):  # the partition's slice mode has no view
-            for kern in (1, 2, 3, 4, 5, 6):
+            for kern in (1, 2, 3, 4, 5, 6, 7):
                 for mb in (1, 2, 3, 4):
                     cfg = {"traversal": trav, "kernel": kern, "min_blocks": mb, "chunk": 512}
                     _check_close(F.mttkrp(m, Ud, cfg=cfg).cpu().numpy(), want[m], (R, m, cfg))
     m0, m1 = F.pair_modes()
-    for kern in (2, 3, 4, 5, 6):
-        for mb in (1, 2, 3):
+    for kern in (2, 3, 4, 5, 6, 7):
+        for mb in (1, 2, 3, 4):
             outs = F.mttkrp_pair(Ud, cfg={"kernel": kern, "min_blocks": mb, "chunk": 512})
             for m in (m0, m1):
                 _check_close(outs[m].cpu().numpy(), want[m], ("pair", R, kern, mb, m))

@@ -387,17 +387,20 @@ int mmcsf_format_values(const mmcsf_format* F, const float** d_vals, uint64_t* n
  * first iteration) or after max_iters. Differences from the reference: the fit
  * uses the full symmetric Gram product and the max-norm is a true maximum
  * (both are wrong in the reference, src/cpd_cpu.cu:383-385 and :298-303). */
-#define MMCSF_CPD_FP32 0       /* FP32 factors and small-matrix math; host checks the fit each iteration */
-#define MMCSF_CPD_BF16 1       /* BF16 factors, FP32 MTTKRP accumulation, FP64 Gram/solve/lambda/fit; one CUDA
-                                  graph launch for the whole loop (needs a non-default stream) */
-#define MMCSF_CPD_FP64_SOLVE 2 /* FP32 factors with the FP64 small-matrix math, host-driven */
+#define MMCSF_CPD_FP32 0       /* FP32 factors and small-matrix math */
+#define MMCSF_CPD_BF16 1       /* BF16 factors, FP32 MTTKRP accumulation, FP64 Gram/solve/lambda/fit */
+#define MMCSF_CPD_FP64_SOLVE 2 /* FP32 factors with the FP64 small-matrix math */
+/* Every form runs the whole loop as one CUDA graph launch (a WHILE node over one
+ * captured iteration) unless no_graph is set. The graph needs a non-default
+ * stream: on the default stream the FP32 forms run host-driven (the host reads
+ * the fit back every iteration) and the BF16 form returns MMCSF_ERR_INVALID. */
 #define MMCSF_CPD_MAX_HISTORY 1000
 typedef struct {
   int rank;       /* 4, 8, 16, 32 or 64 */
   int max_iters;  /* 0 = the reference's 10 (src/util.h:210) */
   double tol;     /* 0 = the reference's 1e-5 (src/cpd_cpu.cu:494) */
   int precision;  /* MMCSF_CPD_* */
-  int no_graph;   /* 1: run the BF16 form host-driven too */
+  int no_graph;   /* 1: run the loop host-driven (one iteration at a time), at any precision */
   uint64_t seed;  /* initial factors uniform in [0,1) when d_init is NULL */
   int profile;    /* 1: time every phase of every iteration with CUDA events (host-driven loop, also for
                      BF16) into mmcsf_cpd_result.phase_ms; the events add a few microseconds per phase */

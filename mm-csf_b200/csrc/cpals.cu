@@ -9,13 +9,16 @@
 // factor. After the last mode, the fit. Everything stays on the device.
 //
 // Two forms:
-//   * precision MMCSF_CPD_FP32: FP32 factors and FP32 small-matrix math, one
-//     host-driven iteration at a time (the fit is read back to test
-//     convergence), like the reference's structure;
+//   * precision MMCSF_CPD_FP32: FP32 factors and FP32 small-matrix math;
 //   * precision MMCSF_CPD_BF16: BF16 factors (the MTTKRP inputs) with FP32
 //     accumulation, and the Gram Hadamard / Cholesky solve / lambda / fit in
-//     FP64; the whole loop is ONE CUDA graph launch: a WHILE conditional node
-//     whose body is one iteration, the fit kernel setting the condition.
+//     FP64.
+// Either form runs the whole loop as ONE CUDA graph launch (a WHILE
+// conditional node whose body is one iteration, the fit kernel setting the
+// condition) unless opts.no_graph is set; on the default stream, which cannot
+// be captured, the FP32 forms run host-driven instead (one iteration at a time,
+// the fit read back to test convergence, like the reference's structure) and
+// the BF16 form is refused.
 //
 // Deviations from the reference, on purpose: the fit uses the full symmetric
 // Gram product (the reference reads the unwritten triangle,
@@ -39,6 +42,7 @@ using mmcsf::set_error;
 namespace mmcsf {
 int mttkrp_mode(const mmcsf_format* F, int mode, int R, int dtype, const void* const* U, float* out,
                 const mmcsf_kernel_cfg* cfg, cudaStream_t s, int* launches);
+int reserve_leaf_scratch(mmcsf_format* F, int R, int dtype);
 
 namespace {
 
@@ -434,6 +438,7 @@ struct Als {
     MMCSF_CUDA(st.alloc(sizeof(State)));
     MMCSF_CUDA(hist.alloc((uint64_t)maxit * sizeof(double)));
     MMCSF_CUDA(status.alloc(sizeof(int)));
+    MMCSF_TRY(reserve_leaf_scratch(F, R, dtype));  // nothing allocates inside the iteration (it may be captured)
     MMCSF_CUDA(cudaMemsetAsync(st.p, 0, sizeof(State), s));
     MMCSF_CUDA(cudaMemsetAsync(hist.p, 0, (uint64_t)maxit * sizeof(double), s));
     MMCSF_CUDA(cudaMemsetAsync(grams.p, 0, (uint64_t)nd * R * R * sizeof(A), s));
@@ -574,7 +579,7 @@ int run_cpd(mmcsf_format* F, const mmcsf_cpd_opts* o, const float* const* d_init
   MMCSF_CUDA(cudaEventRecord(e0, s));
   typename Als<T, A>::Prof prof;
   if (o->profile) MMCSF_TRY(prof.init());
-  if (o->precision == MMCSF_CPD_BF16 && !o->no_graph && !o->profile) {
+  if (!o->no_graph && !o->profile && (o->precision == MMCSF_CPD_BF16 || s != nullptr)) {
     // the whole loop as one graph: WHILE node, body = one iteration
     cudaGraph_t g = nullptr;
     cudaGraphExec_t ge = nullptr;

@@ -92,6 +92,20 @@ __global__ void k_add_f64(const double* __restrict__ in, uint64_t n, float* __re
     out[i] = (float)((double)out[i] + in[i]);
 }
 
+// The format's scratch buffers grow on first use. cudaMalloc and cudaFree are
+// not allowed while a stream is being captured (the failed call would also
+// invalidate the capture), so a growth needed under capture is refused with a
+// clear error instead: run the same call once uncaptured first (mmcsf_cpd
+// allocates what its loop needs before it captures).
+int no_alloc_in_capture(cudaStream_t s) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone)
+    return set_error(MMCSF_ERR_UNSUPPORTED,
+                     "a scratch buffer of the format must grow, which cannot happen during stream capture: "
+                     "run the call once before capturing it");
+  return MMCSF_OK;
+}
+
 // MTTKRP on one part for tensor mode `mode`; out must be zeroed by the caller.
 int part_mttkrp(const mmcsf_format* F, const CsfPart& P, int mode, int R, int dtype, const void* const* U,
                 float* out, const mmcsf_kernel_cfg* cfg, cudaStream_t s, int* launches,
@@ -122,7 +136,10 @@ int part_mttkrp(const mmcsf_format* F, const CsfPart& P, int mode, int R, int dt
   double* o64 = nullptr;
   if (leaf) {
     mmcsf_format* Fm = const_cast<mmcsf_format*>(F);
-    if (Fm->leaf64.bytes < nout * 8) MMCSF_CUDA(Fm->leaf64.alloc(nout * 8));
+    if (Fm->leaf64.bytes < nout * 8) {
+      MMCSF_TRY(no_alloc_in_capture(s));
+      MMCSF_CUDA(Fm->leaf64.alloc(nout * 8));
+    }
     o64 = Fm->leaf64.as<double>();
     MMCSF_CUDA(cudaMemsetAsync(o64, 0, nout * 8, s));
   }
@@ -179,7 +196,10 @@ int mttkrp_mode_vals(const mmcsf_format* F, int mode, int R, int dtype, const vo
     const float* vv = nullptr;
     if (vals) {
       mmcsf_format* Fm = const_cast<mmcsf_format*>(F);
-      if (Fm->vals_scratch.bytes < V.nnz * 4) MMCSF_CUDA(Fm->vals_scratch.alloc(V.nnz * 4));
+      if (Fm->vals_scratch.bytes < V.nnz * 4) {
+        MMCSF_TRY(no_alloc_in_capture(s));
+        MMCSF_CUDA(Fm->vals_scratch.alloc(V.nnz * 4));
+      }
       k_reorder_vals<<<grid_for(V.nnz, 256), 256, 0, s>>>(vals, V.from_part.as<uint32_t>(), V.nnz,
                                                           Fm->vals_scratch.as<float>());
       MMCSF_LAUNCH_CHECK();
@@ -203,6 +223,24 @@ int mttkrp_mode_vals(const mmcsf_format* F, int mode, int R, int dtype, const vo
 int mttkrp_mode(const mmcsf_format* F, int mode, int R, int dtype, const void* const* U, float* out,
                 const mmcsf_kernel_cfg* cfg, cudaStream_t s, int* launches) {
   return mttkrp_mode_vals(F, mode, R, dtype, U, nullptr, out, cfg, s, launches);
+}
+
+// Allocate, now, the FP64 scratch that mttkrp_mode (default cfg) needs for
+// every mode it walks at a partition's leaf level, so that later calls,
+// captured ones included, allocate nothing.
+int reserve_leaf_scratch(mmcsf_format* F, int R, int dtype) {
+  const int d = dtype == MMCSF_DTYPE_BF16 ? 1 : 0;
+  uint64_t need = 0;
+  for (int m = 0; m < F->nd; ++m) {
+    const int trav = F->plan_traversal[d][m] ? F->plan_traversal[d][m] : (F->views[m].present ? 2 : 1);
+    if (trav == 2) continue;  // a view walks the mode at level 0
+    for (int p = 0; p < F->nd; ++p) {
+      const CsfPart& P = F->parts[p];
+      if (P.present && P.nnz && P.order[P.nd - 1] == m) need = std::max(need, F->dims[m] * (uint64_t)R * 8);
+    }
+  }
+  if (need > F->leaf64.bytes) MMCSF_CUDA(F->leaf64.alloc(need));
+  return MMCSF_OK;
 }
 
 }  // namespace mmcsf

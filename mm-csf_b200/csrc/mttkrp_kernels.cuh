@@ -20,6 +20,7 @@
 // Correct for every R (the reference's kernels keep one scalar accumulator per
 // lane across the rank loop and are wrong for R > 32).
 #include <algorithm>
+#include <atomic>
 #include <cuda_bf16.h>
 
 #include <cstring>
@@ -2016,8 +2017,18 @@ cudaError_t launch_stg_d(Args<T> a, cudaStream_t s) {
   a.cslc = nullptr;
   const size_t smem = (size_t)wpb * SS::WARP_BYTES;
   auto k = k_mttkrp_stg<PAIR, G, V, T, GS, D>;
-  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  // the shared-memory opt-in, once per device (the first launch on a device
+  // sets it; later launches, captured ones included, only launch)
+  static std::atomic<uint64_t> opted{0};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
+  const uint64_t bit = 1ull << (dev & 63);
+  if (!(opted.load() & bit)) {
+    e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    opted.fetch_or(bit);
+  }
   k<<<(unsigned)blocks, wpb * 32, smem, s>>>(a);
   return cudaGetLastError();
 }

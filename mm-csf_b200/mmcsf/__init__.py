@@ -526,8 +526,10 @@ class Format:
     def cpd(self, rank, max_iters=10, tol=1e-5, precision="fp32", init=None, seed=0, graph=True, stream=None,
             profile=False):
         """CP-ALS on the device (mmcsf_cpd). precision: "fp32" (FP32 factors and
-        small-matrix math, host-driven), "bf16" (BF16 factors, FP64 solve/fit,
-        one CUDA graph for the loop unless graph=False) or "fp64solve".
+        small-matrix math), "bf16" (BF16 factors, FP64 solve/fit) or
+        "fp64solve" (FP32 factors, FP64 solve/fit). graph: the whole loop as one
+        CUDA graph launch (on a side stream unless `stream` is given; the FP32
+        forms run host-driven on the default stream); False: host-driven.
         init: optional list of FP32 CUDA tensors (dims[m] x rank). profile:
         time every phase (host-driven loop). Returns a dict with fit, iters,
         converged, seconds, history, lambda, factors (and phase_ms)."""
@@ -552,7 +554,10 @@ class Format:
         res = CpdResult()
         st = stream
         if st is None:
-            st = torch.cuda.Stream(device=dev) if (prec == 1 and graph) else torch.cuda.current_stream(dev)
+            st = torch.cuda.Stream(device=dev) if graph else torch.cuda.current_stream(dev)
+        cur = torch.cuda.current_stream(dev)
+        if st != cur:
+            st.wait_stream(cur)  # the initial factors (and their FP32 copies) come from the current stream
         check(lib().mmcsf_cpd(self._h, ctypes.byref(o), ip, op, lam, ctypes.byref(res), _stream(st)))
         torch.cuda.synchronize(dev)
         return {"fit": res.fit, "iters": res.iters, "converged": bool(res.converged), "seconds": res.seconds,

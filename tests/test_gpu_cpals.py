@@ -5,7 +5,9 @@ reference's cpd() (oracle/cpals_oracle.py), started from the same factors.
   close; the FP64-solve form tighter (1e-6 on the fit);
 * BF16 form (BF16 factors, FP64 Gram/solve/fit, the whole loop in one CUDA
   graph): on a planted low-rank tensor it converges to the FP64 run's fit
-  within 1e-4, and the graph and host-driven runs agree.
+  within 1e-4, and the graph and host-driven runs agree;
+* every form: the one-graph loop and the host-driven loop give the same fit
+  history; on the default stream the FP32 forms run host-driven.
 """
 import numpy as np
 import pytest
@@ -117,3 +119,25 @@ def test_cpd_resume_from_checkpoint(torch_cuda):
     ck[0] = ck[0] * torch.tensor(first["lambda"], dtype=torch.float32, device="cuda")
     second = F.cpd(8, max_iters=3, tol=1e-12, precision="fp64solve", init=ck)
     assert np.max(np.abs(np.array(second["history"]) - np.array(full["history"][3:]))) <= 1e-6
+
+
+@pytest.mark.parametrize("precision", ["fp32", "fp64solve", "bf16"])
+def test_cpd_graph_matches_host_driven(precision, torch_cuda):
+    import mmcsf
+    torch = torch_cuda
+    dims = [60, 45, 50]
+    X, _, _ = _tensor(dims, 8000, seed=21, planted=4, noise=0.01)
+    F = mmcsf.Format(X, impl=mmcsf.IMPL_MMCSF, views=1)
+    _, Ud = _init(torch, dims, 8, seed=22)
+    g = F.cpd(8, max_iters=12, tol=1e-5, precision=precision, init=Ud, graph=True)
+    h = F.cpd(8, max_iters=12, tol=1e-5, precision=precision, init=Ud, graph=False)
+    assert g["graph"] and not h["graph"]
+    assert g["iters"] == h["iters"] and g["converged"] == h["converged"]
+    assert np.max(np.abs(np.array(g["history"]) - np.array(h["history"]))) <= 1e-6, (g["history"], h["history"])
+    for a, b in zip(g["factors"], h["factors"]):
+        assert torch.allclose(a, b, rtol=1e-4, atol=1e-6)
+    if precision != "bf16":  # the default stream cannot be captured: the FP32 forms run host-driven there
+        d = F.cpd(8, max_iters=12, tol=1e-5, precision=precision, init=Ud, graph=True,
+                  stream=torch.cuda.default_stream())
+        assert not d["graph"] and d["iters"] == h["iters"]
+        assert np.max(np.abs(np.array(d["history"]) - np.array(h["history"]))) <= 1e-6

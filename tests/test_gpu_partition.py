@@ -206,8 +206,16 @@ def test_cpals_over_partitions(torch_cuda):
     init = [torch.tensor(rng.random((d, 8)).astype(np.float32), device="cuda") for d in dims]
     runs = []
     for rule in (0, 1):
+        # no views: the loop walks one mode at a partition's leaf level, whose FP64
+        # scratch mmcsf_cpd allocates before it captures the loop into a graph
         F = mmcsf.Format(X, impl=mmcsf.IMPL_MMCSF, partition_rule=rule)
         runs.append(F.cpd(8, max_iters=6, tol=0, precision="fp32", init=init))
+        assert runs[-1]["graph"]
+        h = F.cpd(8, max_iters=6, tol=0, precision="fp32", init=init, graph=False)
+        assert np.max(np.abs(np.array(h["history"]) - np.array(runs[-1]["history"]))) <= 1e-6
+        b = F.cpd(8, max_iters=6, tol=0, precision="bf16", init=init)  # the BF16 form's graph on the same format
+        assert b["graph"] and b["iters"] == 6
+        assert abs(b["history"][-1] - runs[-1]["history"][-1]) <= 1e-2, (b["history"], runs[-1]["history"])
     h0, h1 = np.array(runs[0]["history"]), np.array(runs[1]["history"])
     assert len(h0) == len(h1)
     assert np.max(np.abs(h0 - h1)) <= 1e-4, (h0, h1)

@@ -8,7 +8,10 @@ reference's -f, which it leaves to the user).
   factors: every mode matches the FP64 oracle of the factors that mode read
   (BF16-rounded or FP32) within 1e-5, and the plan's measured error of each
   BF16 mode is its actual change against the FP32-factor output;
-* set_plan of that plan reproduces it exactly (a fresh format);
+* set_plan of that plan reproduces it on a fresh format: the same outputs up
+  to the order of the FP32 vector reductions, which varies from launch to
+  launch (two launches of one format already differ by ~1e-6 relative on
+  Zipf-hot rows), so within the suite's 1e-5;
 * mmcsf_autotune picks one of the candidate thresholds, builds that format
   (its arrays are the ones the threshold gives), and its outputs match;
 * the mttkrp command without -w / -f reports the threshold it chose."""
@@ -80,12 +83,13 @@ def test_precision_plan(R, torch_cuda):
                 (p1["pair"]["use"] and m in F.pair_modes() and p1["pair"]["dtype"] == "bf16")
                 or (not (p1["pair"]["use"] and m in F.pair_modes()) and p1[m]["dtype"] == "bf16"))
             _close(outs[m].cpu().numpy(), ref16[m] if read_bf16 else ref32[m], ("mixed", m, read_bf16))
-    # the plan installs on a fresh format and gives the same outputs
+    # the plan installs on a fresh format and gives the same outputs (up to the
+    # order of the atomic reductions)
     G = mmcsf.Format(X, impl=mmcsf.IMPL_MMCSF, views=1)
     G.set_plan(p1)
     outs2 = G.mttkrp_all(Ud)
     for m in range(3):
-        assert torch.allclose(outs2[m], outs[m], rtol=1e-6, atol=0), m
+        assert torch.allclose(outs2[m], outs[m], rtol=RTOL, atol=0), m
 
 
 def test_autotune_fiber_threshold(torch_cuda):

@@ -603,29 +603,38 @@ extern "C" int mmcsf_tune(mmcsf_format* F, int R, int factor_dtype, const void* 
           if (!all0) continue;
         }
       }
-      for (int mbv = 1; mbv <= 4; ++mbv) {
+      // one launch to warm up, the next one timed
+      auto time_cfg = [&](int c, int mbv, float* ms) {
+        mmcsf_kernel_cfg cfg{};
+        cfg.chunk = c;
+        cfg.traversal = trav;
+        cfg.min_blocks = mbv;
+        cfg.kernel = kern;
+        if ((st = mmcsf_mttkrp(F, m, R, factor_dtype, d_factors, d_outs[m], &cfg, stream)) != MMCSF_OK) return;
+        if (cudaEventRecord(e0, s) != cudaSuccess) { st = MMCSF_ERR_CUDA; return; }
+        if ((st = mmcsf_mttkrp(F, m, R, factor_dtype, d_factors, d_outs[m], &cfg, stream)) != MMCSF_OK) return;
+        if (cudaEventRecord(e1, s) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess) {
+          st = MMCSF_ERR_CUDA;
+          return;
+        }
+        cudaEventElapsedTime(ms, e0, e1);
+        if (*ms < best) { best = *ms; bt = trav; bc = c; bm = mbv; bk = kern; }
+      };
+      // a traversal and kernel more than twice as slow as the best so far at
+      // a middle launch shape is not swept over every shape
+      if (best < 1e30f) {
+        float probe = 0;
+        time_cfg(512, 2, &probe);
+        if (st != MMCSF_OK) break;
+        if (probe > 2.f * best) continue;
+      }
+      for (int mbv = 1; mbv <= 4 && st == MMCSF_OK; ++mbv) {
         for (int c : chunks) {
           if (kern == 7 && c != chunks[0]) break;  // kernel 7 sizes its own ranges: one timing per level
-          mmcsf_kernel_cfg cfg{};
-          cfg.chunk = c;
-          cfg.traversal = trav;
-          cfg.min_blocks = mbv;
-          cfg.kernel = kern;
           float ms = 0;
-          for (int rep = 0; rep < 2; ++rep) {  // the second run is timed
-            if ((st = mmcsf_mttkrp(F, m, R, factor_dtype, d_factors, d_outs[m], &cfg, stream)) != MMCSF_OK) break;
-            if (cudaEventRecord(e0, s) != cudaSuccess) { st = MMCSF_ERR_CUDA; break; }
-            if ((st = mmcsf_mttkrp(F, m, R, factor_dtype, d_factors, d_outs[m], &cfg, stream)) != MMCSF_OK) break;
-            if (cudaEventRecord(e1, s) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess) {
-              st = MMCSF_ERR_CUDA;
-              break;
-            }
-            cudaEventElapsedTime(&ms, e0, e1);
-          }
+          time_cfg(c, mbv, &ms);
           if (st != MMCSF_OK) break;
-          if (ms < best) { best = ms; bt = trav; bc = c; bm = mbv; bk = kern; }
         }
-        if (st != MMCSF_OK) break;
       }
       }
     }
